@@ -1,0 +1,287 @@
+/*
+ * soup_b200.h -- C ABI of the B200 soup MD step.
+ *
+ * This is the drop-in boundary under the reference's TypeScript simulation API
+ * (nefayran/protocell-genesis, soup/src/soup-types.ts:181-442 `SoupSystem`, created by
+ * `createSoup` at soup/src/sim.ts:95).  Every entry point below names the reference member it
+ * replaces.  Plain C types only: pointers, sizes, fixed-layout structs; no CUDA or torch types.
+ *
+ * Conventions
+ *  - Every call returns an int status (SOUP_OK = 0).  On failure the handle keeps a message that
+ *    soup_last_error() returns; calls that fail before a handle exists leave it in
+ *    soup_last_error(NULL).  The wording follows the reference's thrown Errors
+ *    (soup/src/soup-health.ts, soup/src/soup-grid-verlet.ts:266-313, soup/src/soup-plan.ts).
+ *  - Readbacks write into CALLER-OWNED host buffers, in the ORIGINAL particle order, in the
+ *    reference's layouts: positions f32x4 (w = kind index), velocities/forces f32x4 (w = 0),
+ *    bond slots u32x3 with 0xFFFFFFFF = empty, everything else one 32-bit word per particle.
+ *    `bytes` must equal the exact size of the array; otherwise SOUP_E_ARG.
+ *  - A handle is not thread-safe.  Distinct handles may be used concurrently from different
+ *    threads; each owns one CUDA stream on the device that was current when it was created.
+ */
+#ifndef SOUP_B200_H
+#define SOUP_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SOUP_ABI_VERSION 1u
+#define SOUP_NONE 0xFFFFFFFFu
+#define SOUP_MAX_KINDS 8
+#define SOUP_MAX_RULES 4
+
+/* Status codes (the reference throws Errors; the ABI returns these). */
+enum {
+  SOUP_OK = 0,
+  SOUP_E_ARG = 1,           /* bad argument, size mismatch, NULL pointer */
+  SOUP_E_NONFINITE = 2,     /* soup/src/soup-health.ts assertStateFinite */
+  SOUP_E_LIST_OVERFLOW = 3, /* soup/src/soup-grid-verlet.ts:270-275 */
+  SOUP_E_ES_OVERFLOW = 4,   /* soup/src/soup-grid-verlet.ts:281-291 */
+  SOUP_E_DRIFT = 5,         /* soup/src/soup-grid-verlet.ts:301-312 */
+  SOUP_E_GEOMETRY = 6,      /* soup/src/soup-plan.ts:76-157 grid / drift-bound refusals */
+  SOUP_E_OOM = 7,           /* device allocation failed */
+  SOUP_E_TIMEOUT = 8,       /* a bounded device-side wait gave up */
+  SOUP_E_CUDA = 9,          /* any other CUDA runtime error */
+  SOUP_E_STATE = 10         /* call not allowed in this state (e.g. relax after step 0) */
+};
+
+/* Species class (soup/src/soup-attraction.ts speciesClassOf). */
+enum { SOUP_CLASS_APOLAR = 0, SOUP_CLASS_POLAR = 1, SOUP_CLASS_SOLVENT = 2, SOUP_CLASS_MINERAL = 3 };
+
+/* Slot role (soup/src/soup-plan.ts slotRole): 0 carbon chain pool, 1 carbon head slot, 2 head. */
+enum { SOUP_ROLE_CHAIN = 0, SOUP_ROLE_HEAD_SLOT = 1, SOUP_ROLE_HEAD = 2 };
+
+/*
+ * Fully resolved configuration of one system.  The host fills it from data/params.json,
+ * data/soup.json and CreateSoupOpts exactly the way the reference fills its uniforms:
+ *   Params          engine/wgsl/forces.wgsl:1-10, engine/src/params.ts:33-47
+ *   Species/AttrScale soup/wgsl/pair.wgsl:43-62, soup/src/soup-attraction.ts
+ *   GridDims / VL   soup/src/soup-plan.ts:121-157, soup/src/sim.ts (deriveListCapacity)
+ *   ES / ES2        soup/src/electrostatics.ts:166-274 (makeEsBasis, esUniform, esUniform2)
+ *   BondParams      soup/wgsl/bond-common.wgsl:54-80, soup/src/soup-buffers.ts:344-410
+ *   WALL            soup/wgsl/wall.wgsl:40, soup/src/soup-confine.ts wallUniformBytes
+ * Real numbers are given in double precision (JavaScript numbers); the library rounds to f32
+ * wherever the reference uploads a Float32Array, and keeps FP64 where the reference computes on
+ * the host in JavaScript doubles (the constant-pH sweep, the closure and aggregate analyses).
+ */
+typedef struct SoupConfig {
+  uint32_t abi_version;            /* must be SOUP_ABI_VERSION */
+  uint32_t n;                      /* number of particles (sum of counts) */
+  uint32_t n_kinds;                /* monomer kinds, <= SOUP_MAX_KINDS */
+  uint32_t seed;                   /* CreateSoupOpts.seed */
+  uint32_t counts[SOUP_MAX_KINDS]; /* particles per kind, kinds in data/soup.json order */
+  double box[3];                   /* live box, sigma */
+
+  /* Params (data/params.json; kT is CreateSoupOpts.kT) */
+  double sigma, epsilon, b_tt, k_fene, r_inf, k_bend, r_bend, wc, kT, gamma, dt;
+
+  /* Species, per kind */
+  double radius[SOUP_MAX_KINDS];      /* radiusSigma */
+  uint32_t kind_class[SOUP_MAX_KINDS];/* SOUP_CLASS_* */
+  double attr_scale[4][4];            /* class-pair attraction depth table */
+  double acid_soap_scale;             /* AttrScale.pair.x */
+
+  /* Neighbour grid and Verlet list (soup/src/soup-plan.ts:121-157) */
+  double interaction_range;        /* wca_cut(sigma*max radius) + wc */
+  double skin;                     /* verletList.skin */
+  double list_range;               /* interaction_range + skin */
+  uint32_t rebuild_every;          /* verletList.rebuildEvery (fixed-cadence mode) */
+  uint32_t rebuild_on_drift;       /* 1: rebuild when max drift > skin/2 (no fixed cadence) */
+  uint32_t list_capacity;          /* per-particle list capacity; 0 = library derives it */
+
+  /* Electrostatics (EsBasis, soup/src/electrostatics.ts:77-131) */
+  uint32_t es_enabled;
+  int32_t charged_kind;            /* titratable kind, -1 = none */
+  double charge_deprotonated;
+  double es_coeff_a, es_kappa, es_cutoff, es_shift_u, es_shift_f;
+  double es_split_radius;          /* = interaction_range */
+  double es_list_range;            /* es_cutoff + skin */
+  uint32_t es_list_capacity;       /* per-head capacity; 0 = library derives it */
+  double pka_intrinsic, ph;
+  uint32_t sweep_every;            /* sweepEverySteps */
+  uint32_t protonation_rng;        /* PcgState.state of the constant-pH chain */
+  double rc_attr;                  /* wca_cut(sigma*b_tt), the acid-soap well onset */
+
+  /* Bond chemistry (BondParams) */
+  uint32_t n_rules;
+  int32_t rule_kind_a[SOUP_MAX_RULES], rule_kind_b[SOUP_MAX_RULES];
+  double attempt_form[SOUP_MAX_RULES], attempt_break[SOUP_MAX_RULES];
+  double accept_form[SOUP_MAX_RULES], accept_break[SOUP_MAX_RULES];
+  uint32_t requires_catalyst[SOUP_MAX_RULES];
+  uint32_t role_a[SOUP_MAX_RULES], role_b[SOUP_MAX_RULES];
+  int32_t catalyst_kind;
+  uint32_t head_terminal_only, head_chain_capacity;
+  uint32_t max_hold_steps, bond_interval;
+
+  /* Confinement wall (0 radius = none) */
+  double wall_radius, wall_k;
+
+  /* Schedule (soup/src/soup-integrate.ts:136-175) */
+  uint64_t global_step;            /* starting step (resume.globalStep) */
+  uint32_t chunk_steps;            /* steps per submission chunk; the reference uses 1000 */
+  uint32_t reserved[7];
+} SoupConfig;
+
+/* Initial state: the resume arrays of CreateSoupOpts.resume (soup/src/soup-types.ts:145-178) plus
+ * the frozen flags.  Any pointer may be NULL, in which case the fresh-creation value is used
+ * (soup/src/soup-init-state.ts:58-307, soup/src/soup-protonation.ts:38-49). */
+typedef struct SoupInitState {
+  const float* positions;       /* f32 x4 */
+  const float* velocities;      /* f32 x4 */
+  const uint32_t* bond_slots;   /* u32 x3 */
+  const uint32_t* center_link;  /* u32 */
+  const uint32_t* center_held;  /* u32 */
+  const uint32_t* bond_rng;     /* u32 */
+  const uint32_t* thermo_rng;   /* u32 */
+  const float* charges;         /* f32 */
+  const uint32_t* frozen;       /* u32 */
+  const uint32_t* events;       /* u32 x (2*n_rules): bond, break per rule */
+  const uint32_t* desorb_events;/* u32 x2: stretch, timeout */
+} SoupInitState;
+
+/* Result of one constant-pH sweep (soup/src/electrostatics.ts:317-326 SweepResult). */
+typedef struct SoupSweepResult {
+  uint32_t attempts, accepted, heads, deprotonated;
+  double alpha;
+  double d_es_mean_kt;
+} SoupSweepResult;
+
+/* Result of the closure flood fill (soup/src/water-closure.ts:198-245 EncapsulatedWaterResult). */
+typedef struct SoupClosureResult {
+  uint32_t encapsulated_count, total_water;
+  double bulk_water_density;
+  double threshold_count;       /* NaN when no bulk water was reached */
+  uint32_t closed;
+  uint32_t total_empty_cells, unreached_cells;
+  uint32_t seed_cell;
+  double seed_dist_from_centre;
+} SoupClosureResult;
+
+/* Handle state summary. */
+typedef struct SoupInfo {
+  uint32_t n;
+  uint64_t global_step;
+  uint32_t list_capacity, es_list_capacity, heads;
+  uint64_t rebuilds, sweeps;
+  double box[3];
+  double max_drift;             /* sqrt of the last measured max drift^2 */
+} SoupInfo;
+
+typedef struct SoupHandle SoupHandle;
+typedef struct SoupBatch SoupBatch;
+
+/* ---- lifecycle ------------------------------------------------------------------------------ */
+
+/* createSoup (soup/src/sim.ts:95): allocates device state, uploads `init` (NULL = fresh lattice),
+ * runs the priming rebuild + force pass (sim.ts:396-408).  Device = the current CUDA device. */
+int soup_create(const SoupConfig* cfg, const SoupInitState* init, SoupHandle** out);
+/* SoupSystem.dispose (soup/src/soup-types.ts:441). */
+void soup_destroy(SoupHandle* h);
+/* Message of the last failed call on `h` (NULL: the last failure with no handle). */
+const char* soup_last_error(const SoupHandle* h);
+int soup_get_info(SoupHandle* h, SoupInfo* out);
+
+/* Fresh-creation arrays on the host: buildInitialState (soup/src/soup-init-state.ts:58-307) and
+ * initialCharges (soup/src/soup-protonation.ts:38-49).  Any output pointer may be NULL. */
+int soup_fresh_state(const SoupConfig* cfg, float* positions, float* velocities, uint32_t* frozen,
+                     uint32_t* bond_rng, uint32_t* thermo_rng);
+int soup_initial_charges(const SoupConfig* cfg, const float* positions, float* charges,
+                         uint32_t* protonation_rng);
+
+/* ---- stepping ------------------------------------------------------------------------------- */
+
+/* SoupSystem.step(n) (soup/src/soup-integrate.ts:136-175): the same global-step schedule
+ * (rebuild on step % rebuild_every == 0 or on half-skin drift, bonds on step % bond_interval == 0,
+ * guards and the constant-pH sweep at chunk boundaries). */
+int soup_step(SoupHandle* h, uint64_t n);
+/* relaxColdStart (soup/src/soup-relax.ts:113-185): capped steepest descent, only at step 0.
+ * out2 receives {maxForceBefore, maxForceAfter}; may be NULL. */
+int soup_relax_cold_start(SoupHandle* h, uint32_t iterations, double max_displacement_sigma,
+                          double* out2);
+
+/* ---- readbacks (soup/src/soup-readback.ts:13-190) ------------------------------------------- */
+int soup_read_pos(SoupHandle* h, void* dst, size_t bytes);          /* particles()    */
+int soup_read_vel(SoupHandle* h, void* dst, size_t bytes);          /* velocities()   */
+int soup_read_force(SoupHandle* h, void* dst, size_t bytes);        /* forcesNoRebuildDEBUG() */
+int soup_forces(SoupHandle* h, void* dst, size_t bytes);            /* forces(): rebuild + force */
+int soup_forces_brute(SoupHandle* h, void* dst, size_t bytes);      /* forcesBruteForce() */
+int soup_read_slots(SoupHandle* h, void* dst, size_t bytes);        /* bondSlots()    */
+int soup_read_center_link(SoupHandle* h, void* dst, size_t bytes);  /* centerLinks()  */
+int soup_read_center_held(SoupHandle* h, void* dst, size_t bytes);  /* centerHeldSteps() */
+int soup_read_charges(SoupHandle* h, void* dst, size_t bytes);      /* charges()      */
+int soup_read_rng_bond(SoupHandle* h, void* dst, size_t bytes);     /* rngState().bond */
+int soup_read_rng_thermo(SoupHandle* h, void* dst, size_t bytes);   /* rngState().thermo */
+int soup_read_frozen(SoupHandle* h, void* dst, size_t bytes);       /* frozen()       */
+int soup_read_events(SoupHandle* h, void* dst, size_t bytes);       /* events(): u32 x 2*n_rules */
+int soup_read_desorb(SoupHandle* h, void* dst, size_t bytes);       /* desorbEvents(): u32 x2 */
+/* nonFiniteCount() (soup/src/soup-health.ts scanNonFinite): out2 = {pos, vel} components. */
+int soup_nonfinite_count(SoupHandle* h, uint32_t* out2);
+/* The Verlet list of every particle as ORIGINAL indices: counts u32[n] and, when `lists` is not
+ * NULL, each particle's neighbours sorted ascending in a CSR layout (offsets = prefix of counts).
+ * `lists_cap` is the element capacity of `lists`.  Diagnostic/parity access. */
+int soup_read_verlet(SoupHandle* h, uint32_t* counts, uint32_t* lists, size_t lists_cap);
+/* Protonation chain state (SoupSystem.protonationRngState). */
+int soup_read_protonation_rng(SoupHandle* h, uint32_t* out);
+
+/* ---- writes --------------------------------------------------------------------------------- */
+/* writeBuffer(chargeBuf) (soup/src/soup-protonation.ts:60); marks forces stale. */
+int soup_write_charges(SoupHandle* h, const float* src, size_t bytes);
+/* Live box change (soup/src/soup-box-scale.ts resizeSoupGrid); positions are not moved. */
+int soup_set_box(SoupHandle* h, const double box[3]);
+/* Replace the whole state (CreateSoupOpts.resume semantics); NULL members keep current values. */
+int soup_write_state(SoupHandle* h, const SoupInitState* st);
+
+/* ---- Monte Carlo and analysis -------------------------------------------------------------- */
+/* protonationSweepDEBUG (soup/src/sim.ts): one constant-pH sweep now on the device, then the
+ * rebuild + force recompute (soup/src/soup-protonation.ts:52-77). */
+int soup_protonation_sweep(SoupHandle* h, SoupSweepResult* out);
+
+/* encapsulatedWaterVolume (soup/src/water-closure.ts:271-363) on the current positions.
+ * member_idx / water_idx are ORIGINAL particle indices; centre from periodicCentreOf. */
+int soup_closure(SoupHandle* h, const uint32_t* member_idx, uint32_t n_members,
+                 const uint32_t* water_idx, uint32_t n_water, const double centre[3],
+                 double cell, double radius, double enclosed_volume_min, SoupClosureResult* out);
+
+/* findAmphiphiles (soup/src/amphiphile.ts:55-141) on the current bond graph: head_of[i] = the
+ * head index of the amphiphile particle i belongs to, or SOUP_NONE.  n_out = amphiphile count. */
+int soup_amphiphile_labels(SoupHandle* h, uint32_t* head_of, uint32_t* n_out);
+
+/* clusterComponents (engine/src/aggregate.ts:201-212) over the member particles (periodic on all
+ * three axes, pair joined when r^2 <= cutoff^2): labels[k] = the minimum ORIGINAL index in the
+ * component of member_idx[k].  n_components may be NULL. */
+int soup_aggregate_labels(SoupHandle* h, const uint32_t* member_idx, uint32_t n_members,
+                          double cutoff, uint32_t* labels, uint32_t* n_components);
+
+/* ---- single phases ------------------------------------------------------------------------- */
+/* One phase of the step on the current device state, so each kernel can be checked in isolation
+ * (the reference times phases the same way: stepPhasesDEBUG, soup/src/soup-readback.ts:191-245).
+ *   REBUILD     encodeVerletRebuild (soup/src/soup-grid-verlet.ts:236-248)
+ *   FORCE       encodeSoupForceList: list force + far ES + wall (soup/src/soup-integrate.ts:64-71)
+ *   KICK_DRIFT  kick_drift_wrap_main (soup/wgsl/step.wgsl:96)
+ *   KICK_THERMO kick_thermostat_main (soup/wgsl/step.wgsl:110)
+ *   BONDS       bond formation then breaking (soup/src/soup-bond-chemistry.ts)
+ *   MAX_DRIFT   soup_max_drift_main (soup/wgsl/verlet.wgsl:113) */
+enum {
+  SOUP_PHASE_REBUILD = 1, SOUP_PHASE_FORCE = 2, SOUP_PHASE_KICK_DRIFT = 3,
+  SOUP_PHASE_KICK_THERMO = 4, SOUP_PHASE_BONDS = 5, SOUP_PHASE_MAX_DRIFT = 6
+};
+int soup_debug_phase(SoupHandle* h, int phase);
+
+/* ---- batched replicas (no reference counterpart: one system per device there) -------------- */
+/* Many independent systems of uneven size stepped together: one launch per kernel per step covers
+ * every replica.  cfgs[r] / inits[r] as for soup_create (inits may be NULL). */
+int soup_batch_create(const SoupConfig* cfgs, const SoupInitState* inits, uint32_t n_replicas,
+                      SoupBatch** out);
+int soup_batch_step(SoupBatch* b, uint64_t n);
+/* Borrowed per-replica handle for readbacks; valid until soup_batch_destroy. */
+SoupHandle* soup_batch_replica(SoupBatch* b, uint32_t r);
+const char* soup_batch_last_error(const SoupBatch* b);
+void soup_batch_destroy(SoupBatch* b);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* SOUP_B200_H */

@@ -1,0 +1,245 @@
+// kernels_force.cu -- the force: list pair force + bonded terms + wall, the far Debye-Hueckel half,
+// and the O(N^2) brute-force twin.
+//
+// Reference: soup/wgsl/verlet.wgsl:132-149 soup_force_list_main (bondedForce + sum over the list of
+// nonbondedSoup), soup/wgsl/step.wgsl:152-193 bondedForce, soup/wgsl/electrostatics-long.wgsl:63-103
+// (far half, accumulated), soup/wgsl/wall.wgsl:42-56 (wall, accumulated), step.wgsl:277-292 brute.
+//
+// TPP threads cooperate on one particle: lane t takes list entries t, t+TPP, ... and bonded terms
+// t, t+TPP, ...; the group reduces with shuffles and lane 0 writes the force.  No atomics: every
+// particle's force is produced by exactly one group (full list, no Newton-3), so the sum order is
+// fixed and the result is run-to-run deterministic.
+#include "soup_internal.h"
+
+namespace soup {
+
+namespace {
+
+constexpr int kBlock = 256;
+inline unsigned nblocks(uint64_t n, int b = kBlock) { return (unsigned)((n + b - 1) / b); }
+
+// One bonded term of particle (slot k, original id gi), term index t in [0, 13):
+//   t < 3         FENE to slot partner t
+//   3 <= t < 12   bend to partner-of-partner ((t-3)/3, (t-3)%3), skipping i itself
+//   t == 12       FENE tether to the adsorbing catalyst (centerLink)
+__device__ __forceinline__ void bonded_term(const Shared& S, const SysParams& P, int t, uint32_t gi, const float4& xi,
+                                            const uint32_t* __restrict__ sl, uint32_t owner,
+                                            const uint32_t* __restrict__ slots, const uint32_t* __restrict__ slot_of,
+                                            const float4* __restrict__ pos, float& fx, float& fy, float& fz) {
+  uint32_t other;
+  bool fene;
+  if (t < 3) { other = sl[t]; fene = true; }
+  else if (t < 12) {
+    uint32_t m = sl[(t - 3) / 3];
+    if (m == SOUP_NONE_U32) return;
+    other = slots[3 * slot_of[m] + (t - 3) % 3];
+    if (other == gi) return;
+    fene = false;
+  } else { other = owner; fene = true; }
+  if (other == SOUP_NONE_U32) return;
+  float4 xo = pos[slot_of[other]];
+  float dx = fast_mi(xi.x - xo.x, P.box[0], P.inv_box[0]);
+  float dy = fast_mi(xi.y - xo.y, P.box[1], P.inv_box[1]);
+  float dz = fast_mi(xi.z - xo.z, P.box[2], P.inv_box[2]);
+  float s = bonded_scalar(S, dx * dx + dy * dy + dz * dz, fene);
+  fx += s * dx; fy += s * dy; fz += s * dz;
+}
+
+template <int TPP>
+__global__ void __launch_bounds__(256) k_force(
+    const Shared* __restrict__ Sg, const SysParams* __restrict__ sp, const uint8_t* __restrict__ sysid, uint32_t N,
+    const float4* __restrict__ pos, const float* __restrict__ charge, const uint32_t* __restrict__ slots,
+    const uint32_t* __restrict__ center, const uint32_t* __restrict__ id, const uint32_t* __restrict__ slot_of,
+    const uint32_t* __restrict__ nl, const uint32_t* __restrict__ nl_cnt, uint32_t cap, float4* __restrict__ force) {
+  __shared__ Shared S;
+  for (int w = threadIdx.x; w < (int)(sizeof(Shared) / 4); w += blockDim.x)
+    reinterpret_cast<uint32_t*>(&S)[w] = reinterpret_cast<const uint32_t*>(Sg)[w];
+  __syncthreads();
+  const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t k = gtid / TPP;
+  const int lane = (int)(gtid % TPP);
+  const bool active = k < N;
+  float fx = 0.f, fy = 0.f, fz = 0.f;
+  if (active) {
+    const SysParams& P = sp[sysid[k]];
+    const float4 xi = pos[k];
+    const int ki = (int)xi.w;
+    const float qi = charge[k];
+    const bool needq = (qi != 0.f) || (S.cls[ki] == 1u && P.acid > 0.f);
+    const uint32_t cnt = nl_cnt[k];
+    const uint32_t* row = nl + (size_t)k * cap;
+    const PairConst* prow = &S.pair[ki * SOUP_KMAX];
+    for (uint32_t s = lane; s < cnt; s += TPP) {
+      const uint32_t j = __ldg(row + s);
+      const float4 xj = __ldg(pos + j);
+      const float dx = fast_mi(xi.x - xj.x, P.box[0], P.inv_box[0]);
+      const float dy = fast_mi(xi.y - xj.y, P.box[1], P.inv_box[1]);
+      const float dz = fast_mi(xi.z - xj.z, P.box[2], P.inv_box[2]);
+      const float r2 = dx * dx + dy * dy + dz * dz;
+      if (r2 >= S.rmax2 || r2 < 1e-12f) continue;
+      const int kj = (int)xj.w;
+      const float qj = needq ? __ldg(charge + j) : 0.f;
+      const float sc = pair_scalar(S, P, prow[kj], r2, ki, kj, qi, qj);
+      fx += sc * dx; fy += sc * dy; fz += sc * dz;
+    }
+    // bonded terms (bondedForce), spread over the group
+    uint32_t sl[3] = {slots[3 * k], slots[3 * k + 1], slots[3 * k + 2]};
+    uint32_t owner = center[k];
+    if ((sl[0] & sl[1] & sl[2] & owner) != SOUP_NONE_U32) {
+      const uint32_t gi = id[k];
+      for (int t = lane; t < 13; t += TPP) bonded_term(S, P, t, gi, xi, sl, owner, slots, slot_of, pos, fx, fy, fz);
+    }
+  }
+#pragma unroll
+  for (int o = TPP / 2; o > 0; o >>= 1) {
+    fx += __shfl_xor_sync(0xffffffffu, fx, o);
+    fy += __shfl_xor_sync(0xffffffffu, fy, o);
+    fz += __shfl_xor_sync(0xffffffffu, fz, o);
+  }
+  if (active && lane == 0) {
+    const SysParams& P = sp[sysid[k]];
+    if (P.wall_r > 0.f) {   // wall.wgsl:42-56
+      const float4 xi = pos[k];
+      float d0 = xi.x - P.box[0] * 0.5f, d1 = xi.y - P.box[1] * 0.5f, d2 = xi.z - P.box[2] * 0.5f;
+      float r = sqrtf(d0 * d0 + d1 * d1 + d2 * d2);
+      if (r > P.wall_r) {
+        float w = -P.wall_k * (r - P.wall_r) / fmaxf(r, 1e-6f);
+        fx += w * d0; fy += w * d1; fz += w * d2;
+      }
+    }
+    force[k] = make_float4(fx, fy, fz, 0.f);
+  }
+}
+
+// soup/wgsl/electrostatics-long.wgsl:63-82 soup_es_force_far_main, a warp per head.
+__global__ void __launch_bounds__(256) k_es_far(const SysParams* __restrict__ sp, const uint32_t* __restrict__ heads,
+                                                const uint32_t* __restrict__ head_sys, uint32_t H,
+                                                const uint32_t* __restrict__ slot_of, const float4* __restrict__ pos,
+                                                const float* __restrict__ charge, const uint32_t* __restrict__ es_nl,
+                                                const uint32_t* __restrict__ es_cnt, uint32_t cap,
+                                                float4* __restrict__ force) {
+  const uint32_t h = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (h >= H) return;   // warp-uniform
+  const SysParams& P = sp[head_sys[h]];
+  const uint32_t ks = slot_of[heads[h]];
+  const float qi = charge[ks];
+  if (qi == 0.f || P.es_A == 0.f) return;
+  const float4 xi = pos[ks];
+  float fx = 0.f, fy = 0.f, fz = 0.f;
+  const uint32_t cnt = es_cnt[h];
+  const uint32_t* row = es_nl + (size_t)h * cap;
+  for (uint32_t s = lane; s < cnt; s += 32) {
+    const uint32_t j = __ldg(row + s);
+    const float qj = __ldg(charge + j);
+    if (qj == 0.f) continue;
+    const float4 xj = __ldg(pos + j);
+    const float dx = fast_mi(xi.x - xj.x, P.box[0], P.inv_box[0]);
+    const float dy = fast_mi(xi.y - xj.y, P.box[1], P.inv_box[1]);
+    const float dz = fast_mi(xi.z - xj.z, P.box[2], P.inv_box[2]);
+    const float r2 = dx * dx + dy * dy + dz * dz;
+    const float rinv = rsqrtf(r2);
+    const float r = r2 * rinv;
+    if (r < P.es_split || r >= P.es_rc) continue;   // esForceFar (electrostatics.wgsl:87-90)
+    const float u = P.es_A * __expf(-P.es_kappa * r) * rinv;
+    const float sc = qi * qj * (u * (rinv + P.es_kappa) - P.es_fc) * rinv;
+    fx += sc * dx; fy += sc * dy; fz += sc * dz;
+  }
+  for (int o = 16; o > 0; o >>= 1) {
+    fx += __shfl_xor_sync(0xffffffffu, fx, o);
+    fy += __shfl_xor_sync(0xffffffffu, fy, o);
+    fz += __shfl_xor_sync(0xffffffffu, fz, o);
+  }
+  if (lane == 0) {
+    float4 f = force[ks];
+    force[ks] = make_float4(f.x + fx, f.y + fy, f.z + fz, 0.f);
+  }
+}
+
+// soup/wgsl/step.wgsl:277-292 + electrostatics-long.wgsl:88-103 + wall: every pair of the replica.
+__global__ void __launch_bounds__(128) k_force_brute(
+    const Shared* __restrict__ Sg, const SysParams* __restrict__ sp, const uint8_t* __restrict__ sysid, uint32_t N,
+    const float4* __restrict__ pos, const float* __restrict__ charge, const uint32_t* __restrict__ slots,
+    const uint32_t* __restrict__ center, const uint32_t* __restrict__ id, const uint32_t* __restrict__ slot_of,
+    float4* __restrict__ force) {
+  __shared__ Shared S;
+  for (int w = threadIdx.x; w < (int)(sizeof(Shared) / 4); w += blockDim.x)
+    reinterpret_cast<uint32_t*>(&S)[w] = reinterpret_cast<const uint32_t*>(Sg)[w];
+  __syncthreads();
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= N) return;
+  const SysParams& P = sp[sysid[k]];
+  const float4 xi = pos[k];
+  const int ki = (int)xi.w;
+  const float qi = charge[k];
+  float fx = 0.f, fy = 0.f, fz = 0.f;
+  for (uint32_t j = P.slot_off; j < P.slot_off + P.n; ++j) {
+    if (j == k) continue;
+    const float4 xj = pos[j];
+    const float dx = fast_mi(xi.x - xj.x, P.box[0], P.inv_box[0]);
+    const float dy = fast_mi(xi.y - xj.y, P.box[1], P.inv_box[1]);
+    const float dz = fast_mi(xi.z - xj.z, P.box[2], P.inv_box[2]);
+    const float r2 = dx * dx + dy * dy + dz * dz;
+    if (r2 < 1e-12f) continue;
+    const int kj = (int)xj.w;
+    const float qj = charge[j];
+    if (r2 < S.rmax2) {
+      const float sc = pair_scalar(S, P, S.pair[ki * SOUP_KMAX + kj], r2, ki, kj, qi, qj);
+      fx += sc * dx; fy += sc * dy; fz += sc * dz;
+    }
+    const float qq = qi * qj;
+    if (qq != 0.f && P.es_A != 0.f) {
+      const float r = sqrtf(r2);
+      if (r >= P.es_split && r < P.es_rc) {
+        const float u = P.es_A * __expf(-P.es_kappa * r) / r;
+        const float s = qq * (u * (1.0f / r + P.es_kappa) - P.es_fc) / r;
+        fx += s * dx; fy += s * dy; fz += s * dz;
+      }
+    }
+  }
+  uint32_t sl[3] = {slots[3 * k], slots[3 * k + 1], slots[3 * k + 2]};
+  uint32_t owner = center[k];
+  const uint32_t gi = id[k];
+  for (int t = 0; t < 13; ++t) bonded_term(S, P, t, gi, xi, sl, owner, slots, slot_of, pos, fx, fy, fz);
+  if (P.wall_r > 0.f) {
+    float d0 = xi.x - P.box[0] * 0.5f, d1 = xi.y - P.box[1] * 0.5f, d2 = xi.z - P.box[2] * 0.5f;
+    float r = sqrtf(d0 * d0 + d1 * d1 + d2 * d2);
+    if (r > P.wall_r) {
+      float w = -P.wall_k * (r - P.wall_r) / fmaxf(r, 1e-6f);
+      fx += w * d0; fy += w * d1; fz += w * d2;
+    }
+  }
+  force[k] = make_float4(fx, fy, fz, 0.f);
+}
+
+template <int TPP>
+void launch_force_tpp(Batch& b) {
+  const uint64_t threads = (uint64_t)b.N * TPP;
+  k_force<TPP><<<nblocks(threads, 256), 256, 0, b.stream>>>(b.shared, b.sp, b.sysid, b.N, b.pos, b.charge, b.slots,
+                                                            b.center, b.id, b.slot_of, b.nl, b.nl_cnt, b.list_cap,
+                                                            b.force);
+}
+
+}  // namespace
+
+void launch_force(Batch& b) {
+  switch (b.tpp) {
+    case 1: launch_force_tpp<1>(b); break;
+    case 2: launch_force_tpp<2>(b); break;
+    case 4: launch_force_tpp<4>(b); break;
+    case 16: launch_force_tpp<16>(b); break;
+    case 32: launch_force_tpp<32>(b); break;
+    default: launch_force_tpp<8>(b); break;
+  }
+  if (b.H > 0) {
+    k_es_far<<<nblocks((uint64_t)b.H * 32, 256), 256, 0, b.stream>>>(b.sp, b.heads, b.head_sys, b.H, b.slot_of, b.pos,
+                                                                     b.charge, b.es_nl, b.es_cnt, b.es_cap, b.force);
+  }
+}
+
+void launch_force_brute(Batch& b) {
+  k_force_brute<<<nblocks(b.N, 128), 128, 0, b.stream>>>(b.shared, b.sp, b.sysid, b.N, b.pos, b.charge, b.slots,
+                                                         b.center, b.id, b.slot_of, b.force);
+}
+
+}  // namespace soup

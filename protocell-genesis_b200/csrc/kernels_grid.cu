@@ -1,0 +1,341 @@
+// kernels_grid.cu -- cell binning, the deterministic re-sort, and the Verlet / head list builds.
+//
+// Reference: engine/wgsl/neighbor.wgsl:19-64 (clear/count/prefix/fill: an atomic counting sort with a
+// one-thread prefix sum and an atomic, run-to-run varying fill order), soup/wgsl/verlet.wgsl:53-92
+// (per-particle walk of (2R+1)^3 cells, keep |mi3(xi-xj)| < listRange), soup/wgsl/
+// electrostatics-long.wgsl:15-56 (serial head compaction, O(N_h^2) head list).
+//
+// Here: a parallel counting sort whose order inside a cell is fixed (ascending original index), so
+// every array is physically reordered into cell order at each rebuild (coalesced neighbour reads);
+// list membership uses the exact f32 test of the reference, so the lists equal the oracle's sets.
+// Walks are over x-rows of cells (contiguous slot ranges), a row at a time.
+#include "soup_internal.h"
+
+namespace soup {
+
+namespace {
+
+constexpr int kBlock = 256;
+inline unsigned nblocks(uint64_t n, int b = kBlock) { return (unsigned)((n + b - 1) / b); }
+
+__global__ void k_cell_index(const float4* __restrict__ pos, const uint8_t* __restrict__ sysid,
+                             const SysParams* __restrict__ sp, uint32_t N, uint32_t* __restrict__ cell_of,
+                             uint32_t* __restrict__ count) {
+  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= N) return;
+  const SysParams& P = sp[sysid[k]];
+  float4 p = pos[k];
+  int cx = ex_cell_axis(p.x, P.box[0], P.dims[0]);
+  int cy = ex_cell_axis(p.y, P.box[1], P.dims[1]);
+  int cz = ex_cell_axis(p.z, P.box[2], P.dims[2]);
+  uint32_t c = P.cell_off + (uint32_t)(cx + P.dims[0] * (cy + P.dims[1] * cz));
+  cell_of[k] = c;
+  atomicAdd(&count[c], 1u);
+}
+
+// Exclusive scan, 4 elements per thread, 1024 threads per block: block-local scan + block totals.
+__global__ void k_scan_block(const uint32_t* __restrict__ in, uint32_t* __restrict__ out, uint32_t n,
+                             uint32_t* __restrict__ block_sums) {
+  __shared__ uint32_t warp_tot[32];
+  const uint32_t base = blockIdx.x * 4096u + threadIdx.x * 4u;
+  uint32_t v[4];
+  uint32_t t = 0;
+  for (int e = 0; e < 4; ++e) { v[e] = (base + e < n) ? in[base + e] : 0u; t += v[e]; }
+  const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+  uint32_t incl = t;
+  for (int o = 1; o < 32; o <<= 1) {
+    uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+    if (lane >= o) incl += y;
+  }
+  if (lane == 31) warp_tot[w] = incl;
+  __syncthreads();
+  if (w == 0) {
+    uint32_t x = warp_tot[lane];
+    uint32_t xi = x;
+    for (int o = 1; o < 32; o <<= 1) {
+      uint32_t y = __shfl_up_sync(0xffffffffu, xi, o);
+      if (lane >= o) xi += y;
+    }
+    warp_tot[lane] = xi - x;  // exclusive
+    if (lane == 31 && block_sums) block_sums[blockIdx.x] = xi;
+  }
+  __syncthreads();
+  uint32_t run = warp_tot[w] + incl - t;
+  for (int e = 0; e < 4; ++e) {
+    if (base + e < n) out[base + e] = run;
+    run += v[e];
+  }
+}
+__global__ void k_scan_add(uint32_t* __restrict__ out, uint32_t n, const uint32_t* __restrict__ block_offs) {
+  uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) out[i] += block_offs[i / 4096u];
+}
+__global__ void k_set_total(uint32_t* __restrict__ start, const uint32_t* __restrict__ count, uint32_t n) {
+  start[n] = start[n - 1] + count[n - 1];
+}
+
+}  // namespace
+
+// exclusive scan of in[0..n) into out[0..n), out[n] = total; tmp must hold >= 2*ceil(n/4096)+2 words
+void exclusive_scan(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* tmp, cudaStream_t st) {
+  if (n == 0) return;
+  uint32_t nb = (n + 4095) / 4096;
+  if (nb == 1) {
+    k_scan_block<<<1, 1024, 0, st>>>(in, out, n, nullptr);
+  } else {
+    uint32_t* sums = tmp;
+    uint32_t* offs = tmp + nb + 1;
+    k_scan_block<<<nb, 1024, 0, st>>>(in, out, n, sums);
+    exclusive_scan(sums, offs, nb, offs + nb + 1, st);
+    k_scan_add<<<nblocks(n), kBlock, 0, st>>>(out, n, offs);
+  }
+  k_set_total<<<1, 1, 0, st>>>(out, in, n);
+}
+
+namespace {
+
+__global__ void k_scatter(const uint32_t* __restrict__ cell_of, const uint32_t* __restrict__ start, uint32_t N,
+                          uint32_t* __restrict__ cursor, uint32_t* __restrict__ perm) {
+  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= N) return;
+  uint32_t c = cell_of[k];
+  perm[start[c] + atomicAdd(&cursor[c], 1u)] = k;
+}
+
+// Inside each cell, order by original index: the atomic scatter order above varies run to run, this
+// makes the slot order (and therefore every summation order) deterministic.
+__global__ void k_sort_cells(const uint32_t* __restrict__ start, uint32_t ncells, const uint32_t* __restrict__ id,
+                             uint32_t* __restrict__ perm) {
+  uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncells) return;
+  uint32_t a = start[c], e = start[c + 1];
+  for (uint32_t x = a + 1; x < e; ++x) {
+    uint32_t v = perm[x];
+    uint32_t key = id[v];
+    uint32_t y = x;
+    while (y > a && id[perm[y - 1]] > key) { perm[y] = perm[y - 1]; --y; }
+    perm[y] = v;
+  }
+}
+
+__global__ void k_gather(uint32_t N, const uint32_t* __restrict__ perm,
+                         const float4* __restrict__ pos, const float4* __restrict__ vel, const float4* __restrict__ force,
+                         const float* __restrict__ charge, const uint32_t* __restrict__ slots,
+                         const uint32_t* __restrict__ center, const uint32_t* __restrict__ held,
+                         const uint32_t* __restrict__ brng, const uint32_t* __restrict__ trng,
+                         const uint8_t* __restrict__ frozen, const uint32_t* __restrict__ id,
+                         float4* __restrict__ pos2, float4* __restrict__ vel2, float4* __restrict__ force2,
+                         float* __restrict__ charge2, uint32_t* __restrict__ slots2, uint32_t* __restrict__ center2,
+                         uint32_t* __restrict__ held2, uint32_t* __restrict__ brng2, uint32_t* __restrict__ trng2,
+                         uint8_t* __restrict__ frozen2, uint32_t* __restrict__ id2, uint32_t* __restrict__ slot_of,
+                         float4* __restrict__ pos_ref) {
+  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= N) return;
+  uint32_t o = perm[k];
+  float4 p = pos[o];
+  pos2[k] = p;
+  pos_ref[k] = p;
+  vel2[k] = vel[o];
+  force2[k] = force[o];
+  charge2[k] = charge[o];
+  slots2[3 * k + 0] = slots[3 * o + 0];
+  slots2[3 * k + 1] = slots[3 * o + 1];
+  slots2[3 * k + 2] = slots[3 * o + 2];
+  center2[k] = center[o];
+  held2[k] = held[o];
+  brng2[k] = brng[o];
+  trng2[k] = trng[o];
+  frozen2[k] = frozen[o];
+  uint32_t g = id[o];
+  id2[k] = g;
+  slot_of[g] = k;
+}
+
+// Distinct wrapped cell coordinates of a +-R walk along one axis, as at most two [lo,hi] intervals.
+struct AxisRange { int lo[2], hi[2], n; };
+__device__ __forceinline__ AxisRange axis_ranges(int q, int R, int dim) {
+  AxisRange a;
+  int lo = q - R, hi = q + R;
+  if (hi - lo + 1 >= dim) { a.n = 1; a.lo[0] = 0; a.hi[0] = dim - 1; }
+  else if (lo < 0) { a.n = 2; a.lo[0] = lo + dim; a.hi[0] = dim - 1; a.lo[1] = 0; a.hi[1] = hi; }
+  else if (hi >= dim) { a.n = 2; a.lo[0] = lo; a.hi[0] = dim - 1; a.lo[1] = 0; a.hi[1] = hi - dim; }
+  else { a.n = 1; a.lo[0] = lo; a.hi[0] = hi; }
+  return a;
+}
+
+// soup/wgsl/verlet.wgsl:53-92, thread per particle, rows of cells as contiguous slot ranges.
+__global__ void __launch_bounds__(128) k_build_list(
+    const float4* __restrict__ pos, const uint8_t* __restrict__ sysid, const SysParams* __restrict__ sp,
+    const uint32_t* __restrict__ cell_of, const uint32_t* __restrict__ start, uint32_t N, uint32_t cap,
+    uint32_t* __restrict__ nl, uint32_t* __restrict__ nl_cnt, uint32_t* __restrict__ flags) {
+  uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= N) return;
+  const SysParams& P = sp[sysid[k]];
+  const float4 xi = pos[k];
+  const float box[3] = {P.box[0], P.box[1], P.box[2]};
+  const float lr = P.list_range;
+  uint32_t c = cell_of[k] - P.cell_off;
+  int qx = (int)(c % (uint32_t)P.dims[0]);
+  int qy = (int)((c / (uint32_t)P.dims[0]) % (uint32_t)P.dims[1]);
+  int qz = (int)(c / ((uint32_t)P.dims[0] * (uint32_t)P.dims[1]));
+  const int R = P.walk;
+  AxisRange ax = axis_ranges(qx, R, P.dims[0]);
+  // distinct y and z coordinates in walk order
+  int ys[16], zs[16], ny = 0, nz = 0;
+  for (int d = -R; d <= R; ++d) {
+    int y = ((qy + d) % P.dims[1] + P.dims[1]) % P.dims[1];
+    bool dup = false;
+    for (int t = 0; t < ny; ++t) dup |= ys[t] == y;
+    if (!dup) ys[ny++] = y;
+    int z = ((qz + d) % P.dims[2] + P.dims[2]) % P.dims[2];
+    dup = false;
+    for (int t = 0; t < nz; ++t) dup |= zs[t] == z;
+    if (!dup) zs[nz++] = z;
+  }
+  uint32_t cnt = 0;
+  uint32_t* row = nl + (size_t)k * cap;
+  for (int iz = 0; iz < nz; ++iz) {
+    for (int iy = 0; iy < ny; ++iy) {
+      uint32_t rowbase = P.cell_off + (uint32_t)(P.dims[0] * (ys[iy] + P.dims[1] * zs[iz]));
+      for (int s = 0; s < ax.n; ++s) {
+        uint32_t a = start[rowbase + ax.lo[s]], e = start[rowbase + ax.hi[s] + 1];
+        for (uint32_t j = a; j < e; ++j) {
+          if (j == k) continue;
+          if (ex_dist(xi, pos[j], box) < lr) {
+            if (cnt < cap) row[cnt] = j;
+            ++cnt;
+          }
+        }
+      }
+    }
+  }
+  if (cnt > cap) { flags[0] = 1u; cnt = cap; }
+  nl_cnt[k] = cnt;
+}
+
+// heads: bin into the coarse head grid (replica-local cells), deterministic order inside a cell
+__global__ void k_head_index(const uint32_t* __restrict__ heads, const uint32_t* __restrict__ head_sys, uint32_t H,
+                             const uint32_t* __restrict__ slot_of, const float4* __restrict__ pos,
+                             const SysParams* __restrict__ sp, uint32_t* __restrict__ hcell_of,
+                             uint32_t* __restrict__ hcount) {
+  uint32_t h = blockIdx.x * blockDim.x + threadIdx.x;
+  if (h >= H) return;
+  const SysParams& P = sp[head_sys[h]];
+  float4 p = pos[slot_of[heads[h]]];
+  int cx = ex_cell_axis(p.x, P.box[0], P.hdims[0]);
+  int cy = ex_cell_axis(p.y, P.box[1], P.hdims[1]);
+  int cz = ex_cell_axis(p.z, P.box[2], P.hdims[2]);
+  uint32_t c = P.hcell_off + (uint32_t)(cx + P.hdims[0] * (cy + P.hdims[1] * cz));
+  hcell_of[h] = c;
+  atomicAdd(&hcount[c], 1u);
+}
+__global__ void k_head_scatter(const uint32_t* __restrict__ hcell_of, const uint32_t* __restrict__ hstart, uint32_t H,
+                               uint32_t* __restrict__ hcursor, uint32_t* __restrict__ hsorted) {
+  uint32_t h = blockIdx.x * blockDim.x + threadIdx.x;
+  if (h >= H) return;
+  uint32_t c = hcell_of[h];
+  hsorted[hstart[c] + atomicAdd(&hcursor[c], 1u)] = h;
+}
+__global__ void k_head_sort_cells(const uint32_t* __restrict__ hstart, uint32_t ncells, uint32_t* __restrict__ hsorted) {
+  uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+  if (c >= ncells) return;
+  uint32_t a = hstart[c], e = hstart[c + 1];
+  for (uint32_t x = a + 1; x < e; ++x) {
+    uint32_t v = hsorted[x];
+    uint32_t y = x;
+    while (y > a && hsorted[y - 1] > v) { hsorted[y] = hsorted[y - 1]; --y; }
+    hsorted[y] = v;
+  }
+}
+
+// soup/wgsl/electrostatics-long.wgsl:31-56 head list at rc_es + skin, via the head grid.
+// Entries are the neighbours' SLOT indices.
+__global__ void k_build_es_list(const uint32_t* __restrict__ heads, const uint32_t* __restrict__ head_sys, uint32_t H,
+                                const uint32_t* __restrict__ slot_of, const float4* __restrict__ pos,
+                                const SysParams* __restrict__ sp, const uint32_t* __restrict__ hcell_of,
+                                const uint32_t* __restrict__ hstart, const uint32_t* __restrict__ hsorted,
+                                uint32_t cap, uint32_t* __restrict__ es_nl, uint32_t* __restrict__ es_cnt,
+                                uint32_t* __restrict__ flags) {
+  uint32_t h = blockIdx.x * blockDim.x + threadIdx.x;
+  if (h >= H) return;
+  const SysParams& P = sp[head_sys[h]];
+  const uint32_t ks = slot_of[heads[h]];
+  const float4 xi = pos[ks];
+  const float box[3] = {P.box[0], P.box[1], P.box[2]};
+  uint32_t c = hcell_of[h] - P.hcell_off;
+  int q[3] = {(int)(c % (uint32_t)P.hdims[0]), (int)((c / (uint32_t)P.hdims[0]) % (uint32_t)P.hdims[1]),
+              (int)(c / ((uint32_t)P.hdims[0] * (uint32_t)P.hdims[1]))};
+  const int R = P.hwalk;
+  int ax[3][8], na[3] = {0, 0, 0};
+  for (int a = 0; a < 3; ++a)
+    for (int d = -R; d <= R; ++d) {
+      int v = ((q[a] + d) % P.hdims[a] + P.hdims[a]) % P.hdims[a];
+      bool dup = false;
+      for (int t = 0; t < na[a]; ++t) dup |= ax[a][t] == v;
+      if (!dup) ax[a][na[a]++] = v;
+    }
+  uint32_t cnt = 0;
+  uint32_t* row = es_nl + (size_t)h * cap;
+  for (int iz = 0; iz < na[2]; ++iz)
+    for (int iy = 0; iy < na[1]; ++iy)
+      for (int ix = 0; ix < na[0]; ++ix) {
+        uint32_t cc = P.hcell_off + (uint32_t)(ax[0][ix] + P.hdims[0] * (ax[1][iy] + P.hdims[1] * ax[2][iz]));
+        for (uint32_t t = hstart[cc]; t < hstart[cc + 1]; ++t) {
+          uint32_t g = hsorted[t];
+          if (g == h) continue;
+          uint32_t js = slot_of[heads[g]];
+          if (ex_dist(xi, pos[js], box) < P.es_list_range) {
+            if (cnt < cap) row[cnt] = js;
+            ++cnt;
+          }
+        }
+      }
+  if (cnt > cap) { flags[1] = 1u; cnt = cap; }
+  es_cnt[h] = cnt;
+}
+
+}  // namespace
+
+void launch_cell_index(Batch& b) {
+  cudaMemsetAsync(b.cell_count, 0, sizeof(uint32_t) * (b.ncells + 1), b.stream);
+  k_cell_index<<<nblocks(b.N), kBlock, 0, b.stream>>>(b.pos, b.sysid, b.sp, b.N, b.cell_of_slot, b.cell_count);
+}
+
+void launch_sort_and_gather(Batch& b) {
+  exclusive_scan(b.cell_count, b.cell_start, b.ncells, b.scan_tmp, b.stream);
+  cudaMemsetAsync(b.cell_cursor, 0, sizeof(uint32_t) * b.ncells, b.stream);
+  k_scatter<<<nblocks(b.N), kBlock, 0, b.stream>>>(b.cell_of_slot, b.cell_start, b.N, b.cell_cursor, b.perm);
+  k_sort_cells<<<nblocks(b.ncells), kBlock, 0, b.stream>>>(b.cell_start, b.ncells, b.id, b.perm);
+  k_gather<<<nblocks(b.N), kBlock, 0, b.stream>>>(b.N, b.perm, b.pos, b.vel, b.force, b.charge, b.slots, b.center,
+                                                   b.held, b.brng, b.trng, b.frozen, b.id, b.pos2, b.vel2, b.force2,
+                                                   b.charge2, b.slots2, b.center2, b.held2, b.brng2, b.trng2,
+                                                   b.frozen2, b.id2, b.slot_of, b.pos_ref);
+  std::swap(b.pos, b.pos2); std::swap(b.vel, b.vel2); std::swap(b.force, b.force2);
+  std::swap(b.charge, b.charge2); std::swap(b.slots, b.slots2); std::swap(b.center, b.center2);
+  std::swap(b.held, b.held2); std::swap(b.brng, b.brng2); std::swap(b.trng, b.trng2);
+  std::swap(b.frozen, b.frozen2); std::swap(b.id, b.id2);
+  // the cell of every new slot: cell_start is monotone, so recompute from the sorted positions
+  cudaMemsetAsync(b.cell_count, 0, sizeof(uint32_t) * (b.ncells + 1), b.stream);
+  k_cell_index<<<nblocks(b.N), kBlock, 0, b.stream>>>(b.pos, b.sysid, b.sp, b.N, b.cell_of_slot, b.cell_count);
+}
+
+void launch_build_lists(Batch& b) {
+  k_build_list<<<nblocks(b.N, 128), 128, 0, b.stream>>>(b.pos, b.sysid, b.sp, b.cell_of_slot, b.cell_start, b.N,
+                                                        b.list_cap, b.nl, b.nl_cnt, b.flags);
+}
+
+void launch_build_es_lists(Batch& b) {
+  if (b.H == 0) return;
+  cudaMemsetAsync(b.hcell_count, 0, sizeof(uint32_t) * (b.nhcells + 1), b.stream);
+  k_head_index<<<nblocks(b.H), kBlock, 0, b.stream>>>(b.heads, b.head_sys, b.H, b.slot_of, b.pos, b.sp, b.hcell_of,
+                                                       b.hcell_count);
+  exclusive_scan(b.hcell_count, b.hcell_start, b.nhcells, b.scan_tmp, b.stream);
+  cudaMemsetAsync(b.hcell_cursor, 0, sizeof(uint32_t) * b.nhcells, b.stream);
+  k_head_scatter<<<nblocks(b.H), kBlock, 0, b.stream>>>(b.hcell_of, b.hcell_start, b.H, b.hcell_cursor, b.hsorted);
+  k_head_sort_cells<<<nblocks(b.nhcells), kBlock, 0, b.stream>>>(b.hcell_start, b.nhcells, b.hsorted);
+  k_build_es_list<<<nblocks(b.H, 128), 128, 0, b.stream>>>(b.heads, b.head_sys, b.H, b.slot_of, b.pos, b.sp,
+                                                           b.hcell_of, b.hcell_start, b.hsorted, b.es_cap, b.es_nl,
+                                                           b.es_cnt, b.flags);
+}
+
+}  // namespace soup

@@ -1,0 +1,902 @@
+// soup_capi.cu -- the C ABI (include/soup_b200.h): lifecycle, uploads/readbacks, the step schedule.
+//
+// Reference: soup/src/sim.ts:95-600 (createSoup and the SoupSystem surface), soup/src/soup-integrate.ts
+// :83-175 (per-step dispatch order and the chunked stepper with its guards and the constant-pH sweep),
+// soup/src/soup-grid-verlet.ts:236-313 (rebuild sequence and assertVerletSafety), soup/src/soup-health.ts
+// (assertStateFinite), soup/src/soup-readback.ts (readbacks), soup/src/soup-relax.ts:87-185.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "soup_internal.h"
+
+using namespace soup;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+constexpr uint32_t NONE = SOUP_NONE_U32;
+constexpr uint32_t FLAG_WORDS = 16;
+
+template <class T> T* dalloc(size_t n) {
+  T* p = nullptr;
+  if (n == 0) n = 1;
+  cudaError_t e = cudaMalloc(&p, n * sizeof(T));
+  if (e != cudaSuccess) throw CudaError(e, "cudaMalloc", __FILE__, __LINE__);
+  return p;
+}
+template <class T> void dfree(T*& p) { if (p) cudaFree(p); p = nullptr; }
+
+struct SoupException {
+  int code;
+  std::string msg;
+};
+[[noreturn]] void fail(int code, const std::string& m) { throw SoupException{code, m}; }
+
+float sigma_v_f32(float gamma, float kT, float dt) {
+  volatile float t = 2.0f * gamma;   // step.wgsl:130: sqrt(2.0 * P.gamma * P.kT * P.dt), f32, in order
+  t = t * kT;
+  t = t * dt;
+  return std::sqrt((float)t);
+}
+
+// ---- parameters ----------------------------------------------------------------------------
+void check_config(const SoupConfig& c) {
+  if (c.abi_version != SOUP_ABI_VERSION) fail(SOUP_E_ARG, "SoupConfig.abi_version does not match this library");
+  if (c.n == 0) fail(SOUP_E_ARG, "createSoup: the starting composition is empty");
+  if (c.n_kinds == 0 || c.n_kinds > SOUP_MAX_KINDS) fail(SOUP_E_ARG, "n_kinds must be 1..8");
+  uint64_t sum = 0;
+  for (uint32_t k = 0; k < c.n_kinds; ++k) sum += c.counts[k];
+  if (sum != c.n) fail(SOUP_E_ARG, "SoupConfig.n must equal the sum of counts");
+  for (int a = 0; a < 3; ++a)
+    if (!(c.box[a] > 0)) fail(SOUP_E_GEOMETRY, "box sides must be positive");
+  if (!(c.list_range > 0) || c.list_capacity == 0) fail(SOUP_E_ARG, "list_range and list_capacity must be positive");
+  if (c.n_rules > SOUP_MAX_RULES) fail(SOUP_E_ARG, "at most 4 bond rules");
+  if (c.bond_interval == 0) fail(SOUP_E_ARG, "bond_interval must be >= 1");
+  if (!c.rebuild_on_drift && c.rebuild_every == 0) fail(SOUP_E_ARG, "rebuild_every must be >= 1");
+  if (c.es_enabled && (c.charged_kind < 0 || c.charged_kind >= (int)c.n_kinds)) fail(SOUP_E_ARG, "charged_kind out of range");
+  if (c.es_enabled && c.es_list_capacity == 0) fail(SOUP_E_ARG, "es_list_capacity must be positive");
+  if (c.es_enabled && c.sweep_every == 0) fail(SOUP_E_ARG, "sweep_every must be >= 1");
+}
+
+Shared make_shared(const SoupConfig& c) {
+  Shared s{};
+  s.n_kinds = c.n_kinds;
+  s.sigma = (float)c.sigma; s.eps = (float)c.epsilon; s.b_tt = (float)c.b_tt; s.k_fene = (float)c.k_fene;
+  s.r_inf = (float)c.r_inf; s.k_bend = (float)c.k_bend; s.r_bend = (float)c.r_bend; s.wc = (float)c.wc;
+  s.c6 = (float)std::pow(2.0, (double)0.16666667f);
+  { volatile float t = s.c6 * s.b_tt; s.rc_attr = t; }
+  s.attr_k = 3.14159265f / (2.0f * s.wc);
+  s.attr_amp = s.eps * 3.14159265f / (2.0f * s.wc);
+  float rmax = s.rc_attr + s.wc;
+  for (uint32_t k = 0; k < SOUP_KMAX; ++k) {
+    s.radius[k] = (float)c.radius[k];
+    s.cls[k] = c.kind_class[k] & 3u;
+  }
+  for (uint32_t i = 0; i < SOUP_KMAX; ++i)
+    for (uint32_t j = 0; j < SOUP_KMAX; ++j) {
+      volatile float b = s.sigma * (s.radius[i] + s.radius[j]);
+      b = b * 0.5f;
+      volatile float w = s.c6 * b;
+      PairConst& p = s.pair[i * SOUP_KMAX + j];
+      p.wcut = w; p.wcut2 = w * w; p.b2 = b * b;
+      p.attr = (float)c.attr_scale[s.cls[i]][s.cls[j]];
+      if (i < c.n_kinds && j < c.n_kinds) rmax = std::max(rmax, (float)w);
+    }
+  if (c.es_enabled) rmax = std::max(rmax, (float)c.es_split_radius);
+  s.rmax2 = rmax * rmax * 1.0001f;
+  for (uint32_t r = 0; r < SOUP_RMAX; ++r) {
+    const bool on = r < c.n_rules;
+    s.kindA[r] = on ? (float)c.rule_kind_a[r] : -1.f; s.kindB[r] = on ? (float)c.rule_kind_b[r] : -1.f;
+    s.att_form[r] = on ? (float)c.attempt_form[r] : 0.f; s.att_break[r] = on ? (float)c.attempt_break[r] : 0.f;
+    s.acc_form[r] = on ? (float)c.accept_form[r] : 0.f; s.acc_break[r] = on ? (float)c.accept_break[r] : 0.f;
+    s.req_cat[r] = on ? (float)c.requires_catalyst[r] : 0.f;
+    s.roleA[r] = on ? (float)c.role_a[r] : 0.f; s.roleB[r] = on ? (float)c.role_b[r] : 0.f;
+  }
+  s.cat_kind = (float)c.catalyst_kind; s.head_terminal = (float)c.head_terminal_only;
+  s.head_cap = (float)c.head_chain_capacity; s.max_hold = (float)c.max_hold_steps; s.interval = (float)c.bond_interval;
+  return s;
+}
+
+void grid_of(const double box[3], double range, int walk, int dims[3]) {
+  const double cell = range / walk;
+  for (int a = 0; a < 3; ++a) dims[a] = std::max(1, (int)std::floor(box[a] / cell));
+}
+
+SysParams make_sys(const SoupConfig& c) {
+  SysParams p{};
+  for (int a = 0; a < 3; ++a) { p.box[a] = (float)c.box[a]; p.inv_box[a] = 1.0f / p.box[a]; p.d_box[a] = c.box[a]; }
+  p.list_range = (float)c.list_range;
+  const bool es = c.es_enabled != 0;
+  p.es_on = es ? 1u : 0u;
+  p.es_A = es ? (float)c.es_coeff_a : 0.f;
+  p.es_kappa = (float)c.es_kappa; p.es_rc = (float)c.es_cutoff; p.es_fc = (float)c.es_shift_f;
+  p.es_split = (float)c.es_split_radius; p.es_list_range = (float)c.es_list_range;
+  p.wall_r = (float)c.wall_radius; p.wall_k = (float)c.wall_k;
+  p.kT = (float)c.kT; p.gamma = (float)c.gamma; p.dt = (float)c.dt;
+  { volatile float t = 0.5f * p.dt; p.hdt = t; volatile float g = p.gamma * p.dt; p.gdt = g; }
+  p.sigma_v = sigma_v_f32(p.gamma, p.kT, p.dt);
+  p.acid = (float)c.acid_soap_scale;
+  p.skin_half2 = (float)(0.25 * c.skin * c.skin);
+  p.walk = 2;
+  grid_of(c.box, c.list_range, p.walk, p.dims);
+  p.hwalk = 2;
+  grid_of(c.box, es ? c.es_list_range : c.list_range, p.hwalk, p.hdims);
+  p.list_cap = c.list_capacity;
+  p.es_cap = c.es_list_capacity;
+  p.charged_kind = c.charged_kind;
+  p.d_A = es ? c.es_coeff_a : 0.0; p.d_kappa = c.es_kappa; p.d_rc = c.es_cutoff; p.d_shiftU = c.es_shift_u;
+  p.d_shiftF = c.es_shift_f; p.d_pka = c.pka_intrinsic; p.d_ph = c.ph; p.d_kT = c.kT; p.d_q = c.charge_deprotonated;
+  p.d_acid = c.acid_soap_scale; p.d_rcattr = c.rc_attr; p.d_wc = c.wc; p.d_eps = c.epsilon;
+  return p;
+}
+
+uint64_t cells_of(const int d[3]) { return (uint64_t)d[0] * d[1] * d[2]; }
+
+// ---- batch construction ----------------------------------------------------------------------
+void alloc_grids(Batch& b) {
+  dfree(b.cell_count); dfree(b.cell_start); dfree(b.cell_cursor); dfree(b.scan_tmp);
+  dfree(b.hcell_count); dfree(b.hcell_start); dfree(b.hcell_cursor);
+  uint64_t nc = 0, nh = 0;
+  for (uint32_t r = 0; r < b.R; ++r) {
+    b.hsp[r].cell_off = (uint32_t)nc;
+    nc += cells_of(b.hsp[r].dims);
+    b.hsp[r].hcell_off = (uint32_t)nh;
+    nh += cells_of(b.hsp[r].hdims);
+  }
+  if (nc > 0x7fffffffull || nh > 0x7fffffffull) fail(SOUP_E_GEOMETRY, "neighbour grid too large");
+  b.ncells = (uint32_t)nc;
+  b.nhcells = (uint32_t)nh;
+  b.cell_count = dalloc<uint32_t>(nc + 1);
+  b.cell_start = dalloc<uint32_t>(nc + 1);
+  b.cell_cursor = dalloc<uint32_t>(nc + 1);
+  b.hcell_count = dalloc<uint32_t>(nh + 1);
+  b.hcell_start = dalloc<uint32_t>(nh + 1);
+  b.hcell_cursor = dalloc<uint32_t>(nh + 1);
+  const uint64_t m = std::max(nc, nh);
+  b.scan_tmp = dalloc<uint32_t>(4 * (m / 4096 + 64) + 256);
+}
+
+void upload_params(Batch& b) {
+  SOUP_CUDA_TRY(cudaMemcpyAsync(b.sp, b.hsp.data(), sizeof(SysParams) * b.R, cudaMemcpyHostToDevice, b.stream));
+  SOUP_CUDA_TRY(cudaMemcpyAsync(b.shared, &b.hs, sizeof(Shared), cudaMemcpyHostToDevice, b.stream));
+}
+
+void rebuild(Batch& b) {
+  launch_cell_index(b);
+  launch_sort_and_gather(b);
+  launch_build_lists(b);
+  launch_build_es_lists(b);
+  SOUP_CUDA_TRY(cudaMemsetAsync(b.drift_bits, 0, sizeof(uint32_t) * b.R, b.stream));
+  b.rebuilds++;
+}
+
+void force_pass(Batch& b) {   // encodeVerletRebuild + encodeSoupForceList (the priming / recompute pass)
+  rebuild(b);
+  launch_force(b);
+  b.force_fresh = true;
+}
+
+// Upload replica r's state from original-order host arrays (NULL members: fresh values).
+void upload_replica(Batch& b, uint32_t r, const SoupInitState* init, bool fresh_allowed) {
+  const SoupConfig& c = b.cfg[r];
+  const uint32_t n = c.n, off = b.hsp[r].slot_off;
+  std::vector<float> pos(4 * (size_t)n), vel(4 * (size_t)n), charge(n);
+  std::vector<uint32_t> slots(3 * (size_t)n, NONE), center(n, NONE), held(n, 0), brng(n), trng(n), frozen32(n, 0);
+  if (fresh_allowed) host_fresh_state(c, pos.data(), vel.data(), frozen32.data(), brng.data(), trng.data());
+  if (init) {
+    if (init->positions) std::memcpy(pos.data(), init->positions, 16 * (size_t)n);
+    if (init->velocities) std::memcpy(vel.data(), init->velocities, 16 * (size_t)n);
+    if (init->bond_slots) std::memcpy(slots.data(), init->bond_slots, 12 * (size_t)n);
+    if (init->center_link) std::memcpy(center.data(), init->center_link, 4 * (size_t)n);
+    if (init->center_held) std::memcpy(held.data(), init->center_held, 4 * (size_t)n);
+    if (init->bond_rng) std::memcpy(brng.data(), init->bond_rng, 4 * (size_t)n);
+    if (init->thermo_rng) std::memcpy(trng.data(), init->thermo_rng, 4 * (size_t)n);
+    if (init->frozen) std::memcpy(frozen32.data(), init->frozen, 4 * (size_t)n);
+  }
+  uint32_t prot = c.protonation_rng;
+  if (init && init->charges) {
+    std::memcpy(charge.data(), init->charges, 4 * (size_t)n);
+  } else {
+    uint32_t pr = 0;
+    host_initial_charges(c, pos.data(), charge.data(), &pr);
+    if (c.protonation_rng == 0) prot = pr;
+  }
+  b.prot_rng[r] = prot;
+  for (uint32_t i = 0; i < n; ++i) {
+    for (int a = 0; a < 3; ++a) {
+      uint32_t& v = slots[3 * (size_t)i + a];
+      if (v != NONE) { if (v >= n) fail(SOUP_E_ARG, "bond_slots names a particle outside the system"); v += off; }
+    }
+    if (center[i] != NONE) { if (center[i] >= n) fail(SOUP_E_ARG, "center_link names a particle outside the system"); center[i] += off; }
+    const float kf = pos[4 * (size_t)i + 3];
+    if (!(kf >= 0.f && kf < (float)c.n_kinds) || kf != std::floor(kf)) fail(SOUP_E_ARG, "positions[4i+3] must hold a kind index");
+  }
+  std::vector<uint8_t> frozen(n);
+  std::vector<uint32_t> ids(n);
+  for (uint32_t i = 0; i < n; ++i) { frozen[i] = frozen32[i] ? 1 : 0; ids[i] = off + i; }
+  auto up = [&](void* dst, const void* src, size_t bytes) {
+    SOUP_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, b.stream));
+  };
+  up(b.pos + off, pos.data(), 16 * (size_t)n);
+  up(b.vel + off, vel.data(), 16 * (size_t)n);
+  SOUP_CUDA_TRY(cudaMemsetAsync(b.force + off, 0, 16 * (size_t)n, b.stream));
+  up(b.charge + off, charge.data(), 4 * (size_t)n);
+  up(b.slots + 3 * (size_t)off, slots.data(), 12 * (size_t)n);
+  up(b.center + off, center.data(), 4 * (size_t)n);
+  up(b.held + off, held.data(), 4 * (size_t)n);
+  up(b.brng + off, brng.data(), 4 * (size_t)n);
+  up(b.trng + off, trng.data(), 4 * (size_t)n);
+  up(b.frozen + off, frozen.data(), n);
+  up(b.id + off, ids.data(), 4 * (size_t)n);
+  up(b.slot_of + off, ids.data(), 4 * (size_t)n);
+  if (init && init->events) up(b.events + 2 * SOUP_MAX_RULES * r, init->events, 8 * (size_t)c.n_rules);
+  if (init && init->desorb_events) up(b.desorb + 2 * r, init->desorb_events, 8);
+  up(b.prot_rng_dev + r, &b.prot_rng[r], 4);
+  SOUP_CUDA_TRY(cudaStreamSynchronize(b.stream));   // host vectors go out of scope
+}
+
+Batch* make_batch(const SoupConfig* cfgs, const SoupInitState* inits, uint32_t R) {
+  if (!cfgs || R == 0) fail(SOUP_E_ARG, "no configuration given");
+  if (R > 255) fail(SOUP_E_ARG, "at most 255 replicas per batch");
+  std::unique_ptr<Batch> bp(new Batch());
+  Batch& b = *bp;
+  b.R = R;
+  b.cfg.assign(cfgs, cfgs + R);
+  for (uint32_t r = 0; r < R; ++r) check_config(b.cfg[r]);
+  SOUP_CUDA_TRY(cudaGetDevice(&b.device));
+  b.hs = make_shared(b.cfg[0]);
+  for (uint32_t r = 1; r < R; ++r) {
+    Shared o = make_shared(b.cfg[r]);
+    o.rmax2 = b.hs.rmax2 = std::max(o.rmax2, b.hs.rmax2);
+    if (std::memcmp(&o, &b.hs, sizeof(Shared)) != 0)
+      fail(SOUP_E_ARG, "replicas of one batch must share the monomer table, force field and bond rules");
+    if (b.cfg[r].global_step != b.cfg[0].global_step || b.cfg[r].bond_interval != b.cfg[0].bond_interval ||
+        b.cfg[r].rebuild_on_drift != b.cfg[0].rebuild_on_drift || b.cfg[r].rebuild_every != b.cfg[0].rebuild_every ||
+        (b.cfg[r].es_enabled && b.cfg[0].es_enabled && b.cfg[r].sweep_every != b.cfg[0].sweep_every) ||
+        b.cfg[r].chunk_steps != b.cfg[0].chunk_steps)
+      fail(SOUP_E_ARG, "replicas of one batch must share the step schedule");
+  }
+  uint64_t N = 0, H = 0;
+  b.hsp.resize(R);
+  b.list_cap = 0;
+  b.es_cap = 0;
+  std::vector<std::vector<uint32_t>> heads(R);
+  for (uint32_t r = 0; r < R; ++r) {
+    const SoupConfig& c = b.cfg[r];
+    b.hsp[r] = make_sys(c);
+    b.hsp[r].slot_off = (uint32_t)N;
+    b.hsp[r].n = c.n;
+    N += c.n;
+    b.list_cap = std::max(b.list_cap, c.list_capacity);
+    if (c.es_enabled) b.es_cap = std::max(b.es_cap, c.es_list_capacity);
+  }
+  if (N > 0xFFFFFFF0ull) fail(SOUP_E_ARG, "too many particles");
+  b.N = (uint32_t)N;
+  b.list_cap = (b.list_cap + 7u) & ~7u;
+  b.prot_rng.assign(R, 0);
+  b.step.assign(R, 0);
+  b.next_sweep.assign(R, UINT64_MAX);
+  SOUP_CUDA_TRY(cudaStreamCreateWithFlags(&b.stream, cudaStreamNonBlocking));
+
+  const size_t n = b.N;
+  b.pos = dalloc<float4>(n); b.vel = dalloc<float4>(n); b.force = dalloc<float4>(n); b.pos_ref = dalloc<float4>(n);
+  b.charge = dalloc<float>(n); b.slots = dalloc<uint32_t>(3 * n); b.center = dalloc<uint32_t>(n);
+  b.held = dalloc<uint32_t>(n); b.brng = dalloc<uint32_t>(n); b.trng = dalloc<uint32_t>(n); b.frozen = dalloc<uint8_t>(n);
+  b.id = dalloc<uint32_t>(n); b.slot_of = dalloc<uint32_t>(n);
+  b.pos2 = dalloc<float4>(n); b.vel2 = dalloc<float4>(n); b.force2 = dalloc<float4>(n); b.charge2 = dalloc<float>(n);
+  b.slots2 = dalloc<uint32_t>(3 * n); b.center2 = dalloc<uint32_t>(n); b.held2 = dalloc<uint32_t>(n);
+  b.brng2 = dalloc<uint32_t>(n); b.trng2 = dalloc<uint32_t>(n); b.frozen2 = dalloc<uint8_t>(n); b.id2 = dalloc<uint32_t>(n);
+  b.cell_of_slot = dalloc<uint32_t>(n); b.perm = dalloc<uint32_t>(n);
+  b.nl = dalloc<uint32_t>(n * (size_t)b.list_cap); b.nl_cnt = dalloc<uint32_t>(n);
+  b.sysid = dalloc<uint8_t>(n);
+  b.sp = dalloc<SysParams>(R); b.shared = dalloc<Shared>(1);
+  b.flags = dalloc<uint32_t>(FLAG_WORDS + 2 * (size_t)R);
+  b.events = dalloc<uint32_t>(2 * SOUP_MAX_RULES * (size_t)R);
+  b.desorb = dalloc<uint32_t>(2 * (size_t)R);
+  b.drift_bits = dalloc<uint32_t>(R);
+  b.bond_items = dalloc<uint32_t>(10 * n); b.bond_nitems = dalloc<uint32_t>(1);
+  b.uf_parent = dalloc<uint32_t>(n); b.comp_min = dalloc<uint32_t>(n); b.item_done = dalloc<uint8_t>(n);
+  b.has_item = dalloc<uint32_t>(n);
+  b.prot_rng_dev = dalloc<uint32_t>(R);
+  b.sweep_out = dalloc<double>(4 * (size_t)R);
+  SOUP_CUDA_TRY(cudaMemsetAsync(b.flags, 0, sizeof(uint32_t) * (FLAG_WORDS + 2 * R), b.stream));
+  SOUP_CUDA_TRY(cudaMemsetAsync(b.events, 0, sizeof(uint32_t) * 2 * SOUP_MAX_RULES * R, b.stream));
+  SOUP_CUDA_TRY(cudaMemsetAsync(b.desorb, 0, sizeof(uint32_t) * 2 * R, b.stream));
+  SOUP_CUDA_TRY(cudaMemsetAsync(b.drift_bits, 0, sizeof(uint32_t) * R, b.stream));
+  {
+    std::vector<uint8_t> sid(n);
+    for (uint32_t r = 0; r < R; ++r)
+      std::fill(sid.begin() + b.hsp[r].slot_off, sid.begin() + b.hsp[r].slot_off + b.cfg[r].n, (uint8_t)r);
+    SOUP_CUDA_TRY(cudaMemcpyAsync(b.sysid, sid.data(), n, cudaMemcpyHostToDevice, b.stream));
+    SOUP_CUDA_TRY(cudaStreamSynchronize(b.stream));
+  }
+  // state, per replica
+  for (uint32_t r = 0; r < R; ++r) {
+    upload_replica(b, r, inits ? &inits[r] : nullptr, true);
+    b.step[r] = b.cfg[r].global_step;
+    b.next_sweep[r] = b.cfg[r].es_enabled ? b.cfg[r].global_step + b.cfg[r].sweep_every : UINT64_MAX;
+  }
+  // heads: titratable beads in index order (static, electrostatics-long.wgsl:15-29)
+  std::vector<uint32_t> hall, hsys;
+  for (uint32_t r = 0; r < R; ++r) {
+    const SoupConfig& c = b.cfg[r];
+    b.hsp[r].head_off = (uint32_t)hall.size();
+    if (c.es_enabled) {
+      std::vector<float> pos(4 * (size_t)c.n);
+      SOUP_CUDA_TRY(cudaMemcpy(pos.data(), b.pos + b.hsp[r].slot_off, 16 * (size_t)c.n, cudaMemcpyDeviceToHost));
+      for (uint32_t i = 0; i < c.n; ++i)
+        if (pos[4 * (size_t)i + 3] == (float)c.charged_kind) { hall.push_back(b.hsp[r].slot_off + i); hsys.push_back(r); }
+    }
+    b.hsp[r].nheads = (uint32_t)hall.size() - b.hsp[r].head_off;
+  }
+  b.H = (uint32_t)hall.size();
+  b.heads = dalloc<uint32_t>(b.H); b.head_sys = dalloc<uint32_t>(b.H);
+  b.es_nl = dalloc<uint32_t>((size_t)b.H * std::max<uint32_t>(b.es_cap, 1)); b.es_cnt = dalloc<uint32_t>(b.H);
+  b.hcell_of = dalloc<uint32_t>(b.H); b.hsorted = dalloc<uint32_t>(b.H);
+  if (b.H) {
+    SOUP_CUDA_TRY(cudaMemcpy(b.heads, hall.data(), 4 * (size_t)b.H, cudaMemcpyHostToDevice));
+    SOUP_CUDA_TRY(cudaMemcpy(b.head_sys, hsys.data(), 4 * (size_t)b.H, cudaMemcpyHostToDevice));
+  }
+  alloc_grids(b);
+  upload_params(b);
+  b.tpp = 8;
+  force_pass(b);   // priming pass (soup/src/sim.ts:396-408)
+  SOUP_CUDA_TRY(cudaStreamSynchronize(b.stream));
+  SOUP_CUDA_TRY(cudaGetLastError());
+  for (uint32_t r = 0; r < R; ++r) {
+    SoupHandle* h = new SoupHandle();
+    h->b = &b;
+    h->r = r;
+    b.views.push_back(h);
+  }
+  return bp.release();
+}
+
+void destroy_batch(Batch* b) {
+  if (!b) return;
+  cudaStreamSynchronize(b->stream);
+  void* ptrs[] = {b->pos, b->vel, b->force, b->pos_ref, b->charge, b->slots, b->center, b->held, b->brng, b->trng,
+                  b->frozen, b->id, b->slot_of, b->pos2, b->vel2, b->force2, b->charge2, b->slots2, b->center2,
+                  b->held2, b->brng2, b->trng2, b->frozen2, b->id2, b->cell_of_slot, b->cell_count, b->cell_start,
+                  b->cell_cursor, b->perm, b->scan_tmp, b->nl, b->nl_cnt, b->heads, b->head_sys, b->es_nl,
+                  b->es_cnt, b->hcell_count, b->hcell_start, b->hcell_cursor, b->hsorted, b->hcell_of, b->flags,
+                  b->events, b->desorb, b->drift_bits, b->bond_items, b->bond_nitems, b->uf_parent, b->comp_min,
+                  b->item_done, b->has_item, b->sweep_out, b->prot_rng_dev, b->sp, b->shared, b->sysid, b->occ,
+                  b->vis, b->frontier};
+  for (void* p : ptrs) if (p) cudaFree(p);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  for (SoupHandle* h : b->views) delete h;
+  delete b;
+}
+
+// ---- guards (soup/src/soup-health.ts, soup/src/soup-grid-verlet.ts:266-313) ----------------
+void guards(Batch& b, uint64_t chunk_start) {
+  launch_nonfinite(b);
+  std::vector<uint32_t> fl(FLAG_WORDS + 2 * b.R), drift(b.R);
+  SOUP_CUDA_TRY(cudaMemcpyAsync(fl.data(), b.flags, 4 * fl.size(), cudaMemcpyDeviceToHost, b.stream));
+  SOUP_CUDA_TRY(cudaMemcpyAsync(drift.data(), b.drift_bits, 4 * (size_t)b.R, cudaMemcpyDeviceToHost, b.stream));
+  SOUP_CUDA_TRY(cudaStreamSynchronize(b.stream));
+  SOUP_CUDA_TRY(cudaGetLastError());
+  for (uint32_t r = 0; r < b.R; ++r) {
+    const uint32_t np = fl[FLAG_WORDS + 2 * r], nv = fl[FLAG_WORDS + 2 * r + 1];
+    if (np || nv) {
+      char m[512];
+      std::snprintf(m, sizeof m,
+                    "non-finite state at step=%llu: non-finite components of positions=%u, velocities=%u of %u "
+                    "(appeared in the step interval %llu..%llu) -- the computation diverged (Inf/NaN), any further "
+                    "numbers from this run are meaningless",
+                    (unsigned long long)b.step[r], np, nv, 3 * b.cfg[r].n, (unsigned long long)chunk_start,
+                    (unsigned long long)b.step[r]);
+      fail(SOUP_E_NONFINITE, m);
+    }
+  }
+  if (fl[0]) {
+    fail(SOUP_E_LIST_OVERFLOW, "Verlet list: verletList.listCapacity=" + std::to_string(b.list_cap) +
+                                   " was insufficient -- at least one particle found more candidates than the list "
+                                   "holds (data may have been silently dropped)");
+  }
+  if (fl[1]) {
+    fail(SOUP_E_ES_OVERFLOW, "long-range electrostatics list: longRangeListCapacity=" + std::to_string(b.es_cap) +
+                                 " was insufficient -- data may have been silently dropped");
+  }
+  if (fl[6]) fail(SOUP_E_STATE, "bond pass: item buffer overflow");
+  for (uint32_t r = 0; r < b.R; ++r) {
+    float d2;
+    std::memcpy(&d2, &drift[r], 4);
+    const double d = std::sqrt(std::max(0.0, (double)d2));
+    if (!std::isfinite(d))
+      fail(SOUP_E_NONFINITE, "Verlet list: the measured drift is not a number -- the state is already non-finite");
+    if (d > b.cfg[r].skin / 2 + 1e-6) {
+      char m[320];
+      std::snprintf(m, sizeof m,
+                    "Verlet list: the measured drift %.4f exceeds skin/2=%.4f -- the analytic bound (verletList.basis) "
+                    "did not hold for the real trajectory, the rebuild was not frequent enough",
+                    d, b.cfg[r].skin / 2);
+      fail(SOUP_E_DRIFT, m);
+    }
+  }
+}
+
+bool drift_exceeds(Batch& b) {
+  std::vector<uint32_t> drift(b.R);
+  SOUP_CUDA_TRY(cudaMemcpyAsync(drift.data(), b.drift_bits, 4 * (size_t)b.R, cudaMemcpyDeviceToHost, b.stream));
+  SOUP_CUDA_TRY(cudaStreamSynchronize(b.stream));
+  for (uint32_t r = 0; r < b.R; ++r) {
+    float d2;
+    std::memcpy(&d2, &drift[r], 4);
+    if (!(d2 <= b.hsp[r].skin_half2)) return true;
+  }
+  return false;
+}
+
+void sweep_all(Batch& b, std::vector<SoupSweepResult>* out) {
+  launch_sweep(b, SOUP_NONE_U32);
+  std::vector<double> so(4 * (size_t)b.R);
+  SOUP_CUDA_TRY(cudaMemcpyAsync(so.data(), b.sweep_out, 8 * so.size(), cudaMemcpyDeviceToHost, b.stream));
+  SOUP_CUDA_TRY(cudaMemcpyAsync(b.prot_rng.data(), b.prot_rng_dev, 4 * (size_t)b.R, cudaMemcpyDeviceToHost, b.stream));
+  force_pass(b);   // soup/src/soup-protonation.ts:62-73: F(x) is stale after the charges changed
+  SOUP_CUDA_TRY(cudaStreamSynchronize(b.stream));
+  b.sweeps++;
+  if (out) {
+    out->resize(b.R);
+    for (uint32_t r = 0; r < b.R; ++r) {
+      SoupSweepResult& s = (*out)[r];
+      s.heads = (uint32_t)so[4 * r];
+      s.attempts = s.heads;
+      s.accepted = (uint32_t)so[4 * r + 1];
+      s.d_es_mean_kt = so[4 * r + 2];
+      s.deprotonated = (uint32_t)so[4 * r + 3];
+      s.alpha = s.heads ? (double)s.deprotonated / s.heads : 0.0;
+    }
+  }
+}
+
+// soup/src/soup-integrate.ts:136-175, for every replica in lockstep
+void step_batch(Batch& b, uint64_t n) {
+  const SoupConfig& c0 = b.cfg[0];
+  const uint64_t chunk_max = c0.chunk_steps ? c0.chunk_steps : 1000;
+  uint64_t done = 0;
+  while (done < n) {
+    const uint64_t chunk = std::min(chunk_max, n - done);
+    const uint64_t chunk_start = b.step[0];
+    for (uint64_t k = 0; k < chunk; ++k) {
+      const uint64_t g = b.step[0];
+      const bool bonds = g % c0.bond_interval == 0;
+      launch_kick_drift(b);
+      bool reb;
+      if (c0.rebuild_on_drift) reb = drift_exceeds(b);
+      else reb = g % c0.rebuild_every == 0;
+      if (reb) rebuild(b);
+      launch_force(b);
+      if (bonds) launch_bonds(b);
+      launch_kick_thermo(b);
+      for (uint32_t r = 0; r < b.R; ++r) b.step[r]++;
+    }
+    guards(b, chunk_start);
+    bool any = false;
+    for (uint32_t r = 0; r < b.R; ++r)
+      if (b.cfg[r].es_enabled && b.step[r] >= b.next_sweep[r]) { any = true; b.next_sweep[r] = b.step[r] + b.cfg[r].sweep_every; }
+    if (any) sweep_all(b, nullptr);
+    done += chunk;
+  }
+}
+
+// ---- readbacks -------------------------------------------------------------------------------
+// Download one array of replica r in slot order and scatter it into original order.
+template <class T>
+void read_replica(Batch& b, uint32_t r, const T* dev, uint32_t per, T* dst, bool map_ids) {
+  const uint32_t n = b.cfg[r].n, off = b.hsp[r].slot_off;
+  std::vector<T> tmp((size_t)n * per);
+  std::vector<uint32_t> ids(n);
+  SOUP_CUDA_TRY(cudaMemcpyAsync(tmp.data(), dev + (size_t)off * per, sizeof(T) * tmp.size(), cudaMemcpyDeviceToHost, b.stream));
+  SOUP_CUDA_TRY(cudaMemcpyAsync(ids.data(), b.id + off, 4 * (size_t)n, cudaMemcpyDeviceToHost, b.stream));
+  SOUP_CUDA_TRY(cudaStreamSynchronize(b.stream));
+  for (uint32_t k = 0; k < n; ++k) {
+    const uint32_t i = ids[k] - off;
+    for (uint32_t e = 0; e < per; ++e) {
+      T v = tmp[(size_t)k * per + e];
+      if constexpr (std::is_same<T, uint32_t>::value) {
+        if (map_ids && v != NONE) v -= off;
+      }
+      dst[(size_t)i * per + e] = v;
+    }
+  }
+}
+
+void need(size_t bytes, size_t want) {
+  if (bytes != want) fail(SOUP_E_ARG, "destination size " + std::to_string(bytes) + " does not match the array size " + std::to_string(want));
+}
+
+// ---- API plumbing ----------------------------------------------------------------------------
+template <class F> int guarded(SoupHandle* h, F&& f) {
+  try {
+    if (!h || !h->b) fail(SOUP_E_ARG, "NULL handle");
+    SOUP_CUDA_TRY(cudaSetDevice(h->b->device));
+    f(*h->b, h->r);
+    h->err.clear();
+    return SOUP_OK;
+  } catch (const SoupException& e) {
+    if (h) h->err = e.msg;
+    g_last_error = e.msg;
+    return e.code;
+  } catch (const CudaError& e) {
+    std::string m = "CUDA: " + e.msg;
+    if (h) h->err = m;
+    g_last_error = m;
+    return e.code == cudaErrorMemoryAllocation ? SOUP_E_OOM : SOUP_E_CUDA;
+  } catch (const std::exception& e) {
+    if (h) h->err = e.what();
+    g_last_error = e.what();
+    return SOUP_E_STATE;
+  }
+}
+
+}  // namespace
+
+extern "C" {
+
+int soup_create(const SoupConfig* cfg, const SoupInitState* init, SoupHandle** out) {
+  try {
+    if (!out) fail(SOUP_E_ARG, "NULL output handle");
+    *out = nullptr;
+    Batch* b = make_batch(cfg, init, 1);
+    SoupHandle* h = b->views[0];
+    h->owns = true;
+    *out = h;
+    return SOUP_OK;
+  } catch (const SoupException& e) {
+    g_last_error = e.msg;
+    return e.code;
+  } catch (const CudaError& e) {
+    g_last_error = "CUDA: " + e.msg;
+    return e.code == cudaErrorMemoryAllocation ? SOUP_E_OOM : SOUP_E_CUDA;
+  }
+}
+
+void soup_destroy(SoupHandle* h) {
+  if (!h || !h->owns) return;
+  destroy_batch(h->b);
+}
+
+const char* soup_last_error(const SoupHandle* h) { return h ? h->err.c_str() : g_last_error.c_str(); }
+
+int soup_get_info(SoupHandle* h, SoupInfo* out) {
+  return guarded(h, [&](Batch& b, uint32_t r) {
+    if (!out) fail(SOUP_E_ARG, "NULL output");
+    std::memset(out, 0, sizeof *out);
+    out->n = b.cfg[r].n;
+    out->global_step = b.step[r];
+    out->list_capacity = b.cfg[r].list_capacity;
+    out->es_list_capacity = b.cfg[r].es_enabled ? b.cfg[r].es_list_capacity : 0;
+    out->heads = b.hsp[r].nheads;
+    out->rebuilds = b.rebuilds;
+    out->sweeps = b.sweeps;
+    for (int a = 0; a < 3; ++a) out->box[a] = b.cfg[r].box[a];
+    uint32_t bits = 0;
+    SOUP_CUDA_TRY(cudaMemcpy(&bits, b.drift_bits + r, 4, cudaMemcpyDeviceToHost));
+    float d2;
+    std::memcpy(&d2, &bits, 4);
+    out->max_drift = std::sqrt(std::max(0.0, (double)d2));
+  });
+}
+
+int soup_fresh_state(const SoupConfig* cfg, float* positions, float* velocities, uint32_t* frozen, uint32_t* bond_rng,
+                     uint32_t* thermo_rng) {
+  if (!cfg) { g_last_error = "NULL config"; return SOUP_E_ARG; }
+  host_fresh_state(*cfg, positions, velocities, frozen, bond_rng, thermo_rng);
+  return SOUP_OK;
+}
+int soup_initial_charges(const SoupConfig* cfg, const float* positions, float* charges, uint32_t* prot) {
+  if (!cfg || !positions || !charges) { g_last_error = "NULL argument"; return SOUP_E_ARG; }
+  host_initial_charges(*cfg, positions, charges, prot);
+  return SOUP_OK;
+}
+
+int soup_step(SoupHandle* h, uint64_t n) {
+  return guarded(h, [&](Batch& b, uint32_t) {
+    if (b.R != 1) fail(SOUP_E_STATE, "a replica of a batch is stepped with soup_batch_step");
+    step_batch(b, n);
+  });
+}
+
+int soup_relax_cold_start(SoupHandle* h, uint32_t iterations, double max_disp, double* out2) {
+  return guarded(h, [&](Batch& b, uint32_t r) {
+    if (iterations < 1) fail(SOUP_E_ARG, "relaxColdStart: iterations must be an integer >= 1");
+    if (!(max_disp > 0)) fail(SOUP_E_ARG, "relaxColdStart: maxDisplacementSigma must be positive");
+    if (b.step[r] != 0)
+      fail(SOUP_E_STATE, "relaxColdStart: the system is already at step " + std::to_string(b.step[r]) +
+                             " -- minimisation is allowed only before the first step");
+    auto maxf = [&]() {
+      force_pass(b);
+      std::vector<float> f(4 * (size_t)b.N);
+      SOUP_CUDA_TRY(cudaMemcpyAsync(f.data(), b.force, f.size() * 4, cudaMemcpyDeviceToHost, b.stream));
+      SOUP_CUDA_TRY(cudaStreamSynchronize(b.stream));
+      double m = 0;
+      for (size_t i = 0; i < f.size(); ++i)
+        if ((i & 3) != 3 && std::isfinite(f[i])) m = std::max(m, (double)std::fabs(f[i]));
+      return m;
+    };
+    const double before = maxf();
+    const double d0 = max_disp * b.cfg[r].sigma;
+    for (uint32_t k = 0; k < iterations; ++k) {   // soup/src/soup-relax.ts:87-111
+      const float d = (float)(d0 * (1.0 - (double)k / iterations));
+      force_pass(b);
+      launch_relax_step(b, d);
+    }
+    force_pass(b);
+    guards(b, 0);
+    const double after = maxf();
+    if (out2) { out2[0] = before; out2[1] = after; }
+  });
+}
+
+#define SOUP_READ(NAME, DEV, T, PER, MAP)                                                    \
+  int NAME(SoupHandle* h, void* dst, size_t bytes) {                                           \
+    return guarded(h, [&](Batch& b, uint32_t r) {                                              \
+      if (!dst) fail(SOUP_E_ARG, "NULL destination");                                          \
+      need(bytes, sizeof(T) * (PER) * (size_t)b.cfg[r].n);                                     \
+      read_replica<T>(b, r, reinterpret_cast<const T*>(DEV), PER, static_cast<T*>(dst), MAP);  \
+    });                                                                                        \
+  }
+
+SOUP_READ(soup_read_pos, b.pos, float, 4, false)
+SOUP_READ(soup_read_vel, b.vel, float, 4, false)
+SOUP_READ(soup_read_force, b.force, float, 4, false)
+SOUP_READ(soup_read_slots, b.slots, uint32_t, 3, true)
+SOUP_READ(soup_read_center_link, b.center, uint32_t, 1, true)
+SOUP_READ(soup_read_center_held, b.held, uint32_t, 1, false)
+SOUP_READ(soup_read_charges, b.charge, float, 1, false)
+SOUP_READ(soup_read_rng_bond, b.brng, uint32_t, 1, false)
+SOUP_READ(soup_read_rng_thermo, b.trng, uint32_t, 1, false)
+
+int soup_read_frozen(SoupHandle* h, void* dst, size_t bytes) {
+  return guarded(h, [&](Batch& b, uint32_t r) {
+    if (!dst) fail(SOUP_E_ARG, "NULL destination");
+    need(bytes, 4 * (size_t)b.cfg[r].n);
+    std::vector<uint8_t> f(b.cfg[r].n);
+    read_replica<uint8_t>(b, r, b.frozen, 1, f.data(), false);
+    uint32_t* d = static_cast<uint32_t*>(dst);
+    for (uint32_t i = 0; i < b.cfg[r].n; ++i) d[i] = f[i];
+  });
+}
+
+int soup_forces(SoupHandle* h, void* dst, size_t bytes) {
+  return guarded(h, [&](Batch& b, uint32_t r) {
+    if (!dst) fail(SOUP_E_ARG, "NULL destination");
+    need(bytes, 16 * (size_t)b.cfg[r].n);
+    force_pass(b);
+    read_replica<float>(b, r, reinterpret_cast<const float*>(b.force), 4, static_cast<float*>(dst), false);
+  });
+}
+int soup_forces_brute(SoupHandle* h, void* dst, size_t bytes) {
+  return guarded(h, [&](Batch& b, uint32_t r) {
+    if (!dst) fail(SOUP_E_ARG, "NULL destination");
+    need(bytes, 16 * (size_t)b.cfg[r].n);
+    launch_force_brute(b);
+    read_replica<float>(b, r, reinterpret_cast<const float*>(b.force), 4, static_cast<float*>(dst), false);
+  });
+}
+
+int soup_read_events(SoupHandle* h, void* dst, size_t bytes) {
+  return guarded(h, [&](Batch& b, uint32_t r) {
+    need(bytes, 8 * (size_t)b.cfg[r].n_rules);
+    SOUP_CUDA_TRY(cudaMemcpy(dst, b.events + 2 * SOUP_MAX_RULES * r, bytes, cudaMemcpyDeviceToHost));
+  });
+}
+int soup_read_desorb(SoupHandle* h, void* dst, size_t bytes) {
+  return guarded(h, [&](Batch& b, uint32_t r) {
+    need(bytes, 8);
+    SOUP_CUDA_TRY(cudaMemcpy(dst, b.desorb + 2 * r, 8, cudaMemcpyDeviceToHost));
+  });
+}
+int soup_nonfinite_count(SoupHandle* h, uint32_t* out2) {
+  return guarded(h, [&](Batch& b, uint32_t r) {
+    launch_nonfinite(b);
+    SOUP_CUDA_TRY(cudaMemcpyAsync(out2, b.flags + FLAG_WORDS + 2 * r, 8, cudaMemcpyDeviceToHost, b.stream));
+    SOUP_CUDA_TRY(cudaStreamSynchronize(b.stream));
+  });
+}
+int soup_read_protonation_rng(SoupHandle* h, uint32_t* out) {
+  return guarded(h, [&](Batch& b, uint32_t r) { *out = b.prot_rng[r]; });
+}
+
+int soup_read_verlet(SoupHandle* h, uint32_t* counts, uint32_t* lists, size_t lists_cap) {
+  return guarded(h, [&](Batch& b, uint32_t r) {
+    const uint32_t n = b.cfg[r].n, off = b.hsp[r].slot_off;
+    std::vector<uint32_t> cnt(n), ids(b.N), rows((size_t)n * b.list_cap);
+    SOUP_CUDA_TRY(cudaMemcpyAsync(cnt.data(), b.nl_cnt + off, 4 * (size_t)n, cudaMemcpyDeviceToHost, b.stream));
+    SOUP_CUDA_TRY(cudaMemcpyAsync(ids.data(), b.id, 4 * (size_t)b.N, cudaMemcpyDeviceToHost, b.stream));
+    SOUP_CUDA_TRY(cudaMemcpyAsync(rows.data(), b.nl + (size_t)off * b.list_cap, 4 * rows.size(), cudaMemcpyDeviceToHost, b.stream));
+    SOUP_CUDA_TRY(cudaStreamSynchronize(b.stream));
+    std::vector<uint32_t> slot_of_local(n);
+    for (uint32_t k = 0; k < n; ++k) slot_of_local[ids[off + k] - off] = k;
+    uint64_t total = 0;
+    for (uint32_t i = 0; i < n; ++i) { counts[i] = cnt[slot_of_local[i]]; total += counts[i]; }
+    if (!lists) return;
+    if (lists_cap < total) fail(SOUP_E_ARG, "lists buffer too small");
+    uint64_t at = 0;
+    for (uint32_t i = 0; i < n; ++i) {
+      const uint32_t k = slot_of_local[i];
+      uint32_t* o = lists + at;
+      for (uint32_t s = 0; s < cnt[k]; ++s) o[s] = ids[rows[(size_t)k * b.list_cap + s]] - off;
+      std::sort(o, o + cnt[k]);
+      at += cnt[k];
+    }
+  });
+}
+
+int soup_write_charges(SoupHandle* h, const float* src, size_t bytes) {
+  return guarded(h, [&](Batch& b, uint32_t r) {
+    const uint32_t n = b.cfg[r].n, off = b.hsp[r].slot_off;
+    need(bytes, 4 * (size_t)n);
+    std::vector<uint32_t> ids(n);
+    SOUP_CUDA_TRY(cudaMemcpyAsync(ids.data(), b.id + off, 4 * (size_t)n, cudaMemcpyDeviceToHost, b.stream));
+    SOUP_CUDA_TRY(cudaStreamSynchronize(b.stream));
+    std::vector<float> q(n);
+    for (uint32_t k = 0; k < n; ++k) q[k] = src[ids[k] - off];
+    SOUP_CUDA_TRY(cudaMemcpyAsync(b.charge + off, q.data(), 4 * (size_t)n, cudaMemcpyHostToDevice, b.stream));
+    force_pass(b);
+    SOUP_CUDA_TRY(cudaStreamSynchronize(b.stream));
+  });
+}
+
+int soup_write_state(SoupHandle* h, const SoupInitState* st) {
+  return guarded(h, [&](Batch& b, uint32_t r) {
+    if (!st) fail(SOUP_E_ARG, "NULL state");
+    const uint32_t n = b.cfg[r].n, off = b.hsp[r].slot_off;
+    // bring every current array of the replica to original order, overlay the given members
+    std::vector<float> pos(4 * (size_t)n), vel(4 * (size_t)n), q(n);
+    std::vector<uint32_t> slots(3 * (size_t)n), center(n), held(n), brng(n), trng(n);
+    std::vector<uint8_t> fr(n);
+    read_replica<float>(b, r, reinterpret_cast<const float*>(b.pos), 4, pos.data(), false);
+    read_replica<float>(b, r, reinterpret_cast<const float*>(b.vel), 4, vel.data(), false);
+    read_replica<float>(b, r, b.charge, 1, q.data(), false);
+    read_replica<uint32_t>(b, r, b.slots, 3, slots.data(), true);
+    read_replica<uint32_t>(b, r, b.center, 1, center.data(), true);
+    read_replica<uint32_t>(b, r, b.held, 1, held.data(), false);
+    read_replica<uint32_t>(b, r, b.brng, 1, brng.data(), false);
+    read_replica<uint32_t>(b, r, b.trng, 1, trng.data(), false);
+    read_replica<uint8_t>(b, r, b.frozen, 1, fr.data(), false);
+    std::vector<uint32_t> fr32(fr.begin(), fr.end());
+    SoupInitState m{};
+    m.positions = st->positions ? st->positions : pos.data();
+    m.velocities = st->velocities ? st->velocities : vel.data();
+    m.bond_slots = st->bond_slots ? st->bond_slots : slots.data();
+    m.center_link = st->center_link ? st->center_link : center.data();
+    m.center_held = st->center_held ? st->center_held : held.data();
+    m.bond_rng = st->bond_rng ? st->bond_rng : brng.data();
+    m.thermo_rng = st->thermo_rng ? st->thermo_rng : trng.data();
+    m.charges = st->charges ? st->charges : q.data();
+    m.frozen = st->frozen ? st->frozen : fr32.data();
+    m.events = st->events;
+    m.desorb_events = st->desorb_events;
+    // other replicas' slots stay where they are; this replica restarts from identity order
+    upload_replica(b, r, &m, false);
+    force_pass(b);
+    SOUP_CUDA_TRY(cudaStreamSynchronize(b.stream));
+  });
+}
+
+int soup_set_box(SoupHandle* h, const double box[3]) {
+  return guarded(h, [&](Batch& b, uint32_t r) {
+    if (!box) fail(SOUP_E_ARG, "NULL box");
+    for (int a = 0; a < 3; ++a) if (!(box[a] > 0)) fail(SOUP_E_GEOMETRY, "box sides must be positive");
+    for (int a = 0; a < 3; ++a) b.cfg[r].box[a] = box[a];
+    const SysParams old = b.hsp[r];
+    SysParams p = make_sys(b.cfg[r]);
+    p.slot_off = old.slot_off; p.n = old.n; p.head_off = old.head_off; p.nheads = old.nheads;
+    b.hsp[r] = p;
+    alloc_grids(b);
+    upload_params(b);
+    force_pass(b);
+    SOUP_CUDA_TRY(cudaStreamSynchronize(b.stream));
+  });
+}
+
+int soup_protonation_sweep(SoupHandle* h, SoupSweepResult* out) {
+  return guarded(h, [&](Batch& b, uint32_t r) {
+    if (!b.cfg[r].es_enabled) fail(SOUP_E_STATE, "electrostatics is not enabled on this system");
+    launch_sweep(b, r);
+    std::vector<double> so(4);
+    SOUP_CUDA_TRY(cudaMemcpyAsync(so.data(), b.sweep_out + 4 * r, 32, cudaMemcpyDeviceToHost, b.stream));
+    SOUP_CUDA_TRY(cudaMemcpyAsync(&b.prot_rng[r], b.prot_rng_dev + r, 4, cudaMemcpyDeviceToHost, b.stream));
+    force_pass(b);
+    SOUP_CUDA_TRY(cudaStreamSynchronize(b.stream));
+    b.sweeps++;
+    b.next_sweep[r] = b.step[r] + b.cfg[r].sweep_every;
+    if (out) {
+      out->heads = (uint32_t)so[0]; out->attempts = out->heads; out->accepted = (uint32_t)so[1];
+      out->d_es_mean_kt = so[2]; out->deprotonated = (uint32_t)so[3];
+      out->alpha = out->heads ? (double)out->deprotonated / out->heads : 0.0;
+    }
+  });
+}
+
+int soup_debug_phase(SoupHandle* h, int phase) {
+  return guarded(h, [&](Batch& b, uint32_t) {
+    switch (phase) {
+      case SOUP_PHASE_REBUILD: rebuild(b); break;
+      case SOUP_PHASE_FORCE: launch_force(b); break;
+      case SOUP_PHASE_KICK_DRIFT: launch_kick_drift(b); break;
+      case SOUP_PHASE_KICK_THERMO: launch_kick_thermo(b); break;
+      case SOUP_PHASE_BONDS: launch_bonds(b); break;
+      case SOUP_PHASE_MAX_DRIFT: launch_max_drift(b); break;
+      default: fail(SOUP_E_ARG, "unknown phase");
+    }
+    SOUP_CUDA_TRY(cudaStreamSynchronize(b.stream));
+    SOUP_CUDA_TRY(cudaGetLastError());
+  });
+}
+
+int soup_closure(SoupHandle* h, const uint32_t* member_idx, uint32_t n_members, const uint32_t* water_idx,
+                 uint32_t n_water, const double centre[3], double cell, double radius, double vmin,
+                 SoupClosureResult* out) {
+  return guarded(h, [&](Batch& b, uint32_t r) {
+    if (!out || !centre || (n_members && !member_idx) || (n_water && !water_idx)) fail(SOUP_E_ARG, "NULL argument");
+    if (!(cell > 0) || !(radius > 0)) fail(SOUP_E_ARG, "cell and radius must be positive");
+    std::string err;
+    int st = run_closure(b, r, member_idx, n_members, water_idx, n_water, centre, cell, radius, vmin, out, err);
+    if (st) fail(st, err);
+  });
+}
+
+int soup_amphiphile_labels(SoupHandle* h, uint32_t* head_of, uint32_t* n_out) {
+  return guarded(h, [&](Batch& b, uint32_t r) {
+    if (!head_of) fail(SOUP_E_ARG, "NULL argument");
+    std::string err;
+    int st = run_amphiphiles(b, r, head_of, n_out, err);
+    if (st) fail(st, err);
+  });
+}
+
+int soup_aggregate_labels(SoupHandle* h, const uint32_t* member_idx, uint32_t n_members, double cutoff,
+                          uint32_t* labels, uint32_t* n_components) {
+  return guarded(h, [&](Batch& b, uint32_t r) {
+    if ((n_members && (!member_idx || !labels)) || !(cutoff > 0)) fail(SOUP_E_ARG, "bad argument");
+    std::string err;
+    int st = run_aggregates(b, r, member_idx, n_members, cutoff, labels, n_components, err);
+    if (st) fail(st, err);
+  });
+}
+
+int soup_batch_create(const SoupConfig* cfgs, const SoupInitState* inits, uint32_t n_replicas, SoupBatch** out) {
+  try {
+    if (!out) fail(SOUP_E_ARG, "NULL output");
+    *out = nullptr;
+    Batch* b = make_batch(cfgs, inits, n_replicas);
+    *out = new SoupBatch{b};
+    return SOUP_OK;
+  } catch (const SoupException& e) {
+    g_last_error = e.msg;
+    return e.code;
+  } catch (const CudaError& e) {
+    g_last_error = "CUDA: " + e.msg;
+    return e.code == cudaErrorMemoryAllocation ? SOUP_E_OOM : SOUP_E_CUDA;
+  }
+}
+
+int soup_batch_step(SoupBatch* sb, uint64_t n) {
+  if (!sb || !sb->b) return SOUP_E_ARG;
+  SoupHandle* h = sb->b->views[0];
+  int st = guarded(h, [&](Batch& b, uint32_t) { step_batch(b, n); });
+  if (st) sb->b->err = h->err;
+  return st;
+}
+SoupHandle* soup_batch_replica(SoupBatch* sb, uint32_t r) {
+  if (!sb || !sb->b || r >= sb->b->R) return nullptr;
+  return sb->b->views[r];
+}
+const char* soup_batch_last_error(const SoupBatch* sb) { return sb && sb->b ? sb->b->err.c_str() : g_last_error.c_str(); }
+void soup_batch_destroy(SoupBatch* sb) {
+  if (!sb) return;
+  destroy_batch(sb->b);
+  delete sb;
+}
+
+}  // extern "C"

@@ -1,0 +1,165 @@
+// soup_internal.h -- host-side device state of a batch of soup systems and the kernel launchers.
+//
+// A single SoupHandle is a batch of one.  All replicas of a batch share one set of device arrays:
+// particles of replica r occupy slots [slot_off_r, slot_off_r + n_r), and every kernel covers the
+// whole batch in one launch, reading the replica's parameters through a static per-slot system id.
+//
+// Layout in HBM ("slot" order = cell-sorted at the last rebuild, deterministic inside a cell by
+// original index):
+//   pos    float4  x, y, z, kind          vel, force float4 (w = 0)
+//   charge float                          slots  u32 x3  partner ORIGINAL (global) ids
+//   center u32 ORIGINAL id                held, bond_rng, thermo_rng u32;  frozen u8
+//   id     u32 slot -> original id        slot_of u32 original id -> slot
+//   pos_ref float4 positions at the last rebuild (drift reference)
+//   nl     u32 [slot][list_cap] Verlet neighbours as SLOT indices; nl_cnt u32 [slot]
+//   heads  u32 original ids of titratable beads (ascending; static);  es_nl [head][es_cap] slots
+#pragma once
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "../../include/soup_b200.h"
+#include "soup_common.cuh"
+
+namespace soup {
+
+template <class T> struct DevBuf {
+  T* p = nullptr;
+  size_t n = 0;
+};
+
+struct Batch {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  uint32_t R = 0;                    // replicas
+  uint32_t N = 0;                    // total particles
+  std::vector<SoupConfig> cfg;       // per replica
+  std::vector<SysParams> hsp;        // per replica (host copy)
+  Shared hs{};                       // batch-wide constants (host copy)
+  SysParams* sp = nullptr;           // device copy
+  Shared* shared = nullptr;          // device copy
+  uint8_t* sysid = nullptr;          // per slot (static: slots never leave their replica's range)
+
+  // particle state (double-buffered for the re-sort gather)
+  float4 *pos = nullptr, *vel = nullptr, *force = nullptr, *pos_ref = nullptr;
+  float* charge = nullptr;
+  uint32_t *slots = nullptr, *center = nullptr, *held = nullptr, *brng = nullptr, *trng = nullptr;
+  uint8_t* frozen = nullptr;
+  uint32_t *id = nullptr, *slot_of = nullptr;
+  float4 *pos2 = nullptr, *vel2 = nullptr, *force2 = nullptr;
+  float* charge2 = nullptr;
+  uint32_t *slots2 = nullptr, *center2 = nullptr, *held2 = nullptr, *brng2 = nullptr, *trng2 = nullptr;
+  uint8_t* frozen2 = nullptr;
+  uint32_t* id2 = nullptr;
+
+  // grid + list
+  uint32_t ncells = 0;               // total list-build cells over the batch
+  uint32_t *cell_of_slot = nullptr, *cell_count = nullptr, *cell_start = nullptr, *cell_cursor = nullptr;
+  uint32_t* perm = nullptr;          // new slot -> old slot
+  uint32_t* scan_tmp = nullptr;
+  uint32_t list_cap = 0;             // row stride of nl (max over replicas, rounded to 32)
+  uint32_t* nl = nullptr;
+  uint32_t* nl_cnt = nullptr;
+
+  // heads / long-range electrostatics
+  uint32_t H = 0;                    // total heads
+  uint32_t* heads = nullptr;         // global original ids, per replica ascending
+  uint32_t* head_sys = nullptr;      // replica of each head
+  uint32_t es_cap = 0;
+  uint32_t* es_nl = nullptr;
+  uint32_t* es_cnt = nullptr;
+  uint32_t nhcells = 0;
+  uint32_t *hcell_count = nullptr, *hcell_start = nullptr, *hcell_cursor = nullptr, *hsorted = nullptr;
+  uint32_t* hcell_of = nullptr;
+
+  // counters and flags (device): [0] list overflow, [1] es overflow, [2..3] nonfinite pos/vel,
+  // [4] drift^2 bits max (global), [5] rebuild request, [6] timeout flag, [7..] per-replica events
+  uint32_t* flags = nullptr;
+  uint32_t* events = nullptr;        // per replica: 2*SOUP_MAX_RULES
+  uint32_t* desorb = nullptr;        // per replica: 2
+  uint32_t* drift_bits = nullptr;    // per replica max drift^2 bits
+
+  // bond pass scratch
+  uint32_t* bond_items = nullptr;    // item records
+  uint32_t* bond_nitems = nullptr;
+  uint32_t* uf_parent = nullptr;     // per original id
+  uint32_t* comp_min = nullptr;      // per original id
+  uint8_t* item_done = nullptr;
+  uint32_t* has_item = nullptr;
+
+  // constant-pH sweep scratch / host state
+  std::vector<uint32_t> prot_rng;    // per replica
+  double* sweep_out = nullptr;       // per replica: attempts, accepted, dEsSum, dEsCount
+  uint32_t* prot_rng_dev = nullptr;
+
+  // analysis scratch
+  uint8_t *occ = nullptr, *vis = nullptr;
+  size_t grid_cap = 0;
+  uint32_t* frontier = nullptr;
+
+  // host-side schedule
+  std::vector<uint64_t> step;        // per replica global step
+  std::vector<uint64_t> next_sweep;
+  uint64_t rebuilds = 0, sweeps = 0;
+  bool force_fresh = false;          // force array matches positions+charges+lists
+  int tpp = 8;                       // threads per particle in the list kernels
+  std::string err;
+  std::vector<SoupHandle*> views;    // per-replica handle views
+};
+
+}  // namespace soup
+
+struct SoupHandle {
+  soup::Batch* b = nullptr;
+  uint32_t r = 0;
+  bool owns = false;
+  std::string err;
+};
+struct SoupBatch {
+  soup::Batch* b = nullptr;
+};
+
+namespace soup {
+// kernel launchers (kernels_*.cu)
+void launch_cell_index(Batch& b);
+void launch_sort_and_gather(Batch& b);
+void launch_build_lists(Batch& b);
+void launch_build_es_lists(Batch& b);
+void launch_force(Batch& b);
+void launch_force_brute(Batch& b);
+void launch_kick_drift(Batch& b);
+void launch_kick_thermo(Batch& b);
+void launch_max_drift(Batch& b);
+void launch_nonfinite(Batch& b);
+void launch_relax_step(Batch& b, float d);
+void launch_bonds(Batch& b);
+void launch_sweep(Batch& b, uint32_t replica);
+void launch_rebuild_check(Batch& b);
+// analysis
+int run_closure(Batch& b, uint32_t r, const uint32_t* mem, uint32_t nm, const uint32_t* wat, uint32_t nw,
+                const double centre[3], double cell, double radius, double vmin, SoupClosureResult* out,
+                std::string& err);
+int run_amphiphiles(Batch& b, uint32_t r, uint32_t* head_of, uint32_t* n_out, std::string& err);
+int run_aggregates(Batch& b, uint32_t r, const uint32_t* mem, uint32_t nm, double cutoff, uint32_t* labels,
+                   uint32_t* ncomp, std::string& err);
+// host
+void host_fresh_state(const SoupConfig& c, float* pos, float* vel, uint32_t* frozen, uint32_t* brng, uint32_t* trng);
+void host_initial_charges(const SoupConfig& c, const float* pos, float* charges, uint32_t* prot_rng);
+}  // namespace soup
+
+#define SOUP_CUDA_TRY(expr)                                                              \
+  do {                                                                                   \
+    cudaError_t e_ = (expr);                                                             \
+    if (e_ != cudaSuccess) throw soup::CudaError(e_, #expr, __FILE__, __LINE__);         \
+  } while (0)
+
+namespace soup {
+struct CudaError {
+  cudaError_t code;
+  std::string msg;
+  CudaError(cudaError_t c, const char* expr, const char* file, int line)
+      : code(c), msg(std::string(cudaGetErrorString(c)) + " at " + file + ":" + std::to_string(line) + " (" + expr + ")") {}
+};
+}  // namespace soup

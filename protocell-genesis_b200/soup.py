@@ -1,0 +1,319 @@
+"""SoupSystem: the reference's simulation API (soup/src/soup-types.ts:181-442) over the C ABI.
+
+Every method calls libsoup_b200.so; arrays come back in the reference's layouts and original
+particle order.  Method names follow the reference (camelCase aliases are provided for the ones
+soup/cli/campaign.ts and verify/ use).
+"""
+import ctypes as C
+from typing import Dict, Optional
+
+import numpy as np
+
+from . import _abi
+from . import config as _config
+
+
+def _ptr(a):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+def _check(lib, h, st):
+    if st != 0:
+        raise _abi.SoupError(st, lib.soup_last_error(h).decode())
+
+
+def init_state(st: Optional[dict]):
+    """SoupInitState from a dict of numpy arrays (CreateSoupOpts.resume field names accepted)."""
+    alias = {"positions": "positions", "velocities": "velocities", "bondSlots": "bond_slots",
+             "bond_slots": "bond_slots", "centerLink": "center_link", "center_link": "center_link",
+             "centerHeldSteps": "center_held", "center_held": "center_held", "bondRng": "bond_rng",
+             "bond_rng": "bond_rng", "thermoRng": "thermo_rng", "thermo_rng": "thermo_rng",
+             "charges": "charges", "frozen": "frozen", "events": "events", "desorbEvents": "desorb_events",
+             "desorb_events": "desorb_events"}
+    dtypes = {"positions": np.float32, "velocities": np.float32, "charges": np.float32}
+    s = _abi.SoupInitState()
+    keep = []
+    for k, v in (st or {}).items():
+        if k not in alias or v is None:
+            continue
+        name = alias[k]
+        a = np.ascontiguousarray(v, dtype=dtypes.get(name, np.uint32))
+        keep.append(a)
+        setattr(s, name, a.ctypes.data)
+    s._keep = keep
+    return s
+
+
+class SoupSystem:
+    """One soup system on the current CUDA device (createSoup, soup/src/sim.ts:95)."""
+
+    def __init__(self, cfg: _abi.SoupConfig, state: Optional[dict] = None, rule_ids=None):
+        self._lib = _abi.lib()
+        self.cfg = cfg
+        self.n = int(cfg.n)
+        self.rule_ids = rule_ids or _config.rule_ids()
+        h = C.c_void_p()
+        st = init_state(state) if state is not None else None
+        rc = self._lib.soup_create(C.byref(cfg), C.byref(st) if st is not None else None, C.byref(h))
+        if rc != 0:
+            raise _abi.SoupError(rc, self._lib.soup_last_error(None).decode())
+        self._h = h
+        self._owned = True
+
+    @classmethod
+    def _view(cls, lib, handle, cfg, rule_ids):
+        self = cls.__new__(cls)
+        self._lib = lib
+        self.cfg = cfg
+        self.n = int(cfg.n)
+        self.rule_ids = rule_ids
+        self._h = handle
+        self._owned = False
+        return self
+
+    # ---- lifecycle ----
+    def dispose(self):
+        if getattr(self, "_h", None) and self._owned:
+            self._lib.soup_destroy(self._h)
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.dispose()
+        except Exception:
+            pass
+
+    def info(self) -> dict:
+        i = _abi.SoupInfo()
+        _check(self._lib, self._h, self._lib.soup_get_info(self._h, C.byref(i)))
+        return dict(n=i.n, global_step=i.global_step, list_capacity=i.list_capacity,
+                    es_list_capacity=i.es_list_capacity, heads=i.heads, rebuilds=i.rebuilds, sweeps=i.sweeps,
+                    box=tuple(i.box), max_drift=i.max_drift)
+
+    @property
+    def steps(self) -> int:
+        return self.info()["global_step"]
+
+    @property
+    def box(self):
+        return self.info()["box"]
+
+    # ---- stepping ----
+    def step(self, n: int):
+        _check(self._lib, self._h, self._lib.soup_step(self._h, int(n)))
+
+    def relax_cold_start(self, iterations: Optional[int] = None, max_displacement_sigma: Optional[float] = None):
+        P = _config.load_params()
+        it = iterations if iterations is not None else P["coldStartRelax"]["iterations"]
+        md = max_displacement_sigma if max_displacement_sigma is not None else P["coldStartRelax"]["maxDisplacementSigma"]
+        out = (C.c_double * 2)()
+        _check(self._lib, self._h, self._lib.soup_relax_cold_start(self._h, int(it), float(md), out))
+        return dict(iterations=it, maxDisplacementStart=md * self.cfg.sigma,
+                    displacementBound=md * self.cfg.sigma * (it + 1) / 2,
+                    maxForceBefore=out[0], maxForceAfter=out[1])
+
+    relaxColdStart = relax_cold_start
+
+    def debug_phase(self, phase: int):
+        _check(self._lib, self._h, self._lib.soup_debug_phase(self._h, int(phase)))
+
+    # ---- readbacks ----
+    def _read(self, fn, dtype, per):
+        a = np.empty(self.n * per, dtype=dtype)
+        _check(self._lib, self._h, getattr(self._lib, fn)(self._h, _ptr(a), a.nbytes))
+        return a
+
+    def particles(self):
+        return self._read("soup_read_pos", np.float32, 4)
+
+    def velocities(self):
+        return self._read("soup_read_vel", np.float32, 4)
+
+    def forces(self):
+        """soup/src/soup-readback.ts forces(): rebuild + force pass, then read."""
+        return self._read("soup_forces", np.float32, 4)
+
+    def forces_no_rebuild(self):
+        return self._read("soup_read_force", np.float32, 4)
+
+    def forces_brute_force(self):
+        return self._read("soup_forces_brute", np.float32, 4)
+
+    def bond_slots(self):
+        return self._read("soup_read_slots", np.uint32, 3)
+
+    def bonds(self):
+        """soup/src/soup-readback.ts:40-50: (i, j) pairs with j > i, in slot order."""
+        s = self.bond_slots().reshape(-1, 3)
+        out = []
+        for i in np.nonzero((s != _abi.NONE).any(axis=1))[0]:
+            for j in s[i]:
+                if j != _abi.NONE and j > i:
+                    out += [i, j]
+        return np.asarray(out, dtype=np.uint32)
+
+    def center_links(self):
+        return self._read("soup_read_center_link", np.uint32, 1)
+
+    def center_held_steps(self):
+        return self._read("soup_read_center_held", np.uint32, 1)
+
+    def charges(self):
+        return self._read("soup_read_charges", np.float32, 1)
+
+    def frozen(self):
+        return self._read("soup_read_frozen", np.uint32, 1)
+
+    def rng_state(self):
+        return dict(bond=self._read("soup_read_rng_bond", np.uint32, 1),
+                    thermo=self._read("soup_read_rng_thermo", np.uint32, 1))
+
+    def events(self) -> Dict[str, int]:
+        a = np.empty(2 * self.cfg.n_rules, np.uint32)
+        _check(self._lib, self._h, self._lib.soup_read_events(self._h, _ptr(a), a.nbytes))
+        out = {}
+        for r, (b, k) in enumerate(self.rule_ids[: self.cfg.n_rules]):
+            out[b] = int(a[2 * r])
+            out[k] = int(a[2 * r + 1])
+        return out
+
+    def events_raw(self):
+        a = np.empty(2 * self.cfg.n_rules, np.uint32)
+        _check(self._lib, self._h, self._lib.soup_read_events(self._h, _ptr(a), a.nbytes))
+        return a
+
+    def desorb_events(self):
+        a = np.empty(2, np.uint32)
+        _check(self._lib, self._h, self._lib.soup_read_desorb(self._h, _ptr(a), a.nbytes))
+        return dict(stretch=int(a[0]), timeout=int(a[1]))
+
+    def nonfinite_count(self):
+        a = (C.c_uint32 * 2)()
+        _check(self._lib, self._h, self._lib.soup_nonfinite_count(self._h, a))
+        return dict(pos=a[0], vel=a[1])
+
+    def protonation_rng_state(self) -> int:
+        v = C.c_uint32()
+        _check(self._lib, self._h, self._lib.soup_read_protonation_rng(self._h, C.byref(v)))
+        return v.value
+
+    def verlet_lists(self):
+        counts = np.empty(self.n, np.uint32)
+        _check(self._lib, self._h, self._lib.soup_read_verlet(self._h, counts.ctypes.data_as(_abi._U32P), None, 0))
+        lists = np.empty(int(counts.sum(dtype=np.uint64)), np.uint32)
+        _check(self._lib, self._h, self._lib.soup_read_verlet(
+            self._h, counts.ctypes.data_as(_abi._U32P), lists.ctypes.data_as(_abi._U32P), lists.size))
+        return counts, lists
+
+    # ---- writes ----
+    def write_charges(self, q):
+        q = np.ascontiguousarray(q, np.float32)
+        _check(self._lib, self._h, self._lib.soup_write_charges(self._h, _ptr(q), q.nbytes))
+
+    def write_state(self, state: dict):
+        st = init_state(state)
+        _check(self._lib, self._h, self._lib.soup_write_state(self._h, C.byref(st)))
+
+    def set_box(self, box):
+        b = (C.c_double * 3)(*[float(x) for x in box])
+        _check(self._lib, self._h, self._lib.soup_set_box(self._h, b))
+
+    # ---- Monte Carlo and analysis ----
+    def protonation_sweep(self):
+        r = _abi.SoupSweepResult()
+        _check(self._lib, self._h, self._lib.soup_protonation_sweep(self._h, C.byref(r)))
+        return dict(attempts=r.attempts, accepted=r.accepted, heads=r.heads, deprotonated=r.deprotonated,
+                    alpha=r.alpha, dEsMeanKT=r.d_es_mean_kt)
+
+    protonationSweepDEBUG = protonation_sweep
+
+    def closure(self, members, water, centre, cell, radius, enclosed_volume_min):
+        m = np.ascontiguousarray(members, np.uint32)
+        w = np.ascontiguousarray(water, np.uint32)
+        c = (C.c_double * 3)(*[float(x) for x in centre])
+        r = _abi.SoupClosureResult()
+        _check(self._lib, self._h, self._lib.soup_closure(
+            self._h, m.ctypes.data_as(_abi._U32P), m.size, w.ctypes.data_as(_abi._U32P), w.size, c,
+            float(cell), float(radius), float(enclosed_volume_min), C.byref(r)))
+        return dict(encapsulatedCount=r.encapsulated_count, totalWater=r.total_water,
+                    bulkWaterDensity=r.bulk_water_density, encapsulationThresholdCount=r.threshold_count,
+                    closed=bool(r.closed), totalEmptyCells=r.total_empty_cells, unreachedCells=r.unreached_cells,
+                    seedCell=r.seed_cell, seedDistFromCentre=r.seed_dist_from_centre)
+
+    def amphiphile_labels(self):
+        head_of = np.empty(self.n, np.uint32)
+        cnt = C.c_uint32()
+        _check(self._lib, self._h, self._lib.soup_amphiphile_labels(self._h, head_of.ctypes.data_as(_abi._U32P),
+                                                                    C.byref(cnt)))
+        return int(cnt.value), head_of
+
+    def aggregate_labels(self, members, cutoff):
+        m = np.ascontiguousarray(members, np.uint32)
+        labels = np.empty(m.size, np.uint32)
+        nc = C.c_uint32()
+        _check(self._lib, self._h, self._lib.soup_aggregate_labels(
+            self._h, m.ctypes.data_as(_abi._U32P), m.size, float(cutoff), labels.ctypes.data_as(_abi._U32P),
+            C.byref(nc)))
+        return int(nc.value), labels
+
+    # reference-style aliases
+    forcesBruteForce = forces_brute_force
+    forcesNoRebuildDEBUG = forces_no_rebuild
+    bondSlots = bond_slots
+    centerLinks = center_links
+    centerHeldSteps = center_held_steps
+    rngState = rng_state
+    desorbEvents = desorb_events
+    nonFiniteCount = nonfinite_count
+    protonationRngState = protonation_rng_state
+
+
+class SoupBatch:
+    """Many independent replicas stepped together (one launch per kernel per step)."""
+
+    def __init__(self, cfgs, states=None, rule_ids=None):
+        self._lib = _abi.lib()
+        R = len(cfgs)
+        arr = (_abi.SoupConfig * R)(*cfgs)
+        self.cfgs = list(cfgs)
+        sts = None
+        self._keep = []
+        if states is not None:
+            sts = (_abi.SoupInitState * R)()
+            for r, st in enumerate(states):
+                s = init_state(st)
+                self._keep.append(s)
+                sts[r] = s
+        h = C.c_void_p()
+        rc = self._lib.soup_batch_create(arr, sts, R, C.byref(h))
+        if rc != 0:
+            raise _abi.SoupError(rc, self._lib.soup_last_error(None).decode())
+        self._h = h
+        rid = rule_ids or _config.rule_ids()
+        self.replicas = [SoupSystem._view(self._lib, self._lib.soup_batch_replica(h, r), cfgs[r], rid) for r in range(R)]
+
+    def step(self, n: int):
+        rc = self._lib.soup_batch_step(self._h, int(n))
+        if rc != 0:
+            raise _abi.SoupError(rc, self._lib.soup_batch_last_error(self._h).decode())
+
+    def dispose(self):
+        if getattr(self, "_h", None):
+            for r in self.replicas:
+                r._h = None
+            self._lib.soup_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.dispose()
+        except Exception:
+            pass
+
+
+def create_soup(opts: _config.SoupOptions, state: Optional[dict] = None) -> SoupSystem:
+    """createSoup (soup/src/sim.ts:95)."""
+    return SoupSystem(_config.resolve(opts), state)
+
+
+createSoup = create_soup

@@ -1,0 +1,164 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle, on identical inputs.
+
+Bars: Verlet/head lists, positions after the kick+drift, RNG streams, bond slots / centre links /
+event counters after a bond pass, and constant-pH accept decisions are bit-exact; forces are within
+1e-5 relative RMS of the FP64 oracle; the thermostat velocities (logf/cosf differ between libraries)
+within 2e-6 relative.
+"""
+import numpy as np
+import pytest
+
+import oracle_binding as ob
+from helpers import boosted, charged_opts, confined_opts, csr_rows, long_range_opts, plain_opts, rel_rms, water_opts
+from protocell_genesis_b200 import _abi, config as cfgm
+from protocell_genesis_b200.soup import SoupBatch, SoupSystem
+
+pytestmark = pytest.mark.gpu
+
+P = cfgm.load_params()
+FORCE_TOL = 1e-5       # relative RMS against FP64 (the target's force bar)
+THERMO_TOL = 2e-6      # velocities after the Langevin kick (library logf/cosf differ in the last ulps)
+
+
+def oracle_state(o, with_force=False):
+    st = dict(positions=o.read(ob.F_POS), velocities=o.read(ob.F_VEL), bond_slots=o.read(ob.F_SLOTS),
+              center_link=o.read(ob.F_CENTER), center_held=o.read(ob.F_HELD), bond_rng=o.read(ob.F_BOND_RNG),
+              thermo_rng=o.read(ob.F_THERMO_RNG), charges=o.read(ob.F_CHARGES), frozen=o.read(ob.F_FROZEN),
+              events=o.read(ob.F_EVENTS), desorb_events=o.read(ob.F_DESORB))
+    return st
+
+
+def make_pair(opts, relax=30, steps=0, tweak=None):
+    cfg = cfgm.resolve(opts, P)
+    if tweak:
+        tweak(cfg)
+    o = ob.OracleSystem(_abi, cfg)
+    if relax:
+        o.relax(relax, 0.1)
+    if steps:
+        o.step(steps)
+    g = SoupSystem(cfg, oracle_state(o))
+    return cfg, o, g
+
+
+@pytest.mark.parametrize("maker", [plain_opts, charged_opts, long_range_opts, confined_opts])
+def test_lists_are_the_oracle_sets(maker):
+    cfg, o, g = make_pair(maker(), relax=10)
+    gc, gl = g.verlet_lists()
+    oc, ol = o.verlet()
+    assert np.array_equal(gc, oc)
+    assert np.array_equal(gl, ol)
+
+
+@pytest.mark.parametrize("maker", [plain_opts, charged_opts, long_range_opts, confined_opts])
+def test_force_within_fp64_tolerance(maker):
+    cfg, o, g = make_pair(maker(), relax=20, steps=20)
+    f64 = o.forces64()
+    fg = g.forces_no_rebuild()
+    assert rel_rms(fg, f64) < FORCE_TOL
+    fb = g.forces_brute_force()
+    assert rel_rms(fb, f64) < FORCE_TOL
+
+
+def test_kick_drift_bit_exact_and_thermostat():
+    cfg, o, g = make_pair(charged_opts(), relax=20, steps=10)
+    o.write(ob.F_FORCE, g.forces_no_rebuild())          # both integrate the same force array
+    g.debug_phase(_abi.PHASE_KICK_DRIFT)
+    o.phase(_abi.PHASE_KICK_DRIFT)
+    assert np.array_equal(g.particles(), o.read(ob.F_POS))
+    assert np.array_equal(g.velocities(), o.read(ob.F_VEL))
+    g.debug_phase(_abi.PHASE_KICK_THERMO)
+    o.phase(_abi.PHASE_KICK_THERMO)
+    assert np.array_equal(g.rng_state()["thermo"], o.read(ob.F_THERMO_RNG))
+    vg = g.velocities().reshape(-1, 4)[:, :3].astype(np.float64)
+    vo = o.read(ob.F_VEL).reshape(-1, 4)[:, :3].astype(np.float64)
+    assert np.abs(vg - vo).max() <= THERMO_TOL * max(1.0, np.abs(vo).max())
+
+
+def test_bond_passes_bit_exact():
+    cfg, o, g = make_pair(plain_opts(), relax=30, tweak=lambda c: boosted(c, attempt=0.8, accept=1.0, brk=0.2))
+    total = 0
+    for rnd in range(6):
+        o.step(13)
+        g.write_state(oracle_state(o))
+        o.phase(_abi.PHASE_REBUILD)
+        o.phase(_abi.PHASE_BONDS)
+        g.debug_phase(_abi.PHASE_BONDS)
+        assert np.array_equal(g.bond_slots(), o.read(ob.F_SLOTS)), rnd
+        assert np.array_equal(g.center_links(), o.read(ob.F_CENTER)), rnd
+        assert np.array_equal(g.center_held_steps(), o.read(ob.F_HELD)), rnd
+        assert np.array_equal(g.rng_state()["bond"], o.read(ob.F_BOND_RNG)), rnd
+        assert np.array_equal(g.events_raw(), o.read(ob.F_EVENTS)), rnd
+        d = g.desorb_events()
+        assert [d["stretch"], d["timeout"]] == list(o.read(ob.F_DESORB)), rnd
+        total = int(o.read(ob.F_EVENTS).sum())
+    assert total > 50   # the passes really formed and broke bonds
+
+
+def test_protonation_sweep_decisions_match():
+    def tw(c):
+        c.protonation_rng = 12345
+    cfg, o, g = make_pair(water_opts(), relax=30, steps=30, tweak=tw)
+    g.write_state(oracle_state(o))
+    rg = g.protonation_sweep()
+    ro = o.sweep()
+    assert np.array_equal(g.charges(), o.read(ob.F_CHARGES))
+    assert g.protonation_rng_state() == int(o.read(ob.F_PROT_RNG)[0])
+    assert rg["accepted"] == ro.accepted and rg["deprotonated"] == ro.deprotonated
+    assert rg["dEsMeanKT"] == pytest.approx(ro.d_es_mean_kt, rel=1e-9, abs=1e-12)
+    # the sweep recomputed the force with the new charges
+    assert rel_rms(g.forces_no_rebuild(), o.forces64()) < FORCE_TOL
+
+
+def test_short_trajectory_tracks_the_oracle():
+    cfg, o, g = make_pair(charged_opts(), relax=30)
+    g.step(40)
+    o.step(40)
+    assert np.array_equal(g.rng_state()["thermo"], o.read(ob.F_THERMO_RNG))
+    pg_ = g.particles().reshape(-1, 4)
+    po = o.read(ob.F_POS).reshape(-1, 4)
+    d = pg_[:, :3] - po[:, :3]
+    d -= np.rint(d / cfg.box[0]) * cfg.box[0]
+    assert np.abs(d).max() < 1e-3
+    assert np.array_equal(pg_[:, 3], po[:, 3])
+
+
+def test_batch_replicas_equal_single_systems():
+    cfgs = []
+    for k, (ph, ion, seed) in enumerate([(6.0, 0.05, 3), (7.5, 0.01, 4), (8.5, 0.1, 5)]):
+        c = cfgm.resolve(water_opts(n_water=1500 + 400 * k, electrostatics={"enabled": True, "pH": ph,
+                                                                           "ionicStrengthMolar": ion},
+                                    seed=seed, sweep_every=20, chunk_steps=20), P)
+        cfgs.append(c)
+    states = []
+    for c in cfgs:
+        o = ob.OracleSystem(_abi, c)
+        o.relax(20, 0.1)
+        states.append(oracle_state(o))
+    batch = SoupBatch(cfgs, states)
+    batch.step(60)
+    for c, st, rep in zip(cfgs, states, batch.replicas):
+        single = SoupSystem(c, st)
+        single.step(60)
+        assert np.array_equal(rep.particles(), single.particles())
+        assert np.array_equal(rep.charges(), single.charges())
+        assert np.array_equal(rep.bond_slots(), single.bond_slots())
+        single.dispose()
+    batch.dispose()
+
+
+def test_guards_are_loud():
+    cfg, o, g = make_pair(plain_opts(), relax=10)
+    st = oracle_state(o)
+    st["positions"] = st["positions"].copy()
+    st["positions"][4 * 5] = np.nan
+    g.write_state(st)
+    with pytest.raises(_abi.SoupError) as e:
+        g.step(1)
+    assert e.value.code == "SOUP_E_NONFINITE"
+    cfg2 = cfgm.resolve(plain_opts(), P)
+    cfg2.list_capacity = 8
+    g2 = SoupSystem(cfg2, oracle_state(o))
+    with pytest.raises(_abi.SoupError) as e:
+        g2.step(1)
+    assert e.value.code == "SOUP_E_LIST_OVERFLOW"
