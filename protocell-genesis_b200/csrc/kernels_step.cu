@@ -157,8 +157,8 @@ void launch_max_drift(Batch& b) {
   k_max_drift<<<nblocks(b.N), kBlock, 0, b.stream>>>(b.sp, b.sysid, b.N, b.pos, b.pos_ref, b.drift_bits);
 }
 void launch_nonfinite(Batch& b) {
-  cudaMemsetAsync(b.flags + 8, 0, sizeof(uint32_t) * 2 * b.R, b.stream);
-  k_nonfinite<<<nblocks(b.N), kBlock, 0, b.stream>>>(b.sysid, b.N, b.pos, b.vel, b.flags + 8);
+  cudaMemsetAsync(b.flags + kFlagWords, 0, sizeof(uint32_t) * 2 * b.R, b.stream);
+  k_nonfinite<<<nblocks(b.N), kBlock, 0, b.stream>>>(b.sysid, b.N, b.pos, b.vel, b.flags + kFlagWords);
 }
 void launch_relax_step(Batch& b, float d) {
   k_relax_step<<<nblocks(b.N), kBlock, 0, b.stream>>>(b.sp, b.sysid, b.N, b.pos, b.force, b.frozen, d);

@@ -21,7 +21,7 @@ namespace {
 thread_local std::string g_last_error;
 
 constexpr uint32_t NONE = SOUP_NONE_U32;
-constexpr uint32_t FLAG_WORDS = 16;
+constexpr uint32_t FLAG_WORDS = kFlagWords;
 
 template <class T> T* dalloc(size_t n) {
   T* p = nullptr;

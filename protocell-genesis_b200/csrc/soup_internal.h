@@ -25,6 +25,10 @@
 
 namespace soup {
 
+// flags[0] list overflow, [1] head-list overflow, [6] bond item overflow; per-replica non-finite
+// counters (positions, velocities) start at flags[kFlagWords].
+constexpr uint32_t kFlagWords = 16;
+
 template <class T> struct DevBuf {
   T* p = nullptr;
   size_t n = 0;
