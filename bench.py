@@ -1,0 +1,322 @@
+#!/usr/bin/env python
+"""Benchmark: particle-steps/s of the soup MD step at 483,268 beads on B200.
+
+Workload (the reference's full-campaign shape, box 76 sigma, its B76 census C 55,988 / O 18,659 /
+H 55,988 / M 1,452 / W 351,181): seeded fresh lattice + 200-iteration cold-start relax (untimed),
+pH 7 constant-pH Monte Carlo every 10 steps, I = 0.01 M long-range Debye-Hueckel (rc_es 15.2 sigma),
+Verlet rebuild on half-skin drift, bond Monte Carlo every 20 steps.  Inputs (state + lists,
+> 400 MB) are larger than the 126 MB L2, so no flush is needed between steps.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cuda|reference]
+
+One JSON line on rank 0.  N > 1 runs N independent replicas (one per GPU, weak scaling; the single
+system is not split).  --impl reference times the CPU oracle (the reference's step
+restated in C++, OpenMP over the host cores) on the same workload.
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+
+METRIC = "particle-steps/s at 483k beads, plain vs batched, at <=1e-5 force err"
+UNIT = "particle-steps/s"
+# the reference's published full-campaign rate at this size (87.2 ms/step, Apple GPU via WebGPU)
+PUBLISHED = 483268 / 0.0872
+CENSUS = {"C": 55988, "O": 18659, "H": 55988, "M": 1452, "W": 351181}
+
+
+def workload_opts(cfgm, seed=19, skin=1.0, sweep_every=10, scale=1.0):
+    """scale < 1 shrinks the census and the box volume by the same factor (profiling captures)."""
+    start = {k: int(round(v * scale)) for k, v in CENSUS.items()}
+    side = 76.0 * scale ** (1.0 / 3.0)
+    return cfgm.SoupOptions(box=[side, side, side], seed=seed, kT=1.1, start=start,
+                            electrostatics={"enabled": True, "pH": 7.0, "ionicStrengthMolar": 0.01},
+                            skin=skin, rebuild_on_drift=True, sweep_every=sweep_every, chunk_steps=sweep_every)
+
+
+def workload_name(skin):
+    return (f"campaign shape: 483,268 beads, 76 sigma box, pH 7 MC every 10 steps, I 0.01 M (rc_es 15.2), "
+            f"bonds every 20, Verlet skin {skin} rebuilt on half-skin drift")
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons, sampled during the timed region."""
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+         "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+         "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.Q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm = [float(r[1]) for r in self.rows if len(r) > 8 and r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in self.rows if len(r) > 8 and r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in self.rows if len(r) > 8 for i in range(4) if "Active" in r[5 + i]
+                          and "Not" not in r[5 + i]})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.rows)}
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as fh:
+            p = json.load(fh)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def dist_init():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def cpu_sample(pkg, ob, cfg, state, budget_s=12.0, max_steps=40):
+    """Time the CPU oracle (all host threads) on a bounded number of steps of the same workload."""
+    from protocell_genesis_b200 import _abi
+    o = ob.OracleSystem(_abi, cfg, state)
+    threads = ob.lib(_abi).oracle_threads()
+    t0 = time.perf_counter()
+    o.step(1)
+    t1 = time.perf_counter()
+    per = t1 - t0
+    n = int(max(1, min(max_steps, budget_s / max(per, 1e-6))))
+    t0 = time.perf_counter()
+    o.step(n)
+    dt = time.perf_counter() - t0
+    o.close()
+    return {"value": cfg.n * n / dt, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{n} steps of the same 483,268-bead workload from the relaxed start (after 1 warm-up step), "
+                      f"C++ oracle FP32 path, OpenMP {threads} threads"}
+
+
+def run_reference(args):
+    ws, rank, _ = dist_init()
+    if rank != 0:
+        return
+    import __graft_entry__ as ge
+    pkg = ge._package()
+    import oracle_binding as ob
+    from protocell_genesis_b200 import _abi, config as cfgm
+    cfg = cfgm.resolve(workload_opts(cfgm, skin=args.skin))
+    o = ob.OracleSystem(_abi, cfg)
+    o.relax(args.ref_relax, 0.1)
+    threads = ob.lib(_abi).oracle_threads()
+    o.step(max(1, min(args.warmup, 2)))
+    t0 = time.perf_counter()
+    o.step(1)
+    per = time.perf_counter() - t0
+    k = int(max(1, min(args.steps, args.ref_budget / max(per, 1e-6))))
+    t0 = time.perf_counter()
+    o.step(k)
+    dt = time.perf_counter() - t0
+    v = cfg.n * k / dt
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws, "steps": k,
+            "warmup": args.warmup, "ms_per_step": 1e3 * dt / k, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": v / PUBLISHED, "dtype": "f32", "data": "synthetic",
+            "config": {"workload": workload_name(args.skin), "relax_iterations": args.ref_relax},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": f"{k} of the requested {args.steps} steps (bounded to ~{args.ref_budget:.0f} s), "
+                                       f"C++ restatement of the reference step, OpenMP {threads} threads"},
+            "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def run_cuda(args):
+    import ctypes as C
+    import numpy as np
+    import torch
+    ws, rank, local = dist_init()
+    torch.cuda.set_device(local)
+    dist = None
+    if ws > 1:
+        import torch.distributed as dist
+        dist.init_process_group("nccl", device_id=torch.device("cuda", local))
+    import __graft_entry__ as ge
+    pkg = ge._package()
+    from protocell_genesis_b200 import _abi, config as cfgm
+    L = _abi.lib()
+    cfg = cfgm.resolve(workload_opts(cfgm, seed=19 + rank, skin=args.skin, scale=args.scale))
+    n = cfg.n
+    # fresh lattice on the host, relaxed on the device (untimed set-up)
+    host = {}
+    for name, dt, per in (("positions", np.float32, 4), ("velocities", np.float32, 4)):
+        host[name] = np.zeros(n * per, dt)
+    fr = np.zeros(n, np.uint32); br = np.zeros(n, np.uint32); tr = np.zeros(n, np.uint32)
+    p = lambda a: a.ctypes.data_as(C.c_void_p)
+    L.soup_fresh_state(C.byref(cfg), p(host["positions"]), p(host["velocities"]), p(fr), p(br), p(tr))
+    s = pkg.SoupSystem(cfg)
+    relax = s.relax_cold_start(args.relax, 0.1)
+    s.step(args.warmup)
+    stream = torch.cuda.ExternalStream(L.soup_stream(s._h))
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    L.soup_profile(s._h, 1)
+    launches0 = L.soup_launch_count(s._h)
+    info0 = s.info()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    with ClockSampler(local) as clk:
+        torch.cuda.nvtx.range_push("timed")
+        e0.record(stream)
+        s.step(args.steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        torch.cuda.nvtx.range_pop()
+    if dist:
+        dist.barrier()
+    ms = e0.elapsed_time(e1)
+    launches = L.soup_launch_count(s._h) - launches0
+    info1 = s.info()
+    ktime = {}
+    for k, name in enumerate(_abi.K_NAMES):
+        t = C.c_double(); c = C.c_uint64()
+        L.soup_kernel_time(s._h, k, C.byref(t), C.byref(c))
+        ktime[name] = (t.value, c.value)
+    L.soup_profile(s._h, 0)
+    ms_max = ms
+    if dist:
+        tt = torch.tensor([ms], device="cuda")
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        ms_max = float(tt.item())
+    value = ws * n * args.steps / (ms_max / 1e3)
+
+    # roofline of the dominant kernel (the list force), algorithmic bytes per launch:
+    # per particle 4 B per list entry + pos 16 + charge 4 + slots 12 + centre 4 + count 4 + force 16
+    counts = np.empty(n, np.uint32)
+    L.soup_read_verlet(s._h, counts.ctypes.data_as(_abi._U32P), None, 0)
+    mean_list = float(counts.mean())
+    f_ms, f_n = ktime["force"]
+    bytes_per_launch = n * (4.0 * mean_list + 56.0)
+    achieved = bytes_per_launch / (f_ms / max(f_n, 1) / 1e3) / 1e9 if f_n else None
+    peak, peak_kind = peaks()
+    traffic = None
+    tf = os.path.join(ROOT, "profiles", "force_traffic.json")
+    if os.path.exists(tf):
+        try:
+            with open(tf) as fh:
+                traffic = json.load(fh).get("bytes_per_launch")
+        except Exception:
+            traffic = None
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": (achieved / peak) if achieved else None, "traffic": traffic,
+                "kernel": "k_force (list pair force + bonded terms)",
+                "algorithmic_bytes_per_launch": bytes_per_launch, "mean_list_entries": mean_list,
+                "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback 6.65 TB/s"}
+
+    # end to end through the public API with host buffers: create from pinned host arrays
+    # (H2D of the whole state), step in chunks of 10 with the positions read back after each chunk
+    state = {"positions": s.particles(), "velocities": s.velocities(), "charges": s.charges(),
+             "bond_slots": s.bond_slots(), "center_link": s.center_links(), "center_held": s.center_held_steps(),
+             "bond_rng": s.rng_state()["bond"], "thermo_rng": s.rng_state()["thermo"]}
+    pinned = {}
+    for k_, v_ in state.items():
+        t_ = torch.from_numpy(np.ascontiguousarray(v_)).pin_memory()
+        pinned[k_] = t_.numpy()
+    out_pos = torch.empty(4 * n, dtype=torch.float32).pin_memory().numpy()
+    e2e_steps = args.steps if not args.no_e2e else 0
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    s2 = pkg.SoupSystem(cfg, pinned)
+    done = 0
+    while done < e2e_steps:
+        c_ = min(10, e2e_steps - done)
+        s2.step(c_)
+        L.soup_read_pos(s2._h, out_pos.ctypes.data_as(C.c_void_p), out_pos.nbytes)
+        done += c_
+    torch.cuda.synchronize()
+    e2e_s = time.perf_counter() - t0
+    h2d = sum(v_.nbytes for v_ in pinned.values())
+    e2e = None
+    if e2e_steps:
+        e2e = {"value": ws * n * e2e_steps / e2e_s, "unit": UNIT,
+               "h2d_bytes_per_step": h2d / e2e_steps, "d2h_bytes_per_step": 16 * n / 10,
+               "note": "create from pinned host arrays + step(10) + particles() readback per 10 steps, wall clock"}
+    s2.dispose()
+
+    cpu = None
+    if rank == 0 and ws == 1 and not args.no_cpu:
+        import oracle_binding as ob
+        cpu = cpu_sample(pkg, ob, cfg, state, budget_s=args.cpu_budget)
+
+    phases = {name: {"ms_total": t, "launches": c, "ms_per_step": t / args.steps} for name, (t, c) in ktime.items() if c}
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": value / (ws * PUBLISHED), "dtype": "f32", "data": "synthetic",
+            "config": {"workload": workload_name(args.skin), "beads": n, "replicas_per_gpu": 1,
+                       "l2": "inputs larger than L2 (state + lists ~0.5 GB vs 126 MB), no flush",
+                       "relax": {"iterations": args.relax, "max_force_after": relax["maxForceAfter"]},
+                       "rebuilds_in_timed_region": info1["rebuilds"] - info0["rebuilds"],
+                       "sweeps_in_timed_region": info1["sweeps"] - info0["sweeps"],
+                       "tpp": 8},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
+            "clocks": clk.summary(), "phases": phases}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    s.dispose()
+    if dist:
+        dist.destroy_process_group()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=500)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
+    ap.add_argument("--skin", type=float, default=1.0)
+    ap.add_argument("--relax", type=int, default=200)
+    ap.add_argument("--ref-relax", type=int, default=15)
+    ap.add_argument("--ref-budget", type=float, default=90.0)
+    ap.add_argument("--cpu-budget", type=float, default=12.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--scale", type=float, default=1.0, help="census and box-volume factor (profiling captures)")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_cuda(args)
+
+
+if __name__ == "__main__":
+    main()

@@ -270,6 +270,20 @@ enum {
 };
 int soup_debug_phase(SoupHandle* h, int phase);
 
+/* ---- measurement hooks (no reference counterpart; the reference times phases by wall clock) --- */
+enum {
+  SOUP_K_FORCE = 0, SOUP_K_ES_FAR = 1, SOUP_K_LIST = 2, SOUP_K_SORT = 3, SOUP_K_KICK_DRIFT = 4,
+  SOUP_K_KICK_THERMO = 5, SOUP_K_BONDS = 6, SOUP_K_SWEEP = 7, SOUP_K_COUNT = 8
+};
+/* The cudaStream_t this handle launches on, so a caller can record CUDA events on it. */
+void* soup_stream(SoupHandle* h);
+/* enable = 1: bracket the kernels of each SOUP_K_* group with CUDA events on the handle's stream. */
+int soup_profile(SoupHandle* h, int enable);
+/* Device milliseconds and launches of one SOUP_K_* group since profiling was last enabled. */
+int soup_kernel_time(SoupHandle* h, int kernel, double* total_ms, uint64_t* launches);
+/* Kernels this library has launched for the handle's batch since creation. */
+uint64_t soup_launch_count(SoupHandle* h);
+
 /* ---- batched replicas (no reference counterpart: one system per device there) -------------- */
 /* Many independent systems of uneven size stepped together: one launch per kernel per step covers
  * every replica.  cfgs[r] / inits[r] as for soup_create (inits may be NULL). */

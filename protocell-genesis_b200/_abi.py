@@ -158,7 +158,15 @@ SIGNATURES = {
     "soup_batch_last_error": (C.c_char_p, [_P]),
     "soup_batch_destroy": (None, [_P]),
     "soup_debug_phase": (C.c_int, [_P, C.c_int]),
+    "soup_stream": (_P, [_P]),
+    "soup_profile": (C.c_int, [_P, C.c_int]),
+    "soup_kernel_time": (C.c_int, [_P, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_uint64)]),
+    "soup_launch_count": (C.c_uint64, [_P]),
 }
+
+# soup_kernel_time groups
+K_FORCE, K_ES_FAR, K_LIST, K_SORT, K_KICK_DRIFT, K_KICK_THERMO, K_BONDS, K_SWEEP = range(8)
+K_NAMES = ["force", "es_far", "list", "sort", "kick_drift", "kick_thermo", "bonds", "sweep"]
 
 
 def library_path() -> str:

@@ -383,6 +383,8 @@ __global__ void k_bond_break(const Shared* __restrict__ Sg, const uint8_t* __res
 }  // namespace
 
 void launch_bonds(Batch& b) {
+  b.launches += 3;
+  prof_begin(b, SOUP_K_BONDS);
   cudaMemsetAsync(b.bond_nitems, 0, sizeof(uint32_t), b.stream);
   cudaMemsetAsync(b.has_item, 0, sizeof(uint32_t) * b.N, b.stream);
   uint32_t* has_item = b.has_item;
@@ -394,6 +396,7 @@ void launch_bonds(Batch& b) {
                                           b.item_done, b.events, b.desorb, b.flags);
   k_bond_break<<<nblocks(b.N), kBlock, 0, b.stream>>>(b.shared, b.sysid, b.N, b.pos, b.id, b.slot_of, b.slots,
                                                       b.brng, b.events);
+  prof_end(b);
 }
 
 }  // namespace soup

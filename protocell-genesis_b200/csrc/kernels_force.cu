@@ -61,11 +61,13 @@ __global__ void __launch_bounds__(256) k_force(
   const bool active = k < N;
   float fx = 0.f, fy = 0.f, fz = 0.f;
   if (active) {
-    const SysParams& P = sp[sysid[k]];
+    const SysParams& Pg = sp[sysid[k]];
+    const PairP P = PairP::of(Pg);
     const float4 xi = pos[k];
     const int ki = (int)xi.w;
     const float qi = charge[k];
     const bool needq = (qi != 0.f) || (S.cls[ki] == 1u && P.acid > 0.f);
+    const float rmax2 = S.rmax2;
     const uint32_t cnt = nl_cnt[k];
     const uint32_t* row = nl + (size_t)k * cap;
     const PairConst* prow = &S.pair[ki * SOUP_KMAX];
@@ -76,7 +78,7 @@ __global__ void __launch_bounds__(256) k_force(
       const float dy = fast_mi(xi.y - xj.y, P.box[1], P.inv_box[1]);
       const float dz = fast_mi(xi.z - xj.z, P.box[2], P.inv_box[2]);
       const float r2 = dx * dx + dy * dy + dz * dz;
-      if (r2 >= S.rmax2 || r2 < 1e-12f) continue;
+      if (r2 >= rmax2 || r2 < 1e-12f) continue;
       const int kj = (int)xj.w;
       const float qj = needq ? __ldg(charge + j) : 0.f;
       const float sc = pair_scalar(S, P, prow[kj], r2, ki, kj, qi, qj);
@@ -87,7 +89,7 @@ __global__ void __launch_bounds__(256) k_force(
     uint32_t owner = center[k];
     if ((sl[0] & sl[1] & sl[2] & owner) != SOUP_NONE_U32) {
       const uint32_t gi = id[k];
-      for (int t = lane; t < 13; t += TPP) bonded_term(S, P, t, gi, xi, sl, owner, slots, slot_of, pos, fx, fy, fz);
+      for (int t = lane; t < 13; t += TPP) bonded_term(S, Pg, t, gi, xi, sl, owner, slots, slot_of, pos, fx, fy, fz);
     }
   }
 #pragma unroll
@@ -112,9 +114,9 @@ __global__ void __launch_bounds__(256) k_force(
 }
 
 // soup/wgsl/electrostatics-long.wgsl:63-82 soup_es_force_far_main, a warp per head.
-__global__ void __launch_bounds__(256) k_es_far(const SysParams* __restrict__ sp, const uint32_t* __restrict__ heads,
+__global__ void __launch_bounds__(256) k_es_far(const SysParams* __restrict__ sp, const uint32_t* __restrict__ head_slot,
                                                 const uint32_t* __restrict__ head_sys, uint32_t H,
-                                                const uint32_t* __restrict__ slot_of, const float4* __restrict__ pos,
+                                                const float4* __restrict__ pos,
                                                 const float* __restrict__ charge, const uint32_t* __restrict__ es_nl,
                                                 const uint32_t* __restrict__ es_cnt, uint32_t cap,
                                                 float4* __restrict__ force) {
@@ -122,7 +124,7 @@ __global__ void __launch_bounds__(256) k_es_far(const SysParams* __restrict__ sp
   const int lane = threadIdx.x & 31;
   if (h >= H) return;   // warp-uniform
   const SysParams& P = sp[head_sys[h]];
-  const uint32_t ks = slot_of[heads[h]];
+  const uint32_t ks = head_slot[h];
   const float qi = charge[ks];
   if (qi == 0.f || P.es_A == 0.f) return;
   const float4 xi = pos[ks];
@@ -130,7 +132,7 @@ __global__ void __launch_bounds__(256) k_es_far(const SysParams* __restrict__ sp
   const uint32_t cnt = es_cnt[h];
   const uint32_t* row = es_nl + (size_t)h * cap;
   for (uint32_t s = lane; s < cnt; s += 32) {
-    const uint32_t j = __ldg(row + s);
+    const uint32_t j = __ldg(head_slot + __ldg(row + s));
     const float qj = __ldg(charge + j);
     if (qj == 0.f) continue;
     const float4 xj = __ldg(pos + j);
@@ -223,6 +225,18 @@ void launch_force_tpp(Batch& b) {
 }  // namespace
 
 void launch_force(Batch& b) {
+  prof_begin(b, SOUP_K_FORCE);
+  launch_force_list(b);
+  prof_end(b);
+  if (b.H > 0) {
+    prof_begin(b, SOUP_K_ES_FAR);
+    launch_es_far(b);
+    prof_end(b);
+  }
+}
+
+void launch_force_list(Batch& b) {
+  b.launches += 1;
   switch (b.tpp) {
     case 1: launch_force_tpp<1>(b); break;
     case 2: launch_force_tpp<2>(b); break;
@@ -231,13 +245,17 @@ void launch_force(Batch& b) {
     case 32: launch_force_tpp<32>(b); break;
     default: launch_force_tpp<8>(b); break;
   }
-  if (b.H > 0) {
-    k_es_far<<<nblocks((uint64_t)b.H * 32, 256), 256, 0, b.stream>>>(b.sp, b.heads, b.head_sys, b.H, b.slot_of, b.pos,
-                                                                     b.charge, b.es_nl, b.es_cnt, b.es_cap, b.force);
-  }
+}
+
+void launch_es_far(Batch& b) {
+  if (b.H == 0) return;
+  b.launches += 1;
+  k_es_far<<<nblocks((uint64_t)b.H * 32, 256), 256, 0, b.stream>>>(b.sp, b.head_slot, b.head_sys, b.H, b.pos,
+                                                                   b.charge, b.es_nl, b.es_cnt, b.es_cap, b.force);
 }
 
 void launch_force_brute(Batch& b) {
+  b.launches += 1;
   k_force_brute<<<nblocks(b.N, 128), 128, 0, b.stream>>>(b.shared, b.sp, b.sysid, b.N, b.pos, b.charge, b.slots,
                                                          b.center, b.id, b.slot_of, b.force);
 }

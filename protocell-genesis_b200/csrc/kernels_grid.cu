@@ -77,8 +77,10 @@ __global__ void k_set_total(uint32_t* __restrict__ start, const uint32_t* __rest
 }  // namespace
 
 // exclusive scan of in[0..n) into out[0..n), out[n] = total; tmp must hold >= 2*ceil(n/4096)+2 words
+uint64_t g_scan_launches = 0;
 void exclusive_scan(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* tmp, cudaStream_t st) {
   if (n == 0) return;
+  g_scan_launches += 2;
   uint32_t nb = (n + 4095) / 4096;
   if (nb == 1) {
     k_scan_block<<<1, 1024, 0, st>>>(in, out, n, nullptr);
@@ -173,7 +175,11 @@ __global__ void __launch_bounds__(128) k_build_list(
   const SysParams& P = sp[sysid[k]];
   const float4 xi = pos[k];
   const float box[3] = {P.box[0], P.box[1], P.box[2]};
+  const float inv[3] = {P.inv_box[0], P.inv_box[1], P.inv_box[2]};
   const float lr = P.list_range;
+  // fast squared distance decides unless it lies within 1e-5 of the range, where the exact
+  // reference arithmetic decides (the minimum image cannot differ there: range < box/2)
+  const float lr2_lo = lr * lr * (1.0f - 1e-5f), lr2_hi = lr * lr * (1.0f + 1e-5f);
   uint32_t c = cell_of[k] - P.cell_off;
   int qx = (int)(c % (uint32_t)P.dims[0]);
   int qy = (int)((c / (uint32_t)P.dims[0]) % (uint32_t)P.dims[1]);
@@ -201,10 +207,15 @@ __global__ void __launch_bounds__(128) k_build_list(
         uint32_t a = start[rowbase + ax.lo[s]], e = start[rowbase + ax.hi[s] + 1];
         for (uint32_t j = a; j < e; ++j) {
           if (j == k) continue;
-          if (ex_dist(xi, pos[j], box) < lr) {
-            if (cnt < cap) row[cnt] = j;
-            ++cnt;
-          }
+          const float4 xj = pos[j];
+          const float dx = fast_mi(xi.x - xj.x, box[0], inv[0]);
+          const float dy = fast_mi(xi.y - xj.y, box[1], inv[1]);
+          const float dz = fast_mi(xi.z - xj.z, box[2], inv[2]);
+          const float r2 = dx * dx + dy * dy + dz * dz;
+          if (r2 > lr2_hi) continue;
+          if (r2 >= lr2_lo && !(ex_dist(xi, xj, box) < lr)) continue;
+          if (cnt < cap) row[cnt] = j;
+          ++cnt;
         }
       }
     }
@@ -217,11 +228,13 @@ __global__ void __launch_bounds__(128) k_build_list(
 __global__ void k_head_index(const uint32_t* __restrict__ heads, const uint32_t* __restrict__ head_sys, uint32_t H,
                              const uint32_t* __restrict__ slot_of, const float4* __restrict__ pos,
                              const SysParams* __restrict__ sp, uint32_t* __restrict__ hcell_of,
-                             uint32_t* __restrict__ hcount) {
+                             uint32_t* __restrict__ hcount, uint32_t* __restrict__ head_slot) {
   uint32_t h = blockIdx.x * blockDim.x + threadIdx.x;
   if (h >= H) return;
   const SysParams& P = sp[head_sys[h]];
-  float4 p = pos[slot_of[heads[h]]];
+  const uint32_t ks = slot_of[heads[h]];
+  head_slot[h] = ks;
+  float4 p = pos[ks];
   int cx = ex_cell_axis(p.x, P.box[0], P.hdims[0]);
   int cy = ex_cell_axis(p.y, P.box[1], P.hdims[1]);
   int cz = ex_cell_axis(p.z, P.box[2], P.hdims[2]);
@@ -249,7 +262,7 @@ __global__ void k_head_sort_cells(const uint32_t* __restrict__ hstart, uint32_t 
 }
 
 // soup/wgsl/electrostatics-long.wgsl:31-56 head list at rc_es + skin, via the head grid.
-// Entries are the neighbours' SLOT indices.
+// Entries are the neighbours' HEAD indices (head_slot maps them to slots).
 __global__ void k_build_es_list(const uint32_t* __restrict__ heads, const uint32_t* __restrict__ head_sys, uint32_t H,
                                 const uint32_t* __restrict__ slot_of, const float4* __restrict__ pos,
                                 const SysParams* __restrict__ sp, const uint32_t* __restrict__ hcell_of,
@@ -285,7 +298,7 @@ __global__ void k_build_es_list(const uint32_t* __restrict__ heads, const uint32
           if (g == h) continue;
           uint32_t js = slot_of[heads[g]];
           if (ex_dist(xi, pos[js], box) < P.es_list_range) {
-            if (cnt < cap) row[cnt] = js;
+            if (cnt < cap) row[cnt] = g;
             ++cnt;
           }
         }
@@ -297,11 +310,16 @@ __global__ void k_build_es_list(const uint32_t* __restrict__ heads, const uint32
 }  // namespace
 
 void launch_cell_index(Batch& b) {
+  b.launches += 1;
+  prof_begin(b, SOUP_K_SORT);
   cudaMemsetAsync(b.cell_count, 0, sizeof(uint32_t) * (b.ncells + 1), b.stream);
   k_cell_index<<<nblocks(b.N), kBlock, 0, b.stream>>>(b.pos, b.sysid, b.sp, b.N, b.cell_of_slot, b.cell_count);
+  prof_end(b);
 }
 
 void launch_sort_and_gather(Batch& b) {
+  prof_begin(b, SOUP_K_SORT);
+  g_scan_launches = 0;
   exclusive_scan(b.cell_count, b.cell_start, b.ncells, b.scan_tmp, b.stream);
   cudaMemsetAsync(b.cell_cursor, 0, sizeof(uint32_t) * b.ncells, b.stream);
   k_scatter<<<nblocks(b.N), kBlock, 0, b.stream>>>(b.cell_of_slot, b.cell_start, b.N, b.cell_cursor, b.perm);
@@ -317,18 +335,25 @@ void launch_sort_and_gather(Batch& b) {
   // the cell of every new slot: cell_start is monotone, so recompute from the sorted positions
   cudaMemsetAsync(b.cell_count, 0, sizeof(uint32_t) * (b.ncells + 1), b.stream);
   k_cell_index<<<nblocks(b.N), kBlock, 0, b.stream>>>(b.pos, b.sysid, b.sp, b.N, b.cell_of_slot, b.cell_count);
+  b.launches += 5 + g_scan_launches;
+  prof_end(b);
 }
 
 void launch_build_lists(Batch& b) {
+  b.launches += 1;
+  prof_begin(b, SOUP_K_LIST);
   k_build_list<<<nblocks(b.N, 128), 128, 0, b.stream>>>(b.pos, b.sysid, b.sp, b.cell_of_slot, b.cell_start, b.N,
                                                         b.list_cap, b.nl, b.nl_cnt, b.flags);
+  prof_end(b);
 }
 
 void launch_build_es_lists(Batch& b) {
   if (b.H == 0) return;
+  g_scan_launches = 0;
+  prof_begin(b, SOUP_K_LIST);
   cudaMemsetAsync(b.hcell_count, 0, sizeof(uint32_t) * (b.nhcells + 1), b.stream);
   k_head_index<<<nblocks(b.H), kBlock, 0, b.stream>>>(b.heads, b.head_sys, b.H, b.slot_of, b.pos, b.sp, b.hcell_of,
-                                                       b.hcell_count);
+                                                       b.hcell_count, b.head_slot);
   exclusive_scan(b.hcell_count, b.hcell_start, b.nhcells, b.scan_tmp, b.stream);
   cudaMemsetAsync(b.hcell_cursor, 0, sizeof(uint32_t) * b.nhcells, b.stream);
   k_head_scatter<<<nblocks(b.H), kBlock, 0, b.stream>>>(b.hcell_of, b.hcell_start, b.H, b.hcell_cursor, b.hsorted);
@@ -336,6 +361,8 @@ void launch_build_es_lists(Batch& b) {
   k_build_es_list<<<nblocks(b.H, 128), 128, 0, b.stream>>>(b.heads, b.head_sys, b.H, b.slot_of, b.pos, b.sp,
                                                            b.hcell_of, b.hcell_start, b.hsorted, b.es_cap, b.es_nl,
                                                            b.es_cnt, b.flags);
+  b.launches += 5 + g_scan_launches;
+  prof_end(b);
 }
 
 }  // namespace soup

@@ -147,20 +147,29 @@ __global__ void k_relax_step(const SysParams* __restrict__ sp, const uint8_t* __
 }  // namespace
 
 void launch_kick_drift(Batch& b) {
+  b.launches += 1;
+  prof_begin(b, SOUP_K_KICK_DRIFT);
   k_kick_drift<<<nblocks(b.N), kBlock, 0, b.stream>>>(b.sp, b.sysid, b.N, b.pos, b.vel, b.force, b.frozen, b.pos_ref,
                                                        b.drift_bits);
+  prof_end(b);
 }
 void launch_kick_thermo(Batch& b) {
+  b.launches += 1;
+  prof_begin(b, SOUP_K_KICK_THERMO);
   k_kick_thermo<<<nblocks(b.N), kBlock, 0, b.stream>>>(b.sp, b.sysid, b.N, b.vel, b.force, b.frozen, b.trng);
+  prof_end(b);
 }
 void launch_max_drift(Batch& b) {
+  b.launches += 1;
   k_max_drift<<<nblocks(b.N), kBlock, 0, b.stream>>>(b.sp, b.sysid, b.N, b.pos, b.pos_ref, b.drift_bits);
 }
 void launch_nonfinite(Batch& b) {
+  b.launches += 1;
   cudaMemsetAsync(b.flags + kFlagWords, 0, sizeof(uint32_t) * 2 * b.R, b.stream);
   k_nonfinite<<<nblocks(b.N), kBlock, 0, b.stream>>>(b.sysid, b.N, b.pos, b.vel, b.flags + kFlagWords);
 }
 void launch_relax_step(Batch& b, float d) {
+  b.launches += 1;
   k_relax_step<<<nblocks(b.N), kBlock, 0, b.stream>>>(b.sp, b.sysid, b.N, b.pos, b.force, b.frozen, d);
 }
 

@@ -138,6 +138,41 @@ SysParams make_sys(const SoupConfig& c) {
 
 uint64_t cells_of(const int d[3]) { return (uint64_t)d[0] * d[1] * d[2]; }
 
+}  // namespace
+
+namespace soup {
+void prof_begin(Batch& b, int k) {
+  if (!b.prof) return;
+  Batch::Mark m{};
+  for (cudaEvent_t* e : {&m.a, &m.b}) {
+    if (!b.event_pool.empty()) { *e = b.event_pool.back(); b.event_pool.pop_back(); }
+    else SOUP_CUDA_TRY(cudaEventCreate(e));
+  }
+  m.k = k;
+  SOUP_CUDA_TRY(cudaEventRecord(m.a, b.stream));
+  b.marks.push_back(m);
+}
+void prof_end(Batch& b) {
+  if (!b.prof || b.marks.empty()) return;
+  SOUP_CUDA_TRY(cudaEventRecord(b.marks.back().b, b.stream));
+}
+void prof_flush(Batch& b) {
+  if (b.marks.empty()) return;
+  SOUP_CUDA_TRY(cudaStreamSynchronize(b.stream));
+  for (const Batch::Mark& m : b.marks) {
+    float ms = 0.f;
+    SOUP_CUDA_TRY(cudaEventElapsedTime(&ms, m.a, m.b));
+    b.kt_ms[m.k] += ms;
+    b.kt_n[m.k] += 1;
+    b.event_pool.push_back(m.a);
+    b.event_pool.push_back(m.b);
+  }
+  b.marks.clear();
+}
+}  // namespace soup
+
+namespace {
+
 // ---- batch construction ----------------------------------------------------------------------
 void alloc_grids(Batch& b) {
   dfree(b.cell_count); dfree(b.cell_start); dfree(b.cell_cursor); dfree(b.scan_tmp);
@@ -336,7 +371,8 @@ Batch* make_batch(const SoupConfig* cfgs, const SoupInitState* inits, uint32_t R
     b.hsp[r].nheads = (uint32_t)hall.size() - b.hsp[r].head_off;
   }
   b.H = (uint32_t)hall.size();
-  b.heads = dalloc<uint32_t>(b.H); b.head_sys = dalloc<uint32_t>(b.H);
+  b.heads = dalloc<uint32_t>(b.H); b.head_sys = dalloc<uint32_t>(b.H); b.head_slot = dalloc<uint32_t>(b.H);
+  b.head_e = dalloc<double>(b.H);
   b.es_nl = dalloc<uint32_t>((size_t)b.H * std::max<uint32_t>(b.es_cap, 1)); b.es_cnt = dalloc<uint32_t>(b.H);
   b.hcell_of = dalloc<uint32_t>(b.H); b.hsorted = dalloc<uint32_t>(b.H);
   if (b.H) {
@@ -365,11 +401,13 @@ void destroy_batch(Batch* b) {
                   b->frozen, b->id, b->slot_of, b->pos2, b->vel2, b->force2, b->charge2, b->slots2, b->center2,
                   b->held2, b->brng2, b->trng2, b->frozen2, b->id2, b->cell_of_slot, b->cell_count, b->cell_start,
                   b->cell_cursor, b->perm, b->scan_tmp, b->nl, b->nl_cnt, b->heads, b->head_sys, b->es_nl,
-                  b->es_cnt, b->hcell_count, b->hcell_start, b->hcell_cursor, b->hsorted, b->hcell_of, b->flags,
+                  b->es_cnt, b->head_slot, b->head_e, b->hcell_count, b->hcell_start, b->hcell_cursor, b->hsorted, b->hcell_of, b->flags,
                   b->events, b->desorb, b->drift_bits, b->bond_items, b->bond_nitems, b->uf_parent, b->comp_min,
                   b->item_done, b->has_item, b->sweep_out, b->prot_rng_dev, b->sp, b->shared, b->sysid, b->occ,
                   b->vis, b->frontier};
   for (void* p : ptrs) if (p) cudaFree(p);
+  for (const Batch::Mark& m : b->marks) { cudaEventDestroy(m.a); cudaEventDestroy(m.b); }
+  for (cudaEvent_t e : b->event_pool) cudaEventDestroy(e);
   if (b->stream) cudaStreamDestroy(b->stream);
   for (SoupHandle* h : b->views) delete h;
   delete b;
@@ -383,6 +421,7 @@ void guards(Batch& b, uint64_t chunk_start) {
   SOUP_CUDA_TRY(cudaMemcpyAsync(drift.data(), b.drift_bits, 4 * (size_t)b.R, cudaMemcpyDeviceToHost, b.stream));
   SOUP_CUDA_TRY(cudaStreamSynchronize(b.stream));
   SOUP_CUDA_TRY(cudaGetLastError());
+  prof_flush(b);
   for (uint32_t r = 0; r < b.R; ++r) {
     const uint32_t np = fl[FLAG_WORDS + 2 * r], nv = fl[FLAG_WORDS + 2 * r + 1];
     if (np || nv) {
@@ -440,7 +479,11 @@ void sweep_all(Batch& b, std::vector<SoupSweepResult>* out) {
   std::vector<double> so(4 * (size_t)b.R);
   SOUP_CUDA_TRY(cudaMemcpyAsync(so.data(), b.sweep_out, 8 * so.size(), cudaMemcpyDeviceToHost, b.stream));
   SOUP_CUDA_TRY(cudaMemcpyAsync(b.prot_rng.data(), b.prot_rng_dev, 4 * (size_t)b.R, cudaMemcpyDeviceToHost, b.stream));
-  force_pass(b);   // soup/src/soup-protonation.ts:62-73: F(x) is stale after the charges changed
+  // soup/src/soup-protonation.ts:62-73: F(x) is stale after the charges changed.  The reference
+  // re-runs its rebuild+force pass; in drift-triggered mode only the force is recomputed (the lists
+  // are sets that do not depend on charges, and the drift trigger keeps them complete).
+  if (b.cfg[0].rebuild_on_drift) { launch_force(b); b.force_fresh = true; }
+  else force_pass(b);
   SOUP_CUDA_TRY(cudaStreamSynchronize(b.stream));
   b.sweeps++;
   if (out) {
@@ -864,6 +907,27 @@ int soup_aggregate_labels(SoupHandle* h, const uint32_t* member_idx, uint32_t n_
     if (st) fail(st, err);
   });
 }
+
+void* soup_stream(SoupHandle* h) { return (h && h->b) ? (void*)h->b->stream : nullptr; }
+
+int soup_profile(SoupHandle* h, int enable) {
+  return guarded(h, [&](Batch& b, uint32_t) {
+    prof_flush(b);
+    b.prof = enable != 0;
+    for (int k = 0; k < SOUP_K_COUNT; ++k) { b.kt_ms[k] = 0; b.kt_n[k] = 0; }
+  });
+}
+
+int soup_kernel_time(SoupHandle* h, int kernel, double* total_ms, uint64_t* launches) {
+  return guarded(h, [&](Batch& b, uint32_t) {
+    if (kernel < 0 || kernel >= SOUP_K_COUNT) fail(SOUP_E_ARG, "unknown kernel group");
+    prof_flush(b);
+    if (total_ms) *total_ms = b.kt_ms[kernel];
+    if (launches) *launches = b.kt_n[kernel];
+  });
+}
+
+uint64_t soup_launch_count(SoupHandle* h) { return (h && h->b) ? h->b->launches : 0; }
 
 int soup_batch_create(const SoupConfig* cfgs, const SoupInitState* inits, uint32_t n_replicas, SoupBatch** out) {
   try {

@@ -123,9 +123,23 @@ __device__ __forceinline__ int ex_cell_axis(float p, float L, int n) {
 // ---------------------------------------------------------------------------------------------
 __device__ __forceinline__ float fast_mi(float d, float L, float invL) { return fmaf(-rintf(d * invL), L, d); }
 
+// The per-system numbers the pair loop needs, held in registers.
+struct PairP {
+  float box[3], inv_box[3];
+  float es_A, es_kappa, es_rc, es_fc, es_split, acid;
+  __device__ __forceinline__ static PairP of(const SysParams& P) {
+    PairP q;
+    for (int a = 0; a < 3; ++a) { q.box[a] = P.box[a]; q.inv_box[a] = P.inv_box[a]; }
+    q.es_A = P.es_A; q.es_kappa = P.es_kappa; q.es_rc = P.es_rc; q.es_fc = P.es_fc; q.es_split = P.es_split;
+    q.acid = P.acid;
+    return q;
+  }
+};
+
 // Scalar s such that the pair force on i is s * d (d = mi(xi - xj)), for every term the
 // neighbour list carries: WCA, class attraction (+ acid-soap depth), near-half screened Coulomb.
-__device__ __forceinline__ float pair_scalar(const Shared& S, const SysParams& P, const PairConst& pc,
+template <class PP>
+__device__ __forceinline__ float pair_scalar(const Shared& S, const PP& P, const PairConst& pc,
                                              float r2, int ki, int kj, float qi, float qj) {
   float rinv = rsqrtf(r2);
   float r = r2 * rinv;

@@ -14,6 +14,7 @@
 //   nl     u32 [slot][list_cap] Verlet neighbours as SLOT indices; nl_cnt u32 [slot]
 //   heads  u32 original ids of titratable beads (ascending; static);  es_nl [head][es_cap] slots
 #pragma once
+#include <algorithm>
 #include <cstdint>
 #include <string>
 #include <vector>
@@ -71,6 +72,8 @@ struct Batch {
   uint32_t H = 0;                    // total heads
   uint32_t* heads = nullptr;         // global original ids, per replica ascending
   uint32_t* head_sys = nullptr;      // replica of each head
+  uint32_t* head_slot = nullptr;     // current slot of each head (refreshed at every rebuild)
+  double* head_e = nullptr;          // constant-pH flip energy per head (scratch of the sweep)
   uint32_t es_cap = 0;
   uint32_t* es_nl = nullptr;
   uint32_t* es_cnt = nullptr;
@@ -111,7 +114,21 @@ struct Batch {
   int tpp = 8;                       // threads per particle in the list kernels
   std::string err;
   std::vector<SoupHandle*> views;    // per-replica handle views
+
+  // measurement: launch counter and optional per-group event timing
+  uint64_t launches = 0;
+  bool prof = false;
+  struct Mark { cudaEvent_t a, b; int k; };
+  std::vector<Mark> marks;
+  std::vector<cudaEvent_t> event_pool;
+  double kt_ms[SOUP_K_COUNT] = {};
+  uint64_t kt_n[SOUP_K_COUNT] = {};
 };
+
+// bracket one launch group with events when profiling is on
+void prof_begin(Batch& b, int k);
+void prof_end(Batch& b);
+void prof_flush(Batch& b);
 
 }  // namespace soup
 
@@ -131,7 +148,9 @@ void launch_cell_index(Batch& b);
 void launch_sort_and_gather(Batch& b);
 void launch_build_lists(Batch& b);
 void launch_build_es_lists(Batch& b);
-void launch_force(Batch& b);
+void launch_force(Batch& b);       // list force, then the far electrostatics half
+void launch_force_list(Batch& b);
+void launch_es_far(Batch& b);
 void launch_force_brute(Batch& b);
 void launch_kick_drift(Batch& b);
 void launch_kick_thermo(Batch& b);
