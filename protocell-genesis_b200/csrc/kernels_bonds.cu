@@ -214,13 +214,13 @@ struct St {
         const uint32_t prev = held[ks];
         held[ks] = prev + inc;
         if (prev + inc > (uint32_t)S.max_hold) {
-          if (cas(i, tip, NONE)) { cas(tip, i, NONE); held[ks] = 0; desorb[2 * rs + 1]++; }
+          if (cas(i, tip, NONE)) { cas(tip, i, NONE); held[ks] = 0; atomicAdd(&desorb[2 * rs + 1], 1u); }
         }
       }
     } else {
       const uint32_t owner = center[ks];                  // desorbStretch (bond-adsorption.wgsl:283-292)
       if (owner != NONE && dist(i, owner) >= S.r_inf) {
-        if (cas(i, owner, NONE)) { cas(owner, i, NONE); held[sl(owner)] = 0; desorb[2 * rs + 0]++; }
+        if (cas(i, owner, NONE)) { cas(owner, i, NONE); held[sl(owner)] = 0; atomicAdd(&desorb[2 * rs + 0], 1u); }
       }
     }
     for (int c = 0; c < np; ++c) {
@@ -238,7 +238,7 @@ struct St {
       else if (roleI == 1) ok = terminate(i);
       else ok = terminate(j);
       if (!ok) { release(i, sI); release(j, sJ); continue; }
-      events[2 * SOUP_MAX_RULES * rs + 2 * r]++;
+      atomicAdd(&events[2 * SOUP_MAX_RULES * rs + 2 * r], 1u);   // components run concurrently
     }
   }
 };

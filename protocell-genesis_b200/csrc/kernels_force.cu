@@ -71,18 +71,30 @@ __global__ void __launch_bounds__(256) k_force(
     const uint32_t cnt = nl_cnt[k];
     const uint32_t* row = nl + (size_t)k * cap;
     const PairConst* prow = &S.pair[ki * SOUP_KMAX];
-    for (uint32_t s = lane; s < cnt; s += TPP) {
-      const uint32_t j = __ldg(row + s);
-      const float4 xj = __ldg(pos + j);
-      const float dx = fast_mi(xi.x - xj.x, P.box[0], P.inv_box[0]);
-      const float dy = fast_mi(xi.y - xj.y, P.box[1], P.inv_box[1]);
-      const float dz = fast_mi(xi.z - xj.z, P.box[2], P.inv_box[2]);
-      const float r2 = dx * dx + dy * dy + dz * dz;
-      if (r2 >= rmax2 || r2 < 1e-12f) continue;
-      const int kj = (int)xj.w;
-      const float qj = needq ? __ldg(charge + j) : 0.f;
-      const float sc = pair_scalar(S, P, prow[kj], r2, ki, kj, qi, qj);
-      fx += sc * dx; fy += sc * dy; fz += sc * dz;
+    // lane takes entries [c*4*TPP + 4*lane, +4): one 16-byte load (rows are 32-byte aligned); the
+    // next chunk's load is issued before the current chunk is evaluated
+    constexpr uint32_t CH = 4 * TPP;
+    uint32_t base = 4u * (uint32_t)lane;
+    uint4 nxt = base < cnt ? __ldg(reinterpret_cast<const uint4*>(row + base)) : make_uint4(k, k, k, k);
+    for (; base < cnt; base += CH) {
+      const uint4 jj = nxt;
+      if (base + CH < cnt) nxt = __ldg(reinterpret_cast<const uint4*>(row + base + CH));
+      const uint32_t jv[4] = {jj.x, base + 1 < cnt ? jj.y : k, base + 2 < cnt ? jj.z : k, base + 3 < cnt ? jj.w : k};
+      float4 xj[4];
+#pragma unroll
+      for (int e = 0; e < 4; ++e) xj[e] = __ldg(pos + jv[e]);
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const float dx = fast_mi(xi.x - xj[e].x, P.box[0], P.inv_box[0]);
+        const float dy = fast_mi(xi.y - xj[e].y, P.box[1], P.inv_box[1]);
+        const float dz = fast_mi(xi.z - xj[e].z, P.box[2], P.inv_box[2]);
+        const float r2 = dx * dx + dy * dy + dz * dz;
+        if (r2 >= rmax2 || r2 < 1e-12f) continue;
+        const int kj = (int)xj[e].w;
+        const float qj = needq ? __ldg(charge + jv[e]) : 0.f;
+        const float sc = pair_scalar(S, P, prow[kj], r2, ki, kj, qi, qj);
+        fx += sc * dx; fy += sc * dy; fz += sc * dz;
+      }
     }
     // bonded terms (bondedForce), spread over the group
     uint32_t sl[3] = {slots[3 * k], slots[3 * k + 1], slots[3 * k + 2]};

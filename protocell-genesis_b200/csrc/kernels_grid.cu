@@ -261,23 +261,28 @@ __global__ void k_head_sort_cells(const uint32_t* __restrict__ hstart, uint32_t 
   }
 }
 
-// soup/wgsl/electrostatics-long.wgsl:31-56 head list at rc_es + skin, via the head grid.
-// Entries are the neighbours' HEAD indices (head_slot maps them to slots).
-__global__ void k_build_es_list(const uint32_t* __restrict__ heads, const uint32_t* __restrict__ head_sys, uint32_t H,
-                                const uint32_t* __restrict__ slot_of, const float4* __restrict__ pos,
-                                const SysParams* __restrict__ sp, const uint32_t* __restrict__ hcell_of,
-                                const uint32_t* __restrict__ hstart, const uint32_t* __restrict__ hsorted,
-                                uint32_t cap, uint32_t* __restrict__ es_nl, uint32_t* __restrict__ es_cnt,
-                                uint32_t* __restrict__ flags) {
-  uint32_t h = blockIdx.x * blockDim.x + threadIdx.x;
-  if (h >= H) return;
+// soup/wgsl/electrostatics-long.wgsl:31-56 head list at rc_es + skin, via the head grid, a warp per
+// head: lanes test 32 candidates at a time, hits are compacted with a ballot.  Entries are the
+// neighbours' HEAD indices (head_slot maps them to slots); membership uses the exact test near the
+// range, so the set equals the reference's.
+__global__ void __launch_bounds__(256) k_build_es_list(const uint32_t* __restrict__ head_sys, uint32_t H,
+                                                       const uint32_t* __restrict__ head_slot, const float4* __restrict__ pos,
+                                                       const SysParams* __restrict__ sp, const uint32_t* __restrict__ hcell_of,
+                                                       const uint32_t* __restrict__ hstart, const uint32_t* __restrict__ hsorted,
+                                                       uint32_t cap, uint32_t* __restrict__ es_nl, uint32_t* __restrict__ es_cnt,
+                                                       uint32_t* __restrict__ flags) {
+  const uint32_t h = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (h >= H) return;   // warp-uniform
   const SysParams& P = sp[head_sys[h]];
-  const uint32_t ks = slot_of[heads[h]];
-  const float4 xi = pos[ks];
+  const float4 xi = pos[head_slot[h]];
   const float box[3] = {P.box[0], P.box[1], P.box[2]};
-  uint32_t c = hcell_of[h] - P.hcell_off;
-  int q[3] = {(int)(c % (uint32_t)P.hdims[0]), (int)((c / (uint32_t)P.hdims[0]) % (uint32_t)P.hdims[1]),
-              (int)(c / ((uint32_t)P.hdims[0] * (uint32_t)P.hdims[1]))};
+  const float inv[3] = {P.inv_box[0], P.inv_box[1], P.inv_box[2]};
+  const float lr = P.es_list_range;
+  const float lo = lr * lr * (1.0f - 1e-5f), hi = lr * lr * (1.0f + 1e-5f);
+  const uint32_t c = hcell_of[h] - P.hcell_off;
+  const int q[3] = {(int)(c % (uint32_t)P.hdims[0]), (int)((c / (uint32_t)P.hdims[0]) % (uint32_t)P.hdims[1]),
+                    (int)(c / ((uint32_t)P.hdims[0] * (uint32_t)P.hdims[1]))};
   const int R = P.hwalk;
   int ax[3][8], na[3] = {0, 0, 0};
   for (int a = 0; a < 3; ++a)
@@ -289,22 +294,39 @@ __global__ void k_build_es_list(const uint32_t* __restrict__ heads, const uint32
     }
   uint32_t cnt = 0;
   uint32_t* row = es_nl + (size_t)h * cap;
+  const uint32_t lt = (1u << lane) - 1u;
   for (int iz = 0; iz < na[2]; ++iz)
     for (int iy = 0; iy < na[1]; ++iy)
       for (int ix = 0; ix < na[0]; ++ix) {
-        uint32_t cc = P.hcell_off + (uint32_t)(ax[0][ix] + P.hdims[0] * (ax[1][iy] + P.hdims[1] * ax[2][iz]));
-        for (uint32_t t = hstart[cc]; t < hstart[cc + 1]; ++t) {
-          uint32_t g = hsorted[t];
-          if (g == h) continue;
-          uint32_t js = slot_of[heads[g]];
-          if (ex_dist(xi, pos[js], box) < P.es_list_range) {
-            if (cnt < cap) row[cnt] = g;
-            ++cnt;
+        const uint32_t cc = P.hcell_off + (uint32_t)(ax[0][ix] + P.hdims[0] * (ax[1][iy] + P.hdims[1] * ax[2][iz]));
+        const uint32_t a0 = hstart[cc], e0 = hstart[cc + 1];
+        for (uint32_t b0 = a0; b0 < e0; b0 += 32) {
+          const uint32_t t = b0 + lane;
+          bool hit = false;
+          uint32_t g = 0;
+          if (t < e0) {
+            g = hsorted[t];
+            if (g != h) {
+              const float4 xj = pos[head_slot[g]];
+              const float dx = fast_mi(xi.x - xj.x, box[0], inv[0]);
+              const float dy = fast_mi(xi.y - xj.y, box[1], inv[1]);
+              const float dz = fast_mi(xi.z - xj.z, box[2], inv[2]);
+              const float r2 = dx * dx + dy * dy + dz * dz;
+              hit = r2 < lo || (r2 <= hi && ex_dist(xi, xj, box) < lr);
+            }
           }
+          const uint32_t m = __ballot_sync(0xffffffffu, hit);
+          if (hit) {
+            const uint32_t at = cnt + __popc(m & lt);
+            if (at < cap) row[at] = g;
+          }
+          cnt += __popc(m);
         }
       }
-  if (cnt > cap) { flags[1] = 1u; cnt = cap; }
-  es_cnt[h] = cnt;
+  if (lane == 0) {
+    if (cnt > cap) { flags[1] = 1u; cnt = cap; }
+    es_cnt[h] = cnt;
+  }
 }
 
 }  // namespace
@@ -358,9 +380,9 @@ void launch_build_es_lists(Batch& b) {
   cudaMemsetAsync(b.hcell_cursor, 0, sizeof(uint32_t) * b.nhcells, b.stream);
   k_head_scatter<<<nblocks(b.H), kBlock, 0, b.stream>>>(b.hcell_of, b.hcell_start, b.H, b.hcell_cursor, b.hsorted);
   k_head_sort_cells<<<nblocks(b.nhcells), kBlock, 0, b.stream>>>(b.hcell_start, b.nhcells, b.hsorted);
-  k_build_es_list<<<nblocks(b.H, 128), 128, 0, b.stream>>>(b.heads, b.head_sys, b.H, b.slot_of, b.pos, b.sp,
-                                                           b.hcell_of, b.hcell_start, b.hsorted, b.es_cap, b.es_nl,
-                                                           b.es_cnt, b.flags);
+  k_build_es_list<<<nblocks((uint64_t)b.H * 32, 256), 256, 0, b.stream>>>(b.head_sys, b.H, b.head_slot, b.pos, b.sp,
+                                                                         b.hcell_of, b.hcell_start, b.hsorted, b.es_cap,
+                                                                         b.es_nl, b.es_cnt, b.flags);
   b.launches += 5 + g_scan_launches;
   prof_end(b);
 }

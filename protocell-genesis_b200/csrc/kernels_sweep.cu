@@ -39,11 +39,14 @@ __device__ __forceinline__ double acid_well(const SysParams& P, double r) {
   const double c = cos((3.141592653589793 * (r - P.d_rcattr)) / (2.0 * P.d_wc));
   return -P.d_acid * P.d_eps * c * c;
 }
+// squared minimum-image distance, FP64, JavaScript rounding of the image (Math.round(d / L)).  The
+// image index is taken from d * (1/L): it can differ from d / L only within an ulp of a half-box
+// offset, where every pair is beyond the (at most 0.45 L) cutoffs either way.
 __device__ __forceinline__ double dist2(const SysParams& P, const float4& a, const float4& b) {
   double dx = (double)a.x - (double)b.x, dy = (double)a.y - (double)b.y, dz = (double)a.z - (double)b.z;
-  dx -= js_round(dx / P.d_box[0]) * P.d_box[0];
-  dy -= js_round(dy / P.d_box[1]) * P.d_box[1];
-  dz -= js_round(dz / P.d_box[2]) * P.d_box[2];
+  dx -= js_round(dx * P.d_inv_box[0]) * P.d_box[0];
+  dy -= js_round(dy * P.d_inv_box[1]) * P.d_box[1];
+  dz -= js_round(dz * P.d_inv_box[2]) * P.d_box[2];
   return dx * dx + dy * dy + dz * dz;
 }
 // the energy a neighbour of charge qj at squared distance r2 contributes to a site's E
@@ -101,16 +104,76 @@ __device__ __forceinline__ bool metropolis(double dG, double kT, double u) {
   return u < exp(-dG / kT);
 }
 
-constexpr int kWalkThreads = 512;
+// the pcgNext LCG (state' = a state + c mod 2^32) advanced n steps at once
+struct Lcg { uint32_t a, c; };
+__device__ __forceinline__ Lcg lcg_pow(uint32_t n) {
+  Lcg acc{1u, 0u}, b{747796405u, 2891336453u};
+  while (n) {
+    if (n & 1u) acc = Lcg{acc.a * b.a, acc.c * b.a + b.c};
+    b = Lcg{b.a * b.a, b.c * b.a + b.c};
+    n >>= 1;
+  }
+  return acc;
+}
+__device__ __forceinline__ double pcg_out(uint32_t v) {
+  v = ((v >> ((v >> 28u) + 4u)) ^ v) * 277803737u;
+  v = (v >> 22u) ^ v;
+  return (double)v / 4294967296.0;
+}
+
+// Draws of the pcgNext stream, 32 at a time: lane l of every warp holds draw base+l; the walker
+// takes them in order through a shuffle (the same values in every warp).
+struct Stream {
+  uint32_t st;       // state after draw base+lane
+  double u;          // draw base+lane
+  uint32_t base, p;  // first draw held, next draw to hand out
+  Lcg jump32;
+  __device__ void init(uint32_t s0, int lane) {
+    const Lcg j = lcg_pow((uint32_t)lane + 1u);
+    st = j.a * s0 + j.c;
+    u = pcg_out(st);
+    base = 0; p = 0;
+    jump32 = lcg_pow(32u);
+  }
+  __device__ double next() {
+    if (p - base == 32u) {
+      st = jump32.a * st + jump32.c;
+      u = pcg_out(st);
+      base += 32u;
+    }
+    const int l = (int)(p - base);
+    ++p;
+    return __shfl_sync(0xffffffffu, u, l);
+  }
+};
+
+constexpr int kWalkThreads = 1024;
+
+// head positions for the flip updates: by head index (hpos) and in head-cell order with the head
+// index in w (spos), so a flip scans contiguous, L2-resident candidate ranges
+__global__ void k_gather_heads(const uint32_t* __restrict__ head_slot, uint32_t H, const float4* __restrict__ pos,
+                               const uint32_t* __restrict__ hsorted, float4* __restrict__ hpos,
+                               float4* __restrict__ spos) {
+  const uint32_t h = blockIdx.x * blockDim.x + threadIdx.x;
+  if (h >= H) return;
+  hpos[h] = pos[head_slot[h]];
+  const uint32_t g = hsorted[h];
+  const float4 p = pos[head_slot[g]];
+  spos[h] = make_float4(p.x, p.y, p.z, __uint_as_float(g));
+}
 
 template <bool SMEM>
 __global__ void __launch_bounds__(kWalkThreads) k_sweep_walk(const SysParams* __restrict__ sp,
                                                              const uint32_t* __restrict__ head_slot,
-                                                             const float4* __restrict__ pos, float* __restrict__ charge,
+                                                             const float4* __restrict__ hpos, float* __restrict__ charge,
                                                              const uint32_t* __restrict__ es_nl,
                                                              const uint32_t* __restrict__ es_cnt, uint32_t cap,
-                                                             double* __restrict__ Eg, uint32_t* __restrict__ rng_io,
-                                                             double* __restrict__ out, uint32_t only) {
+                                                             const uint32_t* __restrict__ hcell_of,
+                                                             const uint32_t* __restrict__ hstart,
+                                                             const float4* __restrict__ spos,
+                                                             double* __restrict__ Eg, uint8_t* __restrict__ flag_g,
+                                                             uint32_t* __restrict__ rng_io, double* __restrict__ out,
+                                                             uint32_t only) {
   extern __shared__ __align__(16) unsigned char smem[];
   const uint32_t r = (only == SOUP_NONE_U32) ? blockIdx.x : only;
   const SysParams& P = sp[r];
@@ -118,64 +181,96 @@ __global__ void __launch_bounds__(kWalkThreads) k_sweep_walk(const SysParams* __
   if (H == 0 || !P.es_on) return;
   const uint32_t off = P.head_off;
   double* E = SMEM ? reinterpret_cast<double*>(smem) : Eg + off;
-  unsigned char* flag = SMEM ? smem + 8 * (size_t)H : nullptr;
-  __shared__ double s_stats[2];
-  __shared__ uint32_t s_acc;
-  if (SMEM) {
-    for (uint32_t h = threadIdx.x; h < H; h += kWalkThreads) {
-      E[h] = Eg[off + h];
-      flag[h] = charge[head_slot[off + h]] != 0.f ? 1 : 0;
-    }
+  uint8_t* flag = SMEM ? smem + 8 * (size_t)H : flag_g + off;
+  const float qd = (float)P.d_q;
+  // flag: 0 neutral, 1 charged with the deprotonated charge, 2 charged with another value
+  for (uint32_t h = threadIdx.x; h < H; h += kWalkThreads) {
+    if (SMEM) E[h] = Eg[off + h];
+    const float q = charge[head_slot[off + h]];
+    flag[h] = q == 0.f ? 0 : (q == qd ? 1 : 2);
   }
-  if (threadIdx.x == 0) { s_stats[0] = 0.0; s_stats[1] = 0.0; s_acc = 0; }
   __syncthreads();
+  const int lane = threadIdx.x & 31;
   const double kT = P.d_kT;
   const double dGintr = kT * 2.302585092994046 * (P.d_pka - P.d_ph);
   const double cut2 = P.d_rc * P.d_rc, reach = P.d_rcattr + P.d_wc, reach2 = reach * reach;
-  uint32_t rng = rng_io[r];
+  const uint32_t s0 = rng_io[r];
+  Stream rs;
+  rs.init(s0, lane);
+  uint32_t accepted = 0, dcount = 0;
+  double dsum = 0.0;
   for (uint32_t a = 0; a < H; ++a) {
-    const double u = pcg_next(rng);
+    const double u = rs.next();
     const uint32_t s = (uint32_t)fmin((double)(H - 1), floor(u * (double)H));
     const double Es = E[s];
-    const bool ch = SMEM ? flag[s] != 0 : charge[head_slot[off + s]] != 0.f;
+    const uint8_t f = flag[s];
+    const bool ch = f != 0;
     const double dG = ch ? -Es : Es;
     bool acc = dG <= 0.0;
-    if (!acc) acc = metropolis(dG, kT, pcg_next(rng));
+    if (!acc) acc = metropolis(dG, kT, rs.next());
     if (!acc) continue;
-    const uint32_t ks = head_slot[off + s];
-    const float q_old = charge[ks];
-    const float q_new = ch ? 0.f : (float)P.d_q;
-    const float4 xi = pos[ks];
-    const uint32_t cnt = es_cnt[off + s];
-    const uint32_t* row = es_nl + (size_t)(off + s) * cap;
-    for (uint32_t k = threadIdx.x; k < cnt; k += kWalkThreads) {
-      const uint32_t t = row[k];
-      const double r2 = dist2(P, xi, pos[head_slot[t]]);
-      E[t - off] += site_term(P, r2, q_new, cut2, reach2) - site_term(P, r2, q_old, cut2, reach2);
+    const float q_old = f == 0 ? 0.f : (f == 1 ? qd : charge[head_slot[off + s]]);
+    const float q_new = ch ? 0.f : qd;
+    const float4 xi = hpos[off + s];
+    {
+      // candidates: the +-hwalk head cells around the site's cell at the last rebuild (complete for
+      // r < rc_es while every head has drifted less than skin/2), one row of cells per warp
+      const uint32_t c = hcell_of[off + s] - P.hcell_off;
+      const int nx = P.hdims[0], ny = P.hdims[1], nz = P.hdims[2], R = P.hwalk;
+      const int qx = (int)(c % (uint32_t)nx), qy = (int)((c / (uint32_t)nx) % (uint32_t)ny),
+                qz = (int)(c / ((uint32_t)nx * (uint32_t)ny));
+      const int span = 2 * R + 1;
+      const int nyv = span < ny ? span : ny, nzv = span < nz ? span : nz;
+      int xlo[2], xhi[2], nxr;
+      {
+        const int lo = qx - R, hi = qx + R;
+        if (hi - lo + 1 >= nx) { nxr = 1; xlo[0] = 0; xhi[0] = nx - 1; }
+        else if (lo < 0) { nxr = 2; xlo[0] = lo + nx; xhi[0] = nx - 1; xlo[1] = 0; xhi[1] = hi; }
+        else if (hi >= nx) { nxr = 2; xlo[0] = lo; xhi[0] = nx - 1; xlo[1] = 0; xhi[1] = hi - nx; }
+        else { nxr = 1; xlo[0] = lo; xhi[0] = hi; }
+      }
+      const int w = threadIdx.x >> 5;
+      for (int rowi = w; rowi < nyv * nzv; rowi += kWalkThreads / 32) {
+        const int y = (span < ny) ? ((qy - R + rowi % nyv) % ny + ny) % ny : rowi % nyv;
+        const int z = (span < nz) ? ((qz - R + rowi / nyv) % nz + nz) % nz : rowi / nyv;
+        const uint32_t rb = P.hcell_off + (uint32_t)(nx * (y + ny * z));
+        for (int xr = 0; xr < nxr; ++xr) {
+          const uint32_t a0 = hstart[rb + xlo[xr]], e0 = hstart[rb + xhi[xr] + 1];
+          for (uint32_t k = a0 + lane; k < e0; k += 32) {
+            const float4 pj = spos[k];
+            const uint32_t t = __float_as_uint(pj.w);
+            if (t == off + s) continue;
+            const double r2 = dist2(P, xi, pj);
+            if (r2 < cut2 || r2 < reach2)
+              E[t - off] += site_term(P, r2, q_new, cut2, reach2) - site_term(P, r2, q_old, cut2, reach2);
+          }
+        }
+      }
     }
-    __syncthreads();   // every thread has read charge[ks] and E[s] for this attempt
+    __syncthreads();   // every update of this flip is in E; every thread has read this attempt's state
+    flag[s] = ch ? 0 : 1;
     if (threadIdx.x == 0) {
-      charge[ks] = q_new;
-      if (SMEM) flag[s] = ch ? 0 : 1;
-      ++s_acc;
-      if (!ch) { s_stats[0] += (Es - dGintr) / kT; s_stats[1] += 1.0; }
+      charge[head_slot[off + s]] = q_new;
+      ++accepted;
+      if (!ch) { dsum += (Es - dGintr) / kT; ++dcount; }
     }
-    __syncthreads();
   }
-  double dep = 0.0;
-  for (uint32_t h = threadIdx.x; h < H; h += kWalkThreads) dep += charge[head_slot[off + h]] != 0.f ? 1.0 : 0.0;
+  __syncthreads();
+  __shared__ uint32_t s_dep;
+  if (threadIdx.x == 0) s_dep = 0;
+  __syncthreads();
+  uint32_t dep = 0;
+  for (uint32_t h = threadIdx.x; h < H; h += kWalkThreads) dep += flag[h] != 0;
   for (int o = 16; o > 0; o >>= 1) dep += __shfl_xor_sync(0xffffffffu, dep, o);
-  __shared__ double s_dep[kWalkThreads / 32];
-  if ((threadIdx.x & 31) == 0) s_dep[threadIdx.x >> 5] = dep;
+  if (lane == 0) atomicAdd(&s_dep, dep);
   __syncthreads();
   if (threadIdx.x == 0) {
-    double t = 0.0;
-    for (int w = 0; w < kWalkThreads / 32; ++w) t += s_dep[w];
-    rng_io[r] = rng;
+    const Lcg j = lcg_pow(rs.p);
+    rng_io[r] = j.a * s0 + j.c;
     out[4 * r + 0] = (double)H;
-    out[4 * r + 1] = (double)s_acc;
-    out[4 * r + 2] = s_stats[1] > 0 ? s_stats[0] / s_stats[1] : 0.0;
-    out[4 * r + 3] = t;
+    out[4 * r + 1] = (double)accepted;
+    out[4 * r + 2] = dcount > 0 ? dsum / dcount : 0.0;
+    out[4 * r + 3] = (double)s_dep;
   }
 }
 
@@ -187,25 +282,30 @@ void launch_sweep(Batch& b, uint32_t replica) {
   uint32_t hmax = 0;
   for (uint32_t r = 0; r < b.R; ++r)
     if (replica == SOUP_NONE_U32 || r == replica) hmax = std::max(hmax, b.hsp[r].nheads);
-  b.launches += 2;
+  b.launches += 3;
   prof_begin(b, SOUP_K_SWEEP);
+  k_gather_heads<<<(b.H + 255) / 256, 256, 0, b.stream>>>(b.head_slot, b.H, b.pos, b.hsorted, b.head_pos,
+                                                           b.head_spos);
   k_sweep_init<<<(unsigned)(((uint64_t)b.H * 32 + 255) / 256), 256, 0, b.stream>>>(
       b.sp, b.head_sys, b.head_slot, b.H, b.pos, b.charge, b.es_nl, b.es_cnt, b.es_cap, b.head_e, replica);
   const unsigned grid = replica == SOUP_NONE_U32 ? b.R : 1;
   const size_t smem = 9 * (size_t)hmax;
   if (smem <= 200 * 1024) {
-    static bool attr = false;
-    if (!attr) {
-      SOUP_CUDA_TRY(cudaFuncSetAttribute(k_sweep_walk<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
-      attr = true;
-    }
-    k_sweep_walk<true><<<grid, kWalkThreads, smem, b.stream>>>(b.sp, b.head_slot, b.pos, b.charge, b.es_nl, b.es_cnt,
-                                                               b.es_cap, b.head_e, b.prot_rng_dev, b.sweep_out, replica);
+    k_sweep_walk<true><<<grid, kWalkThreads, smem, b.stream>>>(b.sp, b.head_slot, b.head_pos, b.charge, b.es_nl,
+                                                               b.es_cnt, b.es_cap, b.hcell_of, b.hcell_start,
+                                                               b.head_spos, b.head_e, b.head_flag,
+                                                               b.prot_rng_dev, b.sweep_out, replica);
   } else {
-    k_sweep_walk<false><<<grid, kWalkThreads, 0, b.stream>>>(b.sp, b.head_slot, b.pos, b.charge, b.es_nl, b.es_cnt,
-                                                             b.es_cap, b.head_e, b.prot_rng_dev, b.sweep_out, replica);
+    k_sweep_walk<false><<<grid, kWalkThreads, 0, b.stream>>>(b.sp, b.head_slot, b.head_pos, b.charge, b.es_nl,
+                                                             b.es_cnt, b.es_cap, b.hcell_of, b.hcell_start,
+                                                             b.head_spos, b.head_e, b.head_flag,
+                                                             b.prot_rng_dev, b.sweep_out, replica);
   }
   prof_end(b);
+}
+
+void sweep_prepare(Batch& b) {
+  SOUP_CUDA_TRY(cudaFuncSetAttribute(k_sweep_walk<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
 }
 
 }  // namespace soup

@@ -42,7 +42,7 @@ struct SysParams {
   uint32_t es_on;            // electrostatics enabled
   int32_t charged_kind;
   // FP64 host-style numbers for the constant-pH sweep
-  double d_box[3];
+  double d_box[3], d_inv_box[3];
   double d_A, d_kappa, d_rc, d_shiftU, d_shiftF, d_pka, d_ph, d_kT, d_q;
   double d_acid, d_rcattr, d_wc, d_eps;
 };
@@ -138,27 +138,26 @@ struct PairP {
 
 // Scalar s such that the pair force on i is s * d (d = mi(xi - xj)), for every term the
 // neighbour list carries: WCA, class attraction (+ acid-soap depth), near-half screened Coulomb.
+// WCA and the attraction are evaluated unconditionally and selected (no divergent branches); the
+// screened Coulomb term only exists between charged beads and stays a branch.
 template <class PP>
 __device__ __forceinline__ float pair_scalar(const Shared& S, const PP& P, const PairConst& pc,
                                              float r2, int ki, int kj, float qi, float qj) {
-  float rinv = rsqrtf(r2);
-  float r = r2 * rinv;
-  float rinv2 = rinv * rinv;
-  float s = 0.f;
-  if (r2 < pc.wcut2) {                       // forces.wgsl:19-23: -wca_dv(r)/r
-    float s2 = pc.b2 * rinv2;
-    float s6 = s2 * s2 * s2;
-    s = 24.0f * S.eps * (2.0f * s6 * s6 - s6) * rinv2;
-  }
-  float scale = pc.attr;                     // pair.wgsl:188 class depth + acid-soap depth
-  if (P.acid > 0.f && S.cls[ki] == 1u && S.cls[kj] == 1u && ((qi != 0.f) != (qj != 0.f))) scale += P.acid;
-  if (scale > 0.f && r >= S.rc_attr && r <= S.rc_attr + S.wc) {   // forces.wgsl:32-37
-    float x = (r - S.rc_attr) * S.attr_k;
-    s -= scale * S.attr_amp * __sinf(2.0f * x) * rinv;
-  }
-  float qq = qi * qj;                        // electrostatics.wgsl:65-83, near half
+  const float rinv = rsqrtf(r2);
+  const float r = r2 * rinv;
+  const float rinv2 = rinv * rinv;
+  const float s2 = pc.b2 * rinv2;                         // forces.wgsl:19-23: -wca_dv(r)/r
+  const float s6 = s2 * s2 * s2;
+  const float fw = 24.0f * S.eps * (2.0f * s6 * s6 - s6) * rinv2;
+  float s = (r2 < pc.wcut2) ? fw : 0.f;
+  float scale = pc.attr;                                  // pair.wgsl:188 class depth + acid-soap depth
+  if (P.acid > 0.f && ((qi != 0.f) != (qj != 0.f)) && S.cls[ki] == 1u && S.cls[kj] == 1u) scale += P.acid;
+  const float x = (r - S.rc_attr) * S.attr_k;            // forces.wgsl:32-37
+  const float fa = scale * S.attr_amp * __sinf(2.0f * x) * rinv;
+  s -= (r >= S.rc_attr && r <= S.rc_attr + S.wc) ? fa : 0.f;
+  const float qq = qi * qj;                               // electrostatics.wgsl:65-83, near half
   if (qq != 0.f && r < P.es_split && r < P.es_rc && P.es_A != 0.f) {
-    float u = P.es_A * __expf(-P.es_kappa * r) * rinv;
+    const float u = P.es_A * __expf(-P.es_kappa * r) * rinv;
     s += qq * (u * (rinv + P.es_kappa) - P.es_fc) * rinv;
   }
   return s;

@@ -74,6 +74,9 @@ struct Batch {
   uint32_t* head_sys = nullptr;      // replica of each head
   uint32_t* head_slot = nullptr;     // current slot of each head (refreshed at every rebuild)
   double* head_e = nullptr;          // constant-pH flip energy per head (scratch of the sweep)
+  float4* head_pos = nullptr;        // head positions gathered for the sweep
+  float4* head_spos = nullptr;       // head positions in head-cell order (w = head index)
+  uint8_t* head_flag = nullptr;      // charge state per head when the sweep cannot keep it in shared memory
   uint32_t es_cap = 0;
   uint32_t* es_nl = nullptr;
   uint32_t* es_cnt = nullptr;
@@ -159,6 +162,7 @@ void launch_nonfinite(Batch& b);
 void launch_relax_step(Batch& b, float d);
 void launch_bonds(Batch& b);
 void launch_sweep(Batch& b, uint32_t replica);
+void sweep_prepare(Batch& b);
 void launch_rebuild_check(Batch& b);
 // analysis
 int run_closure(Batch& b, uint32_t r, const uint32_t* mem, uint32_t nm, const uint32_t* wat, uint32_t nw,
