@@ -10,7 +10,7 @@ Verlet rebuild on half-skin drift, bond Monte Carlo every 20 steps.  Inputs (sta
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl cuda|reference]
 
 One JSON line on rank 0.  N > 1 runs N independent replicas (one per GPU, weak scaling; the single
-system is not split).  --impl reference times the CPU oracle (the reference's step
+483k-bead system fits one GPU and is not split).  --impl reference times the CPU oracle (the reference's step
 restated in C++, OpenMP over the host cores) on the same workload.
 """
 import argparse

@@ -4,19 +4,26 @@
 // numbers), electrostatics.ts:277-281 esPairEnergy, soup/src/acid-soap.ts:147-198 (acidSoapWell,
 // acidSoapSiteWork), electrostatics.ts:308-315 pcgNext.
 //
-// The attempt chain is inherently sequential (attempt a+1's site depends on how many draws attempt a
-// used, which depends on its free energy).  What is not sequential is the energy: the reference
-// recomputes, per attempt, E_s = kT ln10 (pKa - pH) + sum over neighbours of the screened Coulomb work
-// + the acid-soap pair work, and E_s depends on the site's neighbours' charges only (not its own).
-// So:
-//   k_sweep_init   (all SMs) evaluates E_s for every head in FP64 from the head list.
-//   k_sweep_walk   (one CTA per replica) keeps E in shared memory and walks the attempts.  Every
-//                  thread walks the chain redundantly (same RNG, same shared reads), so a rejected
-//                  attempt needs no barrier; an accepted flip of site s adds its exact change to
-//                  E_t of every neighbour t (cooperatively), then one barrier.
-// Arithmetic is FP64 with JavaScript rounding of the minimum image, as the reference's.  E is
-// summed in a different order than the reference's cell walk, so it agrees to FP64 rounding (the
-// decisions agree unless a draw lands within ~1e-15 of its threshold).
+// The attempt chain is sequential: attempt a+1's site draw depends on whether attempt a took an
+// acceptance draw, which depends on its free energy.  The energy itself is not sequential: the
+// reference recomputes, per attempt, E_s = kT ln10 (pKa - pH) + the screened Coulomb work + the
+// acid-soap pair work over the site's neighbours, and E_s depends on the neighbours' charges only.
+// Positions are fixed during a sweep, so the change of E_t when neighbour s flips is a fixed number
+// per pair.  So:
+//   k_sweep_init  (all SMs, a warp per head) evaluates E_h in FP64 from the head list, and for every
+//                 list entry t of h the change D_ht of E_t when h deprotonates (-D_ht when it
+//                 protonates).
+//   k_sweep_walk  (one CTA per replica) keeps E in shared memory and walks the chain in windows of
+//                 32 draws.  Warp 0 holds the draws, their sites and those sites' positions in its
+//                 lanes (prefetched a window ahead); it resolves the window's attempts one by one (the
+//                 deciding lane, one shuffle), and when a flip is accepted every later lane adds the
+//                 flip's change to its own site energy (exact, the formula of D).  Then all warps add
+//                 the window's flips to E from the D rows, and the next window starts.
+// E and D are fixed point (2^-40 kT, int64): integer adds commute, so E does not depend on the
+// order the updates land in and every run is reproducible.  E_h is the FP64 sum rounded once, each
+// D_ht is rounded once, so the energies agree with the reference's FP64 sums to about 1e-11 kT (the
+// decisions agree unless a draw lands that close to its threshold).
+// Arithmetic is FP64 with JavaScript rounding of the minimum image, as the reference's.
 #include "soup_internal.h"
 
 namespace soup {
@@ -60,12 +67,41 @@ __device__ __forceinline__ double site_term(const SysParams& P, double r2, float
   return e;
 }
 
-// E_h = kT ln10 (pKa - pH) + uEs(h), a warp per head
+constexpr double kFix = 1099511627776.0;            // 2^40 fixed-point units per kT
+constexpr double kUnfix = 1.0 / 1099511627776.0;
+constexpr long long kSameSite = (long long)0x8000000000000000ull;   // M marker: both draws pick one site
+__device__ __forceinline__ long long to_fix(double x) { return __double2ll_rn(x * kFix); }
+// change of a neighbour's E when a site at squared distance r2 goes from charge qo to qn
+// (round-to-nearest-even is odd-symmetric, so the reverse flip gives exactly the negative)
+__device__ __forceinline__ long long flip_delta(const SysParams& P, double r2, float qo, float qn, double cut2,
+                                                double reach2) {
+  return to_fix(site_term(P, r2, qn, cut2, reach2) - site_term(P, r2, qo, cut2, reach2));
+}
+// flip_delta(r2, 0, qd) with one square root (the same operations in the same order, so the same
+// bits); the value of every D entry and of every in-window correction
+__device__ __forceinline__ long long std_delta(const SysParams& P, double r2, float qd, double cut2, double reach2) {
+  double t1 = 0.0, t0 = 0.0;
+  const bool es_in = qd != 0.f && r2 < cut2;
+  const bool ac_in = P.d_acid > 0.0 && r2 < reach2 && r2 > 0.0;
+  if (es_in || ac_in) {
+    const double rr = sqrt(r2);
+    if (es_in) t1 += es_energy(P, rr, P.d_q * (double)qd);
+    if (ac_in) {
+      const double v = acid_well(P, rr);
+      t1 += -v;
+      t0 += v;
+    }
+  }
+  return to_fix(t1 - t0);
+}
+
+// E_h = kT ln10 (pKa - pH) + uEs(h) and the row D_h, a warp per head
 __global__ void __launch_bounds__(256) k_sweep_init(const SysParams* __restrict__ sp, const uint32_t* __restrict__ head_sys,
                                                     const uint32_t* __restrict__ head_slot, uint32_t H,
                                                     const float4* __restrict__ pos, const float* __restrict__ charge,
                                                     const uint32_t* __restrict__ es_nl, const uint32_t* __restrict__ es_cnt,
-                                                    uint32_t cap, double* __restrict__ E, uint32_t only) {
+                                                    uint32_t cap, long long* __restrict__ E, long long* __restrict__ D,
+                                                    uint32_t only) {
   const uint32_t h = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (h >= H) return;
@@ -74,10 +110,12 @@ __global__ void __launch_bounds__(256) k_sweep_init(const SysParams* __restrict_
   const SysParams& P = sp[r];
   if (!P.es_on) return;
   const double cut2 = P.d_rc * P.d_rc, reach = P.d_rcattr + P.d_wc, reach2 = reach * reach;
+  const float qd = (float)P.d_q;
   const float4 xi = pos[head_slot[h]];
   double es = 0.0, w = 0.0;
   const uint32_t cnt = es_cnt[h];
   const uint32_t* row = es_nl + (size_t)h * cap;
+  long long* drow = D + (size_t)h * cap;
   for (uint32_t s = lane; s < cnt; s += 32) {
     const uint32_t js = head_slot[row[s]];
     const float qj = charge[js];
@@ -87,20 +125,25 @@ __global__ void __launch_bounds__(256) k_sweep_init(const SysParams* __restrict_
       const double v = acid_well(P, sqrt(r2));
       w += (qj == 0.f) ? v : -v;
     }
+    drow[s] = std_delta(P, r2, qd, cut2, reach2);
   }
   for (int o = 16; o > 0; o >>= 1) {
     es += __shfl_xor_sync(0xffffffffu, es, o);
     w += __shfl_xor_sync(0xffffffffu, w, o);
   }
-  if (lane == 0) E[h] = P.d_kT * 2.302585092994046 * (P.d_pka - P.d_ph) + (es + w);
+  if (lane == 0) E[h] = to_fix(P.d_kT * 2.302585092994046 * (P.d_pka - P.d_ph) + (es + w));
 }
 
-// exp(-dG/kT) > u  decided by an FP32 estimate when far from the threshold, else in FP64
-__device__ __forceinline__ bool metropolis(double dG, double kT, double u) {
-  const float x = (float)(-dG / kT);
-  const double est = (double)__expf(x);
-  if (u < est * (1.0 - 1e-5)) return true;
-  if (u > est * (1.0 + 1e-5) + 1e-300) return false;
+// u < exp(-dG/kT) for dG > 0.  For -dG/kT > -20 an FP32 estimate decides when u is more than 1e-5
+// (relative) away from it: __expf's error there is below 2 + 1.16*20 ulp and the FP32 rounding of
+// the exponent adds 1e-6, together under 5e-6.  Otherwise, and near the threshold, FP64 decides.
+__device__ __forceinline__ bool metropolis(double dG, double kT, double inv_kT, double u) {
+  const double xd = -dG * inv_kT;
+  if (xd > -20.0) {
+    const double est = (double)__expf((float)xd);
+    if (u < est * (1.0 - 1e-5)) return true;
+    if (u > est * (1.0 + 1e-5)) return false;
+  }
   return u < exp(-dG / kT);
 }
 
@@ -121,45 +164,62 @@ __device__ __forceinline__ double pcg_out(uint32_t v) {
   return (double)v / 4294967296.0;
 }
 
-// Draws of the pcgNext stream, 32 at a time: lane l of every warp holds draw base+l; the walker
-// takes them in order through a shuffle (the same values in every warp).
-struct Stream {
-  uint32_t st;       // state after draw base+lane
-  double u;          // draw base+lane
-  uint32_t base, p;  // first draw held, next draw to hand out
-  Lcg jump32;
-  __device__ void init(uint32_t s0, int lane) {
-    const Lcg j = lcg_pow((uint32_t)lane + 1u);
-    st = j.a * s0 + j.c;
-    u = pcg_out(st);
-    base = 0; p = 0;
-    jump32 = lcg_pow(32u);
-  }
-  __device__ double next() {
-    if (p - base == 32u) {
-      st = jump32.a * st + jump32.c;
-      u = pcg_out(st);
-      base += 32u;
-    }
-    const int l = (int)(p - base);
-    ++p;
-    return __shfl_sync(0xffffffffu, u, l);
-  }
+constexpr int kWalkThreads = 512;
+constexpr int kUpd = 8;
+
+// one draw of the stream as a lane holds it: the LCG state that produced it, the draw, the site it
+// selects when it is a site draw, that site's position and its head-list length
+struct Draw {
+  uint32_t st, site, cnt;
+  double u;
+  float x, y, z;
+};
+__device__ __forceinline__ void draw_from(Draw& d, uint32_t st, uint32_t H, uint32_t off,
+                                          const float4* __restrict__ hpos, const uint32_t* __restrict__ es_cnt) {
+  d.st = st;
+  d.u = pcg_out(st);
+  d.site = (uint32_t)fmin((double)(H - 1), floor(d.u * (double)H));
+  const float4 p = hpos[off + d.site];
+  d.x = p.x; d.y = p.y; d.z = p.z;
+  d.cnt = es_cnt[off + d.site];
+}
+__device__ __forceinline__ Draw shfl_draw(const Draw& d, int src) {
+  Draw o;
+  o.st = __shfl_sync(0xffffffffu, d.st, src);
+  o.site = __shfl_sync(0xffffffffu, d.site, src);
+  o.cnt = __shfl_sync(0xffffffffu, d.cnt, src);
+  o.u = __shfl_sync(0xffffffffu, d.u, src);
+  o.x = __shfl_sync(0xffffffffu, d.x, src);
+  o.y = __shfl_sync(0xffffffffu, d.y, src);
+  o.z = __shfl_sync(0xffffffffu, d.z, src);
+  return o;
+}
+
+// the flips one window accepted, for the cooperative update
+struct Flips {
+  uint32_t site[32];
+  uint32_t start[33];    // prefix of the flipped heads' list lengths
+  float qo[32], qn[32];
+  int sign[32];          // +1 deprotonated, -1 protonated, 0 the old charge was another value
+  uint32_t n, done;
+};
+// the sites and positions of a window's 32 draws, and the pair changes between them:
+// M[k][q] (k < q) = D of draw k's site on draw q's site (the exact value its D row holds), or
+// kSameSite when both draws select the same site
+struct Window {
+  uint32_t site[32];
+  float x[32], y[32], z[32];
+  long long M[32][32];
 };
 
-constexpr int kWalkThreads = 1024;
-
-// head positions for the flip updates: by head index (hpos) and in head-cell order with the head
-// index in w (spos), so a flip scans contiguous, L2-resident candidate ranges
-__global__ void k_gather_heads(const uint32_t* __restrict__ head_slot, uint32_t H, const float4* __restrict__ pos,
-                               const uint32_t* __restrict__ hsorted, float4* __restrict__ hpos,
-                               float4* __restrict__ spos) {
-  const uint32_t h = blockIdx.x * blockDim.x + threadIdx.x;
-  if (h >= H) return;
-  hpos[h] = pos[head_slot[h]];
-  const uint32_t g = hsorted[h];
-  const float4 p = pos[head_slot[g]];
-  spos[h] = make_float4(p.x, p.y, p.z, __uint_as_float(g));
+// one attempt's decision from its site energy: bit 1 accepted, bit 2 took an acceptance draw,
+// bit 4 its acceptance draw is the next window's first (lane 31; decided there)
+__device__ __forceinline__ int decide(long long e, uint32_t f, double u_acc, double kT, double inv_kT, int lane) {
+  const double Es = (double)e * kUnfix;
+  const double dG = f != 0 ? -Es : Es;
+  if (dG <= 0.0) return 1;
+  if (lane == 31) return 4;
+  return (metropolis(dG, kT, inv_kT, u_acc) ? 1 : 0) | 2;
 }
 
 template <bool SMEM>
@@ -167,20 +227,21 @@ __global__ void __launch_bounds__(kWalkThreads) k_sweep_walk(const SysParams* __
                                                              const uint32_t* __restrict__ head_slot,
                                                              const float4* __restrict__ hpos, float* __restrict__ charge,
                                                              const uint32_t* __restrict__ es_nl,
-                                                             const uint32_t* __restrict__ es_cnt, uint32_t cap,
-                                                             const uint32_t* __restrict__ hcell_of,
-                                                             const uint32_t* __restrict__ hstart,
-                                                             const float4* __restrict__ spos,
-                                                             double* __restrict__ Eg, uint8_t* __restrict__ flag_g,
+                                                             const uint32_t* __restrict__ es_cnt,
+                                                             const long long* __restrict__ D, uint32_t cap,
+                                                             long long* __restrict__ Eg, uint8_t* __restrict__ flag_g,
                                                              uint32_t* __restrict__ rng_io, double* __restrict__ out,
                                                              uint32_t only) {
   extern __shared__ __align__(16) unsigned char smem[];
+  __shared__ Flips F;
+  __shared__ Window W;
+  __shared__ uint32_t s_dep;
   const uint32_t r = (only == SOUP_NONE_U32) ? blockIdx.x : only;
   const SysParams& P = sp[r];
   const uint32_t H = P.nheads;
   if (H == 0 || !P.es_on) return;
   const uint32_t off = P.head_off;
-  double* E = SMEM ? reinterpret_cast<double*>(smem) : Eg + off;
+  long long* E = SMEM ? reinterpret_cast<long long*>(smem) : Eg + off;
   uint8_t* flag = SMEM ? smem + 8 * (size_t)H : flag_g + off;
   const float qd = (float)P.d_q;
   // flag: 0 neutral, 1 charged with the deprotonated charge, 2 charged with another value
@@ -189,89 +250,210 @@ __global__ void __launch_bounds__(kWalkThreads) k_sweep_walk(const SysParams* __
     const float q = charge[head_slot[off + h]];
     flag[h] = q == 0.f ? 0 : (q == qd ? 1 : 2);
   }
-  __syncthreads();
+  if (threadIdx.x == 0) { F.n = 0; F.done = 0; F.start[0] = 0; s_dep = 0; }
   const int lane = threadIdx.x & 31;
-  const double kT = P.d_kT;
+  const bool chain = threadIdx.x < 32;
+  const double kT = P.d_kT, inv_kT = 1.0 / P.d_kT;
   const double dGintr = kT * 2.302585092994046 * (P.d_pka - P.d_ph);
   const double cut2 = P.d_rc * P.d_rc, reach = P.d_rcattr + P.d_wc, reach2 = reach * reach;
+  // pairs beyond both cutoffs contribute exactly nothing; the FP32 screen keeps a wide margin
+  const float nr = (float)(fmax(P.d_rc, reach) * 1.001 + 1e-3);
+  const float near2 = nr * nr;
+  const float bx = (float)P.d_box[0], by = (float)P.d_box[1], bz = (float)P.d_box[2];
+  const float ibx = 1.f / bx, iby = 1.f / by, ibz = 1.f / bz;
   const uint32_t s0 = rng_io[r];
-  Stream rs;
-  rs.init(s0, lane);
-  uint32_t accepted = 0, dcount = 0;
+
+  // warp 0: lane l holds draw base+l (A) and base+32+l (B)
+  Draw A{}, B{};
+  uint32_t attempts = 0, consumed = 0, accepted = 0, dcount = 0;
   double dsum = 0.0;
-  for (uint32_t a = 0; a < H; ++a) {
-    const double u = rs.next();
-    const uint32_t s = (uint32_t)fmin((double)(H - 1), floor(u * (double)H));
-    const double Es = E[s];
-    const uint8_t f = flag[s];
-    const bool ch = f != 0;
-    const double dG = ch ? -Es : Es;
-    bool acc = dG <= 0.0;
-    if (!acc) acc = metropolis(dG, kT, rs.next());
-    if (!acc) continue;
-    const float q_old = f == 0 ? 0.f : (f == 1 ? qd : charge[head_slot[off + s]]);
-    const float q_new = ch ? 0.f : qd;
-    const float4 xi = hpos[off + s];
-    {
-      // candidates: the +-hwalk head cells around the site's cell at the last rebuild (complete for
-      // r < rc_es while every head has drifted less than skin/2), one row of cells per warp
-      const uint32_t c = hcell_of[off + s] - P.hcell_off;
-      const int nx = P.hdims[0], ny = P.hdims[1], nz = P.hdims[2], R = P.hwalk;
-      const int qx = (int)(c % (uint32_t)nx), qy = (int)((c / (uint32_t)nx) % (uint32_t)ny),
-                qz = (int)(c / ((uint32_t)nx * (uint32_t)ny));
-      const int span = 2 * R + 1;
-      const int nyv = span < ny ? span : ny, nzv = span < nz ? span : nz;
-      int xlo[2], xhi[2], nxr;
-      {
-        const int lo = qx - R, hi = qx + R;
-        if (hi - lo + 1 >= nx) { nxr = 1; xlo[0] = 0; xhi[0] = nx - 1; }
-        else if (lo < 0) { nxr = 2; xlo[0] = lo + nx; xhi[0] = nx - 1; xlo[1] = 0; xhi[1] = hi; }
-        else if (hi >= nx) { nxr = 2; xlo[0] = lo; xhi[0] = nx - 1; xlo[1] = 0; xhi[1] = hi - nx; }
-        else { nxr = 1; xlo[0] = lo; xhi[0] = hi; }
-      }
-      const int w = threadIdx.x >> 5;
-      for (int rowi = w; rowi < nyv * nzv; rowi += kWalkThreads / 32) {
-        const int y = (span < ny) ? ((qy - R + rowi % nyv) % ny + ny) % ny : rowi % nyv;
-        const int z = (span < nz) ? ((qz - R + rowi / nyv) % nz + nz) % nz : rowi / nyv;
-        const uint32_t rb = P.hcell_off + (uint32_t)(nx * (y + ny * z));
-        for (int xr = 0; xr < nxr; ++xr) {
-          const uint32_t a0 = hstart[rb + xlo[xr]], e0 = hstart[rb + xhi[xr] + 1];
-          for (uint32_t k = a0 + lane; k < e0; k += 32) {
-            const float4 pj = spos[k];
-            const uint32_t t = __float_as_uint(pj.w);
-            if (t == off + s) continue;
-            const double r2 = dist2(P, xi, pj);
-            if (r2 < cut2 || r2 < reach2)
-              E[t - off] += site_term(P, r2, q_new, cut2, reach2) - site_term(P, r2, q_old, cut2, reach2);
+  Lcg j32{1u, 0u};
+  if (chain) {
+    const Lcg j = lcg_pow((uint32_t)lane + 1u);
+    j32 = lcg_pow(32u);
+    const uint32_t sa = j.a * s0 + j.c;
+    draw_from(A, sa, H, off, hpos, es_cnt);
+    draw_from(B, j32.a * sa + j32.c, H, off, hpos, es_cnt);
+    W.site[lane] = A.site; W.x[lane] = A.x; W.y[lane] = A.y; W.z[lane] = A.z;
+  }
+  __syncthreads();
+  bool fill = true;      // the first pass only fills M
+
+  for (;;) {
+    if (!fill) {
+      // ---- add the last window's flips to the neighbours' energies ----
+      // (every load of a pass is issued before the first add; F.start is padded with ~0 above the
+      // last flip, so the flip of an item is a fixed five-step search)
+      const uint32_t total = F.start[F.n];
+      for (uint32_t base = 0; base < total; base += kWalkThreads * kUpd) {
+        uint32_t tv[kUpd], fv[kUpd];
+        long long dv[kUpd];
+#pragma unroll
+        for (int u = 0; u < kUpd; ++u) {
+          const uint32_t it = base + (uint32_t)u * kWalkThreads + threadIdx.x;
+          uint32_t lo = 0;
+#pragma unroll
+          for (uint32_t step = 16; step > 0; step >>= 1)
+            if (F.start[lo + step] <= it) lo += step;
+          const bool ok = it < total;
+          const size_t k = ok ? (size_t)(off + F.site[lo]) * cap + (it - F.start[lo]) : 0;
+          tv[u] = es_nl[k];
+          dv[u] = D[k];
+          fv[u] = ok ? lo : 32u;
+        }
+#pragma unroll
+        for (int u = 0; u < kUpd; ++u) {
+          if (fv[u] == 32u) continue;
+          const int sg = F.sign[fv[u]];
+          long long d = sg > 0 ? dv[u] : -dv[u];
+          if (sg == 0) {
+            const uint32_t h = off + F.site[fv[u]];
+            d = flip_delta(P, dist2(P, hpos[h], hpos[tv[u]]), F.qo[fv[u]], F.qn[fv[u]], cut2, reach2);
           }
+          atomicAdd(reinterpret_cast<unsigned long long*>(E + (tv[u] - off)), (unsigned long long)d);
         }
       }
     }
-    __syncthreads();   // every update of this flip is in E; every thread has read this attempt's state
-    flag[s] = ch ? 0 : 1;
-    if (threadIdx.x == 0) {
-      charge[head_slot[off + s]] = q_new;
-      ++accepted;
-      if (!ch) { dsum += (Es - dGintr) / kT; ++dcount; }
+    // ---- the pair changes of the coming window ----
+    for (uint32_t t = threadIdx.x; t < 1024; t += kWalkThreads) {
+      const int k = (int)(t >> 5), q = (int)(t & 31);
+      if (k >= q) continue;
+      long long m = kSameSite;
+      if (W.site[k] != W.site[q]) {
+        m = 0;
+        float dx = W.x[q] - W.x[k], dy = W.y[q] - W.y[k], dz = W.z[q] - W.z[k];
+        dx -= rintf(dx * ibx) * bx;
+        dy -= rintf(dy * iby) * by;
+        dz -= rintf(dz * ibz) * bz;
+        if (dx * dx + dy * dy + dz * dz < near2)
+          m = std_delta(P, dist2(P, make_float4(W.x[k], W.y[k], W.z[k], 0.f), make_float4(W.x[q], W.y[q], W.z[q], 0.f)),
+                        qd, cut2, reach2);
+      }
+      W.M[k][q] = m;
+    }
+    __syncthreads();
+    if (F.done) break;
+    fill = false;
+    if (chain) {
+      // ---- resolve the window: every lane's decision first, then the chain ----
+      long long e = E[A.site];
+      uint32_t f = flag[A.site];
+      const double u_acc = __shfl_down_sync(0xffffffffu, A.u, 1);   // lane l: draw base+l+1 (l < 31)
+      int res = decide(e, f, u_acc, kT, inv_kT, lane);
+      uint32_t dirty = 0;           // lanes whose energy or state changed since their decision
+      uint32_t p = 0, nf = 0;
+      bool done = false;
+      while (p < 32) {
+        if (attempts == H) { done = true; break; }
+        if ((dirty >> p) & 1u) {
+          if (lane == (int)p) res = decide(e, f, u_acc, kT, inv_kT, lane);
+        }
+        const long long mq = W.M[p][lane];        // used by the lanes after p when p flips
+        const int rp = __shfl_sync(0xffffffffu, res, (int)p);
+        if (rp & 4) break;
+        ++attempts;
+        if (rp & 1) {
+          const uint32_t fo = __shfl_sync(0xffffffffu, f, (int)p);
+          if (lane == (int)p) {
+            const double Es = (double)e * kUnfix;
+            F.site[nf] = A.site;
+            F.qo[nf] = fo == 0 ? 0.f : (fo == 1 ? qd : charge[head_slot[off + A.site]]);
+            F.qn[nf] = fo != 0 ? 0.f : qd;
+            F.sign[nf] = fo == 0 ? 1 : (fo == 1 ? -1 : 0);
+            F.start[nf + 1] = A.cnt;
+            flag[A.site] = fo != 0 ? 0 : 1;
+            ++accepted;
+            if (fo == 0) { dsum += Es - dGintr; ++dcount; }
+          }
+          // the flipped head's list and D rows go to L2 for the update that follows the window
+          {
+            const size_t row = (size_t)(off + __shfl_sync(0xffffffffu, A.site, (int)p)) * cap;
+            const uint32_t cnt = __shfl_sync(0xffffffffu, A.cnt, (int)p);
+            const char* dr = reinterpret_cast<const char*>(D + row);
+            const char* nr = reinterpret_cast<const char*>(es_nl + row);
+            for (uint32_t o = (uint32_t)lane * 128u; o < cnt * 8u; o += 32u * 128u)
+              asm volatile("prefetch.global.L2 [%0];" ::"l"(dr + o));
+            for (uint32_t o = (uint32_t)lane * 128u; o < cnt * 4u; o += 32u * 128u)
+              asm volatile("prefetch.global.L2 [%0];" ::"l"(nr + o));
+          }
+          // every later lane takes the flip into its own site energy (or charge state)
+          bool ch = false;
+          if (lane > (int)p) {
+            if (mq == kSameSite) {
+              f = fo != 0 ? 0 : 1;
+              ch = true;
+            } else if (fo != 2) {
+              if (mq != 0) { e += fo == 0 ? mq : -mq; ch = true; }
+            } else {
+              const float qo = charge[head_slot[off + W.site[p]]];
+              const long long m = flip_delta(P, dist2(P, make_float4(W.x[p], W.y[p], W.z[p], 0.f),
+                                                      make_float4(A.x, A.y, A.z, 0.f)), qo, 0.f, cut2, reach2);
+              if (m != 0) { e += m; ch = true; }
+            }
+          }
+          dirty |= __ballot_sync(0xffffffffu, ch);
+          ++nf;
+        }
+        p += (rp & 2) ? 2 : 1;
+      }
+      const uint32_t c = p;
+      consumed += c;
+      __syncwarp();
+      uint32_t v = lane < (int)nf ? F.start[lane + 1] : 0u;
+      for (int o = 1; o < 32; o <<= 1) {
+        const uint32_t y = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += y;
+      }
+      F.start[lane + 1] = lane < (int)nf ? v : 0xFFFFFFFFu;
+      if (lane == 0) { F.n = nf; F.done = done ? 1u : 0u; }
+      // ---- slide the draws by the c this window consumed; publish the next window's sites ----
+      const int src = lane + (int)c;
+      const Draw a1 = shfl_draw(A, src & 31);
+      const Draw b1 = shfl_draw(B, src & 31);
+      if (src < 32) {
+        A = a1;
+        B = b1;
+      } else {
+        A = b1;
+        draw_from(B, j32.a * b1.st + j32.c, H, off, hpos, es_cnt);
+      }
+      __syncwarp();
+      W.site[lane] = A.site; W.x[lane] = A.x; W.y[lane] = A.y; W.z[lane] = A.z;
+    }
+    __syncthreads();
+  }
+  // the charges from the final states (a head still in state 2 keeps its own value)
+  uint32_t dep = 0;
+  for (uint32_t h = threadIdx.x; h < H; h += kWalkThreads) {
+    const uint8_t f = flag[h];
+    if (f != 2) charge[head_slot[off + h]] = f == 0 ? 0.f : qd;
+    dep += f != 0;
+  }
+  for (int o = 16; o > 0; o >>= 1) dep += __shfl_xor_sync(0xffffffffu, dep, o);
+  if (lane == 0) atomicAdd(&s_dep, dep);
+  if (chain) {
+    for (int o = 16; o > 0; o >>= 1) {
+      accepted += __shfl_xor_sync(0xffffffffu, accepted, o);
+      dcount += __shfl_xor_sync(0xffffffffu, dcount, o);
+      dsum += __shfl_xor_sync(0xffffffffu, dsum, o);
     }
   }
   __syncthreads();
-  __shared__ uint32_t s_dep;
-  if (threadIdx.x == 0) s_dep = 0;
-  __syncthreads();
-  uint32_t dep = 0;
-  for (uint32_t h = threadIdx.x; h < H; h += kWalkThreads) dep += flag[h] != 0;
-  for (int o = 16; o > 0; o >>= 1) dep += __shfl_xor_sync(0xffffffffu, dep, o);
-  if (lane == 0) atomicAdd(&s_dep, dep);
-  __syncthreads();
   if (threadIdx.x == 0) {
-    const Lcg j = lcg_pow(rs.p);
+    const Lcg j = lcg_pow(consumed);
     rng_io[r] = j.a * s0 + j.c;
     out[4 * r + 0] = (double)H;
     out[4 * r + 1] = (double)accepted;
-    out[4 * r + 2] = dcount > 0 ? dsum / dcount : 0.0;
+    out[4 * r + 2] = dcount > 0 ? dsum / kT / dcount : 0.0;
     out[4 * r + 3] = (double)s_dep;
   }
+}
+
+// head positions by head index for the sweep
+__global__ void k_gather_heads(const uint32_t* __restrict__ head_slot, uint32_t H, const float4* __restrict__ pos,
+                               float4* __restrict__ hpos) {
+  const uint32_t h = blockIdx.x * blockDim.x + threadIdx.x;
+  if (h < H) hpos[h] = pos[head_slot[h]];
 }
 
 }  // namespace
@@ -284,21 +466,18 @@ void launch_sweep(Batch& b, uint32_t replica) {
     if (replica == SOUP_NONE_U32 || r == replica) hmax = std::max(hmax, b.hsp[r].nheads);
   b.launches += 3;
   prof_begin(b, SOUP_K_SWEEP);
-  k_gather_heads<<<(b.H + 255) / 256, 256, 0, b.stream>>>(b.head_slot, b.H, b.pos, b.hsorted, b.head_pos,
-                                                           b.head_spos);
+  k_gather_heads<<<(b.H + 255) / 256, 256, 0, b.stream>>>(b.head_slot, b.H, b.pos, b.head_pos);
   k_sweep_init<<<(unsigned)(((uint64_t)b.H * 32 + 255) / 256), 256, 0, b.stream>>>(
-      b.sp, b.head_sys, b.head_slot, b.H, b.pos, b.charge, b.es_nl, b.es_cnt, b.es_cap, b.head_e, replica);
+      b.sp, b.head_sys, b.head_slot, b.H, b.pos, b.charge, b.es_nl, b.es_cnt, b.es_cap, b.head_e, b.head_d, replica);
   const unsigned grid = replica == SOUP_NONE_U32 ? b.R : 1;
   const size_t smem = 9 * (size_t)hmax;
   if (smem <= 200 * 1024) {
     k_sweep_walk<true><<<grid, kWalkThreads, smem, b.stream>>>(b.sp, b.head_slot, b.head_pos, b.charge, b.es_nl,
-                                                               b.es_cnt, b.es_cap, b.hcell_of, b.hcell_start,
-                                                               b.head_spos, b.head_e, b.head_flag,
+                                                               b.es_cnt, b.head_d, b.es_cap, b.head_e, b.head_flag,
                                                                b.prot_rng_dev, b.sweep_out, replica);
   } else {
     k_sweep_walk<false><<<grid, kWalkThreads, 0, b.stream>>>(b.sp, b.head_slot, b.head_pos, b.charge, b.es_nl,
-                                                             b.es_cnt, b.es_cap, b.hcell_of, b.hcell_start,
-                                                             b.head_spos, b.head_e, b.head_flag,
+                                                             b.es_cnt, b.head_d, b.es_cap, b.head_e, b.head_flag,
                                                              b.prot_rng_dev, b.sweep_out, replica);
   }
   prof_end(b);

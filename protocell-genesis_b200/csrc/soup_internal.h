@@ -73,9 +73,10 @@ struct Batch {
   uint32_t* heads = nullptr;         // global original ids, per replica ascending
   uint32_t* head_sys = nullptr;      // replica of each head
   uint32_t* head_slot = nullptr;     // current slot of each head (refreshed at every rebuild)
-  double* head_e = nullptr;          // constant-pH flip energy per head (scratch of the sweep)
+  long long* head_e = nullptr;       // constant-pH site energy per head, fixed point 2^-40 (sweep scratch)
   float4* head_pos = nullptr;        // head positions gathered for the sweep
-  float4* head_spos = nullptr;       // head positions in head-cell order (w = head index)
+  long long* head_d = nullptr;       // [head][es_cap] change of a list neighbour's energy when the head
+                                     // deprotonates, fixed point 2^-40 (sweep scratch)
   uint8_t* head_flag = nullptr;      // charge state per head when the sweep cannot keep it in shared memory
   uint32_t es_cap = 0;
   uint32_t* es_nl = nullptr;

@@ -115,6 +115,25 @@ def test_protonation_sweep_decisions_match():
     assert rel_rms(g.forces_no_rebuild(), o.forces64()) < FORCE_TOL
 
 
+@pytest.mark.parametrize("ph,ionic", [(7.0, 0.01), (4.6, 0.1)])
+def test_consecutive_sweeps_on_many_heads(ph, ionic):
+    """Thousands of heads with many accepted flips per sweep, three sweeps in a row."""
+    def tw(c):
+        c.protonation_rng = 987654321
+    opts = water_opts(n_water=6000, box=24.0, start={"C": 1500, "O": 2500, "H": 0, "M": 60, "W": 6000},
+                      electrostatics={"enabled": True, "pH": ph, "ionicStrengthMolar": ionic})
+    cfg, o, g = make_pair(opts, relax=30, steps=10, tweak=tw)
+    g.write_state(oracle_state(o))
+    for k in range(3):
+        rg = g.protonation_sweep()
+        ro = o.sweep()
+        assert np.array_equal(g.charges(), o.read(ob.F_CHARGES)), k
+        assert g.protonation_rng_state() == int(o.read(ob.F_PROT_RNG)[0]), k
+        assert rg["accepted"] == ro.accepted and rg["deprotonated"] == ro.deprotonated, k
+        assert rg["dEsMeanKT"] == pytest.approx(ro.d_es_mean_kt, rel=1e-9, abs=1e-12), k
+        assert ro.accepted > 300, k
+
+
 def test_short_trajectory_tracks_the_oracle():
     cfg, o, g = make_pair(charged_opts(), relax=30)
     g.step(40)
