@@ -255,6 +255,25 @@ int soup_amphiphile_labels(SoupHandle* h, uint32_t* head_of, uint32_t* n_out);
 int soup_aggregate_labels(SoupHandle* h, const uint32_t* member_idx, uint32_t n_members,
                           double cutoff, uint32_t* labels, uint32_t* n_components);
 
+/* The same labels as soup_aggregate_labels, computed without allocating device memory.  It has no
+ * counterpart in the reference.  soup_aggregate_labels allocates its scratch with cudaMalloc and
+ * frees it with cudaFree on every call; a caller whose device memory is held by another allocator
+ * (a framework's caching allocator that reserved the GPU) may see that cudaMalloc fail, and the
+ * cudaFree stalls every stream on the device.  This entry point keeps its scratch in one fixed
+ * array that the library holds on each GPU it runs on (about 9.4 MB, for as long as the process
+ * lives), so it needs no allocation and no free.
+ *   Limits: n_members <= SOUP_NOALLOC_MAX_MEMBERS and floor(box_x/cutoff) * floor(box_y/cutoff)
+ *   * floor(box_z/cutoff) <= SOUP_NOALLOC_MAX_CELLS; larger requests return SOUP_E_ARG with the
+ *   limit in soup_last_error and compute nothing.
+ *   The first call on each device looks up the array's device address (with lazy module loading
+ *   this also loads the library's device code); make that first call before capturing any stream.
+ *   All handles on one device share the array: calls that can overlap (from several host threads)
+ *   must be serialised by the caller.  The call returns after its results are on the host. */
+#define SOUP_NOALLOC_MAX_MEMBERS (1u << 18)
+#define SOUP_NOALLOC_MAX_CELLS (1u << 18)
+int soup_aggregate_labels_noalloc(SoupHandle* h, const uint32_t* member_idx, uint32_t n_members,
+                                  double cutoff, uint32_t* labels, uint32_t* n_components);
+
 /* ---- single phases ------------------------------------------------------------------------- */
 /* One phase of the step on the current device state, so each kernel can be checked in isolation
  * (the reference times phases the same way: stepPhasesDEBUG, soup/src/soup-readback.ts:191-245).

@@ -151,6 +151,7 @@ SIGNATURES = {
                                C.c_double, C.c_double, C.c_double, C.POINTER(SoupClosureResult)]),
     "soup_amphiphile_labels": (C.c_int, [_P, _U32P, _U32P]),
     "soup_aggregate_labels": (C.c_int, [_P, _U32P, C.c_uint32, C.c_double, _U32P, _U32P]),
+    "soup_aggregate_labels_noalloc": (C.c_int, [_P, _U32P, C.c_uint32, C.c_double, _U32P, _U32P]),
     "soup_batch_create": (C.c_int, [C.POINTER(SoupConfig), C.POINTER(SoupInitState), C.c_uint32,
                                     C.POINTER(_P)]),
     "soup_batch_step": (C.c_int, [_P, C.c_uint64]),

@@ -256,6 +256,17 @@ class SoupSystem:
             C.byref(nc)))
         return int(nc.value), labels
 
+    def aggregate_labels_noalloc(self, members, cutoff):
+        """aggregate_labels without device allocation (scratch in a fixed per-device array of the
+        library; at most SOUP_NOALLOC_MAX_MEMBERS members and cells; overlapping calls race)."""
+        m = np.ascontiguousarray(members, np.uint32)
+        labels = np.empty(m.size, np.uint32)
+        nc = C.c_uint32()
+        _check(self._lib, self._h, self._lib.soup_aggregate_labels_noalloc(
+            self._h, m.ctypes.data_as(_abi._U32P), m.size, float(cutoff), labels.ctypes.data_as(_abi._U32P),
+            C.byref(nc)))
+        return int(nc.value), labels
+
     # reference-style aliases
     forcesBruteForce = forces_brute_force
     forcesNoRebuildDEBUG = forces_no_rebuild
