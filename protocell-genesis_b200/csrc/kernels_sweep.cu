@@ -195,21 +195,25 @@ __device__ __forceinline__ Draw shfl_draw(const Draw& d, int src) {
   return o;
 }
 
-// the flips one window accepted, for the cooperative update
+// the flips one window accepted: the scatter into E that runs during the next window, and the
+// corrections the next window's lanes take before E has them
 struct Flips {
   uint32_t site[32];
-  uint32_t start[33];    // prefix of the flipped heads' list lengths
+  uint32_t start[33];    // prefix of the flipped heads' list lengths; ~0 above the last flip
   float qo[32], qn[32];
+  float x[32], y[32], z[32];
   int sign[32];          // +1 deprotonated, -1 protonated, 0 the old charge was another value
-  uint32_t n, done;
+  uint32_t n;
 };
-// the sites and positions of a window's 32 draws, and the pair changes between them:
-// M[k][q] (k < q) = D of draw k's site on draw q's site (the exact value its D row holds), or
-// kSameSite when both draws select the same site
+// the sites and positions of a window's 32 draws, the pair changes between them
+// (M[k][q], k < q: D of draw k's site on draw q's site, the exact value its D row holds, or
+// kSameSite when both draws select one site) and the previous window's flips summed per draw
 struct Window {
   uint32_t site[32];
   float x[32], y[32], z[32];
   long long M[32][32];
+  long long corr[32];
+  uint32_t done;
 };
 
 // one attempt's decision from its site energy: bit 1 accepted, bit 2 took an acceptance draw,
@@ -222,6 +226,47 @@ __device__ __forceinline__ int decide(long long e, uint32_t f, double u_acc, dou
   return (metropolis(dG, kT, inv_kT, u_acc) ? 1 : 0) | 2;
 }
 
+// add the flips of G to the energies of their neighbours: `t` of `nt` threads, kUpd items per
+// thread per pass, every load of a pass in flight before the first add
+__device__ __forceinline__ void scatter_flips(const Flips& G, const SysParams& P, uint32_t off, uint32_t cap,
+                                              const uint32_t* __restrict__ es_nl, const long long* __restrict__ D,
+                                              const float4* __restrict__ hpos, long long* E, double cut2,
+                                              double reach2, uint32_t t, uint32_t nt) {
+  const uint32_t total = G.start[G.n];
+  for (uint32_t base = 0; base < total; base += nt * kUpd) {
+    uint32_t tv[kUpd], fv[kUpd];
+    long long dv[kUpd];
+#pragma unroll
+    for (int u = 0; u < kUpd; ++u) {
+      const uint32_t it = base + (uint32_t)u * nt + t;
+      uint32_t lo = 0;
+#pragma unroll
+      for (uint32_t step = 16; step > 0; step >>= 1)
+        if (G.start[lo + step] <= it) lo += step;
+      const bool ok = it < total;
+      const size_t k = ok ? (size_t)(off + G.site[lo]) * cap + (it - G.start[lo]) : 0;
+      tv[u] = es_nl[k];
+      dv[u] = D[k];
+      fv[u] = ok ? lo : 32u;
+    }
+#pragma unroll
+    for (int u = 0; u < kUpd; ++u) {
+      if (fv[u] == 32u) continue;
+      const int sg = G.sign[fv[u]];
+      long long d = sg > 0 ? dv[u] : -dv[u];
+      if (sg == 0) {
+        const uint32_t h = off + G.site[fv[u]];
+        d = flip_delta(P, dist2(P, hpos[h], hpos[tv[u]]), G.qo[fv[u]], G.qn[fv[u]], cut2, reach2);
+      }
+      atomicAdd(reinterpret_cast<unsigned long long*>(E + (tv[u] - off)), (unsigned long long)d);
+    }
+  }
+}
+
+// Per window w (two barriers):
+//   X  all warps: M of window w and corr of window w from the flips of window w-1 (not yet in E);
+//      warp 0 reads E and the charge states of its sites (E holds every flip before window w-1)
+//   R  warp 0 resolves window w; warps 1.. scatter window w-1's flips into E meanwhile
 template <bool SMEM>
 __global__ void __launch_bounds__(kWalkThreads) k_sweep_walk(const SysParams* __restrict__ sp,
                                                              const uint32_t* __restrict__ head_slot,
@@ -233,7 +278,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_sweep_walk(const SysParams* __
                                                              uint32_t* __restrict__ rng_io, double* __restrict__ out,
                                                              uint32_t only) {
   extern __shared__ __align__(16) unsigned char smem[];
-  __shared__ Flips F;
+  __shared__ Flips F[2];
   __shared__ Window W;
   __shared__ uint32_t s_dep;
   const uint32_t r = (only == SOUP_NONE_U32) ? blockIdx.x : only;
@@ -250,9 +295,14 @@ __global__ void __launch_bounds__(kWalkThreads) k_sweep_walk(const SysParams* __
     const float q = charge[head_slot[off + h]];
     flag[h] = q == 0.f ? 0 : (q == qd ? 1 : 2);
   }
-  if (threadIdx.x == 0) { F.n = 0; F.done = 0; F.start[0] = 0; s_dep = 0; }
   const int lane = threadIdx.x & 31;
   const bool chain = threadIdx.x < 32;
+  if (chain) {
+    F[0].start[lane + 1] = 0xFFFFFFFFu;
+    F[1].start[lane + 1] = 0xFFFFFFFFu;
+    W.corr[lane] = 0;
+    if (lane == 0) { F[0].n = F[1].n = 0; F[0].start[0] = F[1].start[0] = 0; W.done = 0; s_dep = 0; }
+  }
   const double kT = P.d_kT, inv_kT = 1.0 / P.d_kT;
   const double dGintr = kT * 2.302585092994046 * (P.d_pka - P.d_ph);
   const double cut2 = P.d_rc * P.d_rc, reach = P.d_rcattr + P.d_wc, reach2 = reach * reach;
@@ -268,6 +318,8 @@ __global__ void __launch_bounds__(kWalkThreads) k_sweep_walk(const SysParams* __
   uint32_t attempts = 0, consumed = 0, accepted = 0, dcount = 0;
   double dsum = 0.0;
   Lcg j32{1u, 0u};
+  long long e = 0;
+  uint32_t f = 0;
   if (chain) {
     const Lcg j = lcg_pow((uint32_t)lane + 1u);
     j32 = lcg_pow(32u);
@@ -277,111 +329,91 @@ __global__ void __launch_bounds__(kWalkThreads) k_sweep_walk(const SysParams* __
     W.site[lane] = A.site; W.x[lane] = A.x; W.y[lane] = A.y; W.z[lane] = A.z;
   }
   __syncthreads();
-  bool fill = true;      // the first pass only fills M
 
-  for (;;) {
-    if (!fill) {
-      // ---- add the last window's flips to the neighbours' energies ----
-      // (every load of a pass is issued before the first add; F.start is padded with ~0 above the
-      // last flip, so the flip of an item is a fixed five-step search)
-      const uint32_t total = F.start[F.n];
-      for (uint32_t base = 0; base < total; base += kWalkThreads * kUpd) {
-        uint32_t tv[kUpd], fv[kUpd];
-        long long dv[kUpd];
-#pragma unroll
-        for (int u = 0; u < kUpd; ++u) {
-          const uint32_t it = base + (uint32_t)u * kWalkThreads + threadIdx.x;
-          uint32_t lo = 0;
-#pragma unroll
-          for (uint32_t step = 16; step > 0; step >>= 1)
-            if (F.start[lo + step] <= it) lo += step;
-          const bool ok = it < total;
-          const size_t k = ok ? (size_t)(off + F.site[lo]) * cap + (it - F.start[lo]) : 0;
-          tv[u] = es_nl[k];
-          dv[u] = D[k];
-          fv[u] = ok ? lo : 32u;
-        }
-#pragma unroll
-        for (int u = 0; u < kUpd; ++u) {
-          if (fv[u] == 32u) continue;
-          const int sg = F.sign[fv[u]];
-          long long d = sg > 0 ? dv[u] : -dv[u];
-          if (sg == 0) {
-            const uint32_t h = off + F.site[fv[u]];
-            d = flip_delta(P, dist2(P, hpos[h], hpos[tv[u]]), F.qo[fv[u]], F.qn[fv[u]], cut2, reach2);
-          }
-          atomicAdd(reinterpret_cast<unsigned long long*>(E + (tv[u] - off)), (unsigned long long)d);
-        }
-      }
+  for (uint32_t wnd = 0;; ++wnd) {
+    Flips& Fc = F[wnd & 1];          // this window's flips
+    const Flips& Fp = F[(wnd + 1) & 1];   // the previous window's
+    // ---- X ----
+    if (chain) {
+      e = E[A.site];
+      f = flag[A.site];
     }
-    // ---- the pair changes of the coming window ----
-    for (uint32_t t = threadIdx.x; t < 1024; t += kWalkThreads) {
-      const int k = (int)(t >> 5), q = (int)(t & 31);
-      if (k >= q) continue;
-      long long m = kSameSite;
-      if (W.site[k] != W.site[q]) {
-        m = 0;
-        float dx = W.x[q] - W.x[k], dy = W.y[q] - W.y[k], dz = W.z[q] - W.z[k];
+    for (uint32_t t = threadIdx.x; t < 1024u + 32u * Fp.n; t += kWalkThreads) {
+      if (t < 1024u) {
+        const int k = (int)(t >> 5), q = (int)(t & 31);
+        if (k >= q) continue;
+        long long m = kSameSite;
+        if (W.site[k] != W.site[q]) {
+          m = 0;
+          float dx = W.x[q] - W.x[k], dy = W.y[q] - W.y[k], dz = W.z[q] - W.z[k];
+          dx -= rintf(dx * ibx) * bx;
+          dy -= rintf(dy * iby) * by;
+          dz -= rintf(dz * ibz) * bz;
+          if (dx * dx + dy * dy + dz * dz < near2)
+            m = std_delta(P, dist2(P, make_float4(W.x[k], W.y[k], W.z[k], 0.f),
+                                   make_float4(W.x[q], W.y[q], W.z[q], 0.f)), qd, cut2, reach2);
+        }
+        W.M[k][q] = m;
+      } else {
+        const uint32_t g = (t - 1024u) >> 5, q = (t - 1024u) & 31u;
+        if (Fp.site[g] == W.site[q]) continue;        // a site's own flip leaves its E alone
+        float dx = W.x[q] - Fp.x[g], dy = W.y[q] - Fp.y[g], dz = W.z[q] - Fp.z[g];
         dx -= rintf(dx * ibx) * bx;
         dy -= rintf(dy * iby) * by;
         dz -= rintf(dz * ibz) * bz;
-        if (dx * dx + dy * dy + dz * dz < near2)
-          m = std_delta(P, dist2(P, make_float4(W.x[k], W.y[k], W.z[k], 0.f), make_float4(W.x[q], W.y[q], W.z[q], 0.f)),
-                        qd, cut2, reach2);
+        if (dx * dx + dy * dy + dz * dz < near2) {
+          const double r2 = dist2(P, make_float4(Fp.x[g], Fp.y[g], Fp.z[g], 0.f), make_float4(W.x[q], W.y[q], W.z[q], 0.f));
+          const int sg = Fp.sign[g];
+          long long d;
+          if (sg != 0) {
+            d = std_delta(P, r2, qd, cut2, reach2);
+            if (sg < 0) d = -d;
+          } else {
+            d = flip_delta(P, r2, Fp.qo[g], Fp.qn[g], cut2, reach2);
+          }
+          if (d != 0) atomicAdd(reinterpret_cast<unsigned long long*>(&W.corr[q]), (unsigned long long)d);
+        }
       }
-      W.M[k][q] = m;
     }
     __syncthreads();
-    if (F.done) break;
-    fill = false;
+    if (W.done) break;
+    // ---- R ----
     if (chain) {
-      // ---- resolve the window: every lane's decision first, then the chain ----
-      long long e = E[A.site];
-      uint32_t f = flag[A.site];
+      e += W.corr[lane];
       const double u_acc = __shfl_down_sync(0xffffffffu, A.u, 1);   // lane l: draw base+l+1 (l < 31)
       int res = decide(e, f, u_acc, kT, inv_kT, lane);
-      uint32_t dirty = 0;           // lanes whose energy or state changed since their decision
-      uint32_t p = 0, nf = 0;
+      uint32_t acc_m = __ballot_sync(0xffffffffu, res & 1), need_m = __ballot_sync(0xffffffffu, res & 2);
+      uint32_t nxt_m = __ballot_sync(0xffffffffu, res & 4);
+      uint32_t chg_m = __ballot_sync(0xffffffffu, f != 0), f2_m = __ballot_sync(0xffffffffu, f == 2);
+      uint32_t dirty = 0, flipped = 0;
+      uint32_t p = 0, nf = 0, my_nf = 0, my_fo = 0;
+      long long my_e = 0;
       bool done = false;
       while (p < 32) {
         if (attempts == H) { done = true; break; }
-        if ((dirty >> p) & 1u) {
+        const uint32_t bit = 1u << p;
+        const long long mq = W.M[p][lane];            // used by the lanes after p when p flips
+        if (dirty & bit) {
           if (lane == (int)p) res = decide(e, f, u_acc, kT, inv_kT, lane);
+          acc_m = __ballot_sync(0xffffffffu, res & 1);
+          need_m = __ballot_sync(0xffffffffu, res & 2);
+          nxt_m = __ballot_sync(0xffffffffu, res & 4);
         }
-        const long long mq = W.M[p][lane];        // used by the lanes after p when p flips
-        const int rp = __shfl_sync(0xffffffffu, res, (int)p);
-        if (rp & 4) break;
+        if (nxt_m & bit) break;
         ++attempts;
-        if (rp & 1) {
-          const uint32_t fo = __shfl_sync(0xffffffffu, f, (int)p);
+        if (acc_m & bit) {
+          const uint32_t fo = (chg_m & bit) ? ((f2_m & bit) ? 2u : 1u) : 0u;
           if (lane == (int)p) {
-            const double Es = (double)e * kUnfix;
-            F.site[nf] = A.site;
-            F.qo[nf] = fo == 0 ? 0.f : (fo == 1 ? qd : charge[head_slot[off + A.site]]);
-            F.qn[nf] = fo != 0 ? 0.f : qd;
-            F.sign[nf] = fo == 0 ? 1 : (fo == 1 ? -1 : 0);
-            F.start[nf + 1] = A.cnt;
             flag[A.site] = fo != 0 ? 0 : 1;
-            ++accepted;
-            if (fo == 0) { dsum += Es - dGintr; ++dcount; }
+            my_nf = nf; my_fo = fo; my_e = e;
           }
-          // the flipped head's list and D rows go to L2 for the update that follows the window
-          {
-            const size_t row = (size_t)(off + __shfl_sync(0xffffffffu, A.site, (int)p)) * cap;
-            const uint32_t cnt = __shfl_sync(0xffffffffu, A.cnt, (int)p);
-            const char* dr = reinterpret_cast<const char*>(D + row);
-            const char* nr = reinterpret_cast<const char*>(es_nl + row);
-            for (uint32_t o = (uint32_t)lane * 128u; o < cnt * 8u; o += 32u * 128u)
-              asm volatile("prefetch.global.L2 [%0];" ::"l"(dr + o));
-            for (uint32_t o = (uint32_t)lane * 128u; o < cnt * 4u; o += 32u * 128u)
-              asm volatile("prefetch.global.L2 [%0];" ::"l"(nr + o));
-          }
+          flipped |= bit;
           // every later lane takes the flip into its own site energy (or charge state)
-          bool ch = false;
+          bool ch = false, dup = false;
           if (lane > (int)p) {
             if (mq == kSameSite) {
               f = fo != 0 ? 0 : 1;
-              ch = true;
+              ch = dup = true;
             } else if (fo != 2) {
               if (mq != 0) { e += fo == 0 ? mq : -mq; ch = true; }
             } else {
@@ -392,20 +424,35 @@ __global__ void __launch_bounds__(kWalkThreads) k_sweep_walk(const SysParams* __
             }
           }
           dirty |= __ballot_sync(0xffffffffu, ch);
+          if (__ballot_sync(0xffffffffu, dup)) {
+            chg_m = __ballot_sync(0xffffffffu, f != 0);
+            f2_m = __ballot_sync(0xffffffffu, f == 2);
+          }
           ++nf;
         }
-        p += (rp & 2) ? 2 : 1;
+        p += (need_m & bit) ? 2 : 1;
       }
       const uint32_t c = p;
       consumed += c;
-      __syncwarp();
-      uint32_t v = lane < (int)nf ? F.start[lane + 1] : 0u;
+      // ---- this window's flip records, in lane (= attempt) order ----
+      const bool mine = (flipped >> lane) & 1u;
+      if (mine) {
+        Fc.site[my_nf] = A.site;
+        Fc.qo[my_nf] = my_fo == 0 ? 0.f : (my_fo == 1 ? qd : charge[head_slot[off + A.site]]);
+        Fc.qn[my_nf] = my_fo != 0 ? 0.f : qd;
+        Fc.sign[my_nf] = my_fo == 0 ? 1 : (my_fo == 1 ? -1 : 0);
+        Fc.x[my_nf] = A.x; Fc.y[my_nf] = A.y; Fc.z[my_nf] = A.z;
+        ++accepted;
+        if (my_fo == 0) { dsum += (double)my_e * kUnfix - dGintr; ++dcount; }
+      }
+      uint32_t v = mine ? A.cnt : 0u;
       for (int o = 1; o < 32; o <<= 1) {
         const uint32_t y = __shfl_up_sync(0xffffffffu, v, o);
         if (lane >= o) v += y;
       }
-      F.start[lane + 1] = lane < (int)nf ? v : 0xFFFFFFFFu;
-      if (lane == 0) { F.n = nf; F.done = done ? 1u : 0u; }
+      if (mine) Fc.start[my_nf + 1] = v;
+      if (lane >= (int)nf) Fc.start[lane + 1] = 0xFFFFFFFFu;
+      if (lane == 0) { Fc.n = nf; W.done = done ? 1u : 0u; }
       // ---- slide the draws by the c this window consumed; publish the next window's sites ----
       const int src = lane + (int)c;
       const Draw a1 = shfl_draw(A, src & 31);
@@ -419,15 +466,18 @@ __global__ void __launch_bounds__(kWalkThreads) k_sweep_walk(const SysParams* __
       }
       __syncwarp();
       W.site[lane] = A.site; W.x[lane] = A.x; W.y[lane] = A.y; W.z[lane] = A.z;
+      W.corr[lane] = 0;
+    } else {
+      scatter_flips(Fp, P, off, cap, es_nl, D, hpos, E, cut2, reach2, threadIdx.x - 32u, kWalkThreads - 32u);
     }
     __syncthreads();
   }
   // the charges from the final states (a head still in state 2 keeps its own value)
   uint32_t dep = 0;
   for (uint32_t h = threadIdx.x; h < H; h += kWalkThreads) {
-    const uint8_t f = flag[h];
-    if (f != 2) charge[head_slot[off + h]] = f == 0 ? 0.f : qd;
-    dep += f != 0;
+    const uint8_t fl = flag[h];
+    if (fl != 2) charge[head_slot[off + h]] = fl == 0 ? 0.f : qd;
+    dep += fl != 0;
   }
   for (int o = 16; o > 0; o >>= 1) dep += __shfl_xor_sync(0xffffffffu, dep, o);
   if (lane == 0) atomicAdd(&s_dep, dep);
