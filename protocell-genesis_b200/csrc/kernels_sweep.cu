@@ -136,13 +136,16 @@ __global__ void __launch_bounds__(256) k_sweep_init(const SysParams* __restrict_
 
 // u < exp(-dG/kT) for dG > 0.  For -dG/kT > -20 an FP32 estimate decides when u is more than 1e-5
 // (relative) away from it: __expf's error there is below 2 + 1.16*20 ulp and the FP32 rounding of
-// the exponent adds 1e-6, together under 5e-6.  Otherwise, and near the threshold, FP64 decides.
+// the exponent adds 1e-6, together under 5e-6.  Below -20 only u < 1e-8 can pass.  Otherwise, and
+// near the threshold, FP64 decides.
 __device__ __forceinline__ bool metropolis(double dG, double kT, double inv_kT, double u) {
   const double xd = -dG * inv_kT;
   if (xd > -20.0) {
     const double est = (double)__expf((float)xd);
     if (u < est * (1.0 - 1e-5)) return true;
     if (u > est * (1.0 + 1e-5)) return false;
+  } else if (u >= 1e-8) {
+    return false;                 // exp(-dG/kT) <= e^-20 (1 + 1e-15) < 2.1e-9
   }
   return u < exp(-dG / kT);
 }
@@ -166,6 +169,7 @@ __device__ __forceinline__ double pcg_out(uint32_t v) {
 
 constexpr int kWalkThreads = 512;
 constexpr int kUpd = 8;
+constexpr uint32_t kQueue = 512;
 
 // one draw of the stream as a lane holds it: the LCG state that produced it, the draw, the site it
 // selects when it is a site draw, that site's position and its head-list length
@@ -213,7 +217,53 @@ struct Window {
   float x[32], y[32], z[32];
   long long M[32][32];
   long long corr[32];
-  uint32_t done;
+  uint16_t queue[kQueue];   // pairs within reach awaiting FP64: k*32+q (M), or 1024 + g*32+q (corr)
+  uint32_t nq, done;
+};
+
+// window lane q's share of the previous window's flip g (the exact value g's D row holds for q)
+__device__ __forceinline__ void corr_term(const SysParams& P, const Flips& Fp, Window& W, uint32_t g, uint32_t q,
+                                          float qd, double cut2, double reach2) {
+  const double r2 = dist2(P, make_float4(Fp.x[g], Fp.y[g], Fp.z[g], 0.f), make_float4(W.x[q], W.y[q], W.z[q], 0.f));
+  const int sg = Fp.sign[g];
+  long long d;
+  if (sg != 0) {
+    d = std_delta(P, r2, qd, cut2, reach2);
+    if (sg < 0) d = -d;
+  } else {
+    d = flip_delta(P, r2, Fp.qo[g], Fp.qn[g], cut2, reach2);
+  }
+  if (d != 0) atomicAdd(reinterpret_cast<unsigned long long*>(&W.corr[q]), (unsigned long long)d);
+}
+
+// The site energies of one replica: in shared memory as two 32-bit halves (32-bit shared atomics are
+// native, 64-bit ones are not; an add carries from the low half into the high half exactly, so the
+// sum does not depend on the order of the adds), or in global memory as int64.
+template <bool SMEM>
+struct Energies {
+  uint32_t* lo;
+  int32_t* hi;
+  long long* g;
+  __device__ __forceinline__ long long get(uint32_t i) const {
+    if (SMEM) return (long long)(((unsigned long long)(uint32_t)hi[i] << 32) | lo[i]);
+    return g[i];
+  }
+  __device__ __forceinline__ void set(uint32_t i, long long v) const {
+    if (SMEM) { lo[i] = (uint32_t)(unsigned long long)v; hi[i] = (int32_t)((unsigned long long)v >> 32); }
+    else g[i] = v;
+  }
+  __device__ __forceinline__ void add(uint32_t i, long long d) const {
+    if (SMEM) {
+      const unsigned long long ud = (unsigned long long)d;
+      const uint32_t dl = (uint32_t)ud;
+      const int32_t dh = (int32_t)(ud >> 32);
+      const uint32_t old = atomicAdd(lo + i, dl);
+      const int32_t up = dh + ((uint32_t)(old + dl) < old ? 1 : 0);
+      if (up != 0) atomicAdd(hi + i, up);
+    } else {
+      atomicAdd(reinterpret_cast<unsigned long long*>(g + i), (unsigned long long)d);
+    }
+  }
 };
 
 // one attempt's decision from its site energy: bit 1 accepted, bit 2 took an acceptance draw,
@@ -228,9 +278,10 @@ __device__ __forceinline__ int decide(long long e, uint32_t f, double u_acc, dou
 
 // add the flips of G to the energies of their neighbours: `t` of `nt` threads, kUpd items per
 // thread per pass, every load of a pass in flight before the first add
+template <bool SMEM>
 __device__ __forceinline__ void scatter_flips(const Flips& G, const SysParams& P, uint32_t off, uint32_t cap,
                                               const uint32_t* __restrict__ es_nl, const long long* __restrict__ D,
-                                              const float4* __restrict__ hpos, long long* E, double cut2,
+                                              const float4* __restrict__ hpos, const Energies<SMEM>& E, double cut2,
                                               double reach2, uint32_t t, uint32_t nt) {
   const uint32_t total = G.start[G.n];
   for (uint32_t base = 0; base < total; base += nt * kUpd) {
@@ -258,7 +309,7 @@ __device__ __forceinline__ void scatter_flips(const Flips& G, const SysParams& P
         const uint32_t h = off + G.site[fv[u]];
         d = flip_delta(P, dist2(P, hpos[h], hpos[tv[u]]), G.qo[fv[u]], G.qn[fv[u]], cut2, reach2);
       }
-      atomicAdd(reinterpret_cast<unsigned long long*>(E + (tv[u] - off)), (unsigned long long)d);
+      E.add(tv[u] - off, d);
     }
   }
 }
@@ -286,12 +337,12 @@ __global__ void __launch_bounds__(kWalkThreads) k_sweep_walk(const SysParams* __
   const uint32_t H = P.nheads;
   if (H == 0 || !P.es_on) return;
   const uint32_t off = P.head_off;
-  long long* E = SMEM ? reinterpret_cast<long long*>(smem) : Eg + off;
+  const Energies<SMEM> E{reinterpret_cast<uint32_t*>(smem), reinterpret_cast<int32_t*>(smem + 4 * (size_t)H), Eg + off};
   uint8_t* flag = SMEM ? smem + 8 * (size_t)H : flag_g + off;
   const float qd = (float)P.d_q;
   // flag: 0 neutral, 1 charged with the deprotonated charge, 2 charged with another value
   for (uint32_t h = threadIdx.x; h < H; h += kWalkThreads) {
-    if (SMEM) E[h] = Eg[off + h];
+    if (SMEM) E.set(h, Eg[off + h]);
     const float q = charge[head_slot[off + h]];
     flag[h] = q == 0.f ? 0 : (q == qd ? 1 : 2);
   }
@@ -301,7 +352,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_sweep_walk(const SysParams* __
     F[0].start[lane + 1] = 0xFFFFFFFFu;
     F[1].start[lane + 1] = 0xFFFFFFFFu;
     W.corr[lane] = 0;
-    if (lane == 0) { F[0].n = F[1].n = 0; F[0].start[0] = F[1].start[0] = 0; W.done = 0; s_dep = 0; }
+    if (lane == 0) { F[0].n = F[1].n = 0; F[0].start[0] = F[1].start[0] = 0; W.done = 0; W.nq = 0; s_dep = 0; }
   }
   const double kT = P.d_kT, inv_kT = 1.0 / P.d_kT;
   const double dGintr = kT * 2.302585092994046 * (P.d_pka - P.d_ph);
@@ -335,9 +386,11 @@ __global__ void __launch_bounds__(kWalkThreads) k_sweep_walk(const SysParams* __
     const Flips& Fp = F[(wnd + 1) & 1];   // the previous window's
     // ---- X ----
     if (chain) {
-      e = E[A.site];
+      e = E.get(A.site);
       f = flag[A.site];
     }
+    // pairs within reach are queued and then evaluated in FP64 one per thread, so no warp runs the
+    // FP64 path more than once per pass
     for (uint32_t t = threadIdx.x; t < 1024u + 32u * Fp.n; t += kWalkThreads) {
       if (t < 1024u) {
         const int k = (int)(t >> 5), q = (int)(t & 31);
@@ -349,9 +402,12 @@ __global__ void __launch_bounds__(kWalkThreads) k_sweep_walk(const SysParams* __
           dx -= rintf(dx * ibx) * bx;
           dy -= rintf(dy * iby) * by;
           dz -= rintf(dz * ibz) * bz;
-          if (dx * dx + dy * dy + dz * dz < near2)
-            m = std_delta(P, dist2(P, make_float4(W.x[k], W.y[k], W.z[k], 0.f),
-                                   make_float4(W.x[q], W.y[q], W.z[q], 0.f)), qd, cut2, reach2);
+          if (dx * dx + dy * dy + dz * dz < near2) {
+            const uint32_t slot = atomicAdd(&W.nq, 1u);
+            if (slot < kQueue) W.queue[slot] = (uint16_t)t;
+            else m = std_delta(P, dist2(P, make_float4(W.x[k], W.y[k], W.z[k], 0.f),
+                                        make_float4(W.x[q], W.y[q], W.z[q], 0.f)), qd, cut2, reach2);
+          }
         }
         W.M[k][q] = m;
       } else {
@@ -362,20 +418,28 @@ __global__ void __launch_bounds__(kWalkThreads) k_sweep_walk(const SysParams* __
         dy -= rintf(dy * iby) * by;
         dz -= rintf(dz * ibz) * bz;
         if (dx * dx + dy * dy + dz * dz < near2) {
-          const double r2 = dist2(P, make_float4(Fp.x[g], Fp.y[g], Fp.z[g], 0.f), make_float4(W.x[q], W.y[q], W.z[q], 0.f));
-          const int sg = Fp.sign[g];
-          long long d;
-          if (sg != 0) {
-            d = std_delta(P, r2, qd, cut2, reach2);
-            if (sg < 0) d = -d;
-          } else {
-            d = flip_delta(P, r2, Fp.qo[g], Fp.qn[g], cut2, reach2);
-          }
-          if (d != 0) atomicAdd(reinterpret_cast<unsigned long long*>(&W.corr[q]), (unsigned long long)d);
+          const uint32_t slot = atomicAdd(&W.nq, 1u);
+          if (slot < kQueue) W.queue[slot] = (uint16_t)t;
+          else corr_term(P, Fp, W, g, q, qd, cut2, reach2);
         }
       }
     }
     __syncthreads();
+    {
+      const uint32_t nq = W.nq < kQueue ? W.nq : kQueue;
+      for (uint32_t i = threadIdx.x; i < nq; i += kWalkThreads) {
+        const uint32_t t = W.queue[i];
+        if (t < 1024u) {
+          const uint32_t k = t >> 5, q = t & 31u;
+          W.M[k][q] = std_delta(P, dist2(P, make_float4(W.x[k], W.y[k], W.z[k], 0.f),
+                                         make_float4(W.x[q], W.y[q], W.z[q], 0.f)), qd, cut2, reach2);
+        } else {
+          corr_term(P, Fp, W, (t - 1024u) >> 5, (t - 1024u) & 31u, qd, cut2, reach2);
+        }
+      }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) W.nq = 0;
     if (W.done) break;
     // ---- R ----
     if (chain) {
