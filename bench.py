@@ -227,14 +227,15 @@ def run_cuda(args):
     bytes_per_launch = n * (4.0 * mean_list + 56.0)
     achieved = bytes_per_launch / (f_ms / max(f_n, 1) / 1e3) / 1e9 if f_n else None
     peak, peak_kind = peaks()
+    # DRAM bytes per launch of the force kernel from the committed ncu summary (captured on the
+    # quarter-size case and scaled to 483,268 beads there); scaled again for other sizes
     traffic = None
-    tf = os.path.join(ROOT, "profiles", "force_traffic.json")
+    tf = os.path.join(ROOT, "profiles", "k_force_campaign121k.md")
     if os.path.exists(tf):
-        try:
-            with open(tf) as fh:
-                traffic = json.load(fh).get("bytes_per_launch")
-        except Exception:
-            traffic = None
+        with open(tf) as fh:
+            for line in fh:
+                if line.startswith("traffic_bytes_per_launch_483k:"):
+                    traffic = float(line.split(":", 1)[1]) * n / 483268.0
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                 "kernel": "k_force (list pair force + bonded terms)",
