@@ -393,7 +393,7 @@ def run_cuda(args):
                        "relax": {"iterations": args.relax, "max_force_after": relax["maxForceAfter"]},
                        "rebuilds_in_timed_region": info1["rebuilds"] - info0["rebuilds"],
                        "sweeps_in_timed_region": info1["sweeps"] - info0["sweeps"],
-                       "tpp": 8},
+                       "tpp": int(os.environ.get("SOUP_TPP", 4))},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
             "clocks": clk.summary(), "phases": phases, "batched": batched}
     if rank == 0:

@@ -11,6 +11,12 @@
 // fixed and the result is run-to-run deterministic.
 #include "soup_internal.h"
 
+// four 256-thread blocks per SM (64 registers): the force is latency-bound on its gathers, and the
+// fourth block hides more of it than the registers it costs (a few bytes of spill)
+#ifndef SOUP_FORCE_MINB
+#define SOUP_FORCE_MINB 4
+#endif
+
 namespace soup {
 
 namespace {
@@ -46,7 +52,7 @@ __device__ __forceinline__ void bonded_term(const Shared& S, const SysParams& P,
 }
 
 template <int TPP>
-__global__ void __launch_bounds__(256) k_force(
+__global__ void __launch_bounds__(256, SOUP_FORCE_MINB) k_force(
     const Shared* __restrict__ Sg, const SysParams* __restrict__ sp, const uint8_t* __restrict__ sysid, uint32_t N,
     const float4* __restrict__ pos, const float* __restrict__ charge, const uint32_t* __restrict__ slots,
     const uint32_t* __restrict__ center, const uint32_t* __restrict__ id, const uint32_t* __restrict__ slot_of,
@@ -126,28 +132,36 @@ __global__ void __launch_bounds__(256) k_force(
 }
 
 // soup/wgsl/electrostatics-long.wgsl:63-82 soup_es_force_far_main, a warp per head.
+// positions and charges of the heads by head index (x, y, z, q): the far half reads one 16-byte
+// record per list entry instead of a slot lookup followed by two gathers
+__global__ void k_gather_xq(const uint32_t* __restrict__ head_slot, uint32_t H, const float4* __restrict__ pos,
+                            const float* __restrict__ charge, float4* __restrict__ xq) {
+  const uint32_t h = blockIdx.x * blockDim.x + threadIdx.x;
+  if (h >= H) return;
+  const uint32_t k = head_slot[h];
+  const float4 p = pos[k];
+  xq[h] = make_float4(p.x, p.y, p.z, charge[k]);
+}
+
 __global__ void __launch_bounds__(256) k_es_far(const SysParams* __restrict__ sp, const uint32_t* __restrict__ head_slot,
                                                 const uint32_t* __restrict__ head_sys, uint32_t H,
-                                                const float4* __restrict__ pos,
-                                                const float* __restrict__ charge, const uint32_t* __restrict__ es_nl,
+                                                const float4* __restrict__ xq, const uint32_t* __restrict__ es_nl,
                                                 const uint32_t* __restrict__ es_cnt, uint32_t cap,
                                                 float4* __restrict__ force) {
   const uint32_t h = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   if (h >= H) return;   // warp-uniform
   const SysParams& P = sp[head_sys[h]];
-  const uint32_t ks = head_slot[h];
-  const float qi = charge[ks];
+  const float4 xi = xq[h];
+  const float qi = xi.w;
   if (qi == 0.f || P.es_A == 0.f) return;
-  const float4 xi = pos[ks];
   float fx = 0.f, fy = 0.f, fz = 0.f;
   const uint32_t cnt = es_cnt[h];
   const uint32_t* row = es_nl + (size_t)h * cap;
   for (uint32_t s = lane; s < cnt; s += 32) {
-    const uint32_t j = __ldg(head_slot + __ldg(row + s));
-    const float qj = __ldg(charge + j);
+    const float4 xj = __ldg(xq + __ldg(row + s));
+    const float qj = xj.w;
     if (qj == 0.f) continue;
-    const float4 xj = __ldg(pos + j);
     const float dx = fast_mi(xi.x - xj.x, P.box[0], P.inv_box[0]);
     const float dy = fast_mi(xi.y - xj.y, P.box[1], P.inv_box[1]);
     const float dz = fast_mi(xi.z - xj.z, P.box[2], P.inv_box[2]);
@@ -165,6 +179,7 @@ __global__ void __launch_bounds__(256) k_es_far(const SysParams* __restrict__ sp
     fz += __shfl_xor_sync(0xffffffffu, fz, o);
   }
   if (lane == 0) {
+    const uint32_t ks = head_slot[h];
     float4 f = force[ks];
     force[ks] = make_float4(f.x + fx, f.y + fy, f.z + fz, 0.f);
   }
@@ -252,18 +267,19 @@ void launch_force_list(Batch& b) {
   switch (b.tpp) {
     case 1: launch_force_tpp<1>(b); break;
     case 2: launch_force_tpp<2>(b); break;
-    case 4: launch_force_tpp<4>(b); break;
     case 16: launch_force_tpp<16>(b); break;
     case 32: launch_force_tpp<32>(b); break;
-    default: launch_force_tpp<8>(b); break;
+    case 8: launch_force_tpp<8>(b); break;
+    default: launch_force_tpp<4>(b); break;
   }
 }
 
 void launch_es_far(Batch& b) {
   if (b.H == 0) return;
-  b.launches += 1;
-  k_es_far<<<nblocks((uint64_t)b.H * 32, 256), 256, 0, b.stream>>>(b.sp, b.head_slot, b.head_sys, b.H, b.pos,
-                                                                   b.charge, b.es_nl, b.es_cnt, b.es_cap, b.force);
+  b.launches += 2;
+  k_gather_xq<<<nblocks(b.H), kBlock, 0, b.stream>>>(b.head_slot, b.H, b.pos, b.charge, b.head_xq);
+  k_es_far<<<nblocks((uint64_t)b.H * 32, 256), 256, 0, b.stream>>>(b.sp, b.head_slot, b.head_sys, b.H, b.head_xq,
+                                                                   b.es_nl, b.es_cnt, b.es_cap, b.force);
 }
 
 void launch_force_brute(Batch& b) {

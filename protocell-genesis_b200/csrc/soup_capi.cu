@@ -12,6 +12,8 @@
 #include <string>
 #include <vector>
 
+#include <cstdlib>
+
 #include "soup_internal.h"
 
 using namespace soup;
@@ -374,6 +376,7 @@ Batch* make_batch(const SoupConfig* cfgs, const SoupInitState* inits, uint32_t R
   b.heads = dalloc<uint32_t>(b.H); b.head_sys = dalloc<uint32_t>(b.H); b.head_slot = dalloc<uint32_t>(b.H);
   b.head_e = dalloc<long long>(b.H);
   b.head_pos = dalloc<float4>(b.H);
+  b.head_xq = dalloc<float4>(b.H);
   b.head_flag = dalloc<uint8_t>(b.H);
   sweep_prepare(b);
   b.es_nl = dalloc<uint32_t>((size_t)b.H * std::max<uint32_t>(b.es_cap, 1)); b.es_cnt = dalloc<uint32_t>(b.H);
@@ -385,7 +388,10 @@ Batch* make_batch(const SoupConfig* cfgs, const SoupInitState* inits, uint32_t R
   }
   alloc_grids(b);
   upload_params(b);
-  b.tpp = 8;
+  // lanes per particle in the list force: 4 measured fastest at 483k beads (2: same, 8: +5%,
+  // 16: +16%); SOUP_TPP in the environment overrides it for tuning (1, 2, 4, 8, 16 or 32)
+  b.tpp = 4;
+  if (const char* e = std::getenv("SOUP_TPP")) b.tpp = std::atoi(e);
   force_pass(b);   // priming pass (soup/src/sim.ts:396-408)
   SOUP_CUDA_TRY(cudaStreamSynchronize(b.stream));
   SOUP_CUDA_TRY(cudaGetLastError());
@@ -405,7 +411,7 @@ void destroy_batch(Batch* b) {
                   b->frozen, b->id, b->slot_of, b->pos2, b->vel2, b->force2, b->charge2, b->slots2, b->center2,
                   b->held2, b->brng2, b->trng2, b->frozen2, b->id2, b->cell_of_slot, b->cell_count, b->cell_start,
                   b->cell_cursor, b->perm, b->scan_tmp, b->nl, b->nl_cnt, b->heads, b->head_sys, b->es_nl,
-                  b->es_cnt, b->head_slot, b->head_e, b->head_pos, b->head_d, b->head_flag, b->hcell_count, b->hcell_start, b->hcell_cursor, b->hsorted, b->hcell_of, b->flags,
+                  b->es_cnt, b->head_slot, b->head_e, b->head_pos, b->head_xq, b->head_d, b->head_flag, b->hcell_count, b->hcell_start, b->hcell_cursor, b->hsorted, b->hcell_of, b->flags,
                   b->events, b->desorb, b->drift_bits, b->bond_items, b->bond_nitems, b->uf_parent, b->comp_min,
                   b->item_done, b->has_item, b->sweep_out, b->prot_rng_dev, b->sp, b->shared, b->sysid, b->occ,
                   b->vis, b->frontier};

@@ -75,6 +75,7 @@ struct Batch {
   uint32_t* head_slot = nullptr;     // current slot of each head (refreshed at every rebuild)
   long long* head_e = nullptr;       // constant-pH site energy per head, fixed point 2^-40 (sweep scratch)
   float4* head_pos = nullptr;        // head positions gathered for the sweep
+  float4* head_xq = nullptr;         // head positions and charges by head index, for the far half
   long long* head_d = nullptr;       // [head][es_cap] change of a list neighbour's energy when the head
                                      // deprotonates, fixed point 2^-40 (sweep scratch)
   uint8_t* head_flag = nullptr;      // charge state per head when the sweep cannot keep it in shared memory
@@ -115,7 +116,7 @@ struct Batch {
   std::vector<uint64_t> next_sweep;
   uint64_t rebuilds = 0, sweeps = 0;
   bool force_fresh = false;          // force array matches positions+charges+lists
-  int tpp = 8;                       // threads per particle in the list kernels
+  int tpp = 4;                       // threads per particle in the list force
   std::string err;
   std::vector<SoupHandle*> views;    // per-replica handle views
 
