@@ -107,6 +107,36 @@ def dist_init():
     return ws, rank, local
 
 
+def rank_seeds(rank):
+    """Replicas only: every rank runs its own copy of the workload, seeded apart (plain, batched)."""
+    return 19 + rank, 7 + rank
+
+
+def max_over_ranks(x, dist, device):
+    """The largest per-rank value (a step time) over all ranks; x itself on one rank."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def sum_over_ranks(x, dist, device):
+    """The sum of a per-rank value over all ranks; x itself on one rank."""
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return float(t.item())
+
+
+def aggregate_rate(ws, units_per_rank, steps, ms_max):
+    """Whole-job particle-steps/s: every rank's units over the slowest rank's time."""
+    return ws * units_per_rank * steps / (ms_max / 1e3)
+
+
 def cpu_sample(pkg, ob, cfg, state, budget_s=12.0, max_steps=40):
     """Time the CPU oracle (all host threads) on a bounded number of steps of the same workload."""
     from protocell_genesis_b200 import _abi
@@ -221,7 +251,7 @@ def amphiphile_state(L, cfg, na, seed):
 def run_batched(args, pkg, L, cfgm, rank, torch):
     """The batched form: many uneven replicas stepped together, one launch per kernel per step."""
     import ctypes as C
-    items = batched_configs(cfgm, seed=7 + rank, replicas=args.replicas)
+    items = batched_configs(cfgm, seed=rank_seeds(rank)[1], replicas=args.replicas)
     cfgs, states = [], []
     for cfg, na, sd in items:
         st = amphiphile_state(L, cfg, na, sd)
@@ -264,12 +294,13 @@ def run_cuda(args):
     dist = None
     if ws > 1:
         import torch.distributed as dist
-        dist.init_process_group("nccl", device_id=torch.device("cuda", local))
+        import datetime
+        dist.init_process_group("nccl", device_id=torch.device("cuda", local), timeout=datetime.timedelta(seconds=300))
     import __graft_entry__ as ge
     pkg = ge._package()
     from protocell_genesis_b200 import _abi, config as cfgm
     L = _abi.lib()
-    cfg = cfgm.resolve(workload_opts(cfgm, seed=19 + rank, skin=args.skin, scale=args.scale))
+    cfg = cfgm.resolve(workload_opts(cfgm, seed=rank_seeds(rank)[0], skin=args.skin, scale=args.scale))
     n = cfg.n
     # fresh lattice on the host, relaxed on the device (untimed set-up)
     host = {}
@@ -308,12 +339,8 @@ def run_cuda(args):
         L.soup_kernel_time(s._h, k, C.byref(t), C.byref(c))
         ktime[name] = (t.value, c.value)
     L.soup_profile(s._h, 0)
-    ms_max = ms
-    if dist:
-        tt = torch.tensor([ms], device="cuda")
-        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
-        ms_max = float(tt.item())
-    value = ws * n * args.steps / (ms_max / 1e3)
+    ms_max = max_over_ranks(ms, dist, "cuda")
+    value = aggregate_rate(ws, n, args.steps, ms_max)
 
     # roofline of the dominant kernel (the list force), algorithmic bytes per launch:
     # per particle 4 B per list entry + pos 16 + charge 4 + slots 12 + centre 4 + count 4 + force 16
@@ -378,10 +405,10 @@ def run_cuda(args):
     if not args.no_batched:
         batched = run_batched(args, pkg, L, cfgm, rank, torch)
         if dist:
-            tb = torch.tensor([batched["ms_per_step"]], device="cuda")
-            dist.all_reduce(tb, op=dist.ReduceOp.MAX)
-            batched["ms_per_step"] = float(tb.item())
-            batched["value"] = ws * batched["beads"] * 1e3 / batched["ms_per_step"]
+            # ranks draw different replica sets: all their beads over the slowest rank's step
+            batched["ms_per_step"] = max_over_ranks(batched["ms_per_step"], dist, "cuda")
+            batched["beads"] = int(sum_over_ranks(batched["beads"], dist, "cuda"))
+            batched["value"] = aggregate_rate(1, batched["beads"], 1, batched["ms_per_step"])
         batched["vs_plain"] = batched["value"] / value
 
     phases = {name: {"ms_total": t, "launches": c, "ms_per_step": t / args.steps} for name, (t, c) in ktime.items() if c}
