@@ -438,8 +438,8 @@ def main():
     ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
     ap.add_argument("--skin", type=float, default=1.0)
     ap.add_argument("--relax", type=int, default=200)
-    ap.add_argument("--ref-relax", type=int, default=15)
-    ap.add_argument("--ref-budget", type=float, default=90.0)
+    ap.add_argument("--ref-relax", type=int, default=10)
+    ap.add_argument("--ref-budget", type=float, default=60.0)
     ap.add_argument("--cpu-budget", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
