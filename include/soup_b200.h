@@ -274,6 +274,31 @@ int soup_aggregate_labels(SoupHandle* h, const uint32_t* member_idx, uint32_t n_
 int soup_aggregate_labels_noalloc(SoupHandle* h, const uint32_t* member_idx, uint32_t n_members,
                                   double cutoff, uint32_t* labels, uint32_t* n_components);
 
+/* ---- observables ----------------------------------------------------------------------------- */
+/* pairingStats (soup/src/electrostatics.ts:520-561): for every titratable head, the like / unlike
+ * contacts with the other heads within contact_radius (FP64 distance, JavaScript minimum image) and
+ * whether its nearest such head carries the other charge state.  Exact-distance ties for the nearest
+ * go to the smaller head index (the reference takes the first in its cell walk).  contact_radius must
+ * be below the electrostatics cutoff; the reference passes wca_cut(sigma * head_head). */
+typedef struct SoupPairingStats {
+  uint32_t heads, with_neighbour, unlike_contacts, like_contacts, paired, charged;
+  double unlike_fraction;         /* unlike / (unlike + like) */
+  double unlike_fraction_random;  /* 2 alpha (1 - alpha) */
+  double paired_fraction;         /* paired / heads */
+  double contact_radius;
+  double alpha;                   /* charged / heads */
+} SoupPairingStats;
+int soup_pairing_stats(SoupHandle* h, double contact_radius, SoupPairingStats* out);
+
+/* densityProfileZ (engine/src/metrics.ts:21-47): histogram of the beads' z over [0, box_z) in
+ * `bins` bins, split into heads (kinds whose bit is set in head_kind_mask) and tails (the rest).
+ * The soup profiles polar kinds as heads (soup/src/aggregates.ts:95-109); the engine's own
+ * convention is kind 0 (mask 1).  A bead outside [0, box_z) makes the call fail as the reference
+ * does, unless `escaped` is given: then such beads are left out and counted there (dropEscapedZ,
+ * engine/src/metrics.ts:106-121). */
+int soup_density_profile_z(SoupHandle* h, uint32_t bins, uint32_t head_kind_mask, uint32_t* head_counts,
+                           uint32_t* tail_counts, uint32_t* escaped);
+
 /* ---- single phases ------------------------------------------------------------------------- */
 /* One phase of the step on the current device state, so each kernel can be checked in isolation
  * (the reference times phases the same way: stepPhasesDEBUG, soup/src/soup-readback.ts:191-245).

@@ -1523,6 +1523,59 @@ uint32_t oracle_aggregates(const float* pos, const uint32_t* mem, uint32_t m, co
   return aggregates(pos, mem, m, box, cutoff, labels);
 }
 
+// pairingStats (soup/src/electrostatics.ts:520-561) over every pair of titratable heads; the nearest
+// contact's exact-distance ties go to the smaller head index.  out: with_neighbour, unlike, like,
+// paired, charged, heads.
+int oracle_pairing_stats(const float* pos, const float* charges, uint32_t n, const double box[3], int charged_kind,
+                         double contact, uint32_t* out6) {
+  std::vector<uint32_t> heads;
+  for (uint32_t i = 0; i < n; ++i) if ((int)pos[4 * i + 3] == charged_kind) heads.push_back(i);
+  auto mi = [](double d, double L) { return d - js_round(d / L) * L; };
+  uint32_t with = 0, unlike = 0, like = 0, paired = 0, charged = 0;
+  for (size_t a = 0; a < heads.size(); ++a) {
+    const uint32_t i = heads[a];
+    if (charges[i] != 0.f) ++charged;
+    double best = INFINITY;
+    long best_b = -1;
+    bool any = false;
+    for (size_t b = 0; b < heads.size(); ++b) {
+      if (b == a) continue;
+      const uint32_t j = heads[b];
+      const double dx = mi((double)pos[4 * i] - pos[4 * j], box[0]);
+      const double dy = mi((double)pos[4 * i + 1] - pos[4 * j + 1], box[1]);
+      const double dz = mi((double)pos[4 * i + 2] - pos[4 * j + 2], box[2]);
+      const double r = std::sqrt(dx * dx + dy * dy + dz * dz);
+      if (r > contact) continue;
+      any = true;
+      if ((charges[i] == 0.f) != (charges[j] == 0.f)) ++unlike; else ++like;
+      if (r < best) { best = r; best_b = (long)b; }
+    }
+    if (any) ++with;
+    if (best_b >= 0 && (charges[i] == 0.f) != (charges[heads[best_b]] == 0.f)) ++paired;
+  }
+  out6[0] = with; out6[1] = unlike; out6[2] = like; out6[3] = paired; out6[4] = charged;
+  out6[5] = (uint32_t)heads.size();
+  return SOUP_OK;
+}
+
+// densityProfileZ (engine/src/metrics.ts:21-47) with heads = kinds in head_mask; escaped beads are
+// counted instead of binned (dropEscapedZ, metrics.ts:91-110)
+int oracle_density_profile_z(const float* pos, uint32_t n, double box_z, uint32_t bins, uint32_t head_mask,
+                             uint32_t* head, uint32_t* tail, uint32_t* escaped) {
+  const double dz = box_z / bins;
+  for (uint32_t b = 0; b < bins; ++b) head[b] = tail[b] = 0;
+  uint32_t esc = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    const double z = pos[4 * i + 2];
+    if (!(z >= 0 && z < box_z)) { ++esc; continue; }
+    const uint32_t b = std::min<uint32_t>(bins - 1, (uint32_t)std::floor(z / dz));
+    const uint32_t kind = (uint32_t)(int)pos[4 * i + 3];
+    if (kind < 32 && ((head_mask >> kind) & 1u)) ++head[b]; else ++tail[b];
+  }
+  *escaped = esc;
+  return SOUP_OK;
+}
+
 // relaxIterations (soup/src/soup-relax.ts:87-111)
 int oracle_relax(void* p, uint32_t iterations, double d0) {
   System& s = *static_cast<System*>(p);

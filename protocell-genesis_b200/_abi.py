@@ -103,6 +103,15 @@ class SoupClosureResult(C.Structure):
     ]
 
 
+class SoupPairingStats(C.Structure):
+    _fields_ = [
+        ("heads", C.c_uint32), ("with_neighbour", C.c_uint32), ("unlike_contacts", C.c_uint32),
+        ("like_contacts", C.c_uint32), ("paired", C.c_uint32), ("charged", C.c_uint32),
+        ("unlike_fraction", C.c_double), ("unlike_fraction_random", C.c_double), ("paired_fraction", C.c_double),
+        ("contact_radius", C.c_double), ("alpha", C.c_double),
+    ]
+
+
 class SoupInfo(C.Structure):
     _fields_ = [
         ("n", C.c_uint32), ("global_step", C.c_uint64), ("list_capacity", C.c_uint32),
@@ -151,6 +160,8 @@ SIGNATURES = {
                                C.c_double, C.c_double, C.c_double, C.POINTER(SoupClosureResult)]),
     "soup_amphiphile_labels": (C.c_int, [_P, _U32P, _U32P]),
     "soup_aggregate_labels": (C.c_int, [_P, _U32P, C.c_uint32, C.c_double, _U32P, _U32P]),
+    "soup_pairing_stats": (C.c_int, [_P, C.c_double, C.POINTER(SoupPairingStats)]),
+    "soup_density_profile_z": (C.c_int, [_P, C.c_uint32, C.c_uint32, _U32P, _U32P, _U32P]),
     "soup_aggregate_labels_noalloc": (C.c_int, [_P, _U32P, C.c_uint32, C.c_double, _U32P, _U32P]),
     "soup_batch_create": (C.c_int, [C.POINTER(SoupConfig), C.POINTER(SoupInitState), C.c_uint32,
                                     C.POINTER(_P)]),

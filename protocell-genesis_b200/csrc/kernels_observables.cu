@@ -1,0 +1,148 @@
+// kernels_observables.cu -- trajectory observables on the device.
+//
+// Reference:
+//   engine/src/metrics.ts:21-47 densityProfileZ (+ 106-121 dropEscapedZ): bead z histogram split
+//     into heads and tails (the soup profiles a copy whose w is 0 for polar kinds and 1 otherwise,
+//     soup/src/aggregates.ts:95-109; here a kind mask says which kinds count as heads);
+//   soup/src/electrostatics.ts:520-561 pairingStats: per head, the like/unlike contacts with every
+//     other head within the contact radius and the charge of its nearest one.
+// Both reduce to integer counts (atomics on integers), so the results do not depend on the order the
+// threads finish in.  Distances for pairingStats are FP64 with JavaScript rounding of the minimum
+// image (mi(d, L) = d - Math.round(d / L) * L), as the reference computes them.
+#include "soup_internal.h"
+
+namespace soup {
+
+namespace {
+
+constexpr int kBlock = 256;
+inline unsigned nblocks(uint64_t n, int b = kBlock) { return (unsigned)((n + b - 1) / b); }
+
+__device__ __forceinline__ double js_round(double x) {
+  const double r = floor(x);
+  return (x - r >= 0.5) ? r + 1.0 : r;
+}
+__device__ __forceinline__ double mi_js(double d, double L) { return d - js_round(d / L) * L; }
+
+// counts[0..bins) heads, counts[bins..2 bins) tails, counts[2 bins] escaped
+__global__ void k_profile_z(const float4* __restrict__ pos, uint32_t off, uint32_t n, double box_z, uint32_t bins,
+                            uint32_t head_mask, uint32_t* __restrict__ counts) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const float4 p = pos[off + i];
+  const double z = (double)p.z;
+  if (!(z >= 0.0 && z < box_z)) {
+    atomicAdd(&counts[2 * bins], 1u);
+    return;
+  }
+  const double dz = box_z / (double)bins;
+  const uint32_t b = min(bins - 1u, (uint32_t)floor(z / dz));
+  const uint32_t kind = (uint32_t)(int)p.w;
+  const bool head = kind < 32u && ((head_mask >> kind) & 1u);
+  atomicAdd(&counts[head ? b : bins + b], 1u);
+}
+
+// a warp per head of the replica, over its head list (complete for r < rc_es >= the contact radius)
+// out: [0] heads with a neighbour, [1] unlike contacts, [2] like contacts, [3] paired, [4] charged
+__global__ void k_pairing(const uint32_t* __restrict__ head_slot, uint32_t head_off, uint32_t nheads,
+                          const float4* __restrict__ pos, const float* __restrict__ charge,
+                          const uint32_t* __restrict__ es_nl, const uint32_t* __restrict__ es_cnt, uint32_t cap,
+                          double bx, double by, double bz, double contact, uint32_t* __restrict__ out) {
+  const uint32_t hl = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int lane = threadIdx.x & 31;
+  if (hl >= nheads) return;   // warp-uniform
+  const uint32_t h = head_off + hl;
+  const uint32_t ki = head_slot[h];
+  const float4 xi = pos[ki];
+  const bool qi0 = charge[ki] == 0.f;
+  uint32_t unlike = 0, like = 0;
+  double best = INFINITY;
+  uint32_t best_h = 0xFFFFFFFFu;
+  bool best_unlike = false;
+  const uint32_t cnt = es_cnt[h];
+  const uint32_t* row = es_nl + (size_t)h * cap;
+  for (uint32_t s = lane; s < cnt; s += 32) {
+    const uint32_t g = row[s];
+    const uint32_t kj = head_slot[g];
+    const float4 xj = pos[kj];
+    const double dx = mi_js((double)xi.x - (double)xj.x, bx);
+    const double dy = mi_js((double)xi.y - (double)xj.y, by);
+    const double dz = mi_js((double)xi.z - (double)xj.z, bz);
+    const double r = sqrt(dx * dx + dy * dy + dz * dz);
+    if (r > contact) continue;
+    const bool un = qi0 != (charge[kj] == 0.f);
+    if (un) ++unlike; else ++like;
+    if (r < best || (r == best && g < best_h)) { best = r; best_h = g; best_unlike = un; }
+  }
+  // the nearest over the warp (ties: the smaller head index)
+  for (int o = 16; o > 0; o >>= 1) {
+    const double rb = __shfl_xor_sync(0xffffffffu, best, o);
+    const uint32_t hb = __shfl_xor_sync(0xffffffffu, best_h, o);
+    const bool ub = __shfl_xor_sync(0xffffffffu, (int)best_unlike, o) != 0;
+    if (rb < best || (rb == best && hb < best_h)) { best = rb; best_h = hb; best_unlike = ub; }
+    unlike += __shfl_xor_sync(0xffffffffu, unlike, o);
+    like += __shfl_xor_sync(0xffffffffu, like, o);
+  }
+  if (lane == 0) {
+    if (unlike + like > 0) atomicAdd(&out[0], 1u);
+    atomicAdd(&out[1], unlike);
+    atomicAdd(&out[2], like);
+    if (best_h != 0xFFFFFFFFu && best_unlike) atomicAdd(&out[3], 1u);
+    if (!qi0) atomicAdd(&out[4], 1u);
+  }
+}
+
+}  // namespace
+
+int run_profile_z(Batch& b, uint32_t r, uint32_t bins, uint32_t head_mask, uint32_t* head, uint32_t* tail,
+                  uint32_t* escaped, std::string& err) {
+  const SoupConfig& c = b.cfg[r];
+  std::vector<uint32_t> h(2 * (size_t)bins + 1, 0);
+  uint32_t* d = nullptr;
+  SOUP_CUDA_TRY(cudaMallocAsync(&d, 4 * h.size(), b.stream));
+  SOUP_CUDA_TRY(cudaMemsetAsync(d, 0, 4 * h.size(), b.stream));
+  b.launches += 1;
+  k_profile_z<<<nblocks(c.n), kBlock, 0, b.stream>>>(b.pos, b.hsp[r].slot_off, c.n, c.box[2], bins, head_mask, d);
+  SOUP_CUDA_TRY(cudaGetLastError());
+  SOUP_CUDA_TRY(cudaMemcpyAsync(h.data(), d, 4 * h.size(), cudaMemcpyDeviceToHost, b.stream));
+  SOUP_CUDA_TRY(cudaFreeAsync(d, b.stream));
+  SOUP_CUDA_TRY(cudaStreamSynchronize(b.stream));
+  const uint32_t esc = h[2 * (size_t)bins];
+  if (esc && !escaped) {
+    err = "densityProfileZ: " + std::to_string(esc) + " bead(s) outside [0, " + std::to_string(c.box[2]) +
+          "): the z profile is undefined for escaped beads (z is not periodic), and clamping them into the "
+          "edge bin is not allowed: it creates a false peak";
+    return SOUP_E_ARG;
+  }
+  std::copy(h.begin(), h.begin() + bins, head);
+  std::copy(h.begin() + bins, h.begin() + 2 * (size_t)bins, tail);
+  if (escaped) *escaped = esc;
+  return SOUP_OK;
+}
+
+int run_pairing(Batch& b, uint32_t r, double contact, uint32_t out5[5], std::string& err) {
+  const SysParams& P = b.hsp[r];
+  const SoupConfig& c = b.cfg[r];
+  if (!c.es_enabled || P.nheads == 0) {
+    for (int k = 0; k < 5; ++k) out5[k] = 0;
+    return SOUP_OK;
+  }
+  if (!(contact < c.es_cutoff)) {
+    err = "pairingStats: the contact radius must be below the electrostatics cutoff (the head list's reach)";
+    return SOUP_E_ARG;
+  }
+  uint32_t* d = nullptr;
+  SOUP_CUDA_TRY(cudaMallocAsync(&d, 4 * 5, b.stream));
+  SOUP_CUDA_TRY(cudaMemsetAsync(d, 0, 4 * 5, b.stream));
+  b.launches += 1;
+  k_pairing<<<nblocks((uint64_t)P.nheads * 32, kBlock), kBlock, 0, b.stream>>>(
+      b.head_slot, P.head_off, P.nheads, b.pos, b.charge, b.es_nl, b.es_cnt, b.es_cap, c.box[0], c.box[1], c.box[2],
+      contact, d);
+  SOUP_CUDA_TRY(cudaGetLastError());
+  SOUP_CUDA_TRY(cudaMemcpyAsync(out5, d, 4 * 5, cudaMemcpyDeviceToHost, b.stream));
+  SOUP_CUDA_TRY(cudaFreeAsync(d, b.stream));
+  SOUP_CUDA_TRY(cudaStreamSynchronize(b.stream));
+  return SOUP_OK;
+}
+
+}  // namespace soup

@@ -908,6 +908,36 @@ int soup_amphiphile_labels(SoupHandle* h, uint32_t* head_of, uint32_t* n_out) {
   });
 }
 
+int soup_pairing_stats(SoupHandle* h, double contact_radius, SoupPairingStats* out) {
+  return guarded(h, [&](Batch& b, uint32_t r) {
+    if (!out || !(contact_radius > 0)) fail(SOUP_E_ARG, "pairingStats: bad argument");
+    uint32_t c[5];
+    std::string err;
+    int st = run_pairing(b, r, contact_radius, c, err);
+    if (st) fail(st, err);
+    std::memset(out, 0, sizeof *out);
+    out->heads = b.cfg[r].es_enabled ? b.hsp[r].nheads : 0;
+    out->with_neighbour = c[0]; out->unlike_contacts = c[1]; out->like_contacts = c[2];
+    out->paired = c[3]; out->charged = c[4];
+    out->alpha = out->heads > 0 ? (double)c[4] / out->heads : 0.0;
+    const uint32_t contacts = c[1] + c[2];
+    out->unlike_fraction = contacts > 0 ? (double)c[1] / contacts : 0.0;
+    out->unlike_fraction_random = 2 * out->alpha * (1 - out->alpha);
+    out->paired_fraction = out->heads > 0 ? (double)c[3] / out->heads : 0.0;
+    out->contact_radius = contact_radius;
+  });
+}
+
+int soup_density_profile_z(SoupHandle* h, uint32_t bins, uint32_t head_kind_mask, uint32_t* head_counts,
+                           uint32_t* tail_counts, uint32_t* escaped) {
+  return guarded(h, [&](Batch& b, uint32_t r) {
+    if (bins == 0 || bins > (1u << 24) || !head_counts || !tail_counts) fail(SOUP_E_ARG, "densityProfileZ: bad argument");
+    std::string err;
+    int st = run_profile_z(b, r, bins, head_kind_mask, head_counts, tail_counts, escaped, err);
+    if (st) fail(st, err);
+  });
+}
+
 int soup_aggregate_labels(SoupHandle* h, const uint32_t* member_idx, uint32_t n_members, double cutoff,
                           uint32_t* labels, uint32_t* n_components) {
   return guarded(h, [&](Batch& b, uint32_t r) {

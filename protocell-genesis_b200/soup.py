@@ -256,6 +256,40 @@ class SoupSystem:
             C.byref(nc)))
         return int(nc.value), labels
 
+    def pairing_stats(self, contact_radius):
+        """pairingStats (soup/src/electrostatics.ts:520-561) on the device; keys as the reference's."""
+        r = _abi.SoupPairingStats()
+        _check(self._lib, self._h, self._lib.soup_pairing_stats(self._h, float(contact_radius), C.byref(r)))
+        return dict(heads=r.heads, withNeighbour=r.with_neighbour, unlikeContacts=r.unlike_contacts,
+                    likeContacts=r.like_contacts, unlikeFraction=r.unlike_fraction,
+                    unlikeFractionRandom=r.unlike_fraction_random, paired=r.paired,
+                    pairedFraction=r.paired_fraction, contactRadius=r.contact_radius, alpha=r.alpha)
+
+    def density_profile_z(self, bins, head_kinds=None, drop_escaped=False):
+        """densityProfileZ (engine/src/metrics.ts:21-47) of this system's beads on the device:
+        {z, head, tail} (+ escaped when drop_escaped).  head_kinds: the kind indices counted as
+        heads (default: the polar kinds, as the soup's aggregate stage profiles them)."""
+        if head_kinds is None:
+            head_kinds = [k for k, m in enumerate(_config.load_params()["monomers"]) if m["polar"]]
+        mask = 0
+        for k in head_kinds:
+            mask |= 1 << int(k)
+        head = np.zeros(int(bins), np.uint32)
+        tail = np.zeros(int(bins), np.uint32)
+        esc = C.c_uint32(0)
+        _check(self._lib, self._h, self._lib.soup_density_profile_z(
+            self._h, int(bins), mask, head.ctypes.data_as(_abi._U32P), tail.ctypes.data_as(_abi._U32P),
+            C.byref(esc) if drop_escaped else None))
+        dz = float(self.cfg.box[2]) / int(bins)
+        out = dict(z=[(i + 0.5) * dz for i in range(int(bins))], head=head.astype(np.int64).tolist(),
+                   tail=tail.astype(np.int64).tolist())
+        if drop_escaped:
+            out["escaped"] = int(esc.value)
+        return out
+
+    pairingStats = pairing_stats
+    densityProfileZ = density_profile_z
+
     def aggregate_labels_noalloc(self, members, cutoff):
         """aggregate_labels without device allocation (scratch in a fixed per-device array of the
         library; at most SOUP_NOALLOC_MAX_MEMBERS members and cells; overlapping calls race)."""

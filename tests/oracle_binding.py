@@ -62,6 +62,8 @@ def lib(abi):
                                      C.POINTER(abi.SoupClosureResult), P, P]),
         "oracle_amphiphiles": (C.c_uint32, [P, P, C.c_uint32, P, P]),
         "oracle_aggregates": (C.c_uint32, [P, P, C.c_uint32, P, C.c_double, P]),
+        "oracle_pairing_stats": (C.c_int, [P, P, C.c_uint32, P, C.c_int, C.c_double, P]),
+        "oracle_density_profile_z": (C.c_int, [P, C.c_uint32, C.c_double, C.c_uint32, C.c_uint32, P, P, P]),
         "oracle_relax": (C.c_int, [P, C.c_uint32, C.c_double]),
     }
     for name, (res, args) in sig.items():
@@ -268,3 +270,27 @@ def aggregates(abi, pos, members, box, cutoff):
     box = np.ascontiguousarray(box, np.float64)
     n = L.oracle_aggregates(_ptr(pos), _ptr(members), len(members), _ptr(box), cutoff, _ptr(labels))
     return int(n), labels
+
+
+def pairing_stats(abi, pos, charges, box, charged_kind, contact):
+    """(with_neighbour, unlike, like, paired, charged, heads) from the oracle."""
+    L = lib(abi)
+    pos = np.ascontiguousarray(pos, np.float32)
+    charges = np.ascontiguousarray(charges, np.float32)
+    box = np.ascontiguousarray(box, np.float64)
+    out = np.zeros(6, np.uint32)
+    L.oracle_pairing_stats(_ptr(pos), _ptr(charges), len(pos) // 4, _ptr(box), int(charged_kind), float(contact),
+                           _ptr(out))
+    return tuple(int(v) for v in out)
+
+
+def density_profile_z(abi, pos, box_z, bins, head_mask):
+    """(head counts, tail counts, escaped) from the oracle."""
+    L = lib(abi)
+    pos = np.ascontiguousarray(pos, np.float32)
+    head = np.zeros(bins, np.uint32)
+    tail = np.zeros(bins, np.uint32)
+    esc = np.zeros(1, np.uint32)
+    L.oracle_density_profile_z(_ptr(pos), len(pos) // 4, float(box_z), int(bins), int(head_mask), _ptr(head),
+                               _ptr(tail), _ptr(esc))
+    return head, tail, int(esc[0])
