@@ -290,6 +290,21 @@ typedef struct SoupPairingStats {
 } SoupPairingStats;
 int soup_pairing_stats(SoupHandle* h, double contact_radius, SoupPairingStats* out);
 
+/* shapeOf over unwrapAggregate (engine/src/aggregate.ts:245-262, 308-346) for the components named by
+ * `labels` (one per member, e.g. from soup_aggregate_labels): components largest first (ties: smaller
+ * label first, the order clusterComponents sorts them in), and the first max_shapes of them measured:
+ * members unwrapped around the component's smallest original index (periodic on all three axes,
+ * stored as f32 as the reference does), centre, and the per-member gyration tensor.
+ * n_components receives the number of components. */
+typedef struct SoupAggregateShape {
+  uint32_t size;                  /* members */
+  uint32_t label;                 /* the component's smallest original index */
+  double centre[3];               /* centre of the unwrapped members (frame of the label member) */
+  double gyration[6];             /* Sxx, Syy, Szz, Sxy, Sxz, Syz */
+} SoupAggregateShape;
+int soup_aggregate_shapes(SoupHandle* h, const uint32_t* member_idx, const uint32_t* labels, uint32_t n_members,
+                          uint32_t max_shapes, SoupAggregateShape* out, uint32_t* n_components);
+
 /* densityProfileZ (engine/src/metrics.ts:21-47): histogram of the beads' z over [0, box_z) in
  * `bins` bins, split into heads (kinds whose bit is set in head_kind_mask) and tails (the rest).
  * The soup profiles polar kinds as heads (soup/src/aggregates.ts:95-109); the engine's own

@@ -1576,6 +1576,30 @@ int oracle_density_profile_z(const float* pos, uint32_t n, double box_z, uint32_
   return SOUP_OK;
 }
 
+// shapeOf over unwrapAggregate (engine/src/aggregate.ts:245-262, 308-346) for one component; members
+// ascending, the first one the unwrap reference.  out10: n, centre xyz, Sxx Syy Szz Sxy Sxz Syz.
+int oracle_aggregate_shape(const float* pos, const uint32_t* members, uint32_t m, const double box[3], double* out10) {
+  if (m == 0) return SOUP_E_ARG;
+  auto mi = [](double d, double L) { return d - js_round(d / L) * L; };
+  std::vector<float> u(3 * (size_t)m);
+  const double ref[3] = {pos[4 * members[0]], pos[4 * members[0] + 1], pos[4 * members[0] + 2]};
+  for (uint32_t k = 0; k < m; ++k)
+    for (int a = 0; a < 3; ++a)
+      u[3 * k + a] = (float)(ref[a] + mi((double)pos[4 * members[k] + a] - ref[a], box[a]));
+  double c[3] = {0, 0, 0};
+  for (uint32_t k = 0; k < m; ++k) for (int a = 0; a < 3; ++a) c[a] += u[3 * k + a];
+  for (int a = 0; a < 3; ++a) c[a] /= m;
+  double S[6] = {0, 0, 0, 0, 0, 0};
+  for (uint32_t k = 0; k < m; ++k) {
+    const double dx = u[3 * k] - c[0], dy = u[3 * k + 1] - c[1], dz = u[3 * k + 2] - c[2];
+    S[0] += dx * dx; S[1] += dy * dy; S[2] += dz * dz; S[3] += dx * dy; S[4] += dx * dz; S[5] += dy * dz;
+  }
+  out10[0] = m;
+  for (int a = 0; a < 3; ++a) out10[1 + a] = c[a];
+  for (int q = 0; q < 6; ++q) out10[4 + q] = S[q] / m;
+  return SOUP_OK;
+}
+
 // relaxIterations (soup/src/soup-relax.ts:87-111)
 int oracle_relax(void* p, uint32_t iterations, double d0) {
   System& s = *static_cast<System*>(p);

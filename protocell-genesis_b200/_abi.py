@@ -112,6 +112,10 @@ class SoupPairingStats(C.Structure):
     ]
 
 
+class SoupAggregateShape(C.Structure):
+    _fields_ = [("size", C.c_uint32), ("label", C.c_uint32), ("centre", C.c_double * 3), ("gyration", C.c_double * 6)]
+
+
 class SoupInfo(C.Structure):
     _fields_ = [
         ("n", C.c_uint32), ("global_step", C.c_uint64), ("list_capacity", C.c_uint32),
@@ -162,6 +166,8 @@ SIGNATURES = {
     "soup_aggregate_labels": (C.c_int, [_P, _U32P, C.c_uint32, C.c_double, _U32P, _U32P]),
     "soup_pairing_stats": (C.c_int, [_P, C.c_double, C.POINTER(SoupPairingStats)]),
     "soup_density_profile_z": (C.c_int, [_P, C.c_uint32, C.c_uint32, _U32P, _U32P, _U32P]),
+    "soup_aggregate_shapes": (C.c_int, [_P, _U32P, _U32P, C.c_uint32, C.c_uint32, C.POINTER(SoupAggregateShape),
+                                        _U32P]),
     "soup_aggregate_labels_noalloc": (C.c_int, [_P, _U32P, C.c_uint32, C.c_double, _U32P, _U32P]),
     "soup_batch_create": (C.c_int, [C.POINTER(SoupConfig), C.POINTER(SoupInitState), C.c_uint32,
                                     C.POINTER(_P)]),

@@ -146,3 +146,95 @@ int run_pairing(Batch& b, uint32_t r, double contact, uint32_t out5[5], std::str
 }
 
 }  // namespace soup
+
+namespace soup {
+
+namespace {
+
+// shapeOf over unwrapAggregate (engine/src/aggregate.ts:245-262, 308-346) for one component per
+// block: members[start[c] .. start[c+1]) as original indices, the first one the reference member.
+// Unwrapped coordinates are rounded to f32 as the reference stores them (a Float32Array), then
+// summed in FP64 in two passes (centre, then the second moments about it), each a fixed-order block
+// reduction.  out[c]: n, centre x y z, Sxx Syy Szz Sxy Sxz Syz (per member).
+constexpr int kShapeThreads = 256;
+__device__ __forceinline__ double block_sum(double v, double* sh) {
+  sh[threadIdx.x] = v;
+  __syncthreads();
+  for (int s = kShapeThreads / 2; s > 0; s >>= 1) {
+    if ((int)threadIdx.x < s) sh[threadIdx.x] += sh[threadIdx.x + s];
+    __syncthreads();
+  }
+  const double r = sh[0];
+  __syncthreads();
+  return r;
+}
+__global__ void __launch_bounds__(kShapeThreads) k_shape(const float4* __restrict__ pos, const uint32_t* __restrict__ slot_of,
+                                                         uint32_t off, const uint32_t* __restrict__ members,
+                                                         const uint32_t* __restrict__ start, double bx, double by,
+                                                         double bz, double* __restrict__ out) {
+  __shared__ double sh[kShapeThreads];
+  const uint32_t c = blockIdx.x;
+  const uint32_t a = start[c], e = start[c + 1];
+  const float4 r0 = pos[slot_of[off + members[a]]];
+  const double ref[3] = {(double)r0.x, (double)r0.y, (double)r0.z};
+  const double L[3] = {bx, by, bz};
+  auto unwrap = [&](uint32_t k, double u[3]) {
+    const float4 p = pos[slot_of[off + members[k]]];
+    const double v[3] = {(double)p.x, (double)p.y, (double)p.z};
+    for (int ax = 0; ax < 3; ++ax) u[ax] = (double)(float)(ref[ax] + mi_js(v[ax] - ref[ax], L[ax]));
+  };
+  double s[3] = {0, 0, 0};
+  for (uint32_t k = a + threadIdx.x; k < e; k += kShapeThreads) {
+    double u[3];
+    unwrap(k, u);
+    s[0] += u[0]; s[1] += u[1]; s[2] += u[2];
+  }
+  const double n = (double)(e - a);
+  double cen[3];
+  for (int ax = 0; ax < 3; ++ax) cen[ax] = block_sum(s[ax], sh) / n;
+  double m[6] = {0, 0, 0, 0, 0, 0};
+  for (uint32_t k = a + threadIdx.x; k < e; k += kShapeThreads) {
+    double u[3];
+    unwrap(k, u);
+    const double dx = u[0] - cen[0], dy = u[1] - cen[1], dz = u[2] - cen[2];
+    m[0] += dx * dx; m[1] += dy * dy; m[2] += dz * dz; m[3] += dx * dy; m[4] += dx * dz; m[5] += dy * dz;
+  }
+  double tot[6];
+  for (int q = 0; q < 6; ++q) tot[q] = block_sum(m[q], sh) / n;
+  if (threadIdx.x == 0) {
+    double* o = out + 10 * (size_t)c;
+    o[0] = n;
+    for (int ax = 0; ax < 3; ++ax) o[1 + ax] = cen[ax];
+    for (int q = 0; q < 6; ++q) o[4 + q] = tot[q];
+  }
+}
+
+}  // namespace
+
+int run_shapes(Batch& b, uint32_t r, const uint32_t* members_csr, const uint32_t* start, uint32_t ncomp,
+               double* out10, std::string& err) {
+  const SoupConfig& c = b.cfg[r];
+  if (ncomp == 0) return SOUP_OK;
+  const uint32_t total = start[ncomp];
+  for (uint32_t k = 0; k < total; ++k)
+    if (members_csr[k] >= c.n) { err = "aggregate shapes: member index out of range"; return SOUP_E_ARG; }
+  uint32_t *dm = nullptr, *ds = nullptr;
+  double* dout = nullptr;
+  SOUP_CUDA_TRY(cudaMallocAsync(&dm, 4 * (size_t)std::max<uint32_t>(total, 1), b.stream));
+  SOUP_CUDA_TRY(cudaMallocAsync(&ds, 4 * ((size_t)ncomp + 1), b.stream));
+  SOUP_CUDA_TRY(cudaMallocAsync(&dout, 80 * (size_t)ncomp, b.stream));
+  SOUP_CUDA_TRY(cudaMemcpyAsync(dm, members_csr, 4 * (size_t)total, cudaMemcpyHostToDevice, b.stream));
+  SOUP_CUDA_TRY(cudaMemcpyAsync(ds, start, 4 * ((size_t)ncomp + 1), cudaMemcpyHostToDevice, b.stream));
+  b.launches += 1;
+  k_shape<<<ncomp, kShapeThreads, 0, b.stream>>>(b.pos, b.slot_of, b.hsp[r].slot_off, dm, ds, c.box[0], c.box[1],
+                                                 c.box[2], dout);
+  SOUP_CUDA_TRY(cudaGetLastError());
+  SOUP_CUDA_TRY(cudaMemcpyAsync(out10, dout, 80 * (size_t)ncomp, cudaMemcpyDeviceToHost, b.stream));
+  SOUP_CUDA_TRY(cudaFreeAsync(dm, b.stream));
+  SOUP_CUDA_TRY(cudaFreeAsync(ds, b.stream));
+  SOUP_CUDA_TRY(cudaFreeAsync(dout, b.stream));
+  SOUP_CUDA_TRY(cudaStreamSynchronize(b.stream));
+  return SOUP_OK;
+}
+
+}  // namespace soup

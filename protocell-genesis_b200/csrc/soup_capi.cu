@@ -928,6 +928,44 @@ int soup_pairing_stats(SoupHandle* h, double contact_radius, SoupPairingStats* o
   });
 }
 
+int soup_aggregate_shapes(SoupHandle* h, const uint32_t* member_idx, const uint32_t* labels, uint32_t n_members,
+                          uint32_t max_shapes, SoupAggregateShape* out, uint32_t* n_components) {
+  return guarded(h, [&](Batch& b, uint32_t r) {
+    if (n_members && (!member_idx || !labels)) fail(SOUP_E_ARG, "aggregate shapes: bad argument");
+    if (max_shapes && !out) fail(SOUP_E_ARG, "aggregate shapes: NULL output");
+    // components by label, members ascending; largest first, then the smaller label
+    std::vector<std::pair<uint32_t, uint32_t>> ml(n_members);
+    for (uint32_t k = 0; k < n_members; ++k) ml[k] = {labels[k], member_idx[k]};
+    std::sort(ml.begin(), ml.end());
+    std::vector<std::pair<uint32_t, uint32_t>> comp;   // (begin in ml, size)
+    for (uint32_t k = 0; k < n_members;) {
+      uint32_t e = k;
+      while (e < n_members && ml[e].first == ml[k].first) ++e;
+      comp.push_back({k, e - k});
+      k = e;
+    }
+    std::stable_sort(comp.begin(), comp.end(), [](const auto& x, const auto& y) { return x.second > y.second; });
+    if (n_components) *n_components = (uint32_t)comp.size();
+    const uint32_t ns = (uint32_t)std::min<size_t>(max_shapes, comp.size());
+    if (ns == 0) return;
+    std::vector<uint32_t> csr, start(1, 0);
+    for (uint32_t c = 0; c < ns; ++c) {
+      for (uint32_t k = 0; k < comp[c].second; ++k) csr.push_back(ml[comp[c].first + k].second);
+      start.push_back((uint32_t)csr.size());
+    }
+    std::vector<double> o(10 * (size_t)ns);
+    std::string err;
+    int st = run_shapes(b, r, csr.data(), start.data(), ns, o.data(), err);
+    if (st) fail(st, err);
+    for (uint32_t c = 0; c < ns; ++c) {
+      out[c].size = comp[c].second;
+      out[c].label = ml[comp[c].first].first;
+      for (int a = 0; a < 3; ++a) out[c].centre[a] = o[10 * c + 1 + a];
+      for (int q = 0; q < 6; ++q) out[c].gyration[q] = o[10 * c + 4 + q];
+    }
+  });
+}
+
 int soup_density_profile_z(SoupHandle* h, uint32_t bins, uint32_t head_kind_mask, uint32_t* head_counts,
                            uint32_t* tail_counts, uint32_t* escaped) {
   return guarded(h, [&](Batch& b, uint32_t r) {

@@ -174,6 +174,8 @@ int run_amphiphiles(Batch& b, uint32_t r, uint32_t* head_of, uint32_t* n_out, st
 int run_profile_z(Batch& b, uint32_t r, uint32_t bins, uint32_t head_mask, uint32_t* head, uint32_t* tail,
                   uint32_t* escaped, std::string& err);
 int run_pairing(Batch& b, uint32_t r, double contact, uint32_t out5[5], std::string& err);
+int run_shapes(Batch& b, uint32_t r, const uint32_t* members_csr, const uint32_t* start, uint32_t ncomp,
+               double* out10, std::string& err);
 int run_aggregates(Batch& b, uint32_t r, const uint32_t* mem, uint32_t nm, double cutoff, uint32_t* labels,
                    uint32_t* ncomp, std::string& err);
 // host

@@ -12,6 +12,9 @@ or on host arrays, written here in the reference's terms:
   bilayer_thickness  engine/src/metrics.ts:159-162
   henderson_alpha    soup/src/electrostatics.ts:293-295
   apparent_pka       soup/src/electrostatics.ts:300-303
+  shape_metrics      engine/src/aggregate.ts:268-346 (symmetricEigenvalues3x3, symmetricEigenvector3x3,
+                     shapeOf's derived numbers; the sums come from SoupSystem.aggregate_shapes)
+  analyze_aggregates soup/src/aggregates.ts:499-558, the counting and shape parts
 Errors are raised where the reference throws, with its wording.
 """
 import math
@@ -114,6 +117,87 @@ def apparent_pka(alpha, ph):
     return ph - math.log10(alpha / (1 - alpha))
 
 
+def symmetric_eigenvalues_3x3(sxx, syy, szz, sxy, sxz, syz):
+    """Ascending eigenvalues of a real symmetric 3x3 matrix by Smith's closed form (O. K. Smith,
+    "Eigenvalues of a symmetric 3x3 matrix", CACM 4(4):168, 1961): shift by the mean eigenvalue q,
+    scale by p = sqrt(|A - qI|_F^2 / 6), and read the three angles off acos(det(B) / 2) / 3.  A
+    diagonal matrix (off-diagonal norm below 1e-30) is sorted directly."""
+    p1 = sxy * sxy + sxz * sxz + syz * syz
+    if p1 < 1e-30:
+        return sorted([sxx, syy, szz])
+    q = (sxx + syy + szz) / 3
+    p2 = (sxx - q) ** 2 + (syy - q) ** 2 + (szz - q) ** 2 + 2 * p1
+    p = math.sqrt(p2 / 6)
+    bxx, byy, bzz = (sxx - q) / p, (syy - q) / p, (szz - q) / p
+    bxy, bxz, byz = sxy / p, sxz / p, syz / p
+    det = bxx * (byy * bzz - byz * byz) - bxy * (bxy * bzz - byz * bxz) + bxz * (bxy * byz - byy * bxz)
+    phi = math.acos(max(-1.0, min(1.0, det / 2))) / 3
+    largest = q + 2 * p * math.cos(phi)
+    smallest = q + 2 * p * math.cos(phi + 2 * math.pi / 3)
+    return sorted([smallest, 3 * q - largest - smallest, largest])
+
+
+def symmetric_eigenvector_3x3(sxx, syy, szz, sxy, sxz, syz, lam):
+    """Unit eigenvector of one eigenvalue: the largest cross product of two rows of (A - lam I), or
+    None when every pair degenerates (magnitude below 1e-9: a repeated eigenvalue)."""
+    r = [(sxx - lam, sxy, sxz), (sxy, syy - lam, syz), (sxz, syz, szz - lam)]
+
+    def cross(a, b):
+        return (a[1] * b[2] - a[2] * b[1], a[2] * b[0] - a[0] * b[2], a[0] * b[1] - a[1] * b[0])
+
+    best, best_mag = None, -1.0
+    for a, b in ((0, 1), (0, 2), (1, 2)):
+        c = cross(r[a], r[b])
+        m = math.sqrt(c[0] ** 2 + c[1] ** 2 + c[2] ** 2)
+        if m > best_mag:
+            best, best_mag = c, m
+    if best_mag < 1e-9:
+        return None
+    return [best[0] / best_mag, best[1] / best_mag, best[2] / best_mag]
+
+
+def shape_metrics(shape):
+    """shapeOf's numbers from one device shape {size, label, centre, gyration}: principal moments
+    (ascending), radius of gyration, the smallest-moment axis ([0, 0, 1] when not unique), and the
+    flatness (l0 / l2) and in-plane symmetry (l1 / l2) ratios shapeOfAggregate reports."""
+    g = shape["gyration"]
+    lam = symmetric_eigenvalues_3x3(*g)
+    axis = symmetric_eigenvector_3x3(*g, lam[0]) or [0.0, 0.0, 1.0]
+    l0, l1, l2 = lam
+    return {"size": shape["size"], "label": shape["label"], "centre": list(shape["centre"]),
+            "principalMoments": lam, "radiusOfGyration": math.sqrt(max(0.0, l0 + l1 + l2)), "smallestAxis": axis,
+            "flatnessRatio": l0 / l2 if l2 > 1e-12 else 1.0, "inPlaneSymmetry": l1 / l2 if l2 > 1e-12 else 1.0}
+
+
+def analyze_aggregates(system, cutoff, detail_count=5, min_amphiphiles_per_aggregate=1):
+    """The counting and shape parts of analyzeAggregates on a device system: amphiphiles
+    (findAmphiphiles), their members clustered by `cutoff` on all three periodic axes, amphiphiles
+    per aggregate (largest aggregate first), the qualifying aggregates, and shapeOf for the largest
+    `detail_count`.  The head-shell, cavity and closure detail of shapeOfAggregate (and the lamellar
+    / vesicle classification built on them) is not part of this."""
+    n_amph, head_of = system.amphiphile_labels()
+    none = 0xFFFFFFFF
+    members = np.nonzero(head_of != none)[0].astype(np.uint32)
+    empty = {"aggregateCount": 0, "sizeHistogram": [], "aggregates": [], "qualifyingAggregateCount": 0,
+             "amphiphilesInQualifying": 0, "amphiphileShareInQualifying": 0.0}
+    if members.size == 0:
+        return empty
+    _, labels = system.aggregate_labels(members, cutoff)
+    ncomp, shapes = system.aggregate_shapes(members, labels, max(int(detail_count), 0))
+    # amphiphiles per component: its members that are their amphiphile's head
+    is_head = head_of[members] == members
+    uniq, inv = np.unique(labels, return_inverse=True)
+    size = np.bincount(inv)
+    heads = np.bincount(inv, weights=is_head).astype(np.int64)
+    order = sorted(range(len(uniq)), key=lambda c: (-int(size[c]), int(uniq[c])))
+    hist = [int(heads[c]) for c in order]
+    qual = [h for h in hist if h >= min_amphiphiles_per_aggregate]
+    total = int(n_amph)
+    return {"aggregateCount": int(ncomp), "sizeHistogram": hist, "aggregates": [shape_metrics(s) for s in shapes],
+            "qualifyingAggregateCount": len(qual), "amphiphilesInQualifying": int(sum(qual)),
+            "amphiphileShareInQualifying": (sum(qual) / total) if total > 0 else 0.0}
+
+
 # reference-style names
 areaPerLipid = area_per_lipid
 sumProfiles = sum_profiles
@@ -123,3 +207,5 @@ bilayerPeaks = bilayer_peaks
 bilayerThickness = bilayer_thickness
 hendersonAlpha = henderson_alpha
 apparentPKa = apparent_pka
+symmetricEigenvalues3x3 = symmetric_eigenvalues_3x3
+analyzeAggregates = analyze_aggregates

@@ -287,6 +287,20 @@ class SoupSystem:
             out["escaped"] = int(esc.value)
         return out
 
+    def aggregate_shapes(self, members, labels, max_shapes):
+        """Device shapeOf over unwrapAggregate for the components named by `labels`, largest first:
+        (number of components, [ {size, label, centre, gyration (Sxx Syy Szz Sxy Sxz Syz)} ])."""
+        m = np.ascontiguousarray(members, np.uint32)
+        lab = np.ascontiguousarray(labels, np.uint32)
+        out = (_abi.SoupAggregateShape * max(1, int(max_shapes)))()
+        nc = C.c_uint32()
+        _check(self._lib, self._h, self._lib.soup_aggregate_shapes(
+            self._h, m.ctypes.data_as(_abi._U32P), lab.ctypes.data_as(_abi._U32P), m.size, int(max_shapes), out,
+            C.byref(nc)))
+        k = min(int(max_shapes), int(nc.value))
+        return int(nc.value), [dict(size=out[c].size, label=out[c].label, centre=list(out[c].centre),
+                                    gyration=list(out[c].gyration)) for c in range(k)]
+
     pairingStats = pairing_stats
     densityProfileZ = density_profile_z
 

@@ -64,6 +64,7 @@ def lib(abi):
         "oracle_aggregates": (C.c_uint32, [P, P, C.c_uint32, P, C.c_double, P]),
         "oracle_pairing_stats": (C.c_int, [P, P, C.c_uint32, P, C.c_int, C.c_double, P]),
         "oracle_density_profile_z": (C.c_int, [P, C.c_uint32, C.c_double, C.c_uint32, C.c_uint32, P, P, P]),
+        "oracle_aggregate_shape": (C.c_int, [P, P, C.c_uint32, P, P]),
         "oracle_relax": (C.c_int, [P, C.c_uint32, C.c_double]),
     }
     for name, (res, args) in sig.items():
@@ -294,3 +295,14 @@ def density_profile_z(abi, pos, box_z, bins, head_mask):
     L.oracle_density_profile_z(_ptr(pos), len(pos) // 4, float(box_z), int(bins), int(head_mask), _ptr(head),
                                _ptr(tail), _ptr(esc))
     return head, tail, int(esc[0])
+
+
+def aggregate_shape(abi, pos, members, box):
+    """(n, centre[3], gyration[6]) of one component from the oracle; members ascending."""
+    L = lib(abi)
+    pos = np.ascontiguousarray(pos, np.float32)
+    members = np.ascontiguousarray(np.sort(members), np.uint32)
+    box = np.ascontiguousarray(box, np.float64)
+    out = np.zeros(10, np.float64)
+    L.oracle_aggregate_shape(_ptr(pos), _ptr(members), len(members), _ptr(box), _ptr(out))
+    return int(out[0]), out[1:4].copy(), out[4:10].copy()

@@ -31,11 +31,11 @@ def test_library_exports_every_declared_symbol():
 
 def test_struct_layout_matches_header(tmp_path):
     prog = tmp_path / "layout.c"
-    fields = [(s, f) for s in ("SoupConfig", "SoupInitState", "SoupSweepResult", "SoupClosureResult", "SoupInfo", "SoupPairingStats")
+    fields = [(s, f) for s in ("SoupConfig", "SoupInitState", "SoupSweepResult", "SoupClosureResult", "SoupInfo", "SoupPairingStats", "SoupAggregateShape")
               for f, _ in getattr(_abi, s)._fields_]
     body = "\n".join(f'  printf("{s}.{f} %zu\\n", offsetof({s}, {f}));' for s, f in fields)
     sizes = "\n".join(f'  printf("{s} %zu\\n", sizeof({s}));' for s in
-                      ("SoupConfig", "SoupInitState", "SoupSweepResult", "SoupClosureResult", "SoupInfo", "SoupPairingStats"))
+                      ("SoupConfig", "SoupInitState", "SoupSweepResult", "SoupClosureResult", "SoupInfo", "SoupPairingStats", "SoupAggregateShape"))
     prog.write_text(f'#include <stdio.h>\n#include <stddef.h>\n#include "{HEADER}"\nint main(void) {{\n{body}\n{sizes}\n  return 0;\n}}\n')
     exe = tmp_path / "layout"
     subprocess.run(["gcc", str(prog), "-o", str(exe)], check=True)
@@ -43,7 +43,7 @@ def test_struct_layout_matches_header(tmp_path):
     got = dict(line.rsplit(" ", 1) for line in out if line)
     for s, f in fields:
         assert int(got[f"{s}.{f}"]) == getattr(getattr(_abi, s), f).offset, (s, f)
-    for s in ("SoupConfig", "SoupInitState", "SoupSweepResult", "SoupClosureResult", "SoupInfo", "SoupPairingStats"):
+    for s in ("SoupConfig", "SoupInitState", "SoupSweepResult", "SoupClosureResult", "SoupInfo", "SoupPairingStats", "SoupAggregateShape"):
         assert int(got[s]) == C.sizeof(getattr(_abi, s)), s
 
 

@@ -55,3 +55,38 @@ def test_density_profile_matches_the_oracle():
     d = g.density_profile_z(40, drop_escaped=True)
     assert d["escaped"] == 0
     g.dispose()
+
+
+def test_aggregate_shapes_and_analysis_match_the_oracle():
+    from helpers import boosted, plain_opts
+    opts = plain_opts(box=[15, 15, 15], start={"C": 900, "O": 260, "H": 0, "M": 160, "W": 0})
+    cfg = boosted(cfgm.resolve(opts, P), attempt=0.9, accept=1.0, brk=0.02)
+    o = ob.OracleSystem(_abi, cfg)
+    o.relax(30, 0.1)
+    o.step(400)
+    st = dict(positions=o.read(ob.F_POS), bond_slots=o.read(ob.F_SLOTS), center_link=o.read(ob.F_CENTER))
+    g = SoupSystem(cfg, st)
+    cut = cfgm.wca_cutoff(P["params"]["sigma"] * 1.0) + P["params"]["wc"]
+    res = obs.analyze_aggregates(g, cut, detail_count=5)
+    # the oracle's own labels, amphiphiles and shapes on the same positions
+    polar = np.array([1 if m["polar"] else 0 for m in P["monomers"]] + [0] * (8 - len(P["monomers"])), np.uint32)
+    n_o, head_o = ob.amphiphiles(_abi, st["positions"], st["bond_slots"], polar)
+    members = np.nonzero(head_o != _abi.NONE)[0].astype(np.uint32)
+    nc_o, lab_o = ob.aggregates(_abi, st["positions"], members, cfg.box, cut)
+    assert res["aggregateCount"] == nc_o
+    uniq, inv = np.unique(lab_o, return_inverse=True)
+    size = np.bincount(inv)
+    heads = np.bincount(inv, weights=(head_o[members] == members)).astype(int)
+    order = sorted(range(len(uniq)), key=lambda c: (-int(size[c]), int(uniq[c])))
+    assert res["sizeHistogram"] == [int(heads[c]) for c in order]
+    assert len(res["aggregates"]) == min(5, nc_o)
+    for k, shp in enumerate(res["aggregates"]):
+        c = order[k]
+        n, centre, gy = ob.aggregate_shape(_abi, st["positions"], members[inv == c], cfg.box)
+        assert shp["size"] == n == size[c] and shp["label"] == uniq[c]
+        assert np.allclose(shp["centre"], centre, rtol=1e-12, atol=1e-9)
+        want = obs.shape_metrics({"size": n, "label": int(uniq[c]), "centre": centre, "gyration": list(gy)})
+        assert np.allclose(shp["principalMoments"], want["principalMoments"], rtol=1e-9, atol=1e-9)
+        assert shp["radiusOfGyration"] == pytest.approx(want["radiusOfGyration"], rel=1e-9)
+    assert res["aggregates"][0]["size"] > 20
+    g.dispose()

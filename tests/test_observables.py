@@ -100,3 +100,33 @@ def test_oracle_density_profile_equals_histogram():
     hh = np.histogram(inb[inb[:, 3] == 1, 2], bins=40, range=(0, 20.0))[0]
     tt = np.histogram(inb[inb[:, 3] != 1, 2], bins=40, range=(0, 20.0))[0]
     assert esc == 7 and np.array_equal(head, hh) and np.array_equal(tail, tt)
+
+
+def test_smith_eigenvalues_and_vectors():
+    rng = np.random.default_rng(9)
+    for _ in range(50):
+        a = rng.normal(size=(3, 3))
+        m = a @ a.T
+        g = (m[0, 0], m[1, 1], m[2, 2], m[0, 1], m[0, 2], m[1, 2])
+        lam = obs.symmetric_eigenvalues_3x3(*g)
+        assert np.allclose(lam, np.linalg.eigvalsh(m), rtol=1e-10, atol=1e-12)
+        v = obs.symmetric_eigenvector_3x3(*g, lam[0])
+        assert np.allclose(m @ np.array(v), lam[0] * np.array(v), atol=1e-8)
+    assert obs.symmetric_eigenvalues_3x3(3.0, 1.0, 2.0, 0.0, 0.0, 0.0) == [1.0, 2.0, 3.0]
+    assert obs.symmetric_eigenvector_3x3(1.0, 1.0, 1.0, 0.0, 0.0, 0.0, 1.0) is None   # repeated
+
+
+def test_oracle_shape_of_a_rod_across_the_boundary():
+    # 9 beads 1 sigma apart along x, straddling x = 0 of a 20 sigma box (span 8 < L/2 from any bead):
+    # moments 0, 0, (9^2 - 1)/12
+    box = [20.0] * 3
+    pos = np.zeros((9, 4), np.float32)
+    pos[:, 0] = np.mod(np.arange(9) - 4.0, 20.0)
+    pos[:, 1:3] = 7.0
+    n, centre, g = ob.aggregate_shape(_abi, pos.reshape(-1), np.arange(9), box)
+    m = obs.shape_metrics({"size": n, "label": 0, "centre": centre, "gyration": list(g)})
+    assert n == 9
+    assert m["principalMoments"][2] == pytest.approx(80.0 / 12.0, abs=1e-9)
+    assert m["principalMoments"][0] == pytest.approx(0.0, abs=1e-9)
+    assert m["radiusOfGyration"] == pytest.approx(math.sqrt(80.0 / 12.0))
+    assert m["flatnessRatio"] == pytest.approx(0.0, abs=1e-9)
