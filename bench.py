@@ -248,6 +248,61 @@ def amphiphile_state(L, cfg, na, seed):
                 bond_rng=br, thermo_rng=tr)
 
 
+def bilayer_patch(L, cfgm, lx=32.0, lz=40.0, per_side=32, seed=11, kT=1.0, ph=9.0, ionic=0.01):
+    """A preassembled flat bilayer: per_side^2 five-bead amphiphiles per leaflet on a square lattice
+    spanning lx x lx, heads outward, tails inward, the mid-plane at lz / 2; water at uniform random
+    positions outside the slab |z - lz/2| < 5, to a total density of 0.80.  Bond slots as the
+    reference lays a chain out (see amphiphile_state).  Returns (config, state)."""
+    import ctypes as C
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    na = 2 * per_side * per_side
+    n = int(round(0.80 * lx * lx * lz))
+    nw = n - 5 * na
+    opts = cfgm.SoupOptions(box=[lx, lx, lz], seed=seed, kT=kT, start={"C": 4 * na, "O": na, "H": 0, "M": 0, "W": nw},
+                            electrostatics={"enabled": True, "pH": ph, "ionicStrengthMolar": ionic},
+                            skin=1.0, rebuild_on_drift=True)
+    cfg = cfgm.resolve(opts)
+    pos = np.zeros((n, 4), np.float32)
+    vel = np.zeros(n * 4, np.float32)
+    fr = np.zeros(n, np.uint32); br = np.zeros(n, np.uint32); tr = np.zeros(n, np.uint32)
+    p = lambda a: a.ctypes.data_as(C.c_void_p)
+    L.soup_fresh_state(C.byref(cfg), p(pos), p(vel), p(fr), p(br), p(tr))
+    a = lx / per_side
+    gx, gy = np.meshgrid((np.arange(per_side) + 0.5) * a, (np.arange(per_side) + 0.5) * a, indexing="ij")
+    mid = lz / 2
+    k = 0
+    for side in (1.0, -1.0):
+        for x, y in zip(gx.reshape(-1), gy.reshape(-1)):
+            jitter = rng.normal(scale=0.05, size=2)
+            for b in range(5):   # head at 4.5 from the mid-plane, c1..c4 towards it
+                pos[k * 5 + b, :3] = (x + jitter[0], y + jitter[1], mid + side * (4.5 - 0.95 * b))
+            pos[k * 5:k * 5 + 5, 3] = (1.0, 0.0, 0.0, 0.0, 0.0)
+            k += 1
+    w = []
+    while len(w) < nw:
+        cand = rng.uniform((0, 0, 0), (lx, lx, lz), size=(2 * nw, 3))
+        cand = cand[np.abs(cand[:, 2] - mid) > 5.0]
+        w.extend(cand.tolist())
+    pos[5 * na:, :3] = np.array(w[:nw], np.float32)
+    pos[5 * na:, 3] = 4.0
+    none = 0xFFFFFFFF
+    slots = np.full((n, 3), none, np.uint32)
+    b = 5 * np.arange(na, dtype=np.uint32)
+    slots[b, 0] = b + 1
+    slots[b + 1, 2] = b; slots[b + 1, 0] = b + 2
+    slots[b + 2, 0] = b + 1; slots[b + 2, 1] = b + 3
+    slots[b + 3, 0] = b + 2; slots[b + 3, 1] = b + 4
+    slots[b + 4, 0] = b + 3
+    pos = pos.reshape(-1)
+    charges = np.zeros(n, np.float32)
+    prng = C.c_uint32(0)
+    L.soup_initial_charges(C.byref(cfg), p(pos), p(charges), C.byref(prng))
+    state = dict(positions=pos, velocities=vel, bond_slots=slots.reshape(-1), charges=charges, frozen=fr,
+                 bond_rng=br, thermo_rng=tr)
+    return cfg, state
+
+
 def run_batched(args, pkg, L, cfgm, rank, torch):
     """The batched form: many uneven replicas stepped together, one launch per kernel per step."""
     import ctypes as C

@@ -314,6 +314,31 @@ int soup_aggregate_shapes(SoupHandle* h, const uint32_t* member_idx, const uint3
 int soup_density_profile_z(SoupHandle* h, uint32_t bins, uint32_t head_kind_mask, uint32_t* head_counts,
                            uint32_t* tail_counts, uint32_t* escaped);
 
+/* ---- differentiation ------------------------------------------------------------------------- */
+/* The adjoint of the force + Langevin step.  It has no counterpart in the reference, which only
+ * runs the step forward.  The parameters are SOUP_DIFF_NPARAM numbers, in this order:
+ *   the class-pair attraction depths A[apolar][apolar], A[apolar][polar], A[apolar][solvent],
+ *   A[polar][polar], A[polar][solvent], A[solvent][solvent] (symmetric table, SoupConfig.attr_scale),
+ *   k_fene, k_bend, and kappa = 1 / Debye length.  The electrostatics cutoff and the acid-soap depth
+ *   stay at their values when kappa changes.  Single systems only (not batch replicas). */
+#define SOUP_DIFF_NPARAM 9
+int soup_get_diff_params(SoupHandle* h, double* theta);
+/* Sets the parameters and recomputes the force at the current positions. */
+int soup_set_diff_params(SoupHandle* h, const double* theta);
+/* A differentiable window: `steps` steps from the current state with bond Monte Carlo and the
+ * constant-pH sweep held off (charges and bonds fixed), a checkpoint every `checkpoint_every` steps
+ * (each one re-sorts the particles canonically and recomputes the force, so the reverse pass can
+ * replay a segment bit for bit from it).  traj_device (may be NULL): device memory for steps + 1
+ * frames of n float4 positions in original order (frame 0 the start), 16-byte aligned. */
+int soup_diff_forward(SoupHandle* h, uint32_t steps, uint32_t checkpoint_every, float* traj_device);
+/* The reverse pass of the last soup_diff_forward.  dldx_device: dJ/dx_t for t = 0..steps as steps + 1
+ * frames of n float4 in original order (w ignored), device memory.  theta_grad receives dJ/dtheta
+ * (SOUP_DIFF_NPARAM doubles, host); dx0_device / dv0_device (device, n float4, may be NULL) receive
+ * dJ/dx_0 and dJ/dv_0.  The Langevin noise is fixed by the window's seeds (the adjoint does not depend
+ * on it).  The system is left at the window's end state. */
+int soup_diff_backward(SoupHandle* h, const float* dldx_device, double* theta_grad, float* dx0_device,
+                       float* dv0_device);
+
 /* ---- single phases ------------------------------------------------------------------------- */
 /* One phase of the step on the current device state, so each kernel can be checked in isolation
  * (the reference times phases the same way: stepPhasesDEBUG, soup/src/soup-readback.ts:191-245).

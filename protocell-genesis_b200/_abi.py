@@ -166,6 +166,10 @@ SIGNATURES = {
     "soup_aggregate_labels": (C.c_int, [_P, _U32P, C.c_uint32, C.c_double, _U32P, _U32P]),
     "soup_pairing_stats": (C.c_int, [_P, C.c_double, C.POINTER(SoupPairingStats)]),
     "soup_density_profile_z": (C.c_int, [_P, C.c_uint32, C.c_uint32, _U32P, _U32P, _U32P]),
+    "soup_get_diff_params": (C.c_int, [_P, C.POINTER(C.c_double)]),
+    "soup_set_diff_params": (C.c_int, [_P, C.POINTER(C.c_double)]),
+    "soup_diff_forward": (C.c_int, [_P, C.c_uint32, C.c_uint32, _P]),
+    "soup_diff_backward": (C.c_int, [_P, _P, C.POINTER(C.c_double), _P, _P]),
     "soup_aggregate_shapes": (C.c_int, [_P, _U32P, _U32P, C.c_uint32, C.c_uint32, C.POINTER(SoupAggregateShape),
                                         _U32P]),
     "soup_aggregate_labels_noalloc": (C.c_int, [_P, _U32P, C.c_uint32, C.c_double, _U32P, _U32P]),
@@ -183,6 +187,8 @@ SIGNATURES = {
 }
 
 # soup_kernel_time groups
+DIFF_NPARAM = 9
+
 K_FORCE, K_ES_FAR, K_LIST, K_SORT, K_KICK_DRIFT, K_KICK_THERMO, K_BONDS, K_SWEEP = range(8)
 K_NAMES = ["force", "es_far", "list", "sort", "kick_drift", "kick_thermo", "bonds", "sweep"]
 

@@ -17,7 +17,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC,-ffp-contract=off", "--expt-relaxed-constexpr",
          "-ccbin", "/usr/bin/g++"]
 SOURCES = ["soup_capi.cu", "kernels_grid.cu", "kernels_force.cu", "kernels_step.cu", "kernels_bonds.cu",
-           "kernels_sweep.cu", "kernels_analysis.cu", "kernels_observables.cu", "kernels_noalloc.cu", "host_init.cpp"]
+           "kernels_sweep.cu", "kernels_analysis.cu", "kernels_observables.cu", "kernels_adjoint.cu", "kernels_noalloc.cu", "host_init.cpp"]
 HEADERS = ["soup_internal.h", "soup_common.cuh", os.path.join("..", "..", "include", "soup_b200.h")]
 
 

@@ -416,6 +416,9 @@ void destroy_batch(Batch* b) {
                   b->item_done, b->has_item, b->sweep_out, b->prot_rng_dev, b->sp, b->shared, b->sysid, b->occ,
                   b->vis, b->frontier};
   for (void* p : ptrs) if (p) cudaFree(p);
+  for (void* p : {(void*)b->diff.frames, (void*)b->diff.A, (void*)b->diff.B, (void*)b->diff.g, (void*)b->diff.jg,
+                  (void*)b->diff.frozen_o, (void*)b->diff.partial})
+    if (p) cudaFree(p);
   for (const Batch::Mark& m : b->marks) { cudaEventDestroy(m.a); cudaEventDestroy(m.b); }
   for (cudaEvent_t e : b->event_pool) cudaEventDestroy(e);
   if (b->stream) cudaStreamDestroy(b->stream);
@@ -590,6 +593,49 @@ template <class F> int guarded(SoupHandle* h, F&& f) {
   }
 }
 
+}  // namespace
+
+// ---- differentiation ---------------------------------------------------------------------------
+namespace {
+// one step of the window: the plain step without bond Monte Carlo and without the sweep
+void diff_step(Batch& b) {
+  const SoupConfig& c = b.cfg[0];
+  launch_kick_drift(b);
+  const bool reb = c.rebuild_on_drift ? drift_exceeds(b) : (b.step[0] % c.rebuild_every == 0);
+  if (reb) rebuild(b);
+  launch_force(b);
+  launch_kick_thermo(b);
+  b.step[0]++;
+}
+void diff_read(Batch& b, std::vector<float>& pos, std::vector<float>& vel, std::vector<uint32_t>& trng) {
+  const uint32_t n = b.cfg[0].n;
+  pos.resize(4 * (size_t)n); vel.resize(4 * (size_t)n); trng.resize(n);
+  read_replica<float>(b, 0, reinterpret_cast<const float*>(b.pos), 4, pos.data(), false);
+  read_replica<float>(b, 0, reinterpret_cast<const float*>(b.vel), 4, vel.data(), false);
+  read_replica<uint32_t>(b, 0, b.trng, 1, trng.data(), false);
+}
+// the canonical state at a checkpoint: identity order, then the re-sort and force pass of a restore
+void diff_restore(Batch& b, const std::vector<float>& pos, const std::vector<float>& vel,
+                  const std::vector<uint32_t>& trng) {
+  DiffWindow& w = b.diff;
+  SoupInitState m{};
+  m.positions = pos.data(); m.velocities = vel.data(); m.thermo_rng = trng.data();
+  m.bond_slots = w.slots.data(); m.center_link = w.center.data(); m.center_held = w.held.data();
+  m.bond_rng = w.brng.data(); m.charges = w.charge.data(); m.frozen = w.frozen.data();
+  const uint32_t prot = b.prot_rng[0];
+  upload_replica(b, 0, &m, false);
+  b.prot_rng[0] = prot;
+  force_pass(b);
+}
+template <class T> T* dgrow(T* p, size_t& cap, size_t want) {
+  if (want <= cap) return p;
+  if (p) cudaFree(p);
+  T* q = nullptr;
+  SOUP_CUDA_TRY(cudaMalloc(&q, sizeof(T) * want));
+  cap = want;
+  return q;
+}
+constexpr int kDepthPairs[6][2] = {{0, 0}, {0, 1}, {0, 2}, {1, 1}, {1, 2}, {2, 2}};
 }  // namespace
 
 extern "C" {
@@ -905,6 +951,141 @@ int soup_amphiphile_labels(SoupHandle* h, uint32_t* head_of, uint32_t* n_out) {
     std::string err;
     int st = run_amphiphiles(b, r, head_of, n_out, err);
     if (st) fail(st, err);
+  });
+}
+
+
+int soup_get_diff_params(SoupHandle* h, double* theta) {
+  return guarded(h, [&](Batch& b, uint32_t r) {
+    if (!theta) fail(SOUP_E_ARG, "NULL theta");
+    const SoupConfig& c = b.cfg[r];
+    for (int p = 0; p < 6; ++p) theta[p] = c.attr_scale[kDepthPairs[p][0]][kDepthPairs[p][1]];
+    theta[6] = c.k_fene; theta[7] = c.k_bend; theta[8] = c.es_kappa;
+  });
+}
+
+int soup_set_diff_params(SoupHandle* h, const double* theta) {
+  return guarded(h, [&](Batch& b, uint32_t r) {
+    if (!theta) fail(SOUP_E_ARG, "NULL theta");
+    if (b.R != 1) fail(SOUP_E_STATE, "differentiation works on single systems, not batch replicas");
+    for (int p = 0; p < SOUP_DIFF_NPARAM; ++p) if (!std::isfinite(theta[p])) fail(SOUP_E_ARG, "theta must be finite");
+    if (!(theta[6] > 0) || !(theta[7] > 0) || !(theta[8] > 0)) fail(SOUP_E_ARG, "k_fene, k_bend and kappa must be positive");
+    SoupConfig& c = b.cfg[r];
+    for (int p = 0; p < 6; ++p) {
+      c.attr_scale[kDepthPairs[p][0]][kDepthPairs[p][1]] = theta[p];
+      c.attr_scale[kDepthPairs[p][1]][kDepthPairs[p][0]] = theta[p];
+    }
+    c.k_fene = theta[6]; c.k_bend = theta[7]; c.es_kappa = theta[8];
+    if (c.es_enabled) {
+      c.es_shift_u = c.es_coeff_a * std::exp(-c.es_kappa * c.es_cutoff) / c.es_cutoff;
+      c.es_shift_f = c.es_shift_u * (1 / c.es_cutoff + c.es_kappa);
+    }
+    b.hs = make_shared(c);
+    SysParams& P = b.hsp[r];
+    P.es_kappa = (float)c.es_kappa; P.es_fc = (float)c.es_shift_f;
+    P.d_kappa = c.es_kappa; P.d_shiftU = c.es_shift_u; P.d_shiftF = c.es_shift_f;
+    upload_params(b);
+    launch_force(b);
+    SOUP_CUDA_TRY(cudaStreamSynchronize(b.stream));
+  });
+}
+
+int soup_diff_forward(SoupHandle* h, uint32_t steps, uint32_t checkpoint_every, float* traj_device) {
+  return guarded(h, [&](Batch& b, uint32_t) {
+    if (b.R != 1) fail(SOUP_E_STATE, "differentiation works on single systems, not batch replicas");
+    if (steps == 0 || checkpoint_every == 0) fail(SOUP_E_ARG, "steps and checkpoint_every must be positive");
+    if (traj_device && (reinterpret_cast<uintptr_t>(traj_device) & 15u)) fail(SOUP_E_ARG, "traj_device must be 16-byte aligned");
+    DiffWindow& w = b.diff;
+    const uint32_t n = b.cfg[0].n;
+    w.ready = false;
+    w.charge.resize(n); w.slots.resize(3 * (size_t)n); w.center.resize(n); w.held.resize(n); w.brng.resize(n);
+    std::vector<uint8_t> fr(n);
+    read_replica<float>(b, 0, b.charge, 1, w.charge.data(), false);
+    read_replica<uint32_t>(b, 0, b.slots, 3, w.slots.data(), true);
+    read_replica<uint32_t>(b, 0, b.center, 1, w.center.data(), true);
+    read_replica<uint32_t>(b, 0, b.held, 1, w.held.data(), false);
+    read_replica<uint32_t>(b, 0, b.brng, 1, w.brng.data(), false);
+    read_replica<uint8_t>(b, 0, b.frozen, 1, fr.data(), false);
+    w.frozen.assign(fr.begin(), fr.end());
+    w.steps = steps; w.every = checkpoint_every; w.step0 = b.step[0]; w.prot_rng = b.prot_rng[0];
+    w.ck_pos.clear(); w.ck_vel.clear(); w.ck_trng.clear();
+    float4* traj = reinterpret_cast<float4*>(traj_device);
+    for (uint32_t t = 0; t < steps; ++t) {
+      if (t % checkpoint_every == 0) {
+        w.ck_pos.emplace_back(); w.ck_vel.emplace_back(); w.ck_trng.emplace_back();
+        diff_read(b, w.ck_pos.back(), w.ck_vel.back(), w.ck_trng.back());
+        diff_restore(b, w.ck_pos.back(), w.ck_vel.back(), w.ck_trng.back());
+        if (t == 0 && traj) adj_unpermute(b, traj);
+      }
+      diff_step(b);
+      if (traj) adj_unpermute(b, traj + (size_t)(t + 1) * n);
+    }
+    diff_read(b, w.end_pos, w.end_vel, w.end_trng);
+    w.end_step = b.step[0];
+    guards(b, w.step0);
+    w.ready = true;
+  });
+}
+
+int soup_diff_backward(SoupHandle* h, const float* dldx_device, double* theta_grad, float* dx0_device,
+                       float* dv0_device) {
+  return guarded(h, [&](Batch& b, uint32_t) {
+    DiffWindow& w = b.diff;
+    if (!w.ready) fail(SOUP_E_STATE, "no differentiable window: call soup_diff_forward first");
+    if (!dldx_device || !theta_grad) fail(SOUP_E_ARG, "NULL argument");
+    const uint32_t n = b.cfg[0].n, T = w.steps, K = w.every;
+    const float4* dldx = reinterpret_cast<const float4*>(dldx_device);
+    // scratch
+    size_t cap1 = w.frames_cap;
+    w.frames = dgrow(w.frames, cap1, (size_t)(K + 1) * n);
+    w.frames_cap = cap1;
+    if (!w.A) {
+      SOUP_CUDA_TRY(cudaMalloc(&w.A, 16 * (size_t)n)); SOUP_CUDA_TRY(cudaMalloc(&w.B, 16 * (size_t)n));
+      SOUP_CUDA_TRY(cudaMalloc(&w.g, 16 * (size_t)n)); SOUP_CUDA_TRY(cudaMalloc(&w.jg, 16 * (size_t)n));
+      SOUP_CUDA_TRY(cudaMalloc(&w.frozen_o, (size_t)n));
+    }
+    size_t cap2 = w.partial_cap;
+    w.partial = dgrow(w.partial, cap2, adj_partial_count(b));
+    w.partial_cap = cap2;
+    std::vector<uint8_t> fo(w.frozen.begin(), w.frozen.end());
+    SOUP_CUDA_TRY(cudaMemcpyAsync(w.frozen_o, fo.data(), n, cudaMemcpyHostToDevice, b.stream));
+    SOUP_CUDA_TRY(cudaMemcpyAsync(w.A, dldx + (size_t)T * n, 16 * (size_t)n, cudaMemcpyDeviceToDevice, b.stream));
+    SOUP_CUDA_TRY(cudaMemsetAsync(w.B, 0, 16 * (size_t)n, b.stream));
+    SOUP_CUDA_TRY(cudaMemsetAsync(w.g, 0, 16 * (size_t)n, b.stream));
+    const SysParams& P = b.hsp[0];
+    const float a = 1.0f - P.gdt, hh = P.hdt, dt = P.dt;
+    double theta[SOUP_DIFF_NPARAM] = {0};
+    std::vector<double> host;
+    const uint32_t nseg = (T + K - 1) / K;
+    for (uint32_t seg = nseg; seg-- > 0;) {
+      const uint32_t t0 = seg * K, t1 = std::min(t0 + K, T);
+      b.step[0] = w.step0 + t0;
+      diff_restore(b, w.ck_pos[seg], w.ck_vel[seg], w.ck_trng[seg]);
+      adj_unpermute(b, w.frames);
+      for (uint32_t k = 0; k < t1 - t0; ++k) {
+        diff_step(b);
+        adj_unpermute(b, w.frames + (size_t)(k + 1) * n);
+      }
+      for (uint32_t t = t1; t > t0; --t) {
+        adj_scatter_pos(b, w.frames + (size_t)(t - t0) * n);
+        rebuild(b);
+        adj_hvp(b, w.g, w.jg, theta, w.partial, host);
+        const float coef = (t - 1 == 0) ? hh : hh * (1.0f + a);
+        adj_update(b, n, w.A, w.B, w.jg, dldx + (size_t)(t - 1) * n, w.frozen_o, a, dt, coef, w.g, nullptr);
+      }
+      if (seg == 0) {   // time 0: the force at x_0 only feeds the first half kick
+        if (dv0_device) SOUP_CUDA_TRY(cudaMemcpyAsync(dv0_device, w.B, 16 * (size_t)n, cudaMemcpyDeviceToDevice, b.stream));
+        adj_scatter_pos(b, w.frames);
+        rebuild(b);
+        adj_hvp(b, w.g, w.jg, theta, w.partial, host);
+        adj_update(b, n, w.A, w.B, w.jg, nullptr, w.frozen_o, a, dt, 0.f, w.g, reinterpret_cast<float4*>(dx0_device));
+      }
+    }
+    // back to the end of the window
+    b.step[0] = w.end_step;
+    diff_restore(b, w.end_pos, w.end_vel, w.end_trng);
+    SOUP_CUDA_TRY(cudaStreamSynchronize(b.stream));
+    for (int p = 0; p < SOUP_DIFF_NPARAM; ++p) theta_grad[p] = theta[p];
   });
 }
 

@@ -35,6 +35,26 @@ template <class T> struct DevBuf {
   size_t n = 0;
 };
 
+// The state of one differentiable window (soup_diff_forward / soup_diff_backward): checkpoints in
+// original order, the arrays that stay constant inside the window, and the reverse-pass scratch.
+struct DiffWindow {
+  uint32_t steps = 0, every = 0;
+  uint64_t step0 = 0;
+  bool ready = false;
+  std::vector<std::vector<float>> ck_pos, ck_vel;
+  std::vector<std::vector<uint32_t>> ck_trng;
+  std::vector<float> charge;
+  std::vector<uint32_t> slots, center, held, brng, frozen;
+  std::vector<float> end_pos, end_vel;
+  std::vector<uint32_t> end_trng;
+  uint64_t end_step = 0;
+  uint32_t prot_rng = 0;
+  float4 *frames = nullptr, *A = nullptr, *B = nullptr, *g = nullptr, *jg = nullptr;
+  uint8_t* frozen_o = nullptr;
+  double* partial = nullptr;
+  size_t frames_cap = 0, partial_cap = 0;
+};
+
 struct Batch {
   int device = 0;
   cudaStream_t stream = nullptr;
@@ -117,6 +137,7 @@ struct Batch {
   uint64_t rebuilds = 0, sweeps = 0;
   bool force_fresh = false;          // force array matches positions+charges+lists
   int tpp = 4;                       // threads per particle in the list force
+  DiffWindow diff;
   std::string err;
   std::vector<SoupHandle*> views;    // per-replica handle views
 
@@ -164,6 +185,12 @@ void launch_nonfinite(Batch& b);
 void launch_relax_step(Batch& b, float d);
 void launch_bonds(Batch& b);
 void launch_sweep(Batch& b, uint32_t replica);
+void adj_unpermute(Batch& b, float4* dst);
+void adj_scatter_pos(Batch& b, const float4* src);
+void adj_hvp(Batch& b, const float4* g, float4* jg, double* theta, double* partial_dev, std::vector<double>& host);
+size_t adj_partial_count(const Batch& b);
+void adj_update(Batch& b, uint32_t n, float4* A, float4* B, const float4* jg, const float4* ldx, const uint8_t* frozen_o,
+                float a, float dt, float coef, float4* g, float4* xout);
 void sweep_prepare(Batch& b);
 void launch_rebuild_check(Batch& b);
 // analysis

@@ -301,6 +301,28 @@ class SoupSystem:
         return int(nc.value), [dict(size=out[c].size, label=out[c].label, centre=list(out[c].centre),
                                     gyration=list(out[c].gyration)) for c in range(k)]
 
+    # ---- differentiation (the adjoint of the step; no counterpart in the reference) ----
+    def get_diff_params(self):
+        t = (C.c_double * _abi.DIFF_NPARAM)()
+        _check(self._lib, self._h, self._lib.soup_get_diff_params(self._h, t))
+        return np.array(list(t), np.float64)
+
+    def set_diff_params(self, theta):
+        t = (C.c_double * _abi.DIFF_NPARAM)(*[float(v) for v in theta])
+        _check(self._lib, self._h, self._lib.soup_set_diff_params(self._h, t))
+
+    def diff_forward(self, steps, checkpoint_every, traj_ptr=None):
+        """Differentiable window from the current state; traj_ptr: device pointer for steps + 1 frames."""
+        _check(self._lib, self._h, self._lib.soup_diff_forward(self._h, int(steps), int(checkpoint_every),
+                                                               C.c_void_p(traj_ptr) if traj_ptr else None))
+
+    def diff_backward(self, dldx_ptr, dx0_ptr=None, dv0_ptr=None):
+        t = (C.c_double * _abi.DIFF_NPARAM)()
+        _check(self._lib, self._h, self._lib.soup_diff_backward(
+            self._h, C.c_void_p(dldx_ptr), t, C.c_void_p(dx0_ptr) if dx0_ptr else None,
+            C.c_void_p(dv0_ptr) if dv0_ptr else None))
+        return np.array(list(t), np.float64)
+
     pairingStats = pairing_stats
     densityProfileZ = density_profile_z
 

@@ -65,3 +65,20 @@ def rel_rms(a, b):
 def csr_rows(counts, lists):
     off = np.concatenate([[0], np.cumsum(counts.astype(np.int64))])
     return [lists[off[i]:off[i + 1]] for i in range(len(counts))]
+
+
+def oracle_bilayer_start(lx=15.0, lz=16.0, per_side=10, seed=3, relax=200, steps=100):
+    """A small preassembled bilayer patch (the differentiable-patch workload at lx x lx x lz),
+    relaxed and stepped on the oracle: (config, start state with every field of a checkpoint)."""
+    import bench
+    import oracle_binding as ob
+    cfg, st = bench.bilayer_patch(_abi.lib(), cfgm, lx=lx, lz=lz, per_side=per_side, seed=seed)
+    o = ob.OracleSystem(_abi, cfg, st)
+    o.relax(relax, 0.05)
+    if steps:
+        o.step(steps)
+    start = dict(positions=o.read(ob.F_POS), velocities=o.read(ob.F_VEL), bond_slots=o.read(ob.F_SLOTS),
+                 center_link=o.read(ob.F_CENTER), center_held=o.read(ob.F_HELD), bond_rng=o.read(ob.F_BOND_RNG),
+                 thermo_rng=o.read(ob.F_THERMO_RNG), charges=o.read(ob.F_CHARGES), frozen=o.read(ob.F_FROZEN))
+    o.close()
+    return cfg, start
