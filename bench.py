@@ -340,6 +340,66 @@ def run_batched(args, pkg, L, cfgm, rank, torch):
                         "20, skin 1.0 with drift rebuilds; seeded synthetic, relaxed untimed"}
 
 
+def run_gradient(args, pkg, L, torch):
+    """The differentiable bilayer patch: forward + adjoint of the thickness proxy over a 200-step
+    window (checkpoints every 20) with respect to the nine force-field parameters."""
+    import numpy as np
+    from protocell_genesis_b200 import adjoint, config as cfgm
+    cfg, st = bilayer_patch(L, cfgm)
+    s = pkg.SoupSystem(cfg, st)
+    s.relax_cold_start(args.relax, 0.05)
+    s.step(200)
+    p = s.particles().reshape(-1, 4)
+    slots = s.bond_slots().reshape(-1, 3)
+    heads = torch.tensor(np.nonzero(p[:, 3] == 1)[0], device="cuda")
+    tails = torch.tensor(np.nonzero((p[:, 3] == 0) & np.any(slots != 0xFFFFFFFF, axis=1))[0], device="cuda")
+    bz = float(cfg.box[2])
+    steps, every = args.grad_steps, 20
+    stream = torch.cuda.ExternalStream(L.soup_stream(s._h))
+    theta0 = s.get_diff_params()
+
+    def window():
+        th = torch.tensor(theta0, dtype=torch.float64, requires_grad=True)
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        torch.cuda.synchronize()
+        e0.record(stream)
+        traj = adjoint.SoupWindow.apply(th, s, steps, every)
+        e1.record(stream)
+        loss = adjoint.thickness_proxy(traj, heads, tails, bz)
+        loss.backward()
+        e2.record(stream)
+        torch.cuda.synchronize()
+        return float(loss.detach()), th.grad.numpy(), e0.elapsed_time(e1), e1.elapsed_time(e2)
+
+    window()                                  # untimed: allocates the window's scratch
+    launches0 = L.soup_launch_count(s._h)
+    fwd, bwd = [], []
+    for _ in range(args.grad_windows):
+        loss, grad, f_ms, b_ms = window()
+        fwd.append(f_ms)
+        bwd.append(b_ms)
+    launches = L.soup_launch_count(s._h) - launches0
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    s.step(steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    plain_ms = e0.elapsed_time(e1)
+    n = int(cfg.n)
+    s.dispose()
+    total = (sum(fwd) + sum(bwd)) / len(fwd)
+    return {"value": n * steps / (total / 1e3), "unit": "particle-steps/s (forward + adjoint)",
+            "beads": n, "window_steps": steps, "checkpoint_every": every, "windows": len(fwd),
+            "ms_per_window": total, "forward_ms": sum(fwd) / len(fwd), "backward_ms": sum(bwd) / len(bwd),
+            "plain_step_ms": plain_ms / steps, "window_vs_plain_steps": total / plain_ms,
+            "gpu_launches": int(launches), "loss": "thickness proxy", "value_of_loss": loss,
+            "theta": list(adjoint.PARAM_NAMES), "grad": [float(x) for x in grad],
+            "workload": "preassembled flat bilayer, 2,048 five-bead amphiphiles, water to density 0.80, box "
+                        "32x32x40 sigma, pH 9, I 0.01 M; seeded synthetic, relaxed untimed; bond and charge "
+                        "Monte Carlo held off inside the window"}
+
+
 def run_cuda(args):
     import ctypes as C
     import numpy as np
@@ -466,6 +526,14 @@ def run_cuda(args):
             batched["value"] = aggregate_rate(1, batched["beads"], 1, batched["ms_per_step"])
         batched["vs_plain"] = batched["value"] / value
 
+    gradient = None
+    if not args.no_gradient:
+        gradient = run_gradient(args, pkg, L, torch)
+        if dist:
+            gradient["ms_per_window"] = max_over_ranks(gradient["ms_per_window"], dist, "cuda")
+            gradient["value"] = aggregate_rate(ws, gradient["beads"], gradient["window_steps"],
+                                               gradient["ms_per_window"])
+
     phases = {name: {"ms_total": t, "launches": c, "ms_per_step": t / args.steps} for name, (t, c) in ktime.items() if c}
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
@@ -477,7 +545,7 @@ def run_cuda(args):
                        "sweeps_in_timed_region": info1["sweeps"] - info0["sweeps"],
                        "tpp": int(os.environ.get("SOUP_TPP", 4))},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
-            "clocks": clk.summary(), "phases": phases, "batched": batched}
+            "clocks": clk.summary(), "phases": phases, "batched": batched, "gradient": gradient}
     if rank == 0:
         print(json.dumps(line), flush=True)
     s.dispose()
@@ -502,6 +570,9 @@ def main():
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-replica measurement")
     ap.add_argument("--replicas", type=int, default=64)
     ap.add_argument("--batched-steps", type=int, default=100)
+    ap.add_argument("--no-gradient", action="store_true", help="skip the forward + adjoint window measurement")
+    ap.add_argument("--grad-steps", type=int, default=200)
+    ap.add_argument("--grad-windows", type=int, default=3)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

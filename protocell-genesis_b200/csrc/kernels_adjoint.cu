@@ -133,7 +133,7 @@ __device__ __forceinline__ void block_theta(const ThetaAcc& th, double* __restri
   if (threadIdx.x < SOUP_DIFF_NPARAM) {
     double v = 0.0;
     for (int k = 0; k < (int)(blockDim.x / 32); ++k) v += red[k][threadIdx.x];
-    partial[(size_t)blockIdx.x * SOUP_DIFF_NPARAM + threadIdx.x] = v;
+    partial[(size_t)blockIdx.x * SOUP_DIFF_NPARAM + threadIdx.x] += v;   // this block's running sum over steps
   }
 }
 
@@ -317,9 +317,10 @@ void adj_scatter_pos(Batch& b, const float4* src) {
   k_scatter_pos<<<nblocks(b.N), kBlock, 0, b.stream>>>(src, b.slot_of, b.N, b.pos);
 }
 
-// (J g) at the device's current positions and lists, into jg (original order), and the parameter
-// partials added to theta (summed on the host in block order, so the result is deterministic)
-void adj_hvp(Batch& b, const float4* g, float4* jg, double* theta, double* partial_dev, std::vector<double>& host) {
+// (J g) at the device's current positions and lists, into jg (original order); the parameter
+// partials are added to each block's running sums in partial_dev (zeroed by the caller before the
+// first step, summed by adj_theta_sum after the last), so the reverse pass never waits on the host
+void adj_hvp(Batch& b, const float4* g, float4* jg, double* partial_dev) {
   const unsigned g1 = nblocks((uint64_t)b.N * kTpp, kBlock);
   const unsigned g2 = b.H ? nblocks((uint64_t)b.H * 32, kBlock) : 0;
   b.launches += 1 + (g2 ? 1 : 0);
@@ -328,11 +329,14 @@ void adj_hvp(Batch& b, const float4* g, float4* jg, double* theta, double* parti
   if (g2)
     k_hvp_far<<<g2, kBlock, 0, b.stream>>>(b.sp, b.head_slot, b.head_sys, b.H, b.pos, b.charge, b.id, b.es_nl,
                                            b.es_cnt, b.es_cap, g, jg, partial_dev + (size_t)g1 * SOUP_DIFF_NPARAM);
-  const size_t np = (size_t)(g1 + g2) * SOUP_DIFF_NPARAM;
-  host.resize(np);
+}
+// theta += the blocks' sums, in block order (deterministic)
+void adj_theta_sum(Batch& b, const double* partial_dev, double* theta) {
+  const size_t np = adj_partial_count(b);
+  std::vector<double> host(np);
   SOUP_CUDA_TRY(cudaMemcpyAsync(host.data(), partial_dev, 8 * np, cudaMemcpyDeviceToHost, b.stream));
   SOUP_CUDA_TRY(cudaStreamSynchronize(b.stream));
-  for (size_t k = 0; k < (size_t)(g1 + g2); ++k)
+  for (size_t k = 0; k < np / SOUP_DIFF_NPARAM; ++k)
     for (int p = 0; p < SOUP_DIFF_NPARAM; ++p) theta[p] += host[k * SOUP_DIFF_NPARAM + p];
 }
 size_t adj_partial_count(const Batch& b) {

@@ -1047,6 +1047,7 @@ int soup_diff_backward(SoupHandle* h, const float* dldx_device, double* theta_gr
     size_t cap2 = w.partial_cap;
     w.partial = dgrow(w.partial, cap2, adj_partial_count(b));
     w.partial_cap = cap2;
+    SOUP_CUDA_TRY(cudaMemsetAsync(w.partial, 0, 8 * adj_partial_count(b), b.stream));
     std::vector<uint8_t> fo(w.frozen.begin(), w.frozen.end());
     SOUP_CUDA_TRY(cudaMemcpyAsync(w.frozen_o, fo.data(), n, cudaMemcpyHostToDevice, b.stream));
     SOUP_CUDA_TRY(cudaMemcpyAsync(w.A, dldx + (size_t)T * n, 16 * (size_t)n, cudaMemcpyDeviceToDevice, b.stream));
@@ -1055,7 +1056,6 @@ int soup_diff_backward(SoupHandle* h, const float* dldx_device, double* theta_gr
     const SysParams& P = b.hsp[0];
     const float a = 1.0f - P.gdt, hh = P.hdt, dt = P.dt;
     double theta[SOUP_DIFF_NPARAM] = {0};
-    std::vector<double> host;
     const uint32_t nseg = (T + K - 1) / K;
     for (uint32_t seg = nseg; seg-- > 0;) {
       const uint32_t t0 = seg * K, t1 = std::min(t0 + K, T);
@@ -1069,7 +1069,7 @@ int soup_diff_backward(SoupHandle* h, const float* dldx_device, double* theta_gr
       for (uint32_t t = t1; t > t0; --t) {
         adj_scatter_pos(b, w.frames + (size_t)(t - t0) * n);
         rebuild(b);
-        adj_hvp(b, w.g, w.jg, theta, w.partial, host);
+        adj_hvp(b, w.g, w.jg, w.partial);
         const float coef = (t - 1 == 0) ? hh : hh * (1.0f + a);
         adj_update(b, n, w.A, w.B, w.jg, dldx + (size_t)(t - 1) * n, w.frozen_o, a, dt, coef, w.g, nullptr);
       }
@@ -1077,12 +1077,13 @@ int soup_diff_backward(SoupHandle* h, const float* dldx_device, double* theta_gr
         if (dv0_device) SOUP_CUDA_TRY(cudaMemcpyAsync(dv0_device, w.B, 16 * (size_t)n, cudaMemcpyDeviceToDevice, b.stream));
         adj_scatter_pos(b, w.frames);
         rebuild(b);
-        adj_hvp(b, w.g, w.jg, theta, w.partial, host);
+        adj_hvp(b, w.g, w.jg, w.partial);
         adj_update(b, n, w.A, w.B, w.jg, nullptr, w.frozen_o, a, dt, 0.f, w.g, reinterpret_cast<float4*>(dx0_device));
       }
     }
     // back to the end of the window
     b.step[0] = w.end_step;
+    adj_theta_sum(b, w.partial, theta);
     diff_restore(b, w.end_pos, w.end_vel, w.end_trng);
     SOUP_CUDA_TRY(cudaStreamSynchronize(b.stream));
     for (int p = 0; p < SOUP_DIFF_NPARAM; ++p) theta_grad[p] = theta[p];

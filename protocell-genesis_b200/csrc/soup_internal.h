@@ -187,7 +187,8 @@ void launch_bonds(Batch& b);
 void launch_sweep(Batch& b, uint32_t replica);
 void adj_unpermute(Batch& b, float4* dst);
 void adj_scatter_pos(Batch& b, const float4* src);
-void adj_hvp(Batch& b, const float4* g, float4* jg, double* theta, double* partial_dev, std::vector<double>& host);
+void adj_hvp(Batch& b, const float4* g, float4* jg, double* partial_dev);
+void adj_theta_sum(Batch& b, const double* partial_dev, double* theta);
 size_t adj_partial_count(const Batch& b);
 void adj_update(Batch& b, uint32_t n, float4* A, float4* B, const float4* jg, const float4* ldx, const uint8_t* frozen_o,
                 float a, float dt, float coef, float4* g, float4* xout);
