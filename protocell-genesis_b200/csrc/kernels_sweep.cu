@@ -26,6 +26,9 @@
 // Arithmetic is FP64 with JavaScript rounding of the minimum image, as the reference's.
 #include "soup_internal.h"
 
+#include <cooperative_groups.h>
+namespace cg = cooperative_groups;
+
 namespace soup {
 
 namespace {
@@ -169,22 +172,79 @@ __device__ __forceinline__ double pcg_out(uint32_t v) {
 
 constexpr int kWalkThreads = 512;
 constexpr int kUpd = 8;
-constexpr uint32_t kQueue = 512;
+constexpr uint32_t kBand = 64;    // a band row: one draw's changes on the sites of the next 63 draws
+constexpr uint32_t kRing = 64;    // band rows the walk keeps in shared memory
+constexpr int kWalkSmemMax = 224 * 1024;   // the ring, the energies and the charge states
+
+// Replica r's band rows and draw sites start at these offsets: a sweep consumes at most 2 H draws
+// (an attempt takes a site draw and at most one acceptance draw) and a window reads kBand rows ahead.
+__device__ __forceinline__ size_t band_row0(const SysParams& P, uint32_t r) {
+  return 2 * (size_t)P.head_off + (size_t)kBand * r;
+}
+__device__ __forceinline__ size_t draw_site0(const SysParams& P, uint32_t r) {
+  return 2 * (size_t)P.head_off + 2 * (size_t)kBand * r;
+}
+__device__ __forceinline__ uint32_t site_of(double u, uint32_t H) {
+  return (uint32_t)fmin((double)(H - 1), floor(u * (double)H));
+}
+
+// the site every draw of the sweep's stream selects when it is a site draw (all SMs)
+__global__ void k_sweep_draws(const SysParams* __restrict__ sp, const uint32_t* __restrict__ rng_io, uint32_t only,
+                              uint32_t* __restrict__ draw_site) {
+  const uint32_t r = only == SOUP_NONE_U32 ? blockIdx.y : only;
+  const SysParams& P = sp[r];
+  const uint32_t H = P.nheads;
+  if (H == 0 || !P.es_on) return;
+  const uint32_t d = blockIdx.x * blockDim.x + threadIdx.x;
+  if (d >= 2 * H + 2 * kBand) return;
+  const Lcg j = lcg_pow(d + 1u);
+  draw_site[draw_site0(P, r) + d] = site_of(pcg_out(j.a * rng_io[r] + j.c), H);
+}
+
+// band[d][k] (k = 1..63): the change of draw d+k's site energy when draw d's site deprotonates
+// (std_delta, the value the D rows hold), or kSameSite when both draws select one site.  Positions
+// are fixed during a sweep, so the whole band is known before the walk starts.
+__global__ void k_sweep_band(const SysParams* __restrict__ sp, const float4* __restrict__ hpos,
+                             const uint32_t* __restrict__ draw_site, uint32_t only, long long* __restrict__ band) {
+  const uint32_t r = only == SOUP_NONE_U32 ? blockIdx.y : only;
+  const SysParams& P = sp[r];
+  const uint32_t H = P.nheads;
+  if (H == 0 || !P.es_on) return;
+  const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t row = (uint32_t)(t / kBand), k = (uint32_t)(t % kBand);
+  if (row >= 2 * H + kBand) return;
+  long long m = 0;
+  if (k != 0) {
+    const uint32_t* ds = draw_site + draw_site0(P, r);
+    const uint32_t a = ds[row], c = ds[row + k];
+    if (a == c) {
+      m = kSameSite;
+    } else {
+      const float4 pa = hpos[P.head_off + a], pc = hpos[P.head_off + c];
+      const double cut2 = P.d_rc * P.d_rc, reach = P.d_rcattr + P.d_wc, reach2 = reach * reach;
+      // pairs beyond both cutoffs change nothing; the FP32 screen keeps a wide margin
+      const float nr = (float)(fmax(P.d_rc, reach) * 1.001 + 1e-3);
+      float dx = pc.x - pa.x, dy = pc.y - pa.y, dz = pc.z - pa.z;
+      dx -= rintf(dx * P.inv_box[0]) * P.box[0];
+      dy -= rintf(dy * P.inv_box[1]) * P.box[1];
+      dz -= rintf(dz * P.inv_box[2]) * P.box[2];
+      if (dx * dx + dy * dy + dz * dz < nr * nr) m = std_delta(P, dist2(P, pa, pc), (float)P.d_q, cut2, reach2);
+    }
+  }
+  band[(band_row0(P, r) + row) * kBand + k] = m;
+}
 
 // one draw of the stream as a lane holds it: the LCG state that produced it, the draw, the site it
-// selects when it is a site draw, that site's position and its head-list length
+// selects when it is a site draw and that site's head-list length
 struct Draw {
   uint32_t st, site, cnt;
   double u;
-  float x, y, z;
 };
 __device__ __forceinline__ void draw_from(Draw& d, uint32_t st, uint32_t H, uint32_t off,
-                                          const float4* __restrict__ hpos, const uint32_t* __restrict__ es_cnt) {
+                                          const uint32_t* __restrict__ es_cnt) {
   d.st = st;
   d.u = pcg_out(st);
-  d.site = (uint32_t)fmin((double)(H - 1), floor(d.u * (double)H));
-  const float4 p = hpos[off + d.site];
-  d.x = p.x; d.y = p.y; d.z = p.z;
+  d.site = site_of(d.u, H);
   d.cnt = es_cnt[off + d.site];
 }
 __device__ __forceinline__ Draw shfl_draw(const Draw& d, int src) {
@@ -193,9 +253,6 @@ __device__ __forceinline__ Draw shfl_draw(const Draw& d, int src) {
   o.site = __shfl_sync(0xffffffffu, d.site, src);
   o.cnt = __shfl_sync(0xffffffffu, d.cnt, src);
   o.u = __shfl_sync(0xffffffffu, d.u, src);
-  o.x = __shfl_sync(0xffffffffu, d.x, src);
-  o.y = __shfl_sync(0xffffffffu, d.y, src);
-  o.z = __shfl_sync(0xffffffffu, d.z, src);
   return o;
 }
 
@@ -203,68 +260,32 @@ __device__ __forceinline__ Draw shfl_draw(const Draw& d, int src) {
 // corrections the next window's lanes take before E has them
 struct Flips {
   uint32_t site[32];
+  uint32_t draw[32];     // the flip's draw in the sweep's stream
   uint32_t start[33];    // prefix of the flipped heads' list lengths; ~0 above the last flip
   float qo[32], qn[32];
-  float x[32], y[32], z[32];
   int sign[32];          // +1 deprotonated, -1 protonated, 0 the old charge was another value
   uint32_t n;
 };
-// the sites and positions of a window's 32 draws, the pair changes between them
-// (M[k][q], k < q: D of draw k's site on draw q's site, the exact value its D row holds, or
-// kSameSite when both draws select one site) and the previous window's flips summed per draw
-struct Window {
-  uint32_t site[32];
-  float x[32], y[32], z[32];
-  long long M[32][32];
-  long long corr[32];
-  uint16_t queue[kQueue];   // pairs within reach awaiting FP64: k*32+q (M), or 1024 + g*32+q (corr)
-  uint32_t nq, done;
-};
 
-// window lane q's share of the previous window's flip g (the exact value g's D row holds for q)
-__device__ __forceinline__ void corr_term(const SysParams& P, const Flips& Fp, Window& W, uint32_t g, uint32_t q,
-                                          float qd, double cut2, double reach2) {
-  const double r2 = dist2(P, make_float4(Fp.x[g], Fp.y[g], Fp.z[g], 0.f), make_float4(W.x[q], W.y[q], W.z[q], 0.f));
-  const int sg = Fp.sign[g];
-  long long d;
-  if (sg != 0) {
-    d = std_delta(P, r2, qd, cut2, reach2);
-    if (sg < 0) d = -d;
-  } else {
-    d = flip_delta(P, r2, Fp.qo[g], Fp.qn[g], cut2, reach2);
-  }
-  if (d != 0) atomicAdd(reinterpret_cast<unsigned long long*>(&W.corr[q]), (unsigned long long)d);
+// The attempt lanes of a window from lane p on: an attempt whose need bit is set takes the next
+// draw as its acceptance draw, and the lane after that is an attempt again.  Every run of set need
+// bits (restricted to lanes >= p) therefore starts at an attempt, its attempts are the run's even
+// offsets, and each of them skips the following lane.  Even offsets are read off the prefix parity
+// of the need bits against the parity just before the run (spread over the run by a carry).
+__device__ __forceinline__ uint32_t attempt_mask(uint32_t need_m, uint32_t p) {
+  const uint32_t range = 0xffffffffu << p;
+  const uint32_t x = need_m & range;
+  uint32_t px = x;                      // px bit i: parity of x's bits 0..i
+  px ^= px << 1;
+  px ^= px << 2;
+  px ^= px << 4;
+  px ^= px << 8;
+  px ^= px << 16;
+  const uint32_t starts = ((px & ~x) << 1) & x & ~(x << 1);   // runs whose preceding parity is 1
+  const uint32_t fill = (x ^ (x + starts)) & x;                 // that parity spread over the run
+  const uint32_t even = x & (px ^ fill);                        // the run's even offsets
+  return range & ~(even << 1);
 }
-
-// The site energies of one replica: in shared memory as two 32-bit halves (32-bit shared atomics are
-// native, 64-bit ones are not; an add carries from the low half into the high half exactly, so the
-// sum does not depend on the order of the adds), or in global memory as int64.
-template <bool SMEM>
-struct Energies {
-  uint32_t* lo;
-  int32_t* hi;
-  long long* g;
-  __device__ __forceinline__ long long get(uint32_t i) const {
-    if (SMEM) return (long long)(((unsigned long long)(uint32_t)hi[i] << 32) | lo[i]);
-    return g[i];
-  }
-  __device__ __forceinline__ void set(uint32_t i, long long v) const {
-    if (SMEM) { lo[i] = (uint32_t)(unsigned long long)v; hi[i] = (int32_t)((unsigned long long)v >> 32); }
-    else g[i] = v;
-  }
-  __device__ __forceinline__ void add(uint32_t i, long long d) const {
-    if (SMEM) {
-      const unsigned long long ud = (unsigned long long)d;
-      const uint32_t dl = (uint32_t)ud;
-      const int32_t dh = (int32_t)(ud >> 32);
-      const uint32_t old = atomicAdd(lo + i, dl);
-      const int32_t up = dh + ((uint32_t)(old + dl) < old ? 1 : 0);
-      if (up != 0) atomicAdd(hi + i, up);
-    } else {
-      atomicAdd(reinterpret_cast<unsigned long long*>(g + i), (unsigned long long)d);
-    }
-  }
-};
 
 // one attempt's decision from its site energy: bit 1 accepted, bit 2 took an acceptance draw,
 // bit 4 its acceptance draw is the next window's first (lane 31; decided there)
@@ -276,25 +297,31 @@ __device__ __forceinline__ int decide(long long e, uint32_t f, double u_acc, dou
   return (metropolis(dG, kT, inv_kT, u_acc) ? 1 : 0) | 2;
 }
 
-// add the flips of G to the energies of their neighbours: `t` of `nt` threads, kUpd items per
-// thread per pass, every load of a pass in flight before the first add
-template <bool SMEM>
+// add the flips of G to the energies of their neighbours (global int64, reductions in L2): `t` of
+// `nt` threads of whole warps across the cluster, kUpd items per thread per pass.  An item's flip is
+// counted from the flips' list starts held one per lane; every load of a pass is in flight before
+// the first add.
 __device__ __forceinline__ void scatter_flips(const Flips& G, const SysParams& P, uint32_t off, uint32_t cap,
                                               const uint32_t* __restrict__ es_nl, const long long* __restrict__ D,
-                                              const float4* __restrict__ hpos, const Energies<SMEM>& E, double cut2,
+                                              const float4* __restrict__ hpos, long long* __restrict__ E, double cut2,
                                               double reach2, uint32_t t, uint32_t nt) {
-  const uint32_t total = G.start[G.n];
+  const uint32_t total = G.start[G.n], nfl = G.n;
+  const uint32_t start_next = G.start[(threadIdx.x & 31u) + 1u];   // lane g: start of flip g + 1
   for (uint32_t base = 0; base < total; base += nt * kUpd) {
     uint32_t tv[kUpd], fv[kUpd];
     long long dv[kUpd];
 #pragma unroll
+    for (int u = 0; u < kUpd; ++u) fv[u] = 0;
+    for (uint32_t g = 0; g < nfl; ++g) {
+      const uint32_t sn = __shfl_sync(0xffffffffu, start_next, (int)g);
+#pragma unroll
+      for (int u = 0; u < kUpd; ++u) fv[u] += sn <= base + (uint32_t)u * nt + t ? 1u : 0u;
+    }
+#pragma unroll
     for (int u = 0; u < kUpd; ++u) {
       const uint32_t it = base + (uint32_t)u * nt + t;
-      uint32_t lo = 0;
-#pragma unroll
-      for (uint32_t step = 16; step > 0; step >>= 1)
-        if (G.start[lo + step] <= it) lo += step;
       const bool ok = it < total;
+      const uint32_t lo = fv[u];
       const size_t k = ok ? (size_t)(off + G.site[lo]) * cap + (it - G.start[lo]) : 0;
       tv[u] = es_nl[k];
       dv[u] = D[k];
@@ -309,203 +336,241 @@ __device__ __forceinline__ void scatter_flips(const Flips& G, const SysParams& P
         const uint32_t h = off + G.site[fv[u]];
         d = flip_delta(P, dist2(P, hpos[h], hpos[tv[u]]), G.qo[fv[u]], G.qn[fv[u]], cut2, reach2);
       }
-      E.add(tv[u] - off, d);
+      atomicAdd(reinterpret_cast<unsigned long long*>(E + (tv[u] - off)), (unsigned long long)d);
     }
   }
 }
 
-// Per window w (two barriers):
-//   X  all warps: M of window w and corr of window w from the flips of window w-1 (not yet in E);
-//      warp 0 reads E and the charge states of its sites (E holds every flip before window w-1)
-//   R  warp 0 resolves window w; warps 1.. scatter window w-1's flips into E meanwhile
-template <bool SMEM>
+// band rows [row0, row0 + 32) into the ring, 16 bytes a thread at a time
+__device__ __forceinline__ void fetch_rows(long long (*ring)[kBand], const long long* __restrict__ brow, uint32_t row0,
+                                           uint32_t t, uint32_t nt) {
+  constexpr uint32_t kPairs = kBand / 2;
+  for (uint32_t i = t; i < 32u * kPairs; i += nt) {
+    const uint32_t row = row0 + i / kPairs, c = i % kPairs;
+    reinterpret_cast<longlong2*>(ring[row & (kRing - 1)])[c] =
+        reinterpret_cast<const longlong2*>(brow + (size_t)row * kBand)[c];
+  }
+}
+
+// One cluster per replica.  CTA 0 walks the chain (warp 0) and keeps the charge states and the ring of
+// band rows in shared memory; the site energies E live in global memory and every thread of the
+// cluster but warp 0 of CTA 0 scatters flips into them.  Per window (two cluster barriers):
+//   C  warp 0 reads E and the charge states of its sites (E holds every flip before window w-1)
+//      and adds the flips of window w-1 from the band rows in the ring
+//   R  warp 0 resolves window w; the rest scatter window w-1's flips into E, and CTA 0's other
+//      warps fetch the band rows the next window can need
+// Window w's draws are consumed+0..31; the ring holds band rows [consumed - 32, consumed + 32) at C
+// (rows of window w-1's flips and of window w's draws) and the fetch during R adds rows
+// consumed+32..63, which covers window w+1 (it starts at consumed + 31 or + 32).
 __global__ void __launch_bounds__(kWalkThreads) k_sweep_walk(const SysParams* __restrict__ sp,
                                                              const uint32_t* __restrict__ head_slot,
                                                              const float4* __restrict__ hpos, float* __restrict__ charge,
                                                              const uint32_t* __restrict__ es_nl,
                                                              const uint32_t* __restrict__ es_cnt,
                                                              const long long* __restrict__ D, uint32_t cap,
-                                                             long long* __restrict__ Eg, uint8_t* __restrict__ flag_g,
+                                                             long long* __restrict__ Eg,
+                                                             const long long* __restrict__ band,
                                                              uint32_t* __restrict__ rng_io, double* __restrict__ out,
                                                              uint32_t only) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ Flips F[2];
-  __shared__ Window W;
-  __shared__ uint32_t s_dep;
-  const uint32_t r = (only == SOUP_NONE_U32) ? blockIdx.x : only;
+  __shared__ Flips Fh;                 // a helper CTA's copy of the flips it scatters
+  __shared__ uint32_t s_dep, s_done, s_base;
+  cg::cluster_group cluster = cg::this_cluster();
+  const uint32_t crank = cluster.block_rank(), csize = cluster.num_blocks();
+  const bool lead = crank == 0;
+  const uint32_t r = (only == SOUP_NONE_U32) ? blockIdx.x / csize : only;
   const SysParams& P = sp[r];
   const uint32_t H = P.nheads;
-  if (H == 0 || !P.es_on) return;
+  if (H == 0 || !P.es_on) return;     // the whole cluster leaves together
   const uint32_t off = P.head_off;
-  const Energies<SMEM> E{reinterpret_cast<uint32_t*>(smem), reinterpret_cast<int32_t*>(smem + 4 * (size_t)H), Eg + off};
-  uint8_t* flag = SMEM ? smem + 8 * (size_t)H : flag_g + off;
+  long long (*ring)[kBand] = reinterpret_cast<long long (*)[kBand]>(smem);
+  uint8_t* flag = smem + sizeof(long long) * kRing * kBand;
+  long long* E = Eg + off;
+  const long long* brow = band + band_row0(P, r) * kBand;
   const float qd = (float)P.d_q;
-  // flag: 0 neutral, 1 charged with the deprotonated charge, 2 charged with another value
-  for (uint32_t h = threadIdx.x; h < H; h += kWalkThreads) {
-    if (SMEM) E.set(h, Eg[off + h]);
-    const float q = charge[head_slot[off + h]];
-    flag[h] = q == 0.f ? 0 : (q == qd ? 1 : 2);
-  }
   const int lane = threadIdx.x & 31;
-  const bool chain = threadIdx.x < 32;
-  if (chain) {
-    F[0].start[lane + 1] = 0xFFFFFFFFu;
-    F[1].start[lane + 1] = 0xFFFFFFFFu;
-    W.corr[lane] = 0;
-    if (lane == 0) { F[0].n = F[1].n = 0; F[0].start[0] = F[1].start[0] = 0; W.done = 0; W.nq = 0; s_dep = 0; }
+  const bool chain = lead && threadIdx.x < 32;
+  if (lead) {
+    // flag: 0 neutral, 1 charged with the deprotonated charge, 2 charged with another value
+    for (uint32_t h = threadIdx.x; h < H; h += kWalkThreads) {
+      const float q = charge[head_slot[off + h]];
+      flag[h] = q == 0.f ? 0 : (q == qd ? 1 : 2);
+    }
+    fetch_rows(ring, brow, 0, threadIdx.x, kWalkThreads);
+    if (threadIdx.x < 32) {
+      F[0].start[lane + 1] = 0xFFFFFFFFu;
+      F[1].start[lane + 1] = 0xFFFFFFFFu;
+      if (lane == 0) { F[0].n = F[1].n = 0; F[0].start[0] = F[1].start[0] = 0; s_done = 0; s_base = 0; s_dep = 0; }
+    }
   }
+  // the lead CTA's window state, read by every CTA of the cluster
+  const Flips* lead_F = cluster.map_shared_rank(&F[0], 0);
+  const uint32_t* lead_done = cluster.map_shared_rank(&s_done, 0);
+  const uint32_t* lead_base = cluster.map_shared_rank(&s_base, 0);
+  // scatter threads: CTA 0's warps 1.., then every thread of the other CTAs
+  const uint32_t nscat = (kWalkThreads - 32u) + (csize - 1u) * kWalkThreads;
+  const uint32_t tscat = lead ? threadIdx.x - 32u : (kWalkThreads - 32u) + (crank - 1u) * kWalkThreads + threadIdx.x;
   const double kT = P.d_kT, inv_kT = 1.0 / P.d_kT;
   const double dGintr = kT * 2.302585092994046 * (P.d_pka - P.d_ph);
   const double cut2 = P.d_rc * P.d_rc, reach = P.d_rcattr + P.d_wc, reach2 = reach * reach;
-  // pairs beyond both cutoffs contribute exactly nothing; the FP32 screen keeps a wide margin
-  const float nr = (float)(fmax(P.d_rc, reach) * 1.001 + 1e-3);
-  const float near2 = nr * nr;
-  const float bx = (float)P.d_box[0], by = (float)P.d_box[1], bz = (float)P.d_box[2];
-  const float ibx = 1.f / bx, iby = 1.f / by, ibz = 1.f / bz;
   const uint32_t s0 = rng_io[r];
 
-  // warp 0: lane l holds draw base+l (A) and base+32+l (B)
+  // warp 0: lane l holds draw consumed+l (A) and consumed+32+l (B)
   Draw A{}, B{};
   uint32_t attempts = 0, consumed = 0, accepted = 0, dcount = 0;
   double dsum = 0.0;
   Lcg j32{1u, 0u};
   long long e = 0;
-  uint32_t f = 0;
+  uint32_t f = 0, colmask = 0;
   if (chain) {
     const Lcg j = lcg_pow((uint32_t)lane + 1u);
     j32 = lcg_pow(32u);
     const uint32_t sa = j.a * s0 + j.c;
-    draw_from(A, sa, H, off, hpos, es_cnt);
-    draw_from(B, j32.a * sa + j32.c, H, off, hpos, es_cnt);
-    W.site[lane] = A.site; W.x[lane] = A.x; W.y[lane] = A.y; W.z[lane] = A.z;
+    draw_from(A, sa, H, off, es_cnt);
+    draw_from(B, j32.a * sa + j32.c, H, off, es_cnt);
   }
-  __syncthreads();
+  cluster.sync();
 
   for (uint32_t wnd = 0;; ++wnd) {
-    Flips& Fc = F[wnd & 1];          // this window's flips
+    Flips& Fc = F[wnd & 1];               // this window's flips (lead CTA)
     const Flips& Fp = F[(wnd + 1) & 1];   // the previous window's
-    // ---- X ----
+    // written by warp 0 of CTA 0 during the previous R, read by everyone before this window's barrier
+    if (*lead_done) break;
+    const uint32_t base = *lead_base;
+    if (!lead) {                          // the flips this CTA scatters during R
+      const uint32_t* src = reinterpret_cast<const uint32_t*>(lead_F + ((wnd + 1) & 1));
+      for (uint32_t i = threadIdx.x; i < sizeof(Flips) / 4; i += kWalkThreads) reinterpret_cast<uint32_t*>(&Fh)[i] = src[i];
+    }
+    // ---- C ----
     if (chain) {
-      e = E.get(A.site);
+      e = (long long)__ldcg(reinterpret_cast<const unsigned long long*>(E + A.site));
       f = flag[A.site];
-    }
-    // pairs within reach are queued and then evaluated in FP64 one per thread, so no warp runs the
-    // FP64 path more than once per pass
-    for (uint32_t t = threadIdx.x; t < 1024u + 32u * Fp.n; t += kWalkThreads) {
-      if (t < 1024u) {
-        const int k = (int)(t >> 5), q = (int)(t & 31);
-        if (k >= q) continue;
-        long long m = kSameSite;
-        if (W.site[k] != W.site[q]) {
-          m = 0;
-          float dx = W.x[q] - W.x[k], dy = W.y[q] - W.y[k], dz = W.z[q] - W.z[k];
-          dx -= rintf(dx * ibx) * bx;
-          dy -= rintf(dy * iby) * by;
-          dz -= rintf(dz * ibz) * bz;
-          if (dx * dx + dy * dy + dz * dz < near2) {
-            const uint32_t slot = atomicAdd(&W.nq, 1u);
-            if (slot < kQueue) W.queue[slot] = (uint16_t)t;
-            else m = std_delta(P, dist2(P, make_float4(W.x[k], W.y[k], W.z[k], 0.f),
-                                        make_float4(W.x[q], W.y[q], W.z[q], 0.f)), qd, cut2, reach2);
-          }
+      // four flips at a time with every load in flight first (indices masked into bounds; entries
+      // past the count are dropped); a flip from a charge other than the standard one is rare and
+      // evaluated alone afterwards.  A site's own flip leaves its E alone.
+      const uint32_t n_prev = Fp.n;
+      bool other = false;
+      for (uint32_t g0 = 0; g0 < n_prev; g0 += 4u) {
+        uint32_t gs[4], gdr[4];
+        int sgn[4];
+        long long dv4[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const uint32_t g = (g0 + (uint32_t)k) & 31u;
+          gs[k] = Fp.site[g]; gdr[k] = Fp.draw[g]; sgn[k] = Fp.sign[g];
         }
-        W.M[k][q] = m;
-      } else {
-        const uint32_t g = (t - 1024u) >> 5, q = (t - 1024u) & 31u;
-        if (Fp.site[g] == W.site[q]) continue;        // a site's own flip leaves its E alone
-        float dx = W.x[q] - Fp.x[g], dy = W.y[q] - Fp.y[g], dz = W.z[q] - Fp.z[g];
-        dx -= rintf(dx * ibx) * bx;
-        dy -= rintf(dy * iby) * by;
-        dz -= rintf(dz * ibz) * bz;
-        if (dx * dx + dy * dy + dz * dz < near2) {
-          const uint32_t slot = atomicAdd(&W.nq, 1u);
-          if (slot < kQueue) W.queue[slot] = (uint16_t)t;
-          else corr_term(P, Fp, W, g, q, qd, cut2, reach2);
+#pragma unroll
+        for (int k = 0; k < 4; ++k)
+          dv4[k] = ring[gdr[k] & (kRing - 1)][(consumed + (uint32_t)lane - gdr[k]) & (kBand - 1)];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+          const bool use = g0 + (uint32_t)k < n_prev && gs[k] != A.site;
+          other |= use && sgn[k] == 0;
+          e += (use && sgn[k] != 0) ? (sgn[k] > 0 ? dv4[k] : -dv4[k]) : 0;
         }
       }
-    }
-    __syncthreads();
-    {
-      const uint32_t nq = W.nq < kQueue ? W.nq : kQueue;
-      for (uint32_t i = threadIdx.x; i < nq; i += kWalkThreads) {
-        const uint32_t t = W.queue[i];
-        if (t < 1024u) {
-          const uint32_t k = t >> 5, q = t & 31u;
-          W.M[k][q] = std_delta(P, dist2(P, make_float4(W.x[k], W.y[k], W.z[k], 0.f),
-                                         make_float4(W.x[q], W.y[q], W.z[q], 0.f)), qd, cut2, reach2);
-        } else {
-          corr_term(P, Fp, W, (t - 1024u) >> 5, (t - 1024u) & 31u, qd, cut2, reach2);
-        }
+      if (other)
+        for (uint32_t g = 0; g < n_prev; ++g)
+          if (Fp.sign[g] == 0 && Fp.site[g] != A.site)
+            e += flip_delta(P, dist2(P, hpos[off + Fp.site[g]], hpos[off + A.site]), Fp.qo[g], Fp.qn[g], cut2, reach2);
+      // the earlier lanes of this window whose flip changes this lane (band entry nonzero)
+      colmask = 0;
+#pragma unroll
+      for (uint32_t q = 0; q < 31u; ++q) {   // every load in bounds and independent; lanes <= q drop theirs
+        const long long v = ring[(consumed + q) & (kRing - 1)][((uint32_t)lane - q) & (kBand - 1)];
+        colmask |= (q < (uint32_t)lane && v != 0) ? 1u << q : 0u;
       }
     }
-    __syncthreads();
-    if (threadIdx.x == 0) W.nq = 0;
-    if (W.done) break;
+    cluster.sync();
     // ---- R ----
     if (chain) {
-      e += W.corr[lane];
-      const double u_acc = __shfl_down_sync(0xffffffffu, A.u, 1);   // lane l: draw base+l+1 (l < 31)
+      const double u_acc = __shfl_down_sync(0xffffffffu, A.u, 1);   // lane l: draw consumed+l+1 (l < 31)
       int res = decide(e, f, u_acc, kT, inv_kT, lane);
       uint32_t acc_m = __ballot_sync(0xffffffffu, res & 1), need_m = __ballot_sync(0xffffffffu, res & 2);
       uint32_t nxt_m = __ballot_sync(0xffffffffu, res & 4);
-      uint32_t chg_m = __ballot_sync(0xffffffffu, f != 0), f2_m = __ballot_sync(0xffffffffu, f == 2);
-      uint32_t dirty = 0, flipped = 0;
-      uint32_t p = 0, nf = 0, my_nf = 0, my_fo = 0;
+      uint32_t flipped = 0, p = 0, my_fo = 0;
       long long my_e = 0;
       bool done = false;
-      while (p < 32) {
-        if (attempts == H) { done = true; break; }
-        const uint32_t bit = 1u << p;
-        const long long mq = W.M[p][lane];            // used by the lanes after p when p flips
-        if (dirty & bit) {
-          if (lane == (int)p) res = decide(e, f, u_acc, kT, inv_kT, lane);
+      // the lanes of m flip; no later lane's energy or charge state depends on them
+      auto commit = [&](uint32_t m) {
+        if ((m >> lane) & 1u) {
+          flag[A.site] = f != 0 ? 0 : 1;
+          my_fo = f; my_e = e;
+        }
+        flipped |= m;
+      };
+      // lane q flips and every later lane takes the flip into its own site energy (or charge
+      // state), deciding again if that changed
+      auto flip_at = [&](uint32_t q) {
+        const uint32_t site_q = __shfl_sync(0xffffffffu, A.site, (int)q);
+        const uint32_t fo = __shfl_sync(0xffffffffu, f, (int)q);
+        commit(1u << q);
+        bool ch = false;
+        if (lane > (int)q) {
+          const long long mq = ring[(consumed + q) & (kRing - 1)][(uint32_t)lane - q];
+          if (mq == kSameSite) {
+            f = fo != 0 ? 0 : 1;
+            ch = true;
+          } else if (fo != 2) {
+            if (mq != 0) { e += fo == 0 ? mq : -mq; ch = true; }
+          } else {
+            const float qo = charge[head_slot[off + site_q]];
+            const long long m = flip_delta(P, dist2(P, hpos[off + site_q], hpos[off + A.site]), qo, 0.f, cut2, reach2);
+            if (m != 0) { e += m; ch = true; }
+          }
+        }
+        if (ch) res = decide(e, f, u_acc, kT, inv_kT, lane);
+        if (__ballot_sync(0xffffffffu, ch)) {
           acc_m = __ballot_sync(0xffffffffu, res & 1);
           need_m = __ballot_sync(0xffffffffu, res & 2);
           nxt_m = __ballot_sync(0xffffffffu, res & 4);
         }
-        if (nxt_m & bit) break;
-        ++attempts;
-        if (acc_m & bit) {
-          const uint32_t fo = (chg_m & bit) ? ((f2_m & bit) ? 2u : 1u) : 0u;
-          if (lane == (int)p) {
-            flag[A.site] = fo != 0 ? 0 : 1;
-            my_nf = nf; my_fo = fo; my_e = e;
+      };
+      if (H - attempts > 32u) {
+        // the attempt limit cannot fall inside this window.  From lane p the attempts run up to the
+        // first one that takes an acceptance draw, skip that draw, and so on.  Every flip before the
+        // first flip that changes some later lane (colmask) resolves at once; that flip resolves
+        // alone, and the scan starts again behind it.
+        while (p < 32u) {
+          const uint32_t am = attempt_mask(need_m, p);
+          const uint32_t stop = am & nxt_m;                  // lane 31 decides in the next window
+          const uint32_t fm = am & acc_m & ~stop;
+          const uint32_t hit = colmask & fm;
+          const uint32_t qs = __reduce_min_sync(0xffffffffu, hit ? (uint32_t)(__ffs(hit) - 1) : 32u);
+          if (qs == 32u) {
+            attempts += __popc(am & ~stop);
+            commit(fm);
+            p = stop ? 31u : 32u;
+            break;
           }
-          flipped |= bit;
-          // every later lane takes the flip into its own site energy (or charge state)
-          bool ch = false, dup = false;
-          if (lane > (int)p) {
-            if (mq == kSameSite) {
-              f = fo != 0 ? 0 : 1;
-              ch = dup = true;
-            } else if (fo != 2) {
-              if (mq != 0) { e += fo == 0 ? mq : -mq; ch = true; }
-            } else {
-              const float qo = charge[head_slot[off + W.site[p]]];
-              const long long m = flip_delta(P, dist2(P, make_float4(W.x[p], W.y[p], W.z[p], 0.f),
-                                                      make_float4(A.x, A.y, A.z, 0.f)), qo, 0.f, cut2, reach2);
-              if (m != 0) { e += m; ch = true; }
-            }
-          }
-          dirty |= __ballot_sync(0xffffffffu, ch);
-          if (__ballot_sync(0xffffffffu, dup)) {
-            chg_m = __ballot_sync(0xffffffffu, f != 0);
-            f2_m = __ballot_sync(0xffffffffu, f == 2);
-          }
-          ++nf;
+          const uint32_t below = (1u << qs) - 1u;
+          attempts += __popc(am & below) + 1u;
+          commit(fm & below);
+          flip_at(qs);
+          p = qs + (((need_m >> qs) & 1u) ? 2u : 1u);
         }
-        p += (need_m & bit) ? 2 : 1;
+      } else {
+        // the last attempts of the sweep: one lane at a time, stopping at the limit
+        while (p < 32u) {
+          if (attempts == H) { done = true; break; }
+          const uint32_t bit = 1u << p;
+          if (nxt_m & bit) break;
+          ++attempts;
+          if (acc_m & bit) flip_at(p);
+          p += (need_m & bit) ? 2u : 1u;
+        }
       }
       const uint32_t c = p;
-      consumed += c;
       // ---- this window's flip records, in lane (= attempt) order ----
       const bool mine = (flipped >> lane) & 1u;
+      const uint32_t nf = __popc(flipped), my_nf = __popc(flipped & ((1u << lane) - 1u));
       if (mine) {
         Fc.site[my_nf] = A.site;
+        Fc.draw[my_nf] = consumed + (uint32_t)lane;
         Fc.qo[my_nf] = my_fo == 0 ? 0.f : (my_fo == 1 ? qd : charge[head_slot[off + A.site]]);
         Fc.qn[my_nf] = my_fo != 0 ? 0.f : qd;
         Fc.sign[my_nf] = my_fo == 0 ? 1 : (my_fo == 1 ? -1 : 0);
-        Fc.x[my_nf] = A.x; Fc.y[my_nf] = A.y; Fc.z[my_nf] = A.z;
         ++accepted;
         if (my_fo == 0) { dsum += (double)my_e * kUnfix - dGintr; ++dcount; }
       }
@@ -516,8 +581,9 @@ __global__ void __launch_bounds__(kWalkThreads) k_sweep_walk(const SysParams* __
       }
       if (mine) Fc.start[my_nf + 1] = v;
       if (lane >= (int)nf) Fc.start[lane + 1] = 0xFFFFFFFFu;
-      if (lane == 0) { Fc.n = nf; W.done = done ? 1u : 0u; }
-      // ---- slide the draws by the c this window consumed; publish the next window's sites ----
+      consumed += c;
+      if (lane == 0) { Fc.n = nf; s_done = done ? 1u : 0u; s_base = consumed; }
+      // ---- slide the draws by the c this window consumed ----
       const int src = lane + (int)c;
       const Draw a1 = shfl_draw(A, src & 31);
       const Draw b1 = shfl_draw(B, src & 31);
@@ -526,15 +592,17 @@ __global__ void __launch_bounds__(kWalkThreads) k_sweep_walk(const SysParams* __
         B = b1;
       } else {
         A = b1;
-        draw_from(B, j32.a * b1.st + j32.c, H, off, hpos, es_cnt);
+        draw_from(B, j32.a * b1.st + j32.c, H, off, es_cnt);
       }
-      __syncwarp();
-      W.site[lane] = A.site; W.x[lane] = A.x; W.y[lane] = A.y; W.z[lane] = A.z;
-      W.corr[lane] = 0;
     } else {
-      scatter_flips(Fp, P, off, cap, es_nl, D, hpos, E, cut2, reach2, threadIdx.x - 32u, kWalkThreads - 32u);
+      scatter_flips(lead ? Fp : Fh, P, off, cap, es_nl, D, hpos, E, cut2, reach2, tscat, nscat);
+      if (lead) fetch_rows(ring, brow, base + 32u, threadIdx.x - 32u, kWalkThreads - 32u);
     }
-    __syncthreads();
+    cluster.sync();
+  }
+  if (!lead) {
+    cluster.sync();                       // CTA 0's shared memory stays up until every helper is done
+    return;
   }
   // the charges from the final states (a head still in state 2 keeps its own value)
   uint32_t dep = 0;
@@ -553,6 +621,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_sweep_walk(const SysParams* __
     }
   }
   __syncthreads();
+  cluster.sync();
   if (threadIdx.x == 0) {
     const Lcg j = lcg_pow(consumed);
     rng_io[r] = j.a * s0 + j.c;
@@ -578,27 +647,45 @@ void launch_sweep(Batch& b, uint32_t replica) {
   uint32_t hmax = 0;
   for (uint32_t r = 0; r < b.R; ++r)
     if (replica == SOUP_NONE_U32 || r == replica) hmax = std::max(hmax, b.hsp[r].nheads);
-  b.launches += 3;
+  if (hmax == 0) return;
+  b.launches += 5;
   prof_begin(b, SOUP_K_SWEEP);
+  const unsigned ry = replica == SOUP_NONE_U32 ? b.R : 1;
   k_gather_heads<<<(b.H + 255) / 256, 256, 0, b.stream>>>(b.head_slot, b.H, b.pos, b.head_pos);
   k_sweep_init<<<(unsigned)(((uint64_t)b.H * 32 + 255) / 256), 256, 0, b.stream>>>(
       b.sp, b.head_sys, b.head_slot, b.H, b.pos, b.charge, b.es_nl, b.es_cnt, b.es_cap, b.head_e, b.head_d, replica);
-  const unsigned grid = replica == SOUP_NONE_U32 ? b.R : 1;
-  const size_t smem = 9 * (size_t)hmax;
-  if (smem <= 200 * 1024) {
-    k_sweep_walk<true><<<grid, kWalkThreads, smem, b.stream>>>(b.sp, b.head_slot, b.head_pos, b.charge, b.es_nl,
-                                                               b.es_cnt, b.head_d, b.es_cap, b.head_e, b.head_flag,
-                                                               b.prot_rng_dev, b.sweep_out, replica);
-  } else {
-    k_sweep_walk<false><<<grid, kWalkThreads, 0, b.stream>>>(b.sp, b.head_slot, b.head_pos, b.charge, b.es_nl,
-                                                             b.es_cnt, b.head_d, b.es_cap, b.head_e, b.head_flag,
-                                                             b.prot_rng_dev, b.sweep_out, replica);
-  }
+  k_sweep_draws<<<dim3((2 * hmax + 2 * kBand + 255) / 256, ry), 256, 0, b.stream>>>(b.sp, b.prot_rng_dev, replica,
+                                                                                   b.draw_site);
+  k_sweep_band<<<dim3((unsigned)(((uint64_t)(2 * hmax + kBand) * kBand + 255) / 256), ry), 256, 0, b.stream>>>(
+      b.sp, b.head_pos, b.draw_site, replica, b.sweep_band);
+  // flags (a byte per head) after the ring; one cluster per replica, as wide as the SM count allows
+  const size_t smem = sizeof(long long) * kRing * kBand + (((size_t)hmax + 15) & ~(size_t)15);
+  const unsigned cs = ry <= 16 ? 8u : (ry <= 32 ? 4u : (ry <= 64 ? 2u : 1u));
+  cudaLaunchConfig_t lc = {};
+  lc.gridDim = dim3(ry * cs);
+  lc.blockDim = dim3(kWalkThreads);
+  lc.dynamicSmemBytes = smem;
+  lc.stream = b.stream;
+  cudaLaunchAttribute attr[1];
+  attr[0].id = cudaLaunchAttributeClusterDimension;
+  attr[0].val.clusterDim.x = cs;
+  attr[0].val.clusterDim.y = 1;
+  attr[0].val.clusterDim.z = 1;
+  lc.attrs = attr;
+  lc.numAttrs = 1;
+  SOUP_CUDA_TRY(cudaLaunchKernelEx(&lc, k_sweep_walk, (const SysParams*)b.sp, (const uint32_t*)b.head_slot,
+                                   (const float4*)b.head_pos, b.charge, (const uint32_t*)b.es_nl,
+                                   (const uint32_t*)b.es_cnt, (const long long*)b.head_d, b.es_cap, b.head_e,
+                                   (const long long*)b.sweep_band, b.prot_rng_dev, b.sweep_out, replica));
   prof_end(b);
 }
 
+uint32_t sweep_max_heads() { return (uint32_t)(kWalkSmemMax - sizeof(long long) * kRing * kBand - 16); }
+size_t sweep_band_rows(const Batch& b) { return 2 * (size_t)b.H + (size_t)kBand * b.R; }
+size_t sweep_draw_sites(const Batch& b) { return 2 * (size_t)b.H + 2 * (size_t)kBand * b.R; }
+
 void sweep_prepare(Batch& b) {
-  SOUP_CUDA_TRY(cudaFuncSetAttribute(k_sweep_walk<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+  SOUP_CUDA_TRY(cudaFuncSetAttribute(k_sweep_walk, cudaFuncAttributeMaxDynamicSharedMemorySize, kWalkSmemMax));
 }
 
 }  // namespace soup

@@ -371,6 +371,9 @@ Batch* make_batch(const SoupConfig* cfgs, const SoupInitState* inits, uint32_t R
         if (pos[4 * (size_t)i + 3] == (float)c.charged_kind) { hall.push_back(b.hsp[r].slot_off + i); hsys.push_back(r); }
     }
     b.hsp[r].nheads = (uint32_t)hall.size() - b.hsp[r].head_off;
+    if (b.cfg[r].es_enabled && b.hsp[r].nheads > sweep_max_heads())
+      fail(SOUP_E_ARG, "constant-pH sweep: " + std::to_string(b.hsp[r].nheads) + " heads in one replica exceed the " +
+                           std::to_string(sweep_max_heads()) + " the device sweep holds");
   }
   b.H = (uint32_t)hall.size();
   b.heads = dalloc<uint32_t>(b.H); b.head_sys = dalloc<uint32_t>(b.H); b.head_slot = dalloc<uint32_t>(b.H);
@@ -378,6 +381,8 @@ Batch* make_batch(const SoupConfig* cfgs, const SoupInitState* inits, uint32_t R
   b.head_pos = dalloc<float4>(b.H);
   b.head_xq = dalloc<float4>(b.H);
   b.head_flag = dalloc<uint8_t>(b.H);
+  b.draw_site = dalloc<uint32_t>(std::max<size_t>(sweep_draw_sites(b), 1));
+  b.sweep_band = dalloc<long long>(std::max<size_t>(sweep_band_rows(b) * 64, 1));
   sweep_prepare(b);
   b.es_nl = dalloc<uint32_t>((size_t)b.H * std::max<uint32_t>(b.es_cap, 1)); b.es_cnt = dalloc<uint32_t>(b.H);
   b.head_d = dalloc<long long>((size_t)b.H * std::max<uint32_t>(b.es_cap, 1));
@@ -411,7 +416,7 @@ void destroy_batch(Batch* b) {
                   b->frozen, b->id, b->slot_of, b->pos2, b->vel2, b->force2, b->charge2, b->slots2, b->center2,
                   b->held2, b->brng2, b->trng2, b->frozen2, b->id2, b->cell_of_slot, b->cell_count, b->cell_start,
                   b->cell_cursor, b->perm, b->scan_tmp, b->nl, b->nl_cnt, b->heads, b->head_sys, b->es_nl,
-                  b->es_cnt, b->head_slot, b->head_e, b->head_pos, b->head_xq, b->head_d, b->head_flag, b->hcell_count, b->hcell_start, b->hcell_cursor, b->hsorted, b->hcell_of, b->flags,
+                  b->es_cnt, b->head_slot, b->head_e, b->head_pos, b->head_xq, b->head_d, b->head_flag, b->draw_site, b->sweep_band, b->hcell_count, b->hcell_start, b->hcell_cursor, b->hsorted, b->hcell_of, b->flags,
                   b->events, b->desorb, b->drift_bits, b->bond_items, b->bond_nitems, b->uf_parent, b->comp_min,
                   b->item_done, b->has_item, b->sweep_out, b->prot_rng_dev, b->sp, b->shared, b->sysid, b->occ,
                   b->vis, b->frontier};

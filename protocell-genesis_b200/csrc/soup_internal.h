@@ -99,6 +99,8 @@ struct Batch {
   long long* head_d = nullptr;       // [head][es_cap] change of a list neighbour's energy when the head
                                      // deprotonates, fixed point 2^-40 (sweep scratch)
   uint8_t* head_flag = nullptr;      // charge state per head when the sweep cannot keep it in shared memory
+  uint32_t* draw_site = nullptr;     // the site each draw of a sweep's stream selects (sweep scratch)
+  long long* sweep_band = nullptr;   // [draw][64] changes of the next 63 draws' site energies (sweep scratch)
   uint32_t es_cap = 0;
   uint32_t* es_nl = nullptr;
   uint32_t* es_cnt = nullptr;
@@ -185,6 +187,9 @@ void launch_nonfinite(Batch& b);
 void launch_relax_step(Batch& b, float d);
 void launch_bonds(Batch& b);
 void launch_sweep(Batch& b, uint32_t replica);
+size_t sweep_band_rows(const Batch& b);
+uint32_t sweep_max_heads();   // heads one replica may hold for the device constant-pH sweep
+size_t sweep_draw_sites(const Batch& b);
 void adj_unpermute(Batch& b, float4* dst);
 void adj_scatter_pos(Batch& b, const float4* src);
 void adj_hvp(Batch& b, const float4* g, float4* jg, double* partial_dev);
