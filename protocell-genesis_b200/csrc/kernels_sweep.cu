@@ -202,36 +202,41 @@ __global__ void k_sweep_draws(const SysParams* __restrict__ sp, const uint32_t* 
 }
 
 // band[d][k] (k = 1..63): the change of draw d+k's site energy when draw d's site deprotonates
-// (std_delta, the value the D rows hold), or kSameSite when both draws select one site.  Positions
-// are fixed during a sweep, so the whole band is known before the walk starts.
+// (std_delta, the value the D rows hold), or kSameSite when both draws select one site; band[d][0]
+// is the mask of the row's nonzero entries.  Positions are fixed during a sweep, so the whole band is
+// known before the walk starts.  A warp per row.
+__device__ __forceinline__ long long band_entry(const SysParams& P, const float4* __restrict__ hpos,
+                                                const uint32_t* __restrict__ ds, uint32_t row, uint32_t k) {
+  if (k == 0) return 0;
+  const uint32_t a = ds[row], c = ds[row + k];
+  if (a == c) return kSameSite;
+  const float4 pa = hpos[P.head_off + a], pc = hpos[P.head_off + c];
+  const double cut2 = P.d_rc * P.d_rc, reach = P.d_rcattr + P.d_wc, reach2 = reach * reach;
+  // pairs beyond both cutoffs change nothing; the FP32 screen keeps a wide margin
+  const float nr = (float)(fmax(P.d_rc, reach) * 1.001 + 1e-3);
+  float dx = pc.x - pa.x, dy = pc.y - pa.y, dz = pc.z - pa.z;
+  dx -= rintf(dx * P.inv_box[0]) * P.box[0];
+  dy -= rintf(dy * P.inv_box[1]) * P.box[1];
+  dz -= rintf(dz * P.inv_box[2]) * P.box[2];
+  if (dx * dx + dy * dy + dz * dz >= nr * nr) return 0;
+  return std_delta(P, dist2(P, pa, pc), (float)P.d_q, cut2, reach2);
+}
 __global__ void k_sweep_band(const SysParams* __restrict__ sp, const float4* __restrict__ hpos,
                              const uint32_t* __restrict__ draw_site, uint32_t only, long long* __restrict__ band) {
   const uint32_t r = only == SOUP_NONE_U32 ? blockIdx.y : only;
   const SysParams& P = sp[r];
   const uint32_t H = P.nheads;
   if (H == 0 || !P.es_on) return;
-  const uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const uint32_t row = (uint32_t)(t / kBand), k = (uint32_t)(t % kBand);
-  if (row >= 2 * H + kBand) return;
-  long long m = 0;
-  if (k != 0) {
-    const uint32_t* ds = draw_site + draw_site0(P, r);
-    const uint32_t a = ds[row], c = ds[row + k];
-    if (a == c) {
-      m = kSameSite;
-    } else {
-      const float4 pa = hpos[P.head_off + a], pc = hpos[P.head_off + c];
-      const double cut2 = P.d_rc * P.d_rc, reach = P.d_rcattr + P.d_wc, reach2 = reach * reach;
-      // pairs beyond both cutoffs change nothing; the FP32 screen keeps a wide margin
-      const float nr = (float)(fmax(P.d_rc, reach) * 1.001 + 1e-3);
-      float dx = pc.x - pa.x, dy = pc.y - pa.y, dz = pc.z - pa.z;
-      dx -= rintf(dx * P.inv_box[0]) * P.box[0];
-      dy -= rintf(dy * P.inv_box[1]) * P.box[1];
-      dz -= rintf(dz * P.inv_box[2]) * P.box[2];
-      if (dx * dx + dy * dy + dz * dz < nr * nr) m = std_delta(P, dist2(P, pa, pc), (float)P.d_q, cut2, reach2);
-    }
-  }
-  band[(band_row0(P, r) + row) * kBand + k] = m;
+  const uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const uint32_t lane = threadIdx.x & 31u;
+  if (w >= 2 * (uint64_t)H + kBand) return;   // whole warps
+  const uint32_t row = (uint32_t)w;
+  const uint32_t* ds = draw_site + draw_site0(P, r);
+  const long long m0 = band_entry(P, hpos, ds, row, lane), m1 = band_entry(P, hpos, ds, row, lane + 32u);
+  const uint32_t b0 = __ballot_sync(0xffffffffu, m0 != 0), b1 = __ballot_sync(0xffffffffu, m1 != 0);
+  long long* out = band + (band_row0(P, r) + row) * kBand;
+  out[lane] = lane == 0 ? (long long)(((unsigned long long)b1 << 32) | b0) : m0;
+  out[lane + 32u] = m1;
 }
 
 // one draw of the stream as a lane holds it: the LCG state that produced it, the draw, the site it
@@ -408,9 +413,11 @@ __global__ void __launch_bounds__(kWalkThreads) k_sweep_walk(const SysParams* __
   const Flips* lead_F = cluster.map_shared_rank(&F[0], 0);
   const uint32_t* lead_done = cluster.map_shared_rank(&s_done, 0);
   const uint32_t* lead_base = cluster.map_shared_rank(&s_base, 0);
-  // scatter threads: CTA 0's warps 1.., then every thread of the other CTAs
-  const uint32_t nscat = (kWalkThreads - 32u) + (csize - 1u) * kWalkThreads;
-  const uint32_t tscat = lead ? threadIdx.x - 32u : (kWalkThreads - 32u) + (crank - 1u) * kWalkThreads + threadIdx.x;
+  // scatter threads: every thread of the other CTAs, or CTA 0's warps 1.. when the cluster is one CTA
+  // (then they also fetch the band rows, which is all they do otherwise)
+  const bool lead_scatters = csize == 1u;
+  const uint32_t nscat = lead_scatters ? kWalkThreads - 32u : (csize - 1u) * kWalkThreads;
+  const uint32_t tscat = lead ? threadIdx.x - 32u : (crank - 1u) * kWalkThreads + threadIdx.x;
   const double kT = P.d_kT, inv_kT = 1.0 / P.d_kT;
   const double dGintr = kT * 2.302585092994046 * (P.d_pka - P.d_ph);
   const double cut2 = P.d_rc * P.d_rc, reach = P.d_rcattr + P.d_wc, reach2 = reach * reach;
@@ -422,7 +429,9 @@ __global__ void __launch_bounds__(kWalkThreads) k_sweep_walk(const SysParams* __
   double dsum = 0.0;
   Lcg j32{1u, 0u};
   long long e = 0;
-  uint32_t f = 0, colmask = 0;
+  uint32_t f = 0, inter_m = 0;
+  long long corr = 0;          // the previous window's flips on this lane's site energy
+  bool other_prev = false;     // the previous window flipped a head from a non-standard charge
   if (chain) {
     const Lcg j = lcg_pow((uint32_t)lane + 1u);
     j32 = lcg_pow(32u);
@@ -438,49 +447,21 @@ __global__ void __launch_bounds__(kWalkThreads) k_sweep_walk(const SysParams* __
     // written by warp 0 of CTA 0 during the previous R, read by everyone before this window's barrier
     if (*lead_done) break;
     const uint32_t base = *lead_base;
-    if (!lead) {                          // the flips this CTA scatters during R
-      const uint32_t* src = reinterpret_cast<const uint32_t*>(lead_F + ((wnd + 1) & 1));
-      for (uint32_t i = threadIdx.x; i < sizeof(Flips) / 4; i += kWalkThreads) reinterpret_cast<uint32_t*>(&Fh)[i] = src[i];
-    }
     // ---- C ----
     if (chain) {
       e = (long long)__ldcg(reinterpret_cast<const unsigned long long*>(E + A.site));
       f = flag[A.site];
-      // four flips at a time with every load in flight first (indices masked into bounds; entries
-      // past the count are dropped); a flip from a charge other than the standard one is rare and
-      // evaluated alone afterwards.  A site's own flip leaves its E alone.
-      const uint32_t n_prev = Fp.n;
-      bool other = false;
-      for (uint32_t g0 = 0; g0 < n_prev; g0 += 4u) {
-        uint32_t gs[4], gdr[4];
-        int sgn[4];
-        long long dv4[4];
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-          const uint32_t g = (g0 + (uint32_t)k) & 31u;
-          gs[k] = Fp.site[g]; gdr[k] = Fp.draw[g]; sgn[k] = Fp.sign[g];
-        }
-#pragma unroll
-        for (int k = 0; k < 4; ++k)
-          dv4[k] = ring[gdr[k] & (kRing - 1)][(consumed + (uint32_t)lane - gdr[k]) & (kBand - 1)];
-#pragma unroll
-        for (int k = 0; k < 4; ++k) {
-          const bool use = g0 + (uint32_t)k < n_prev && gs[k] != A.site;
-          other |= use && sgn[k] == 0;
-          e += (use && sgn[k] != 0) ? (sgn[k] > 0 ? dv4[k] : -dv4[k]) : 0;
-        }
-      }
-      if (other)
-        for (uint32_t g = 0; g < n_prev; ++g)
+      // the previous window's flips, accumulated for this window's draws while they were taken; a
+      // flip from a charge other than the standard one is rare and evaluated here.  A site's own
+      // flip leaves its E alone.
+      e += corr;
+      if (other_prev)
+        for (uint32_t g = 0; g < Fp.n; ++g)
           if (Fp.sign[g] == 0 && Fp.site[g] != A.site)
             e += flip_delta(P, dist2(P, hpos[off + Fp.site[g]], hpos[off + A.site]), Fp.qo[g], Fp.qn[g], cut2, reach2);
-      // the earlier lanes of this window whose flip changes this lane (band entry nonzero)
-      colmask = 0;
-#pragma unroll
-      for (uint32_t q = 0; q < 31u; ++q) {   // every load in bounds and independent; lanes <= q drop theirs
-        const long long v = ring[(consumed + q) & (kRing - 1)][((uint32_t)lane - q) & (kBand - 1)];
-        colmask |= (q < (uint32_t)lane && v != 0) ? 1u << q : 0u;
-      }
+      // this lane's flip would change a later lane of the window: its band row's nonzero mask
+      const unsigned long long nz = (unsigned long long)ring[(consumed + (uint32_t)lane) & (kRing - 1)][0];
+      inter_m = __ballot_sync(0xffffffffu, ((nz >> 1) & ((1ull << (31 - lane)) - 1ull)) != 0);
     }
     cluster.sync();
     // ---- R ----
@@ -492,13 +473,27 @@ __global__ void __launch_bounds__(kWalkThreads) k_sweep_walk(const SysParams* __
       uint32_t flipped = 0, p = 0, my_fo = 0;
       long long my_e = 0;
       bool done = false;
-      // the lanes of m flip; no later lane's energy or charge state depends on them
+      // the next window's draws are consumed+31..63: lane l accumulates the flips' changes of draw
+      // consumed+31+l (nc) and lane 31 also of draw consumed+63 (nc2), from the flips' band rows
+      long long nc = 0, nc2 = 0;
+      bool other = false;
+      // the lanes of m flip; no later lane of this window depends on them
       auto commit = [&](uint32_t m) {
         if ((m >> lane) & 1u) {
           flag[A.site] = f != 0 ? 0 : 1;
           my_fo = f; my_e = e;
         }
         flipped |= m;
+        for (uint32_t mm = m; mm; mm &= mm - 1u) {
+          const uint32_t q = (uint32_t)(__ffs(mm) - 1);
+          const uint32_t fq = __shfl_sync(0xffffffffu, f, (int)q);
+          if (fq == 2u) { other = true; continue; }
+          const long long* row = ring[(consumed + q) & (kRing - 1)];
+          const long long v = row[(31u + (uint32_t)lane - q) & (kBand - 1)];
+          const long long v2 = row[(63u - q) & (kBand - 1)];
+          if (31u + (uint32_t)lane != q && v != kSameSite) nc += fq == 0 ? v : -v;
+          if (lane == 31 && v2 != kSameSite) nc2 += fq == 0 ? v2 : -v2;
+        }
       };
       // lane q flips and every later lane takes the flip into its own site energy (or charge
       // state), deciding again if that changed
@@ -530,14 +525,14 @@ __global__ void __launch_bounds__(kWalkThreads) k_sweep_walk(const SysParams* __
       if (H - attempts > 32u) {
         // the attempt limit cannot fall inside this window.  From lane p the attempts run up to the
         // first one that takes an acceptance draw, skip that draw, and so on.  Every flip before the
-        // first flip that changes some later lane (colmask) resolves at once; that flip resolves
+        // first flip that changes some later lane (inter_m) resolves at once; that flip resolves
         // alone, and the scan starts again behind it.
         while (p < 32u) {
           const uint32_t am = attempt_mask(need_m, p);
           const uint32_t stop = am & nxt_m;                  // lane 31 decides in the next window
           const uint32_t fm = am & acc_m & ~stop;
-          const uint32_t hit = colmask & fm;
-          const uint32_t qs = __reduce_min_sync(0xffffffffu, hit ? (uint32_t)(__ffs(hit) - 1) : 32u);
+          const uint32_t hit = inter_m & fm;
+          const uint32_t qs = hit ? (uint32_t)(__ffs(hit) - 1) : 32u;
           if (qs == 32u) {
             attempts += __popc(am & ~stop);
             commit(fm);
@@ -583,7 +578,13 @@ __global__ void __launch_bounds__(kWalkThreads) k_sweep_walk(const SysParams* __
       if (lane >= (int)nf) Fc.start[lane + 1] = 0xFFFFFFFFu;
       consumed += c;
       if (lane == 0) { Fc.n = nf; s_done = done ? 1u : 0u; s_base = consumed; }
-      // ---- slide the draws by the c this window consumed ----
+      // ---- slide the draws by the c this window consumed (31 or 32 unless the sweep is done) ----
+      {
+        const long long ncs = __shfl_sync(0xffffffffu, nc, (lane + (int)c - 31) & 31);
+        const long long nc2s = __shfl_sync(0xffffffffu, nc2, 31);
+        corr = (c == 32u && lane == 31) ? nc2s : ncs;
+        other_prev = __any_sync(0xffffffffu, other);
+      }
       const int src = lane + (int)c;
       const Draw a1 = shfl_draw(A, src & 31);
       const Draw b1 = shfl_draw(B, src & 31);
@@ -595,7 +596,12 @@ __global__ void __launch_bounds__(kWalkThreads) k_sweep_walk(const SysParams* __
         draw_from(B, j32.a * b1.st + j32.c, H, off, es_cnt);
       }
     } else {
-      scatter_flips(lead ? Fp : Fh, P, off, cap, es_nl, D, hpos, E, cut2, reach2, tscat, nscat);
+      if (!lead) {                        // a copy of the flips this CTA scatters
+        const uint32_t* src = reinterpret_cast<const uint32_t*>(lead_F + ((wnd + 1) & 1));
+        for (uint32_t i = threadIdx.x; i < sizeof(Flips) / 4; i += kWalkThreads) reinterpret_cast<uint32_t*>(&Fh)[i] = src[i];
+        __syncthreads();
+      }
+      if (!lead || lead_scatters) scatter_flips(lead ? Fp : Fh, P, off, cap, es_nl, D, hpos, E, cut2, reach2, tscat, nscat);
       if (lead) fetch_rows(ring, brow, base + 32u, threadIdx.x - 32u, kWalkThreads - 32u);
     }
     cluster.sync();
@@ -656,7 +662,7 @@ void launch_sweep(Batch& b, uint32_t replica) {
       b.sp, b.head_sys, b.head_slot, b.H, b.pos, b.charge, b.es_nl, b.es_cnt, b.es_cap, b.head_e, b.head_d, replica);
   k_sweep_draws<<<dim3((2 * hmax + 2 * kBand + 255) / 256, ry), 256, 0, b.stream>>>(b.sp, b.prot_rng_dev, replica,
                                                                                    b.draw_site);
-  k_sweep_band<<<dim3((unsigned)(((uint64_t)(2 * hmax + kBand) * kBand + 255) / 256), ry), 256, 0, b.stream>>>(
+  k_sweep_band<<<dim3((unsigned)(((uint64_t)(2 * hmax + kBand) * 32 + 255) / 256), ry), 256, 0, b.stream>>>(
       b.sp, b.head_pos, b.draw_site, replica, b.sweep_band);
   // flags (a byte per head) after the ring; one cluster per replica, as wide as the SM count allows
   const size_t smem = sizeof(long long) * kRing * kBand + (((size_t)hmax + 15) & ~(size_t)15);
