@@ -153,6 +153,25 @@ __global__ void k_gather(uint32_t N, const uint32_t* __restrict__ perm,
   slot_of[g] = k;
 }
 
+// the gathered arrays back into the primary buffers, so every array keeps its address across rebuilds
+// (a captured step graph holds them as kernel arguments)
+__global__ void k_copy_back(uint32_t N, const float4* __restrict__ pos2, const float4* __restrict__ vel2,
+                            const float4* __restrict__ force2, const float* __restrict__ charge2,
+                            const uint32_t* __restrict__ slots2, const uint32_t* __restrict__ center2,
+                            const uint32_t* __restrict__ held2, const uint32_t* __restrict__ brng2,
+                            const uint32_t* __restrict__ trng2, const uint8_t* __restrict__ frozen2,
+                            const uint32_t* __restrict__ id2, float4* __restrict__ pos, float4* __restrict__ vel,
+                            float4* __restrict__ force, float* __restrict__ charge, uint32_t* __restrict__ slots,
+                            uint32_t* __restrict__ center, uint32_t* __restrict__ held, uint32_t* __restrict__ brng,
+                            uint32_t* __restrict__ trng, uint8_t* __restrict__ frozen, uint32_t* __restrict__ id) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= N) return;
+  pos[k] = pos2[k]; vel[k] = vel2[k]; force[k] = force2[k]; charge[k] = charge2[k];
+  slots[3 * k] = slots2[3 * k]; slots[3 * k + 1] = slots2[3 * k + 1]; slots[3 * k + 2] = slots2[3 * k + 2];
+  center[k] = center2[k]; held[k] = held2[k]; brng[k] = brng2[k]; trng[k] = trng2[k]; frozen[k] = frozen2[k];
+  id[k] = id2[k];
+}
+
 // Distinct wrapped cell coordinates of a +-R walk along one axis, as at most two [lo,hi] intervals.
 struct AxisRange { int lo[2], hi[2], n; };
 __device__ __forceinline__ AxisRange axis_ranges(int q, int R, int dim) {
@@ -350,14 +369,14 @@ void launch_sort_and_gather(Batch& b) {
                                                    b.held, b.brng, b.trng, b.frozen, b.id, b.pos2, b.vel2, b.force2,
                                                    b.charge2, b.slots2, b.center2, b.held2, b.brng2, b.trng2,
                                                    b.frozen2, b.id2, b.slot_of, b.pos_ref);
-  std::swap(b.pos, b.pos2); std::swap(b.vel, b.vel2); std::swap(b.force, b.force2);
-  std::swap(b.charge, b.charge2); std::swap(b.slots, b.slots2); std::swap(b.center, b.center2);
-  std::swap(b.held, b.held2); std::swap(b.brng, b.brng2); std::swap(b.trng, b.trng2);
-  std::swap(b.frozen, b.frozen2); std::swap(b.id, b.id2);
+  k_copy_back<<<nblocks(b.N), kBlock, 0, b.stream>>>(b.N, b.pos2, b.vel2, b.force2, b.charge2, b.slots2, b.center2,
+                                                      b.held2, b.brng2, b.trng2, b.frozen2, b.id2, b.pos, b.vel, b.force,
+                                                      b.charge, b.slots, b.center, b.held, b.brng, b.trng, b.frozen,
+                                                      b.id);
   // the cell of every new slot: cell_start is monotone, so recompute from the sorted positions
   cudaMemsetAsync(b.cell_count, 0, sizeof(uint32_t) * (b.ncells + 1), b.stream);
   k_cell_index<<<nblocks(b.N), kBlock, 0, b.stream>>>(b.pos, b.sysid, b.sp, b.N, b.cell_of_slot, b.cell_count);
-  b.launches += 5 + g_scan_launches;
+  b.launches += 6 + g_scan_launches;
   prof_end(b);
 }
 

@@ -144,7 +144,25 @@ __global__ void k_relax_step(const SysParams* __restrict__ sp, const uint8_t* __
   pos[k] = x;
 }
 
+// the drift-triggered rebuild decision of a captured step: any replica whose largest drift since its
+// last rebuild exceeds skin/2 (or is not a number) sets the graph's conditional node
+__global__ void k_rebuild_decide(const SysParams* __restrict__ sp, const uint32_t* __restrict__ drift_bits, uint32_t R,
+                                 cudaGraphConditionalHandle h, uint32_t* __restrict__ count) {
+  bool any = false;
+  for (uint32_t r = threadIdx.x; r < R; r += 32) any |= !(__uint_as_float(drift_bits[r]) <= sp[r].skin_half2);
+  any = __any_sync(0xffffffffu, any);
+  if (threadIdx.x == 0) {
+    cudaGraphSetConditional(h, any ? 1u : 0u);
+    if (any) *count += 1u;
+  }
+}
+
 }  // namespace
+
+void launch_rebuild_decide(Batch& b, cudaGraphConditionalHandle h) {
+  b.launches += 1;
+  k_rebuild_decide<<<1, 32, 0, b.stream>>>(b.sp, b.drift_bits, b.R, h, b.rebuild_count);
+}
 
 void launch_kick_drift(Batch& b) {
   b.launches += 1;

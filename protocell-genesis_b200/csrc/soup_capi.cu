@@ -204,12 +204,15 @@ void upload_params(Batch& b) {
   SOUP_CUDA_TRY(cudaMemcpyAsync(b.shared, &b.hs, sizeof(Shared), cudaMemcpyHostToDevice, b.stream));
 }
 
-void rebuild(Batch& b) {
+void rebuild_launches(Batch& b) {
   launch_cell_index(b);
   launch_sort_and_gather(b);
   launch_build_lists(b);
   launch_build_es_lists(b);
   SOUP_CUDA_TRY(cudaMemsetAsync(b.drift_bits, 0, sizeof(uint32_t) * b.R, b.stream));
+}
+void rebuild(Batch& b) {
+  rebuild_launches(b);
   b.rebuilds++;
 }
 
@@ -320,6 +323,9 @@ Batch* make_batch(const SoupConfig* cfgs, const SoupInitState* inits, uint32_t R
   b.step.assign(R, 0);
   b.next_sweep.assign(R, UINT64_MAX);
   SOUP_CUDA_TRY(cudaStreamCreateWithFlags(&b.stream, cudaStreamNonBlocking));
+  SOUP_CUDA_TRY(cudaStreamCreateWithFlags(&b.cap_stream, cudaStreamNonBlocking));
+  // step chunks run as captured graphs; SOUP_NO_GRAPH=1 in the environment launches them one by one
+  if (const char* e = std::getenv("SOUP_NO_GRAPH")) b.graphs_enabled = std::atoi(e) == 0;
 
   const size_t n = b.N;
   b.pos = dalloc<float4>(n); b.vel = dalloc<float4>(n); b.force = dalloc<float4>(n); b.pos_ref = dalloc<float4>(n);
@@ -341,6 +347,8 @@ Batch* make_batch(const SoupConfig* cfgs, const SoupInitState* inits, uint32_t R
   b.uf_parent = dalloc<uint32_t>(n); b.comp_min = dalloc<uint32_t>(n); b.item_done = dalloc<uint8_t>(n);
   b.has_item = dalloc<uint32_t>(n);
   b.prot_rng_dev = dalloc<uint32_t>(R);
+  b.rebuild_count = dalloc<uint32_t>(1);
+  SOUP_CUDA_TRY(cudaMemsetAsync(b.rebuild_count, 0, 4, b.stream));
   b.sweep_out = dalloc<double>(4 * (size_t)R);
   SOUP_CUDA_TRY(cudaMemsetAsync(b.flags, 0, sizeof(uint32_t) * (FLAG_WORDS + 2 * R), b.stream));
   SOUP_CUDA_TRY(cudaMemsetAsync(b.events, 0, sizeof(uint32_t) * 2 * SOUP_MAX_RULES * R, b.stream));
@@ -409,10 +417,14 @@ Batch* make_batch(const SoupConfig* cfgs, const SoupInitState* inits, uint32_t R
   return bp.release();
 }
 
+void drop_graphs(Batch& b);
+
 void destroy_batch(Batch* b) {
   if (!b) return;
   cudaStreamSynchronize(b->stream);
-  void* ptrs[] = {b->pos, b->vel, b->force, b->pos_ref, b->charge, b->slots, b->center, b->held, b->brng, b->trng,
+  drop_graphs(*b);
+  if (b->cap_stream) cudaStreamDestroy(b->cap_stream);
+  void* ptrs[] = {b->rebuild_count, b->pos, b->vel, b->force, b->pos_ref, b->charge, b->slots, b->center, b->held, b->brng, b->trng,
                   b->frozen, b->id, b->slot_of, b->pos2, b->vel2, b->force2, b->charge2, b->slots2, b->center2,
                   b->held2, b->brng2, b->trng2, b->frozen2, b->id2, b->cell_of_slot, b->cell_count, b->cell_start,
                   b->cell_cursor, b->perm, b->scan_tmp, b->nl, b->nl_cnt, b->heads, b->head_sys, b->es_nl,
@@ -518,6 +530,107 @@ void sweep_all(Batch& b, std::vector<SoupSweepResult>* out) {
   }
 }
 
+void drop_graphs(Batch& b) {
+  for (auto& g : b.graphs) cudaGraphExecDestroy(g.exec);
+  b.graphs.clear();
+}
+
+// Capture `chunk` steps starting at global step `start` (soup-integrate.ts's per-step schedule) as one
+// graph.  With drift-triggered rebuilds each step holds a one-thread decision kernel and a
+// conditional node whose body is the rebuild, so the graph never waits on the host.
+Batch::ChunkGraph capture_chunk(Batch& b, uint64_t chunk, uint64_t start, uint64_t key) {
+  const SoupConfig& c0 = b.cfg[0];
+  const uint64_t l0 = b.launches;
+  uint64_t fixed_rebuilds = 0;
+  cudaStream_t main = b.stream;
+  SOUP_CUDA_TRY(cudaStreamBeginCapture(main, cudaStreamCaptureModeThreadLocal));
+  try {
+    for (uint64_t k = 0; k < chunk; ++k) {
+      const uint64_t g = start + k;
+      launch_kick_drift(b);
+      if (c0.rebuild_on_drift) {
+        cudaStreamCaptureStatus st;
+        cudaGraph_t cg = nullptr;
+        const cudaGraphNode_t* deps = nullptr;
+        size_t nd = 0;
+        SOUP_CUDA_TRY(cudaStreamGetCaptureInfo(main, &st, nullptr, &cg, nullptr, nullptr));
+        cudaGraphConditionalHandle h;
+        SOUP_CUDA_TRY(cudaGraphConditionalHandleCreate(&h, cg, 0, 0));
+        launch_rebuild_decide(b, h);
+        SOUP_CUDA_TRY(cudaStreamGetCaptureInfo(main, &st, nullptr, &cg, &deps, &nd));
+        cudaGraphNodeParams np = {};
+        np.type = cudaGraphNodeTypeConditional;
+        np.conditional.handle = h;
+        np.conditional.type = cudaGraphCondTypeIf;
+        np.conditional.size = 1;
+        cudaGraphNode_t node;
+        SOUP_CUDA_TRY(cudaGraphAddNode(&node, cg, deps, nd, &np));
+        const uint64_t lb = b.launches;
+        b.stream = b.cap_stream;
+        SOUP_CUDA_TRY(cudaStreamBeginCaptureToGraph(b.cap_stream, np.conditional.phGraph_out[0], nullptr, nullptr, 0,
+                                                    cudaStreamCaptureModeThreadLocal));
+        rebuild_launches(b);
+        cudaGraph_t body = nullptr;
+        SOUP_CUDA_TRY(cudaStreamEndCapture(b.cap_stream, &body));
+        b.stream = main;
+        b.body_launches = b.launches - lb;
+        b.launches = lb;
+        SOUP_CUDA_TRY(cudaStreamUpdateCaptureDependencies(main, &node, 1, cudaStreamSetCaptureDependencies));
+      } else if (g % c0.rebuild_every == 0) {
+        rebuild_launches(b);
+        ++fixed_rebuilds;
+      }
+      launch_force(b);
+      if (g % c0.bond_interval == 0) launch_bonds(b);
+      launch_kick_thermo(b);
+    }
+  } catch (...) {
+    b.stream = main;
+    cudaGraph_t broken = nullptr;
+    cudaStreamEndCapture(main, &broken);
+    if (broken) cudaGraphDestroy(broken);
+    b.launches = l0;
+    throw;
+  }
+  cudaGraph_t graph = nullptr;
+  SOUP_CUDA_TRY(cudaStreamEndCapture(main, &graph));
+  Batch::ChunkGraph cgr{key, nullptr, b.launches - l0, fixed_rebuilds};
+  b.launches = l0;
+  const cudaError_t e = cudaGraphInstantiate(&cgr.exec, graph, 0);
+  cudaGraphDestroy(graph);
+  SOUP_CUDA_TRY(e);
+  return cgr;
+}
+
+// one chunk from its cached graph (captured on first use); the host bookkeeping of the steps
+void run_chunk_graph(Batch& b, uint64_t chunk, uint64_t start) {
+  const SoupConfig& c0 = b.cfg[0];
+  const uint64_t key = chunk | ((start % c0.bond_interval) << 20) |
+                       (c0.rebuild_on_drift ? 0ull : ((start % c0.rebuild_every) << 40));
+  const Batch::ChunkGraph* g = nullptr;
+  for (auto& x : b.graphs)
+    if (x.key == key) g = &x;
+  if (!g) {
+    if (b.graphs.size() >= 16) drop_graphs(b);
+    b.graphs.push_back(capture_chunk(b, chunk, start, key));
+    g = &b.graphs.back();
+  }
+  SOUP_CUDA_TRY(cudaGraphLaunch(g->exec, b.stream));
+  b.launches += g->launches;
+  b.rebuilds += g->rebuilds_fixed;
+  for (uint32_t r = 0; r < b.R; ++r) b.step[r] += chunk;
+}
+
+// the rebuilds the conditional nodes took since the last call (the stream is synchronised)
+void count_graph_rebuilds(Batch& b) {
+  uint32_t c = 0;
+  SOUP_CUDA_TRY(cudaMemcpy(&c, b.rebuild_count, 4, cudaMemcpyDeviceToHost));
+  const uint32_t d = c - b.rebuild_count_seen;
+  b.rebuild_count_seen = c;
+  b.rebuilds += d;
+  b.launches += (uint64_t)d * b.body_launches;
+}
+
 // soup/src/soup-integrate.ts:136-175, for every replica in lockstep
 void step_batch(Batch& b, uint64_t n) {
   const SoupConfig& c0 = b.cfg[0];
@@ -526,20 +639,26 @@ void step_batch(Batch& b, uint64_t n) {
   while (done < n) {
     const uint64_t chunk = std::min(chunk_max, n - done);
     const uint64_t chunk_start = b.step[0];
-    for (uint64_t k = 0; k < chunk; ++k) {
-      const uint64_t g = b.step[0];
-      const bool bonds = g % c0.bond_interval == 0;
-      launch_kick_drift(b);
-      bool reb;
-      if (c0.rebuild_on_drift) reb = drift_exceeds(b);
-      else reb = g % c0.rebuild_every == 0;
-      if (reb) rebuild(b);
-      launch_force(b);
-      if (bonds) launch_bonds(b);
-      launch_kick_thermo(b);
-      for (uint32_t r = 0; r < b.R; ++r) b.step[r]++;
+    const bool graph = b.graphs_enabled && !b.prof && chunk >= 4;
+    if (graph) {
+      run_chunk_graph(b, chunk, chunk_start);
+    } else {
+      for (uint64_t k = 0; k < chunk; ++k) {
+        const uint64_t g = b.step[0];
+        const bool bonds = g % c0.bond_interval == 0;
+        launch_kick_drift(b);
+        bool reb;
+        if (c0.rebuild_on_drift) reb = drift_exceeds(b);
+        else reb = g % c0.rebuild_every == 0;
+        if (reb) rebuild(b);
+        launch_force(b);
+        if (bonds) launch_bonds(b);
+        launch_kick_thermo(b);
+        for (uint32_t r = 0; r < b.R; ++r) b.step[r]++;
+      }
     }
     guards(b, chunk_start);
+    if (graph) count_graph_rebuilds(b);
     bool any = false;
     for (uint32_t r = 0; r < b.R; ++r)
       if (b.cfg[r].es_enabled && b.step[r] >= b.next_sweep[r]) { any = true; b.next_sweep[r] = b.step[r] + b.cfg[r].sweep_every; }
@@ -896,6 +1015,7 @@ int soup_set_box(SoupHandle* h, const double box[3]) {
     SysParams p = make_sys(b.cfg[r]);
     p.slot_off = old.slot_off; p.n = old.n; p.head_off = old.head_off; p.nheads = old.nheads;
     b.hsp[r] = p;
+    drop_graphs(b);
     alloc_grids(b);
     upload_params(b);
     force_pass(b);

@@ -140,6 +140,15 @@ struct Batch {
   bool force_fresh = false;          // force array matches positions+charges+lists
   int tpp = 4;                       // threads per particle in the list force
   DiffWindow diff;
+  // captured step chunks (CUDA graphs), keyed by length and schedule phase; the drift-triggered
+  // rebuild is a conditional node whose condition a one-thread kernel sets
+  struct ChunkGraph { uint64_t key; cudaGraphExec_t exec; uint64_t launches, rebuilds_fixed; };
+  std::vector<ChunkGraph> graphs;
+  bool graphs_enabled = true;
+  cudaStream_t cap_stream = nullptr;     // captures the rebuild body
+  uint64_t body_launches = 0;            // kernels in one rebuild body
+  uint32_t* rebuild_count = nullptr;     // device: rebuilds the conditional nodes took
+  uint32_t rebuild_count_seen = 0;
   std::string err;
   std::vector<SoupHandle*> views;    // per-replica handle views
 
@@ -182,6 +191,7 @@ void launch_es_far(Batch& b);
 void launch_force_brute(Batch& b);
 void launch_kick_drift(Batch& b);
 void launch_kick_thermo(Batch& b);
+void launch_rebuild_decide(Batch& b, cudaGraphConditionalHandle h);
 void launch_max_drift(Batch& b);
 void launch_nonfinite(Batch& b);
 void launch_relax_step(Batch& b, float d);
