@@ -318,6 +318,7 @@ def run_batched(args, pkg, L, cfgm, rank, torch):
         states.append(st)
     batch = pkg.SoupBatch(cfgs, states)
     total = sum(int(c.n) for c in cfgs)
+    tune = batch.autotune(steps=20) if not args.no_tune else None   # untimed; the choice stays in effect
     batch.step(args.warmup)
     h0 = batch.replicas[0]._h
     stream = torch.cuda.ExternalStream(L.soup_stream(h0))
@@ -334,10 +335,11 @@ def run_batched(args, pkg, L, cfgm, rank, torch):
     launches = L.soup_launch_count(h0) - launches0
     batch.dispose()
     return {"value": total * steps / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / steps, "steps": steps,
-            "replicas": len(cfgs), "beads": total, "gpu_launches": int(launches),
+            "replicas": len(cfgs), "beads": total, "gpu_launches": int(launches), "autotune": tune,
             "workload": "uneven replicas: box U[29,53] sigma, density 0.80, 15% beads in preassembled 5-bead "
                         "amphiphiles, rest water, pH U[5,9], I log-U[0.001,0.1] M, sweep every 10, bonds every "
-                        "20, skin 1.0 with drift rebuilds; seeded synthetic, relaxed untimed"}
+                        "20, skin planned 1.0 with drift rebuilds, lanes per particle, cell size and skin "
+                        "autotuned (untimed); steps in captured CUDA graphs; seeded synthetic, relaxed untimed"}
 
 
 def run_gradient(args, pkg, L, torch):
@@ -578,6 +580,7 @@ def main():
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-replica measurement")
     ap.add_argument("--replicas", type=int, default=64)
     ap.add_argument("--batched-steps", type=int, default=100)
+    ap.add_argument("--no-tune", action="store_true", help="skip the batched form's autotuning")
     ap.add_argument("--no-gradient", action="store_true", help="skip the forward + adjoint window measurement")
     ap.add_argument("--prof-steps", type=int, default=100, help="steps of the profiled segment (per-kernel split)")
     ap.add_argument("--grad-steps", type=int, default=200)

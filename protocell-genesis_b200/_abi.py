@@ -116,6 +116,13 @@ class SoupAggregateShape(C.Structure):
     _fields_ = [("size", C.c_uint32), ("label", C.c_uint32), ("centre", C.c_double * 3), ("gyration", C.c_double * 6)]
 
 
+class SoupTuneResult(C.Structure):
+    _fields_ = [
+        ("tpp", C.c_uint32), ("walk", C.c_uint32), ("tpp_before", C.c_uint32), ("walk_before", C.c_uint32),
+        ("skin_scale", C.c_double), ("ms_per_step_before", C.c_double), ("ms_per_step_after", C.c_double),
+    ]
+
+
 class SoupInfo(C.Structure):
     _fields_ = [
         ("n", C.c_uint32), ("global_step", C.c_uint64), ("list_capacity", C.c_uint32),
@@ -158,6 +165,7 @@ SIGNATURES = {
     "soup_read_protonation_rng": (C.c_int, [_P, _U32P]),
     "soup_write_charges": (C.c_int, [_P, _P, _SZ]),
     "soup_set_box": (C.c_int, [_P, C.POINTER(C.c_double)]),
+    "soup_autotune": (C.c_int, [_P, C.c_uint32, C.POINTER(SoupTuneResult)]),
     "soup_write_state": (C.c_int, [_P, C.POINTER(SoupInitState)]),
     "soup_protonation_sweep": (C.c_int, [_P, C.POINTER(SoupSweepResult)]),
     "soup_closure": (C.c_int, [_P, _U32P, C.c_uint32, _U32P, C.c_uint32, C.POINTER(C.c_double),

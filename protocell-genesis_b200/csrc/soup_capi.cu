@@ -762,6 +762,98 @@ template <class T> T* dgrow(T* p, size_t& cap, size_t want) {
 constexpr int kDepthPairs[6][2] = {{0, 0}, {0, 1}, {0, 2}, {1, 1}, {1, 2}, {2, 2}};
 }  // namespace
 
+// ---- autotuning -------------------------------------------------------------------------------
+namespace {
+// Every replica's state in original order and the host schedule, to restore after trial steps.
+struct TuneSnapshot {
+  std::vector<std::vector<float>> pos, vel, q;
+  std::vector<std::vector<uint32_t>> slots, center, held, brng, trng, frozen;
+  std::vector<uint64_t> step, next_sweep;
+  std::vector<uint32_t> prot_rng, events, desorb;
+  uint64_t rebuilds = 0, sweeps = 0;
+};
+TuneSnapshot tune_snapshot(Batch& b) {
+  TuneSnapshot t;
+  const uint32_t R = b.R;
+  t.pos.resize(R); t.vel.resize(R); t.q.resize(R); t.slots.resize(R); t.center.resize(R); t.held.resize(R);
+  t.brng.resize(R); t.trng.resize(R); t.frozen.resize(R);
+  for (uint32_t r = 0; r < R; ++r) {
+    const uint32_t n = b.cfg[r].n;
+    t.pos[r].resize(4 * (size_t)n); t.vel[r].resize(4 * (size_t)n); t.q[r].resize(n); t.slots[r].resize(3 * (size_t)n);
+    t.center[r].resize(n); t.held[r].resize(n); t.brng[r].resize(n); t.trng[r].resize(n); t.frozen[r].resize(n);
+    std::vector<uint8_t> fr(n);
+    read_replica<float>(b, r, reinterpret_cast<const float*>(b.pos), 4, t.pos[r].data(), false);
+    read_replica<float>(b, r, reinterpret_cast<const float*>(b.vel), 4, t.vel[r].data(), false);
+    read_replica<float>(b, r, b.charge, 1, t.q[r].data(), false);
+    read_replica<uint32_t>(b, r, b.slots, 3, t.slots[r].data(), true);
+    read_replica<uint32_t>(b, r, b.center, 1, t.center[r].data(), true);
+    read_replica<uint32_t>(b, r, b.held, 1, t.held[r].data(), false);
+    read_replica<uint32_t>(b, r, b.brng, 1, t.brng[r].data(), false);
+    read_replica<uint32_t>(b, r, b.trng, 1, t.trng[r].data(), false);
+    read_replica<uint8_t>(b, r, b.frozen, 1, fr.data(), false);
+    t.frozen[r].assign(fr.begin(), fr.end());
+  }
+  t.events.resize(2 * SOUP_MAX_RULES * (size_t)R);
+  t.desorb.resize(2 * (size_t)R);
+  SOUP_CUDA_TRY(cudaMemcpy(t.events.data(), b.events, 4 * t.events.size(), cudaMemcpyDeviceToHost));
+  SOUP_CUDA_TRY(cudaMemcpy(t.desorb.data(), b.desorb, 4 * t.desorb.size(), cudaMemcpyDeviceToHost));
+  t.step = b.step; t.next_sweep = b.next_sweep; t.prot_rng = b.prot_rng;
+  t.rebuilds = b.rebuilds; t.sweeps = b.sweeps;
+  return t;
+}
+void tune_restore(Batch& b, const TuneSnapshot& t) {
+  for (uint32_t r = 0; r < b.R; ++r) {
+    SoupInitState m{};
+    m.positions = t.pos[r].data(); m.velocities = t.vel[r].data(); m.charges = t.q[r].data();
+    m.bond_slots = t.slots[r].data(); m.center_link = t.center[r].data(); m.center_held = t.held[r].data();
+    m.bond_rng = t.brng[r].data(); m.thermo_rng = t.trng[r].data(); m.frozen = t.frozen[r].data();
+    upload_replica(b, r, &m, false);
+  }
+  SOUP_CUDA_TRY(cudaMemcpyAsync(b.events, t.events.data(), 4 * t.events.size(), cudaMemcpyHostToDevice, b.stream));
+  SOUP_CUDA_TRY(cudaMemcpyAsync(b.desorb, t.desorb.data(), 4 * t.desorb.size(), cudaMemcpyHostToDevice, b.stream));
+  b.step = t.step; b.next_sweep = t.next_sweep; b.prot_rng = t.prot_rng;
+  for (uint32_t r = 0; r < b.R; ++r) SOUP_CUDA_TRY(cudaMemcpyAsync(b.prot_rng_dev + r, &b.prot_rng[r], 4, cudaMemcpyHostToDevice, b.stream));
+  b.rebuilds = t.rebuilds; b.sweeps = t.sweeps;
+  force_pass(b);
+  SOUP_CUDA_TRY(cudaStreamSynchronize(b.stream));
+}
+// every replica's list geometry for a skin (scaled from the planned one) and a list-walk radius
+// (the neighbour cell is list range / walk)
+void tune_plan(Batch& b, const std::vector<double>& skin, int walk) {
+  for (uint32_t r = 0; r < b.R; ++r) {
+    SoupConfig& c = b.cfg[r];
+    const double ds = skin[r] - c.skin;
+    c.list_range += ds;
+    if (c.es_enabled) c.es_list_range += ds;
+    c.skin = skin[r];
+    const SysParams old = b.hsp[r];
+    SysParams p = make_sys(c);
+    p.walk = walk;
+    grid_of(c.box, c.list_range, walk, p.dims);
+    p.slot_off = old.slot_off; p.n = old.n; p.head_off = old.head_off; p.nheads = old.nheads;
+    b.hsp[r] = p;
+  }
+  drop_graphs(b);
+  alloc_grids(b);
+  upload_params(b);
+}
+template <class F> double tune_time(Batch& b, int reps, F&& f) {
+  cudaEvent_t e0, e1;
+  SOUP_CUDA_TRY(cudaEventCreate(&e0));
+  SOUP_CUDA_TRY(cudaEventCreate(&e1));
+  f();   // warm
+  SOUP_CUDA_TRY(cudaEventRecord(e0, b.stream));
+  for (int k = 0; k < reps; ++k) f();
+  SOUP_CUDA_TRY(cudaEventRecord(e1, b.stream));
+  SOUP_CUDA_TRY(cudaEventSynchronize(e1));
+  float ms = 0.f;
+  SOUP_CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return ms / reps;
+}
+}  // namespace
+
 extern "C" {
 
 int soup_create(const SoupConfig* cfg, const SoupInitState* init, SoupHandle** out) {
@@ -1020,6 +1112,65 @@ int soup_set_box(SoupHandle* h, const double box[3]) {
     upload_params(b);
     force_pass(b);
     SOUP_CUDA_TRY(cudaStreamSynchronize(b.stream));
+  });
+}
+
+int soup_autotune(SoupHandle* h, uint32_t steps, SoupTuneResult* out) {
+  return guarded(h, [&](Batch& b, uint32_t) {
+    if (steps < 10) fail(SOUP_E_ARG, "autotune: at least 10 steps per candidate");
+    const TuneSnapshot snap = tune_snapshot(b);
+    const bool prof = b.prof;
+    b.prof = false;
+    std::vector<double> planned(b.R);
+    for (uint32_t r = 0; r < b.R; ++r) planned[r] = b.cfg[r].skin;
+    const int walk0 = b.hsp[0].walk;
+    const int tpp0 = b.tpp;
+    auto steps_ms = [&]() { return tune_time(b, 1, [&] { step_batch(b, steps); }) / steps; };
+    SoupTuneResult res{};
+    res.ms_per_step_before = steps_ms();
+    tune_restore(b, snap);
+    // block shape: lanes per particle of the list force, timed on the force alone
+    const int tpps[3] = {2, 4, 8};
+    double best = 1e30;
+    for (int t : tpps) {
+      b.tpp = t;
+      const double ms = tune_time(b, 5, [&] { launch_force_list(b); });
+      if (ms < best) { best = ms; res.tpp = (uint32_t)t; }
+    }
+    b.tpp = (int)res.tpp;
+    drop_graphs(b);
+    // cell size: the list-walk radius (cell = list range / walk), timed on the list build
+    best = 1e30;
+    for (int w : {2, 3}) {
+      tune_plan(b, planned, w);
+      force_pass(b);
+      const double ms = tune_time(b, 3, [&] { launch_cell_index(b); launch_build_lists(b); });
+      if (ms < best) { best = ms; res.walk = (uint32_t)w; }
+    }
+    // skin (drift-triggered rebuilds only): at most the planned one, which sized the list capacity;
+    // timed on whole steps, rebuilds and sweeps included
+    res.skin_scale = 1.0;
+    if (b.cfg[0].rebuild_on_drift) {
+      best = 1e30;
+      for (double f : {0.6, 0.8, 1.0}) {
+        std::vector<double> sk(b.R);
+        for (uint32_t r = 0; r < b.R; ++r) sk[r] = planned[r] * f;
+        tune_plan(b, sk, (int)res.walk);
+        tune_restore(b, snap);
+        const double ms = steps_ms();
+        if (ms < best) { best = ms; res.skin_scale = f; }
+      }
+    }
+    std::vector<double> sk(b.R);
+    for (uint32_t r = 0; r < b.R; ++r) sk[r] = planned[r] * res.skin_scale;
+    tune_plan(b, sk, (int)res.walk);
+    tune_restore(b, snap);
+    res.ms_per_step_after = steps_ms();
+    tune_restore(b, snap);
+    b.prof = prof;
+    res.tpp_before = (uint32_t)tpp0;
+    res.walk_before = (uint32_t)walk0;
+    if (out) *out = res;
   });
 }
 

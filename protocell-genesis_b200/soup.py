@@ -218,6 +218,12 @@ class SoupSystem:
         b = (C.c_double * 3)(*[float(x) for x in box])
         _check(self._lib, self._h, self._lib.soup_set_box(self._h, b))
 
+    def autotune(self, steps: int = 20) -> dict:
+        """Pick the list force's lanes per particle, the neighbour-cell size and (with drift-triggered
+        rebuilds) the skin for this system's whole batch by timing them, keep the choice, and restore
+        the state (see soup_autotune in include/soup_b200.h)."""
+        return _autotune(self._lib, self._h, steps)
+
     # ---- Monte Carlo and analysis ----
     def protonation_sweep(self):
         r = _abi.SoupSweepResult()
@@ -349,6 +355,14 @@ class SoupSystem:
     protonationRngState = protonation_rng_state
 
 
+def _autotune(lib, h, steps):
+    r = _abi.SoupTuneResult()
+    _check(lib, h, lib.soup_autotune(h, int(steps), C.byref(r)))
+    return dict(tpp=r.tpp, walk=r.walk, tpp_before=r.tpp_before, walk_before=r.walk_before,
+                skin_scale=r.skin_scale, ms_per_step_before=r.ms_per_step_before,
+                ms_per_step_after=r.ms_per_step_after)
+
+
 class SoupBatch:
     """Many independent replicas stepped together (one launch per kernel per step)."""
 
@@ -377,6 +391,10 @@ class SoupBatch:
         rc = self._lib.soup_batch_step(self._h, int(n))
         if rc != 0:
             raise _abi.SoupError(rc, self._lib.soup_batch_last_error(self._h).decode())
+
+    def autotune(self, steps: int = 20) -> dict:
+        """soup_autotune for the whole batch (through replica 0's handle, which addresses the batch)."""
+        return _autotune(self._lib, self.replicas[0]._h, steps)
 
     def dispose(self):
         if getattr(self, "_h", None):
