@@ -44,7 +44,7 @@ def workload_opts(cfgm, seed=19, skin=1.0, sweep_every=10, scale=1.0):
 
 def workload_name(skin):
     return (f"campaign shape: 483,268 beads, 76 sigma box, pH 7 MC every 10 steps, I 0.01 M (rc_es 15.2), "
-            f"bonds every 20, Verlet skin {skin} rebuilt on half-skin drift")
+            f"bonds every 20, Verlet skin planned {skin} (scaled by the autotuner) rebuilt on half-skin drift")
 
 
 class ClockSampler:
@@ -428,6 +428,7 @@ def run_cuda(args):
     L.soup_fresh_state(C.byref(cfg), p(host["positions"]), p(host["velocities"]), p(fr), p(br), p(tr))
     s = pkg.SoupSystem(cfg)
     relax = s.relax_cold_start(args.relax, 0.1)
+    tune = s.autotune(steps=20) if not args.no_tune else None   # untimed; the choice stays in effect
     s.step(args.warmup)
     stream = torch.cuda.ExternalStream(L.soup_stream(s._h))
     e0 = torch.cuda.Event(enable_timing=True)
@@ -473,14 +474,20 @@ def run_cuda(args):
     achieved = bytes_per_launch / (f_ms / max(f_n, 1) / 1e3) / 1e9 if f_n else None
     peak, peak_kind = peaks()
     # DRAM bytes per launch of the force kernel from the committed ncu summary (captured on the
-    # quarter-size case and scaled to 483,268 beads there); scaled again for other sizes
+    # quarter-size case and scaled there to 483,268 beads at its mean list length); scaled again by
+    # particles x list entries, which the traffic follows
     traffic = None
     tf = os.path.join(ROOT, "profiles", "k_force_campaign121k.md")
     if os.path.exists(tf):
+        t483 = l483 = None
         with open(tf) as fh:
             for line in fh:
                 if line.startswith("traffic_bytes_per_launch_483k:"):
-                    traffic = float(line.split(":", 1)[1]) * n / 483268.0
+                    t483 = float(line.split(":", 1)[1])
+                if line.startswith("mean_list_entries_483k:"):
+                    l483 = float(line.split(":", 1)[1])
+        if t483 is not None:
+            traffic = t483 * (n * mean_list) / (483268.0 * (l483 or mean_list))
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": (achieved / peak) if achieved else None, "traffic": traffic,
                 "kernel": "k_force (list pair force + bonded terms)",
@@ -549,7 +556,7 @@ def run_cuda(args):
                        "relax": {"iterations": args.relax, "max_force_after": relax["maxForceAfter"]},
                        "rebuilds_in_timed_region": info1["rebuilds"] - info0["rebuilds"],
                        "sweeps_in_timed_region": info1["sweeps"] - info0["sweeps"],
-                       "tpp": int(os.environ.get("SOUP_TPP", 4)),
+                       "autotune": tune,
                        "execution": "steps in captured CUDA graphs of 10 (one sweep period), the drift-triggered "
                                     "rebuild a conditional node",
                        "split": f"phases and the force roofline from a profiled segment of {args.prof_steps} steps "
@@ -580,7 +587,7 @@ def main():
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-replica measurement")
     ap.add_argument("--replicas", type=int, default=64)
     ap.add_argument("--batched-steps", type=int, default=100)
-    ap.add_argument("--no-tune", action="store_true", help="skip the batched form's autotuning")
+    ap.add_argument("--no-tune", action="store_true", help="skip the autotuning (plain and batched)")
     ap.add_argument("--no-gradient", action="store_true", help="skip the forward + adjoint window measurement")
     ap.add_argument("--prof-steps", type=int, default=100, help="steps of the profiled segment (per-kernel split)")
     ap.add_argument("--grad-steps", type=int, default=200)
