@@ -320,6 +320,7 @@ def run_batched(args, pkg, L, cfgm, rank, torch):
     total = sum(int(c.n) for c in cfgs)
     tune = batch.autotune(steps=20) if not args.no_tune else None   # untimed; the choice stays in effect
     batch.step(args.warmup)
+    batch.prepare_graphs()
     h0 = batch.replicas[0]._h
     stream = torch.cuda.ExternalStream(L.soup_stream(h0))
     e0 = torch.cuda.Event(enable_timing=True)
@@ -430,6 +431,7 @@ def run_cuda(args):
     relax = s.relax_cold_start(args.relax, 0.1)
     tune = s.autotune(steps=20) if not args.no_tune else None   # untimed; the choice stays in effect
     s.step(args.warmup)
+    s.prepare_graphs()   # every chunk graph of the schedule captured before the timed region
     stream = torch.cuda.ExternalStream(L.soup_stream(s._h))
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)

@@ -247,6 +247,9 @@ typedef struct SoupTuneResult {
   double ms_per_step_before, ms_per_step_after;
 } SoupTuneResult;
 int soup_autotune(SoupHandle* h, uint32_t steps, SoupTuneResult* out);
+/* soup_step runs chunks of chunkSteps steps (at least 4) as captured CUDA graphs, captured on first
+ * use; this captures every chunk graph of the current schedule now, without stepping. */
+int soup_prepare_graphs(SoupHandle* h);
 /* Replace the whole state (CreateSoupOpts.resume semantics); NULL members keep current values. */
 int soup_write_state(SoupHandle* h, const SoupInitState* st);
 

@@ -5,6 +5,7 @@
 // soup/src/soup-grid-verlet.ts:236-313 (rebuild sequence and assertVerletSafety), soup/src/soup-health.ts
 // (assertStateFinite), soup/src/soup-readback.ts (readbacks), soup/src/soup-relax.ts:87-185.
 #include <algorithm>
+#include <numeric>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
@@ -602,14 +603,32 @@ Batch::ChunkGraph capture_chunk(Batch& b, uint64_t chunk, uint64_t start, uint64
   return cgr;
 }
 
+uint64_t chunk_key(const Batch& b, uint64_t chunk, uint64_t start) {
+  const SoupConfig& c0 = b.cfg[0];
+  return chunk | ((start % c0.bond_interval) << 20) | (c0.rebuild_on_drift ? 0ull : ((start % c0.rebuild_every) << 40));
+}
+const Batch::ChunkGraph* find_graph(const Batch& b, uint64_t key) {
+  for (auto& x : b.graphs)
+    if (x.key == key) return &x;
+  return nullptr;
+}
+// capture (without running) the graphs of every schedule phase the chunks from `start` go through
+void prepare_graphs(Batch& b, uint64_t chunk, uint64_t start) {
+  const SoupConfig& c0 = b.cfg[0];
+  const uint64_t period = c0.rebuild_on_drift ? c0.bond_interval : std::lcm<uint64_t>(c0.bond_interval, c0.rebuild_every);
+  for (uint64_t s0 = start, k = 0; k < period; ++k, s0 += chunk) {
+    const uint64_t key = chunk_key(b, chunk, s0);
+    if (find_graph(b, key)) continue;
+    if (b.graphs.size() >= 16) return;
+    b.graphs.push_back(capture_chunk(b, chunk, s0, key));
+    if (chunk_key(b, chunk, s0 + chunk) == chunk_key(b, chunk, start)) return;   // the phases repeat
+  }
+}
+
 // one chunk from its cached graph (captured on first use); the host bookkeeping of the steps
 void run_chunk_graph(Batch& b, uint64_t chunk, uint64_t start) {
-  const SoupConfig& c0 = b.cfg[0];
-  const uint64_t key = chunk | ((start % c0.bond_interval) << 20) |
-                       (c0.rebuild_on_drift ? 0ull : ((start % c0.rebuild_every) << 40));
-  const Batch::ChunkGraph* g = nullptr;
-  for (auto& x : b.graphs)
-    if (x.key == key) g = &x;
+  const uint64_t key = chunk_key(b, chunk, start);
+  const Batch::ChunkGraph* g = find_graph(b, key);
   if (!g) {
     if (b.graphs.size() >= 16) drop_graphs(b);
     b.graphs.push_back(capture_chunk(b, chunk, start, key));
@@ -1112,6 +1131,13 @@ int soup_set_box(SoupHandle* h, const double box[3]) {
     upload_params(b);
     force_pass(b);
     SOUP_CUDA_TRY(cudaStreamSynchronize(b.stream));
+  });
+}
+
+int soup_prepare_graphs(SoupHandle* h) {
+  return guarded(h, [&](Batch& b, uint32_t) {
+    const uint64_t chunk = b.cfg[0].chunk_steps ? b.cfg[0].chunk_steps : 1000;
+    if (b.graphs_enabled && chunk >= 4) prepare_graphs(b, chunk, b.step[0]);
   });
 }
 

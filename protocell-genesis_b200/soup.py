@@ -218,6 +218,10 @@ class SoupSystem:
         b = (C.c_double * 3)(*[float(x) for x in box])
         _check(self._lib, self._h, self._lib.soup_set_box(self._h, b))
 
+    def prepare_graphs(self):
+        """Capture the step graphs of the current schedule now (soup_step captures them on first use)."""
+        _check(self._lib, self._h, self._lib.soup_prepare_graphs(self._h))
+
     def autotune(self, steps: int = 20) -> dict:
         """Pick the list force's lanes per particle, the neighbour-cell size and (with drift-triggered
         rebuilds) the skin for this system's whole batch by timing them, keep the choice, and restore
@@ -391,6 +395,10 @@ class SoupBatch:
         rc = self._lib.soup_batch_step(self._h, int(n))
         if rc != 0:
             raise _abi.SoupError(rc, self._lib.soup_batch_last_error(self._h).decode())
+
+    def prepare_graphs(self):
+        """soup_prepare_graphs for the whole batch."""
+        _check(self._lib, self.replicas[0]._h, self._lib.soup_prepare_graphs(self.replicas[0]._h))
 
     def autotune(self, steps: int = 20) -> dict:
         """soup_autotune for the whole batch (through replica 0's handle, which addresses the batch)."""
