@@ -687,25 +687,33 @@ void step_batch(Batch& b, uint64_t n) {
 }
 
 // ---- readbacks -------------------------------------------------------------------------------
-// Download one array of replica r in slot order and scatter it into original order.
+// Replica r's array in original order, gathered on the device into scratch (the gather's staging
+// buffer, free outside a rebuild) and copied out in one piece; bond partners and centre links map
+// from global slots back to replica indices.
+template <class T>
+__global__ void k_to_original(const T* __restrict__ src, const uint32_t* __restrict__ id, uint32_t off, uint32_t n,
+                              uint32_t per, bool map_ids, T* __restrict__ dst) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const uint32_t i = id[off + k] - off;
+  for (uint32_t e = 0; e < per; ++e) {
+    T v = src[(size_t)(off + k) * per + e];
+    if constexpr (std::is_same<T, uint32_t>::value) {
+      if (map_ids && v != NONE) v -= off;
+    }
+    dst[(size_t)i * per + e] = v;
+  }
+}
 template <class T>
 void read_replica(Batch& b, uint32_t r, const T* dev, uint32_t per, T* dst, bool map_ids) {
   const uint32_t n = b.cfg[r].n, off = b.hsp[r].slot_off;
-  std::vector<T> tmp((size_t)n * per);
-  std::vector<uint32_t> ids(n);
-  SOUP_CUDA_TRY(cudaMemcpyAsync(tmp.data(), dev + (size_t)off * per, sizeof(T) * tmp.size(), cudaMemcpyDeviceToHost, b.stream));
-  SOUP_CUDA_TRY(cudaMemcpyAsync(ids.data(), b.id + off, 4 * (size_t)n, cudaMemcpyDeviceToHost, b.stream));
+  static_assert(sizeof(T) <= 16, "scratch holds 16 bytes a particle");
+  if (sizeof(T) * per > 16) fail(SOUP_E_ARG, "readback wider than the scratch");
+  T* scratch = reinterpret_cast<T*>(b.pos2);
+  if (n) k_to_original<T><<<(n + 255) / 256, 256, 0, b.stream>>>(dev, b.id, off, n, per, map_ids, scratch);
+  SOUP_CUDA_TRY(cudaGetLastError());
+  SOUP_CUDA_TRY(cudaMemcpyAsync(dst, scratch, sizeof(T) * (size_t)n * per, cudaMemcpyDeviceToHost, b.stream));
   SOUP_CUDA_TRY(cudaStreamSynchronize(b.stream));
-  for (uint32_t k = 0; k < n; ++k) {
-    const uint32_t i = ids[k] - off;
-    for (uint32_t e = 0; e < per; ++e) {
-      T v = tmp[(size_t)k * per + e];
-      if constexpr (std::is_same<T, uint32_t>::value) {
-        if (map_ids && v != NONE) v -= off;
-      }
-      dst[(size_t)i * per + e] = v;
-    }
-  }
 }
 
 void need(size_t bytes, size_t want) {
