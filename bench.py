@@ -303,6 +303,128 @@ def bilayer_patch(L, cfgm, lx=32.0, lz=40.0, per_side=32, seed=11, kT=1.0, ph=9.
     return cfg, state
 
 
+def parcel_configs(cfgm, seed, replicas, n=60000, density=1.1):
+    """Finite water parcels: n beads inside a neutral spherical wall (stiffness 100) at the reference's
+    confined density, 12% of the beads in five-bead amphiphiles, the rest water; pH ~ U[6, 8] with
+    the heads' initial charges from initialCharges, I = 0.01 M for every replica (one Debye kappa,
+    which the batched gradient window needs)."""
+    import math
+    import numpy as np
+    rng = np.random.default_rng(seed)
+    radius = (n / density / (4.0 / 3.0 * math.pi)) ** (1.0 / 3.0)
+    side = 2.0 * radius + 34.0   # the face clearance must exceed the head-list range (16.2 sigma at 0.01 M)
+    na = int(0.12 * n) // 5
+    out = []
+    for r in range(replicas):
+        opts = cfgm.SoupOptions(box=[side] * 3, seed=int(seed * 1000 + r), kT=1.1,
+                                start={"C": 4 * na, "O": na, "H": 0, "M": 0, "W": n - 5 * na},
+                                electrostatics={"enabled": True, "pH": float(rng.uniform(6.0, 8.0)),
+                                                "ionicStrengthMolar": 0.01},
+                                confine={"radiusSigma": radius, "stiffness": 100.0},
+                                skin=1.0, rebuild_on_drift=True, sweep_every=10, chunk_steps=10,
+                                es_list_capacity=na)   # a parcel is smaller than the head-list range
+        out.append((cfgm.resolve(opts), na, int(rng.integers(1 << 31)), radius))
+    return out
+
+
+def parcel_state(L, cfg, na, seed, radius):
+    """amphiphile_state inside the parcel: chain centres uniform in the ball of radius - 3, water
+    uniform in the ball of radius - 0.5, about the box centre."""
+    import numpy as np
+    st = amphiphile_state(L, cfg, na, seed)
+    rng = np.random.default_rng(seed + 1)
+    centre = np.array(list(cfg.box), np.float64) / 2.0
+
+    def ball(k, rad):
+        out = np.empty((0, 3))
+        while len(out) < k:
+            c = rng.uniform(-rad, rad, (2 * k + 16, 3))
+            out = np.concatenate([out, c[np.linalg.norm(c, axis=1) < rad]])
+        return out[:k]
+
+    pos = st["positions"].reshape(-1, 4)
+    u = rng.normal(size=(na, 3))
+    u /= np.linalg.norm(u, axis=1, keepdims=True)
+    chain = ball(na, radius - 3.0)[:, None, :] + ((np.arange(5) - 2.0) * 0.95)[None, :, None] * u[:, None, :]
+    pos[:5 * na, :3] = (chain.reshape(-1, 3) + centre).astype(np.float32)
+    pos[5 * na:, :3] = (ball(cfg.n - 5 * na, radius - 0.5) + centre).astype(np.float32)
+    st["positions"] = pos.reshape(-1)
+    return st
+
+
+def run_gradient_batched(args, pkg, L, torch):
+    """Batched replicas + adjoint: 16 finite water parcels of 60k beads stepped as one batch; forward
+    + adjoint of the encapsulated-water proxy over a window, with respect to the nine parameters
+    (the head-water depth A_polar_solvent among them)."""
+    import numpy as np
+    from protocell_genesis_b200 import adjoint, config as cfgm
+    items = parcel_configs(cfgm, seed=3, replicas=args.parcel_replicas)
+    cfgs, states = [], []
+    for cfg, na, sd, radius in items:
+        st = parcel_state(L, cfg, na, sd, radius)
+        s_ = pkg.SoupSystem(cfg, st)
+        s_.relax_cold_start(args.relax, 0.1)
+        st["positions"] = s_.particles()
+        s_.dispose()
+        cfgs.append(cfg)
+        states.append(st)
+    batch = pkg.SoupBatch(cfgs, states)
+    batch.step(20)
+    N = batch.n
+    kinds = np.concatenate([st["positions"].reshape(-1, 4)[:, 3] for st in states])
+    rep = np.concatenate([np.full(c.n, r) for r, c in enumerate(cfgs)])
+    heads = torch.tensor(kinds == 1.0, device="cuda")
+    water = torch.tensor(kinds == 4.0, device="cuda")
+    rep_t = torch.tensor(rep, device="cuda")
+    R = len(cfgs)
+    centre = torch.tensor(list(cfgs[0].box), dtype=torch.float64, device="cuda") / 2.0
+    nh = torch.zeros(R, dtype=torch.float64, device="cuda").index_add_(0, rep_t[heads], torch.ones(int(heads.sum()), dtype=torch.float64, device="cuda"))
+
+    def encapsulated(traj):
+        # per replica and frame: the heads' mean distance from the parcel centre; the loss counts the
+        # water inside it smoothly (logistic of width 0.5 sigma), summed over replicas, averaged over frames
+        rad = (traj[:, :, :3].double() - centre).norm(dim=-1)
+        shell = torch.zeros((traj.shape[0], R), dtype=torch.float64, device="cuda")
+        shell = shell.index_add(1, rep_t[heads], rad[:, heads]) / nh
+        inside = torch.sigmoid((shell[:, rep_t[water]] - rad[:, water]) / 0.5)
+        return inside.sum(dim=1).mean()
+
+    steps, every = args.parcel_steps, 20
+    stream = torch.cuda.ExternalStream(L.soup_stream(batch.replicas[0]._h))
+    theta0 = batch.get_diff_params()
+
+    def window():
+        th = torch.tensor(theta0, dtype=torch.float64, requires_grad=True)
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        torch.cuda.synchronize()
+        e0.record(stream)
+        traj = adjoint.SoupWindow.apply(th, batch, steps, every)
+        e1.record(stream)
+        loss = encapsulated(traj)
+        loss.backward()
+        e2.record(stream)
+        torch.cuda.synchronize()
+        return float(loss.detach()), th.grad.numpy(), e0.elapsed_time(e1), e1.elapsed_time(e2)
+
+    window()
+    fwd, bwd = [], []
+    for _ in range(args.grad_windows):
+        loss, grad, f_ms, b_ms = window()
+        fwd.append(f_ms)
+        bwd.append(b_ms)
+    batch.dispose()
+    total = (sum(fwd) + sum(bwd)) / len(fwd)
+    return {"value": N * steps / (total / 1e3), "unit": "particle-steps/s (forward + adjoint)", "replicas": R,
+            "beads": N, "window_steps": steps, "checkpoint_every": every, "windows": len(fwd),
+            "ms_per_window": total, "forward_ms": sum(fwd) / len(fwd), "backward_ms": sum(bwd) / len(bwd),
+            "loss": "encapsulated-water proxy", "value_of_loss": loss,
+            "theta": list(adjoint.PARAM_NAMES), "grad": [float(x) for x in grad],
+            "workload": f"{R} spherical water parcels of {cfgs[0].n} beads (radius {items[0][3]:.1f} sigma, "
+                        f"density 1.1 as the reference's confined composition) behind a neutral wall, 12% "
+                        f"beads in five-bead amphiphiles, pH U[6,8], I 0.01 M; a {steps}-step window with bond "
+                        f"and charge Monte Carlo held off; seeded synthetic, relaxed untimed"}
+
+
 def run_batched(args, pkg, L, cfgm, rank, torch):
     """The batched form: many uneven replicas stepped together, one launch per kernel per step."""
     import ctypes as C
@@ -541,6 +663,14 @@ def run_cuda(args):
             batched["value"] = aggregate_rate(1, batched["beads"], 1, batched["ms_per_step"])
         batched["vs_plain"] = batched["value"] / value
 
+    gradient_batched = None
+    if not args.no_gradient:
+        gradient_batched = run_gradient_batched(args, pkg, L, torch)
+        if dist:
+            gradient_batched["ms_per_window"] = max_over_ranks(gradient_batched["ms_per_window"], dist, "cuda")
+            gradient_batched["value"] = aggregate_rate(ws, gradient_batched["beads"], gradient_batched["window_steps"],
+                                                       gradient_batched["ms_per_window"])
+
     gradient = None
     if not args.no_gradient:
         gradient = run_gradient(args, pkg, L, torch)
@@ -564,7 +694,8 @@ def run_cuda(args):
                        "split": f"phases and the force roofline from a profiled segment of {args.prof_steps} steps "
                                 "right after the timed region"},
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
-            "clocks": clk.summary(), "phases": phases, "batched": batched, "gradient": gradient}
+            "clocks": clk.summary(), "phases": phases, "batched": batched, "gradient": gradient,
+            "gradient_batched": gradient_batched}
     if rank == 0:
         print(json.dumps(line), flush=True)
     s.dispose()
@@ -594,6 +725,8 @@ def main():
     ap.add_argument("--prof-steps", type=int, default=100, help="steps of the profiled segment (per-kernel split)")
     ap.add_argument("--grad-steps", type=int, default=200)
     ap.add_argument("--grad-windows", type=int, default=3)
+    ap.add_argument("--parcel-replicas", type=int, default=16)
+    ap.add_argument("--parcel-steps", type=int, default=200)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -339,7 +339,10 @@ int soup_density_profile_z(SoupHandle* h, uint32_t bins, uint32_t head_kind_mask
  *   the class-pair attraction depths A[apolar][apolar], A[apolar][polar], A[apolar][solvent],
  *   A[polar][polar], A[polar][solvent], A[solvent][solvent] (symmetric table, SoupConfig.attr_scale),
  *   k_fene, k_bend, and kappa = 1 / Debye length.  The electrostatics cutoff and the acid-soap depth
- *   stay at their values when kappa changes.  Single systems only (not batch replicas). */
+ *   stay at their values when kappa changes.  On a batch the parameters are shared by every replica
+ *   (which must agree on dt, gamma and, with electrostatics, kappa) and the trajectory, the loss
+ *   gradients and dx0 / dv0 hold every replica's particles in the batch's original order; theta_grad
+ *   sums the replicas. */
 #define SOUP_DIFF_NPARAM 9
 int soup_get_diff_params(SoupHandle* h, double* theta);
 /* Sets the parameters and recomputes the force at the current positions. */

@@ -748,7 +748,8 @@ template <class F> int guarded(SoupHandle* h, F&& f) {
 
 // ---- differentiation ---------------------------------------------------------------------------
 namespace {
-// one step of the window: the plain step without bond Monte Carlo and without the sweep
+// one step of the window: the plain step without bond Monte Carlo and without the sweep, every
+// replica in lockstep
 void diff_step(Batch& b) {
   const SoupConfig& c = b.cfg[0];
   launch_kick_drift(b);
@@ -756,26 +757,32 @@ void diff_step(Batch& b) {
   if (reb) rebuild(b);
   launch_force(b);
   launch_kick_thermo(b);
-  b.step[0]++;
+  for (uint32_t r = 0; r < b.R; ++r) b.step[r]++;
 }
-void diff_read(Batch& b, std::vector<float>& pos, std::vector<float>& vel, std::vector<uint32_t>& trng) {
-  const uint32_t n = b.cfg[0].n;
-  pos.resize(4 * (size_t)n); vel.resize(4 * (size_t)n); trng.resize(n);
-  read_replica<float>(b, 0, reinterpret_cast<const float*>(b.pos), 4, pos.data(), false);
-  read_replica<float>(b, 0, reinterpret_cast<const float*>(b.vel), 4, vel.data(), false);
-  read_replica<uint32_t>(b, 0, b.trng, 1, trng.data(), false);
+using ReplicaArrays = std::vector<std::vector<float>>;
+using ReplicaWords = std::vector<std::vector<uint32_t>>;
+void diff_read(Batch& b, ReplicaArrays& pos, ReplicaArrays& vel, ReplicaWords& trng) {
+  pos.resize(b.R); vel.resize(b.R); trng.resize(b.R);
+  for (uint32_t r = 0; r < b.R; ++r) {
+    const uint32_t n = b.cfg[r].n;
+    pos[r].resize(4 * (size_t)n); vel[r].resize(4 * (size_t)n); trng[r].resize(n);
+    read_replica<float>(b, r, reinterpret_cast<const float*>(b.pos), 4, pos[r].data(), false);
+    read_replica<float>(b, r, reinterpret_cast<const float*>(b.vel), 4, vel[r].data(), false);
+    read_replica<uint32_t>(b, r, b.trng, 1, trng[r].data(), false);
+  }
 }
 // the canonical state at a checkpoint: identity order, then the re-sort and force pass of a restore
-void diff_restore(Batch& b, const std::vector<float>& pos, const std::vector<float>& vel,
-                  const std::vector<uint32_t>& trng) {
+void diff_restore(Batch& b, const ReplicaArrays& pos, const ReplicaArrays& vel, const ReplicaWords& trng) {
   DiffWindow& w = b.diff;
-  SoupInitState m{};
-  m.positions = pos.data(); m.velocities = vel.data(); m.thermo_rng = trng.data();
-  m.bond_slots = w.slots.data(); m.center_link = w.center.data(); m.center_held = w.held.data();
-  m.bond_rng = w.brng.data(); m.charges = w.charge.data(); m.frozen = w.frozen.data();
-  const uint32_t prot = b.prot_rng[0];
-  upload_replica(b, 0, &m, false);
-  b.prot_rng[0] = prot;
+  for (uint32_t r = 0; r < b.R; ++r) {
+    SoupInitState m{};
+    m.positions = pos[r].data(); m.velocities = vel[r].data(); m.thermo_rng = trng[r].data();
+    m.bond_slots = w.slots[r].data(); m.center_link = w.center[r].data(); m.center_held = w.held[r].data();
+    m.bond_rng = w.brng[r].data(); m.charges = w.charge[r].data(); m.frozen = w.frozen[r].data();
+    const uint32_t prot = b.prot_rng[r];
+    upload_replica(b, r, &m, false);
+    b.prot_rng[r] = prot;
+  }
   force_pass(b);
 }
 template <class T> T* dgrow(T* p, size_t& cap, size_t want) {
@@ -1274,26 +1281,43 @@ int soup_get_diff_params(SoupHandle* h, double* theta) {
   });
 }
 
+// the window's parameters are shared by the batch: every replica must agree on kappa (when its
+// electrostatics is on), dt and gamma
+void diff_check_batch(const Batch& b) {
+  for (uint32_t r = 1; r < b.R; ++r) {
+    if (b.cfg[r].dt != b.cfg[0].dt || b.cfg[r].gamma != b.cfg[0].gamma)
+      fail(SOUP_E_STATE, "differentiation of a batch needs one dt and gamma for every replica");
+    if (b.cfg[r].es_enabled && b.cfg[0].es_enabled && b.cfg[r].es_kappa != b.cfg[0].es_kappa)
+      fail(SOUP_E_STATE, "differentiation of a batch needs one Debye kappa for every replica (equal ionic strength)");
+  }
+}
+
 int soup_set_diff_params(SoupHandle* h, const double* theta) {
-  return guarded(h, [&](Batch& b, uint32_t r) {
+  return guarded(h, [&](Batch& b, uint32_t) {
     if (!theta) fail(SOUP_E_ARG, "NULL theta");
-    if (b.R != 1) fail(SOUP_E_STATE, "differentiation works on single systems, not batch replicas");
+    diff_check_batch(b);
     for (int p = 0; p < SOUP_DIFF_NPARAM; ++p) if (!std::isfinite(theta[p])) fail(SOUP_E_ARG, "theta must be finite");
     if (!(theta[6] > 0) || !(theta[7] > 0) || !(theta[8] > 0)) fail(SOUP_E_ARG, "k_fene, k_bend and kappa must be positive");
-    SoupConfig& c = b.cfg[r];
-    for (int p = 0; p < 6; ++p) {
-      c.attr_scale[kDepthPairs[p][0]][kDepthPairs[p][1]] = theta[p];
-      c.attr_scale[kDepthPairs[p][1]][kDepthPairs[p][0]] = theta[p];
+    for (uint32_t r = 0; r < b.R; ++r) {
+      SoupConfig& c = b.cfg[r];
+      for (int p = 0; p < 6; ++p) {
+        c.attr_scale[kDepthPairs[p][0]][kDepthPairs[p][1]] = theta[p];
+        c.attr_scale[kDepthPairs[p][1]][kDepthPairs[p][0]] = theta[p];
+      }
+      c.k_fene = theta[6]; c.k_bend = theta[7]; c.es_kappa = theta[8];
+      if (c.es_enabled) {
+        c.es_shift_u = c.es_coeff_a * std::exp(-c.es_kappa * c.es_cutoff) / c.es_cutoff;
+        c.es_shift_f = c.es_shift_u * (1 / c.es_cutoff + c.es_kappa);
+      }
+      SysParams& P = b.hsp[r];
+      P.es_kappa = (float)c.es_kappa; P.es_fc = (float)c.es_shift_f;
+      P.d_kappa = c.es_kappa; P.d_shiftU = c.es_shift_u; P.d_shiftF = c.es_shift_f;
     }
-    c.k_fene = theta[6]; c.k_bend = theta[7]; c.es_kappa = theta[8];
-    if (c.es_enabled) {
-      c.es_shift_u = c.es_coeff_a * std::exp(-c.es_kappa * c.es_cutoff) / c.es_cutoff;
-      c.es_shift_f = c.es_shift_u * (1 / c.es_cutoff + c.es_kappa);
+    b.hs = make_shared(b.cfg[0]);
+    for (uint32_t r = 1; r < b.R; ++r) {
+      const Shared o = make_shared(b.cfg[r]);
+      b.hs.rmax2 = std::max(b.hs.rmax2, o.rmax2);
     }
-    b.hs = make_shared(c);
-    SysParams& P = b.hsp[r];
-    P.es_kappa = (float)c.es_kappa; P.es_fc = (float)c.es_shift_f;
-    P.d_kappa = c.es_kappa; P.d_shiftU = c.es_shift_u; P.d_shiftF = c.es_shift_f;
     upload_params(b);
     launch_force(b);
     SOUP_CUDA_TRY(cudaStreamSynchronize(b.stream));
@@ -1302,22 +1326,27 @@ int soup_set_diff_params(SoupHandle* h, const double* theta) {
 
 int soup_diff_forward(SoupHandle* h, uint32_t steps, uint32_t checkpoint_every, float* traj_device) {
   return guarded(h, [&](Batch& b, uint32_t) {
-    if (b.R != 1) fail(SOUP_E_STATE, "differentiation works on single systems, not batch replicas");
+    diff_check_batch(b);
     if (steps == 0 || checkpoint_every == 0) fail(SOUP_E_ARG, "steps and checkpoint_every must be positive");
     if (traj_device && (reinterpret_cast<uintptr_t>(traj_device) & 15u)) fail(SOUP_E_ARG, "traj_device must be 16-byte aligned");
     DiffWindow& w = b.diff;
-    const uint32_t n = b.cfg[0].n;
+    const uint32_t N = b.N, R = b.R;
     w.ready = false;
-    w.charge.resize(n); w.slots.resize(3 * (size_t)n); w.center.resize(n); w.held.resize(n); w.brng.resize(n);
-    std::vector<uint8_t> fr(n);
-    read_replica<float>(b, 0, b.charge, 1, w.charge.data(), false);
-    read_replica<uint32_t>(b, 0, b.slots, 3, w.slots.data(), true);
-    read_replica<uint32_t>(b, 0, b.center, 1, w.center.data(), true);
-    read_replica<uint32_t>(b, 0, b.held, 1, w.held.data(), false);
-    read_replica<uint32_t>(b, 0, b.brng, 1, w.brng.data(), false);
-    read_replica<uint8_t>(b, 0, b.frozen, 1, fr.data(), false);
-    w.frozen.assign(fr.begin(), fr.end());
-    w.steps = steps; w.every = checkpoint_every; w.step0 = b.step[0]; w.prot_rng = b.prot_rng[0];
+    w.charge.resize(R); w.slots.resize(R); w.center.resize(R); w.held.resize(R); w.brng.resize(R); w.frozen.resize(R);
+    for (uint32_t r = 0; r < R; ++r) {
+      const uint32_t n = b.cfg[r].n;
+      w.charge[r].resize(n); w.slots[r].resize(3 * (size_t)n); w.center[r].resize(n); w.held[r].resize(n);
+      w.brng[r].resize(n);
+      std::vector<uint8_t> fr(n);
+      read_replica<float>(b, r, b.charge, 1, w.charge[r].data(), false);
+      read_replica<uint32_t>(b, r, b.slots, 3, w.slots[r].data(), true);
+      read_replica<uint32_t>(b, r, b.center, 1, w.center[r].data(), true);
+      read_replica<uint32_t>(b, r, b.held, 1, w.held[r].data(), false);
+      read_replica<uint32_t>(b, r, b.brng, 1, w.brng[r].data(), false);
+      read_replica<uint8_t>(b, r, b.frozen, 1, fr.data(), false);
+      w.frozen[r].assign(fr.begin(), fr.end());
+    }
+    w.steps = steps; w.every = checkpoint_every; w.step0 = b.step[0]; w.prot_rng = b.prot_rng;
     w.ck_pos.clear(); w.ck_vel.clear(); w.ck_trng.clear();
     float4* traj = reinterpret_cast<float4*>(traj_device);
     for (uint32_t t = 0; t < steps; ++t) {
@@ -1328,7 +1357,7 @@ int soup_diff_forward(SoupHandle* h, uint32_t steps, uint32_t checkpoint_every, 
         if (t == 0 && traj) adj_unpermute(b, traj);
       }
       diff_step(b);
-      if (traj) adj_unpermute(b, traj + (size_t)(t + 1) * n);
+      if (traj) adj_unpermute(b, traj + (size_t)(t + 1) * N);
     }
     diff_read(b, w.end_pos, w.end_vel, w.end_trng);
     w.end_step = b.step[0];
@@ -1343,58 +1372,62 @@ int soup_diff_backward(SoupHandle* h, const float* dldx_device, double* theta_gr
     DiffWindow& w = b.diff;
     if (!w.ready) fail(SOUP_E_STATE, "no differentiable window: call soup_diff_forward first");
     if (!dldx_device || !theta_grad) fail(SOUP_E_ARG, "NULL argument");
-    const uint32_t n = b.cfg[0].n, T = w.steps, K = w.every;
+    const uint32_t N = b.N, T = w.steps, K = w.every;
     const float4* dldx = reinterpret_cast<const float4*>(dldx_device);
     // scratch
     size_t cap1 = w.frames_cap;
-    w.frames = dgrow(w.frames, cap1, (size_t)(K + 1) * n);
+    w.frames = dgrow(w.frames, cap1, (size_t)(K + 1) * N);
     w.frames_cap = cap1;
     if (!w.A) {
-      SOUP_CUDA_TRY(cudaMalloc(&w.A, 16 * (size_t)n)); SOUP_CUDA_TRY(cudaMalloc(&w.B, 16 * (size_t)n));
-      SOUP_CUDA_TRY(cudaMalloc(&w.g, 16 * (size_t)n)); SOUP_CUDA_TRY(cudaMalloc(&w.jg, 16 * (size_t)n));
-      SOUP_CUDA_TRY(cudaMalloc(&w.frozen_o, (size_t)n));
+      SOUP_CUDA_TRY(cudaMalloc(&w.A, 16 * (size_t)N)); SOUP_CUDA_TRY(cudaMalloc(&w.B, 16 * (size_t)N));
+      SOUP_CUDA_TRY(cudaMalloc(&w.g, 16 * (size_t)N)); SOUP_CUDA_TRY(cudaMalloc(&w.jg, 16 * (size_t)N));
+      SOUP_CUDA_TRY(cudaMalloc(&w.frozen_o, (size_t)N));
     }
     size_t cap2 = w.partial_cap;
     w.partial = dgrow(w.partial, cap2, adj_partial_count(b));
     w.partial_cap = cap2;
     SOUP_CUDA_TRY(cudaMemsetAsync(w.partial, 0, 8 * adj_partial_count(b), b.stream));
-    std::vector<uint8_t> fo(w.frozen.begin(), w.frozen.end());
-    SOUP_CUDA_TRY(cudaMemcpyAsync(w.frozen_o, fo.data(), n, cudaMemcpyHostToDevice, b.stream));
-    SOUP_CUDA_TRY(cudaMemcpyAsync(w.A, dldx + (size_t)T * n, 16 * (size_t)n, cudaMemcpyDeviceToDevice, b.stream));
-    SOUP_CUDA_TRY(cudaMemsetAsync(w.B, 0, 16 * (size_t)n, b.stream));
-    SOUP_CUDA_TRY(cudaMemsetAsync(w.g, 0, 16 * (size_t)n, b.stream));
+    std::vector<uint8_t> fo(N, 0);   // by the batch's original index: replica r from its slot offset
+    for (uint32_t r = 0; r < b.R; ++r)
+      for (uint32_t i = 0; i < b.cfg[r].n; ++i) fo[b.hsp[r].slot_off + i] = (uint8_t)w.frozen[r][i];
+    SOUP_CUDA_TRY(cudaMemcpyAsync(w.frozen_o, fo.data(), N, cudaMemcpyHostToDevice, b.stream));
+    SOUP_CUDA_TRY(cudaMemcpyAsync(w.A, dldx + (size_t)T * N, 16 * (size_t)N, cudaMemcpyDeviceToDevice, b.stream));
+    SOUP_CUDA_TRY(cudaMemsetAsync(w.B, 0, 16 * (size_t)N, b.stream));
+    SOUP_CUDA_TRY(cudaMemsetAsync(w.g, 0, 16 * (size_t)N, b.stream));
     const SysParams& P = b.hsp[0];
     const float a = 1.0f - P.gdt, hh = P.hdt, dt = P.dt;
     double theta[SOUP_DIFF_NPARAM] = {0};
+    auto set_step = [&](uint64_t s0) { for (uint32_t r = 0; r < b.R; ++r) b.step[r] = s0; };
     const uint32_t nseg = (T + K - 1) / K;
     for (uint32_t seg = nseg; seg-- > 0;) {
       const uint32_t t0 = seg * K, t1 = std::min(t0 + K, T);
-      b.step[0] = w.step0 + t0;
+      set_step(w.step0 + t0);
       diff_restore(b, w.ck_pos[seg], w.ck_vel[seg], w.ck_trng[seg]);
       adj_unpermute(b, w.frames);
       for (uint32_t k = 0; k < t1 - t0; ++k) {
         diff_step(b);
-        adj_unpermute(b, w.frames + (size_t)(k + 1) * n);
+        adj_unpermute(b, w.frames + (size_t)(k + 1) * N);
       }
       for (uint32_t t = t1; t > t0; --t) {
-        adj_scatter_pos(b, w.frames + (size_t)(t - t0) * n);
+        adj_scatter_pos(b, w.frames + (size_t)(t - t0) * N);
         rebuild(b);
         adj_hvp(b, w.g, w.jg, w.partial);
         const float coef = (t - 1 == 0) ? hh : hh * (1.0f + a);
-        adj_update(b, n, w.A, w.B, w.jg, dldx + (size_t)(t - 1) * n, w.frozen_o, a, dt, coef, w.g, nullptr);
+        adj_update(b, N, w.A, w.B, w.jg, dldx + (size_t)(t - 1) * N, w.frozen_o, a, dt, coef, w.g, nullptr);
       }
       if (seg == 0) {   // time 0: the force at x_0 only feeds the first half kick
-        if (dv0_device) SOUP_CUDA_TRY(cudaMemcpyAsync(dv0_device, w.B, 16 * (size_t)n, cudaMemcpyDeviceToDevice, b.stream));
+        if (dv0_device) SOUP_CUDA_TRY(cudaMemcpyAsync(dv0_device, w.B, 16 * (size_t)N, cudaMemcpyDeviceToDevice, b.stream));
         adj_scatter_pos(b, w.frames);
         rebuild(b);
         adj_hvp(b, w.g, w.jg, w.partial);
-        adj_update(b, n, w.A, w.B, w.jg, nullptr, w.frozen_o, a, dt, 0.f, w.g, reinterpret_cast<float4*>(dx0_device));
+        adj_update(b, N, w.A, w.B, w.jg, nullptr, w.frozen_o, a, dt, 0.f, w.g, reinterpret_cast<float4*>(dx0_device));
       }
     }
     // back to the end of the window
-    b.step[0] = w.end_step;
+    set_step(w.end_step);
     adj_theta_sum(b, w.partial, theta);
     diff_restore(b, w.end_pos, w.end_vel, w.end_trng);
+    b.prot_rng = w.prot_rng;
     SOUP_CUDA_TRY(cudaStreamSynchronize(b.stream));
     for (int p = 0; p < SOUP_DIFF_NPARAM; ++p) theta_grad[p] = theta[p];
   });

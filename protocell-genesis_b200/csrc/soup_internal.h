@@ -41,14 +41,16 @@ struct DiffWindow {
   uint32_t steps = 0, every = 0;
   uint64_t step0 = 0;
   bool ready = false;
-  std::vector<std::vector<float>> ck_pos, ck_vel;
-  std::vector<std::vector<uint32_t>> ck_trng;
-  std::vector<float> charge;
-  std::vector<uint32_t> slots, center, held, brng, frozen;
-  std::vector<float> end_pos, end_vel;
-  std::vector<uint32_t> end_trng;
+  // per checkpoint, per replica: positions, velocities, thermostat states in original order
+  std::vector<std::vector<std::vector<float>>> ck_pos, ck_vel;
+  std::vector<std::vector<std::vector<uint32_t>>> ck_trng;
+  // per replica, fixed over the window
+  std::vector<std::vector<float>> charge;
+  std::vector<std::vector<uint32_t>> slots, center, held, brng, frozen;
+  std::vector<std::vector<float>> end_pos, end_vel;
+  std::vector<std::vector<uint32_t>> end_trng;
   uint64_t end_step = 0;
-  uint32_t prot_rng = 0;
+  std::vector<uint32_t> prot_rng;
   float4 *frames = nullptr, *A = nullptr, *B = nullptr, *g = nullptr, *jg = nullptr;
   uint8_t* frozen_o = nullptr;
   double* partial = nullptr;

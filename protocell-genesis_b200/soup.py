@@ -396,6 +396,25 @@ class SoupBatch:
         if rc != 0:
             raise _abi.SoupError(rc, self._lib.soup_batch_last_error(self._h).decode())
 
+    @property
+    def n(self) -> int:
+        """Particles of the whole batch (replica r's original indices follow replica r-1's)."""
+        return sum(int(r.n) for r in self.replicas)
+
+    # the differentiable window over the whole batch: the parameters are shared by every replica,
+    # the trajectory holds every replica's particles (soup_diff_forward / soup_diff_backward)
+    def get_diff_params(self):
+        return self.replicas[0].get_diff_params()
+
+    def set_diff_params(self, theta):
+        self.replicas[0].set_diff_params(theta)
+
+    def diff_forward(self, steps, checkpoint_every, traj_ptr=None):
+        self.replicas[0].diff_forward(steps, checkpoint_every, traj_ptr)
+
+    def diff_backward(self, dldx_ptr, dx0_ptr=None, dv0_ptr=None):
+        return self.replicas[0].diff_backward(dldx_ptr, dx0_ptr, dv0_ptr)
+
     def prepare_graphs(self):
         """soup_prepare_graphs for the whole batch."""
         _check(self._lib, self.replicas[0]._h, self._lib.soup_prepare_graphs(self.replicas[0]._h))

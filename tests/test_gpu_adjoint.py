@@ -215,3 +215,36 @@ def test_thickness_gradient_over_the_200_step_window(patch):
           "\nrel nudged", spread)
     assert v == pytest.approx(v64, rel=1e-5)
     assert np.all(np.abs(grad - grad64) <= 5e-2 * np.abs(grad64)), (grad, grad64)
+
+
+def test_batched_window_equals_its_replicas():
+    """A batch of two patches differentiates as one window with shared parameters: its frames are
+    the replicas' own frames bit for bit, and its gradient is the sum of theirs."""
+    from protocell_genesis_b200.soup import SoupBatch
+    c1, s1 = oracle_bilayer_start(seed=3, relax=300, steps=200)
+    c2, s2 = oracle_bilayer_start(seed=4, relax=300, steps=200)
+    n1, n2 = c1.n, c2.n
+    gen = torch.Generator().manual_seed(7)
+    w = torch.randn((STEPS + 1, n1 + n2, 4), generator=gen, dtype=torch.float64)
+    w[:, :, 3] = 0
+    w[0] = 0
+    box = torch.tensor(list(c1.box) + [1.0], dtype=torch.float64, device="cuda")
+
+    def run(sys_, wt):
+        th = torch.tensor(sys_.get_diff_params(), dtype=torch.float64, requires_grad=True)
+        traj = adjoint.SoupWindow.apply(th, sys_, STEPS, EVERY)
+        loss = _displacement_loss(traj, wt.cuda(), box)
+        loss.backward()
+        return float(loss.detach()), th.grad.numpy().copy(), traj.detach().cpu().numpy()
+
+    batch = SoupBatch([c1, c2], [s1, s2])
+    lb, gb, tb = run(batch, w)
+    batch.dispose()
+    parts = []
+    for c, st, sl in ((c1, s1, slice(0, n1)), (c2, s2, slice(n1, n1 + n2))):
+        g = SoupSystem(c, st)
+        parts.append(run(g, w[:, sl]))
+        g.dispose()
+    assert np.array_equal(tb[:, :n1], parts[0][2]) and np.array_equal(tb[:, n1:], parts[1][2])
+    assert lb == pytest.approx(parts[0][0] + parts[1][0], rel=1e-12)
+    assert np.allclose(gb, parts[0][1] + parts[1][1], rtol=1e-9, atol=1e-12)
