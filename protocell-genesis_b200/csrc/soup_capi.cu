@@ -435,7 +435,7 @@ void destroy_batch(Batch* b) {
                   b->vis, b->frontier};
   for (void* p : ptrs) if (p) cudaFree(p);
   for (void* p : {(void*)b->diff.frames, (void*)b->diff.A, (void*)b->diff.B, (void*)b->diff.g, (void*)b->diff.jg,
-                  (void*)b->diff.frozen_o, (void*)b->diff.partial})
+                  (void*)b->diff.frozen_o, (void*)b->diff.partial, (void*)b->diff.all})
     if (p) cudaFree(p);
   for (const Batch::Mark& m : b->marks) { cudaEventDestroy(m.a); cudaEventDestroy(m.b); }
   for (cudaEvent_t e : b->event_pool) cudaEventDestroy(e);
@@ -784,6 +784,18 @@ void diff_restore(Batch& b, const ReplicaArrays& pos, const ReplicaArrays& vel, 
     b.prot_rng[r] = prot;
   }
   force_pass(b);
+}
+// lists valid for the positions now in b.pos: kept while no particle has moved more than skin/2
+// from where the lists were built (the forward step's own test), rebuilt otherwise
+void refresh_lists(Batch& b) {
+  SOUP_CUDA_TRY(cudaMemsetAsync(b.drift_bits, 0, sizeof(uint32_t) * b.R, b.stream));
+  launch_max_drift(b);
+  if (drift_exceeds(b)) rebuild(b);
+}
+// the device budget for keeping every frame of a window (SOUP_DIFF_FRAME_BUDGET_MB, default 8 GiB)
+size_t frame_budget() {
+  if (const char* e = std::getenv("SOUP_DIFF_FRAME_BUDGET_MB")) return (size_t)std::atoll(e) << 20;
+  return (size_t)8 << 30;
 }
 template <class T> T* dgrow(T* p, size_t& cap, size_t want) {
   if (want <= cap) return p;
@@ -1349,7 +1361,19 @@ int soup_diff_forward(SoupHandle* h, uint32_t steps, uint32_t checkpoint_every, 
     w.steps = steps; w.every = checkpoint_every; w.step0 = b.step[0]; w.prot_rng = b.prot_rng;
     w.ck_pos.clear(); w.ck_vel.clear(); w.ck_trng.clear();
     float4* traj = reinterpret_cast<float4*>(traj_device);
-    for (uint32_t t = 0; t < steps; ++t) {
+    const size_t frame_bytes = 16 * (size_t)N * (steps + 1);
+    w.stored = frame_bytes <= frame_budget();
+    if (w.stored) {   // keep every frame: the reverse pass reads them instead of replaying segments
+      w.all = dgrow(w.all, w.all_cap, (size_t)N * (steps + 1));
+      force_pass(b);
+      adj_unpermute(b, w.all);
+      for (uint32_t t = 0; t < steps; ++t) {
+        diff_step(b);
+        adj_unpermute(b, w.all + (size_t)(t + 1) * N);
+      }
+      if (traj) SOUP_CUDA_TRY(cudaMemcpyAsync(traj, w.all, frame_bytes, cudaMemcpyDeviceToDevice, b.stream));
+    }
+    for (uint32_t t = 0; t < steps && !w.stored; ++t) {
       if (t % checkpoint_every == 0) {
         w.ck_pos.emplace_back(); w.ck_vel.emplace_back(); w.ck_trng.emplace_back();
         diff_read(b, w.ck_pos.back(), w.ck_vel.back(), w.ck_trng.back());
@@ -1398,7 +1422,21 @@ int soup_diff_backward(SoupHandle* h, const float* dldx_device, double* theta_gr
     const float a = 1.0f - P.gdt, hh = P.hdt, dt = P.dt;
     double theta[SOUP_DIFF_NPARAM] = {0};
     auto set_step = [&](uint64_t s0) { for (uint32_t r = 0; r < b.R; ++r) b.step[r] = s0; };
-    const uint32_t nseg = (T + K - 1) / K;
+    if (w.stored) {
+      for (uint32_t t = T; t > 0; --t) {
+        adj_scatter_pos(b, w.all + (size_t)t * N);
+        refresh_lists(b);
+        adj_hvp(b, w.g, w.jg, w.partial);
+        const float coef = (t - 1 == 0) ? hh : hh * (1.0f + a);
+        adj_update(b, N, w.A, w.B, w.jg, dldx + (size_t)(t - 1) * N, w.frozen_o, a, dt, coef, w.g, nullptr);
+      }
+      if (dv0_device) SOUP_CUDA_TRY(cudaMemcpyAsync(dv0_device, w.B, 16 * (size_t)N, cudaMemcpyDeviceToDevice, b.stream));
+      adj_scatter_pos(b, w.all);
+      refresh_lists(b);
+      adj_hvp(b, w.g, w.jg, w.partial);
+      adj_update(b, N, w.A, w.B, w.jg, nullptr, w.frozen_o, a, dt, 0.f, w.g, reinterpret_cast<float4*>(dx0_device));
+    }
+    const uint32_t nseg = w.stored ? 0 : (T + K - 1) / K;
     for (uint32_t seg = nseg; seg-- > 0;) {
       const uint32_t t0 = seg * K, t1 = std::min(t0 + K, T);
       set_step(w.step0 + t0);
@@ -1410,7 +1448,7 @@ int soup_diff_backward(SoupHandle* h, const float* dldx_device, double* theta_gr
       }
       for (uint32_t t = t1; t > t0; --t) {
         adj_scatter_pos(b, w.frames + (size_t)(t - t0) * N);
-        rebuild(b);
+        refresh_lists(b);
         adj_hvp(b, w.g, w.jg, w.partial);
         const float coef = (t - 1 == 0) ? hh : hh * (1.0f + a);
         adj_update(b, N, w.A, w.B, w.jg, dldx + (size_t)(t - 1) * N, w.frozen_o, a, dt, coef, w.g, nullptr);
@@ -1418,7 +1456,7 @@ int soup_diff_backward(SoupHandle* h, const float* dldx_device, double* theta_gr
       if (seg == 0) {   // time 0: the force at x_0 only feeds the first half kick
         if (dv0_device) SOUP_CUDA_TRY(cudaMemcpyAsync(dv0_device, w.B, 16 * (size_t)N, cudaMemcpyDeviceToDevice, b.stream));
         adj_scatter_pos(b, w.frames);
-        rebuild(b);
+        refresh_lists(b);
         adj_hvp(b, w.g, w.jg, w.partial);
         adj_update(b, N, w.A, w.B, w.jg, nullptr, w.frozen_o, a, dt, 0.f, w.g, reinterpret_cast<float4*>(dx0_device));
       }

@@ -51,6 +51,9 @@ struct DiffWindow {
   std::vector<std::vector<uint32_t>> end_trng;
   uint64_t end_step = 0;
   std::vector<uint32_t> prot_rng;
+  bool stored = false;                  // every frame kept on the device (no checkpoints, no replay)
+  float4* all = nullptr;                 // (steps + 1) frames in original order when stored
+  size_t all_cap = 0;
   float4 *frames = nullptr, *A = nullptr, *B = nullptr, *g = nullptr, *jg = nullptr;
   uint8_t* frozen_o = nullptr;
   double* partial = nullptr;

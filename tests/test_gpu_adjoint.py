@@ -133,13 +133,16 @@ def test_start_state_gradients_match_the_fp64_window(patch):
     assert rx < TOL and rv < TOL
 
 
-def test_checkpoint_spacing_and_repeatability(patch):
-    """Each checkpoint re-sorts the particles, which changes FP32 summation order, so different
-    spacings agree to rounding; the same spacing repeats bit for bit (the segments are replayed
-    exactly from their checkpoints)."""
+def test_checkpoint_spacing_and_repeatability(patch, monkeypatch):
+    """The window keeps every frame on the device when they fit its budget, and otherwise checkpoints
+    and replays segments.  Each checkpoint re-sorts the particles, which changes FP32 summation order,
+    so the two modes and different spacings agree to rounding; the same spacing repeats bit for bit
+    (the segments are replayed exactly from their checkpoints)."""
     cfg, start, w = patch
     g = SoupSystem(cfg, start)
     theta0 = g.get_diff_params()
+    l0, g0 = _gpu(g, start, theta0, w, every=3)                # every frame kept
+    monkeypatch.setenv("SOUP_DIFF_FRAME_BUDGET_MB", "0")      # checkpoints and replay
     l1, g1 = _gpu(g, start, theta0, w, every=3)
     l1b, g1b = _gpu(g, start, theta0, w, every=3)
     l2, g2 = _gpu(g, start, theta0, w, every=STEPS)
@@ -147,6 +150,8 @@ def test_checkpoint_spacing_and_repeatability(patch):
     assert l1 == l1b and np.array_equal(g1, g1b)
     assert l2 == pytest.approx(l1, rel=1e-5)
     assert np.allclose(g2, g1, rtol=1e-3, atol=1e-5 * np.abs(g1).max())
+    assert l0 == pytest.approx(l1, rel=1e-5)
+    assert np.allclose(g0, g1, rtol=1e-3, atol=1e-5 * np.abs(g1).max())
 
 
 def _thickness(cfg, start):
