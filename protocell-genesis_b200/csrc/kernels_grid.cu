@@ -184,7 +184,28 @@ __device__ __forceinline__ AxisRange axis_ranges(int q, int R, int dim) {
   return a;
 }
 
-// soup/wgsl/verlet.wgsl:53-92, thread per particle, rows of cells as contiguous slot ranges.
+// The cells lo..hi (unwrapped, hi - lo + 1 < dim) as at most two wrapped [lo,hi] intervals, in the
+// order axis_ranges gives them.
+__device__ __forceinline__ AxisRange span_ranges(int lo, int hi, int dim) {
+  AxisRange a;
+  if (lo < 0) { a.n = 2; a.lo[0] = lo + dim; a.hi[0] = dim - 1; a.lo[1] = 0; a.hi[1] = hi; }
+  else if (hi >= dim) { a.n = 2; a.lo[0] = lo; a.hi[0] = dim - 1; a.lo[1] = 0; a.hi[1] = hi - dim; }
+  else { a.n = 1; a.lo[0] = lo; a.hi[0] = hi; }
+  if (a.n == 2 && a.lo[1] > a.hi[1]) a.n = 1;
+  if (a.n == 2 && a.lo[0] > a.hi[0]) { a.n = 1; a.lo[0] = a.lo[1]; a.hi[0] = a.hi[1]; }
+  return a;
+}
+// distance from p to the cell interval [c cs, (c + 1) cs) along one axis (unwrapped c), less a
+// margin for the rounding of the cell assignment
+__device__ __forceinline__ float gap_to_cell(float p, int c, float cs) {
+  const float lo = (float)c * cs - p, hi = (float)(c + 1) * cs - p;
+  return fmaxf(0.f, fmaxf(lo, -hi) - 1e-4f);
+}
+
+// soup/wgsl/verlet.wgsl:53-92, thread per particle, rows of cells as contiguous slot ranges.  When
+// the walk does not wrap onto itself, each (y, z) row of cells is trimmed to the x cells that can
+// reach the list sphere (with a margin) and rows wholly outside it are skipped; the accept test is
+// unchanged, so the list is the same set.
 __global__ void __launch_bounds__(128) k_build_list(
     const float4* __restrict__ pos, const uint8_t* __restrict__ sysid, const SysParams* __restrict__ sp,
     const uint32_t* __restrict__ cell_of, const uint32_t* __restrict__ start, uint32_t N, uint32_t cap,
@@ -219,6 +240,44 @@ __global__ void __launch_bounds__(128) k_build_list(
   }
   uint32_t cnt = 0;
   uint32_t* row = nl + (size_t)k * cap;
+  auto take = [&](uint32_t a, uint32_t e) {
+    for (uint32_t j = a; j < e; ++j) {
+      if (j == k) continue;
+      const float4 xj = pos[j];
+      const float dx = fast_mi(xi.x - xj.x, box[0], inv[0]);
+      const float dy = fast_mi(xi.y - xj.y, box[1], inv[1]);
+      const float dz = fast_mi(xi.z - xj.z, box[2], inv[2]);
+      const float r2 = dx * dx + dy * dy + dz * dz;
+      if (r2 > lr2_hi) continue;
+      if (r2 >= lr2_lo && !(ex_dist(xi, xj, box) < lr)) continue;
+      if (cnt < cap) row[cnt] = j;
+      ++cnt;
+    }
+  };
+  if (P.dims[0] >= 2 * R + 1 && P.dims[1] >= 2 * R + 1 && P.dims[2] >= 2 * R + 1) {
+    const float cs[3] = {box[0] / (float)P.dims[0], box[1] / (float)P.dims[1], box[2] / (float)P.dims[2]};
+    const float lrm = lr * (1.0f + 1e-5f) + 1e-3f, lrm2 = lrm * lrm;
+    for (int oz = -R; oz <= R; ++oz) {
+      const float gz = gap_to_cell(xi.z, qz + oz, cs[2]);
+      const int cz = (qz + oz + P.dims[2]) % P.dims[2];
+      for (int oy = -R; oy <= R; ++oy) {
+        const float gy = gap_to_cell(xi.y, qy + oy, cs[1]);
+        const float g2 = gy * gy + gz * gz;
+        if (g2 >= lrm2) continue;
+        const float ext = sqrtf(lrm2 - g2);
+        const int xlo = max(qx - R, (int)floorf((xi.x - ext) / cs[0]));
+        const int xhi = min(qx + R, (int)floorf((xi.x + ext) / cs[0]));
+        if (xlo > xhi) continue;
+        const int cy = (qy + oy + P.dims[1]) % P.dims[1];
+        const uint32_t rowbase = P.cell_off + (uint32_t)(P.dims[0] * (cy + P.dims[1] * cz));
+        const AxisRange xr = span_ranges(xlo, xhi, P.dims[0]);
+        for (int sgi = 0; sgi < xr.n; ++sgi) take(start[rowbase + xr.lo[sgi]], start[rowbase + xr.hi[sgi] + 1]);
+      }
+    }
+    if (cnt > cap) { flags[0] = 1u; cnt = cap; }
+    nl_cnt[k] = cnt;
+    return;
+  }
   for (int iz = 0; iz < nz; ++iz) {
     for (int iy = 0; iy < ny; ++iy) {
       uint32_t rowbase = P.cell_off + (uint32_t)(P.dims[0] * (ys[iy] + P.dims[1] * zs[iz]));
