@@ -373,34 +373,55 @@ __global__ void __launch_bounds__(256) k_build_es_list(const uint32_t* __restric
   uint32_t cnt = 0;
   uint32_t* row = es_nl + (size_t)h * cap;
   const uint32_t lt = (1u << lane) - 1u;
-  for (int iz = 0; iz < na[2]; ++iz)
-    for (int iy = 0; iy < na[1]; ++iy)
-      for (int ix = 0; ix < na[0]; ++ix) {
-        const uint32_t cc = P.hcell_off + (uint32_t)(ax[0][ix] + P.hdims[0] * (ax[1][iy] + P.hdims[1] * ax[2][iz]));
-        const uint32_t a0 = hstart[cc], e0 = hstart[cc + 1];
-        for (uint32_t b0 = a0; b0 < e0; b0 += 32) {
-          const uint32_t t = b0 + lane;
-          bool hit = false;
-          uint32_t g = 0;
-          if (t < e0) {
-            g = hsorted[t];
-            if (g != h) {
-              const float4 xj = pos[head_slot[g]];
-              const float dx = fast_mi(xi.x - xj.x, box[0], inv[0]);
-              const float dy = fast_mi(xi.y - xj.y, box[1], inv[1]);
-              const float dz = fast_mi(xi.z - xj.z, box[2], inv[2]);
-              const float r2 = dx * dx + dy * dy + dz * dz;
-              hit = r2 < lo || (r2 <= hi && ex_dist(xi, xj, box) < lr);
-            }
-          }
-          const uint32_t m = __ballot_sync(0xffffffffu, hit);
-          if (hit) {
-            const uint32_t at = cnt + __popc(m & lt);
-            if (at < cap) row[at] = g;
-          }
-          cnt += __popc(m);
+  auto scan_cell = [&](uint32_t cc) {
+    const uint32_t a0 = hstart[cc], e0 = hstart[cc + 1];
+    for (uint32_t b0 = a0; b0 < e0; b0 += 32) {
+      const uint32_t t = b0 + lane;
+      bool hit = false;
+      uint32_t g = 0;
+      if (t < e0) {
+        g = hsorted[t];
+        if (g != h) {
+          const float4 xj = pos[head_slot[g]];
+          const float dx = fast_mi(xi.x - xj.x, box[0], inv[0]);
+          const float dy = fast_mi(xi.y - xj.y, box[1], inv[1]);
+          const float dz = fast_mi(xi.z - xj.z, box[2], inv[2]);
+          const float r2 = dx * dx + dy * dy + dz * dz;
+          hit = r2 < lo || (r2 <= hi && ex_dist(xi, xj, box) < lr);
         }
       }
+      const uint32_t m = __ballot_sync(0xffffffffu, hit);
+      if (hit) {
+        const uint32_t at = cnt + __popc(m & lt);
+        if (at < cap) row[at] = g;
+      }
+      cnt += __popc(m);
+    }
+  };
+  if (P.hdims[0] >= 2 * R + 1 && P.hdims[1] >= 2 * R + 1 && P.hdims[2] >= 2 * R + 1) {
+    // the walk does not wrap onto itself: cells wholly beyond the list sphere (with a margin) are
+    // skipped, which leaves the list the same set
+    const float cs[3] = {box[0] / (float)P.hdims[0], box[1] / (float)P.hdims[1], box[2] / (float)P.hdims[2]};
+    const float lrm = lr * (1.0f + 1e-5f) + 1e-3f, lrm2 = lrm * lrm;
+    for (int oz = -R; oz <= R; ++oz) {
+      const float gz = gap_to_cell(xi.z, q[2] + oz, cs[2]);
+      for (int oy = -R; oy <= R; ++oy) {
+        const float gy = gap_to_cell(xi.y, q[1] + oy, cs[1]);
+        for (int ox = -R; ox <= R; ++ox) {
+          const float gx = gap_to_cell(xi.x, q[0] + ox, cs[0]);
+          if (gx * gx + gy * gy + gz * gz >= lrm2) continue;
+          const int cx = (q[0] + ox + P.hdims[0]) % P.hdims[0], cy = (q[1] + oy + P.hdims[1]) % P.hdims[1],
+                    cz = (q[2] + oz + P.hdims[2]) % P.hdims[2];
+          scan_cell(P.hcell_off + (uint32_t)(cx + P.hdims[0] * (cy + P.hdims[1] * cz)));
+        }
+      }
+    }
+  } else {
+    for (int iz = 0; iz < na[2]; ++iz)
+      for (int iy = 0; iy < na[1]; ++iy)
+        for (int ix = 0; ix < na[0]; ++ix)
+          scan_cell(P.hcell_off + (uint32_t)(ax[0][ix] + P.hdims[0] * (ax[1][iy] + P.hdims[1] * ax[2][iz])));
+  }
   if (lane == 0) {
     if (cnt > cap) { flags[1] = 1u; cnt = cap; }
     es_cnt[h] = cnt;
