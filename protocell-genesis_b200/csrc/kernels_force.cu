@@ -51,20 +51,23 @@ __device__ __forceinline__ void bonded_term(const Shared& S, const SysParams& P,
   fx += s * dx; fy += s * dy; fz += s * dz;
 }
 
-template <int TPP>
+// SEL: the particles are the nsel slots sel[] (the heads, after a charge sweep) instead of all N
+template <int TPP, bool SEL>
 __global__ void __launch_bounds__(256, SOUP_FORCE_MINB) k_force(
     const Shared* __restrict__ Sg, const SysParams* __restrict__ sp, const uint8_t* __restrict__ sysid, uint32_t N,
     const float4* __restrict__ pos, const float* __restrict__ charge, const uint32_t* __restrict__ slots,
     const uint32_t* __restrict__ center, const uint32_t* __restrict__ id, const uint32_t* __restrict__ slot_of,
-    const uint32_t* __restrict__ nl, const uint32_t* __restrict__ nl_cnt, uint32_t cap, float4* __restrict__ force) {
+    const uint32_t* __restrict__ nl, const uint32_t* __restrict__ nl_cnt, uint32_t cap, float4* __restrict__ force,
+    const uint32_t* __restrict__ sel, uint32_t nsel) {
   __shared__ Shared S;
   for (int w = threadIdx.x; w < (int)(sizeof(Shared) / 4); w += blockDim.x)
     reinterpret_cast<uint32_t*>(&S)[w] = reinterpret_cast<const uint32_t*>(Sg)[w];
   __syncthreads();
   const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
-  const uint32_t k = gtid / TPP;
+  const uint32_t g = gtid / TPP;
   const int lane = (int)(gtid % TPP);
-  const bool active = k < N;
+  const bool active = SEL ? g < nsel : g < N;
+  const uint32_t k = SEL ? (active ? sel[g] : 0u) : g;
   float fx = 0.f, fy = 0.f, fz = 0.f;
   if (active) {
     const SysParams& Pg = sp[sysid[k]];
@@ -242,11 +245,17 @@ __global__ void __launch_bounds__(128) k_force_brute(
 }
 
 template <int TPP>
-void launch_force_tpp(Batch& b) {
-  const uint64_t threads = (uint64_t)b.N * TPP;
-  k_force<TPP><<<nblocks(threads, 256), 256, 0, b.stream>>>(b.shared, b.sp, b.sysid, b.N, b.pos, b.charge, b.slots,
-                                                            b.center, b.id, b.slot_of, b.nl, b.nl_cnt, b.list_cap,
-                                                            b.force);
+void launch_force_tpp(Batch& b, bool heads) {
+  if (heads) {
+    if (b.H == 0) return;
+    k_force<TPP, true><<<nblocks((uint64_t)b.H * TPP, 256), 256, 0, b.stream>>>(
+        b.shared, b.sp, b.sysid, b.N, b.pos, b.charge, b.slots, b.center, b.id, b.slot_of, b.nl, b.nl_cnt, b.list_cap,
+        b.force, b.head_slot, b.H);
+    return;
+  }
+  k_force<TPP, false><<<nblocks((uint64_t)b.N * TPP, 256), 256, 0, b.stream>>>(
+      b.shared, b.sp, b.sysid, b.N, b.pos, b.charge, b.slots, b.center, b.id, b.slot_of, b.nl, b.nl_cnt, b.list_cap,
+      b.force, nullptr, 0u);
 }
 
 }  // namespace
@@ -262,16 +271,26 @@ void launch_force(Batch& b) {
   }
 }
 
-void launch_force_list(Batch& b) {
+void launch_force_list(Batch& b, bool heads) {
   b.launches += 1;
   switch (b.tpp) {
-    case 1: launch_force_tpp<1>(b); break;
-    case 2: launch_force_tpp<2>(b); break;
-    case 16: launch_force_tpp<16>(b); break;
-    case 32: launch_force_tpp<32>(b); break;
-    case 8: launch_force_tpp<8>(b); break;
-    default: launch_force_tpp<4>(b); break;
+    case 1: launch_force_tpp<1>(b, heads); break;
+    case 2: launch_force_tpp<2>(b, heads); break;
+    case 16: launch_force_tpp<16>(b, heads); break;
+    case 32: launch_force_tpp<32>(b, heads); break;
+    case 8: launch_force_tpp<8>(b, heads); break;
+    default: launch_force_tpp<4>(b, heads); break;
   }
+}
+
+// after a charge sweep: only the heads' forces depend on charges (when only heads are charged and
+// the polar class is the heads' kind alone), so they alone are recomputed, with the same arithmetic;
+// timed with the sweep it completes (the force group keeps whole passes only)
+void launch_force_heads(Batch& b) {
+  prof_begin(b, SOUP_K_SWEEP);
+  launch_force_list(b, true);
+  if (b.H > 0) launch_es_far(b);
+  prof_end(b);
 }
 
 void launch_es_far(Batch& b) {

@@ -261,6 +261,12 @@ void upload_replica(Batch& b, uint32_t r, const SoupInitState* init, bool fresh_
   std::vector<uint8_t> frozen(n);
   std::vector<uint32_t> ids(n);
   for (uint32_t i = 0; i < n; ++i) { frozen[i] = frozen32[i] ? 1 : 0; ids[i] = off + i; }
+  b.kinds[r].resize(n);
+  b.off_head_charge[r] = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    b.kinds[r][i] = (uint8_t)pos[4 * (size_t)i + 3];
+    if (charge[i] != 0.f && (int)b.kinds[r][i] != c.charged_kind) b.off_head_charge[r] = 1;
+  }
   auto up = [&](void* dst, const void* src, size_t bytes) {
     SOUP_CUDA_TRY(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, b.stream));
   };
@@ -290,6 +296,12 @@ Batch* make_batch(const SoupConfig* cfgs, const SoupInitState* inits, uint32_t R
   b.R = R;
   b.cfg.assign(cfgs, cfgs + R);
   for (uint32_t r = 0; r < R; ++r) check_config(b.cfg[r]);
+  b.kinds.resize(R);
+  b.off_head_charge.assign(R, 1);
+  b.polar_is_charged_kind = true;
+  for (uint32_t r = 0; r < R; ++r)
+    for (uint32_t k = 0; k < b.cfg[r].n_kinds; ++k)
+      if ((b.cfg[r].kind_class[k] & 3u) == 1u && (int)k != b.cfg[r].charged_kind) b.polar_is_charged_kind = false;
   SOUP_CUDA_TRY(cudaGetDevice(&b.device));
   b.hs = make_shared(b.cfg[0]);
   for (uint32_t r = 1; r < R; ++r) {
@@ -513,7 +525,15 @@ void sweep_all(Batch& b, std::vector<SoupSweepResult>* out) {
   // soup/src/soup-protonation.ts:62-73: F(x) is stale after the charges changed.  The reference
   // re-runs its rebuild+force pass; in drift-triggered mode only the force is recomputed (the lists
   // are sets that do not depend on charges, and the drift trigger keeps them complete).
-  if (b.cfg[0].rebuild_on_drift) { launch_force(b); b.force_fresh = true; }
+  if (b.cfg[0].rebuild_on_drift) {
+    // only head-head terms depend on charges when only heads carry charge and the polar class is
+    // the heads' kind alone: the other particles' forces stand, bit for bit
+    bool heads_only = b.polar_is_charged_kind && !std::getenv("SOUP_SWEEP_FORCE_ALL");
+    for (uint32_t r = 0; r < b.R; ++r) heads_only = heads_only && !b.off_head_charge[r];
+    if (heads_only) launch_force_heads(b);
+    else launch_force(b);
+    b.force_fresh = true;
+  }
   else force_pass(b);
   SOUP_CUDA_TRY(cudaStreamSynchronize(b.stream));
   b.sweeps++;
@@ -1101,6 +1121,9 @@ int soup_write_charges(SoupHandle* h, const float* src, size_t bytes) {
     SOUP_CUDA_TRY(cudaStreamSynchronize(b.stream));
     std::vector<float> q(n);
     for (uint32_t k = 0; k < n; ++k) q[k] = src[ids[k] - off];
+    b.off_head_charge[r] = 0;
+    for (uint32_t i = 0; i < n; ++i)
+      if (src[i] != 0.f && (int)b.kinds[r][i] != b.cfg[r].charged_kind) b.off_head_charge[r] = 1;
     SOUP_CUDA_TRY(cudaMemcpyAsync(b.charge + off, q.data(), 4 * (size_t)n, cudaMemcpyHostToDevice, b.stream));
     force_pass(b);
     SOUP_CUDA_TRY(cudaStreamSynchronize(b.stream));

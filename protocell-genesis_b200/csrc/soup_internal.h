@@ -156,6 +156,12 @@ struct Batch {
   uint32_t rebuild_count_seen = 0;
   std::string err;
   std::vector<SoupHandle*> views;    // per-replica handle views
+  // charge locality: only the charged kind is in the polar class (batch-wide), and per replica the
+  // kinds (host copy, static) and whether any other kind carries a charge; when no replica does,
+  // a charge sweep changes the forces on the heads alone
+  bool polar_is_charged_kind = false;
+  std::vector<std::vector<uint8_t>> kinds;
+  std::vector<uint8_t> off_head_charge;
 
   // measurement: launch counter and optional per-group event timing
   uint64_t launches = 0;
@@ -191,7 +197,8 @@ void launch_sort_and_gather(Batch& b);
 void launch_build_lists(Batch& b);
 void launch_build_es_lists(Batch& b);
 void launch_force(Batch& b);       // list force, then the far electrostatics half
-void launch_force_list(Batch& b);
+void launch_force_list(Batch& b, bool heads = false);
+void launch_force_heads(Batch& b);  // the heads' list force and far half only (after a charge sweep)
 void launch_es_far(Batch& b);
 void launch_force_brute(Batch& b);
 void launch_kick_drift(Batch& b);
