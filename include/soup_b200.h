@@ -233,13 +233,13 @@ int soup_write_charges(SoupHandle* h, const float* src, size_t bytes);
 int soup_set_box(SoupHandle* h, const double box[3]);
 
 /* ---- autotuning (no reference counterpart) ----------------------------------------------------
- * Picks, for the handle's whole batch, the block shape of the list force (lanes per particle, timed
- * on the force), the neighbour-cell size (list-walk radius 2 or 3, timed on the list build) and, with
- * drift-triggered rebuilds, the Verlet skin (0.6, 0.8 or 1.0 of the planned skin, which sized the
- * list capacity; timed on `steps` whole steps).  The choice stays in effect.  The state is restored
- * afterwards: positions, velocities, charges, bonds, RNG states, event counters and the step schedule
- * are as they were, and the particles are re-sorted, so later forces agree with an untuned run to
- * FP32 rounding. */
+ * Picks, for the handle's whole batch, the block shape of the list force (1, 2, 4 or 8 lanes per
+ * particle, timed on the force), the neighbour-cell size (list-walk radius 2 or 3, timed on the
+ * list build) and, with drift-triggered rebuilds, the Verlet skin (0.6, 0.8 or 1.0 of the planned
+ * skin, which sized the list capacity; timed on `steps` whole steps).  The choice stays in effect.
+ * The state is restored afterwards: positions, velocities, charges, bonds, RNG states, event
+ * counters and the step schedule are as they were, and the particles are re-sorted, so later forces
+ * agree with an untuned run to FP32 rounding. */
 typedef struct SoupTuneResult {
   uint32_t tpp, walk;             /* chosen lanes per particle, list-walk radius */
   uint32_t tpp_before, walk_before;

@@ -1206,7 +1206,7 @@ int soup_autotune(SoupHandle* h, uint32_t steps, SoupTuneResult* out) {
     res.ms_per_step_before = steps_ms();
     tune_restore(b, snap);
     // block shape: lanes per particle of the list force, timed on the force alone
-    const int tpps[3] = {2, 4, 8};
+    const int tpps[4] = {1, 2, 4, 8};
     double best = 1e30;
     for (int t : tpps) {
       b.tpp = t;

@@ -37,7 +37,7 @@ def test_choices_stay_and_the_state_is_restored():
     before = _state(g)
     r = g.autotune(steps=10)
     after = _state(g)
-    assert r["tpp"] in (2, 4, 8) and r["walk"] in (2, 3) and r["skin_scale"] in (0.6, 0.8, 1.0)
+    assert r["tpp"] in (1, 2, 4, 8) and r["walk"] in (2, 3) and r["skin_scale"] in (0.6, 0.8, 1.0)
     assert r["ms_per_step_before"] > 0 and r["ms_per_step_after"] > 0
     for k in before:
         assert np.array_equal(np.asarray(before[k]), np.asarray(after[k])), k
@@ -76,7 +76,7 @@ def test_tuned_batch_steps_like_its_replicas():
                            charges=o.read(ob.F_CHARGES)))
     batch = SoupBatch(cfgs, states)
     r = batch.autotune(steps=10)
-    assert r["tpp"] in (2, 4, 8)
+    assert r["tpp"] in (1, 2, 4, 8)
     batch.step(30)
     for c, st, rep in zip(cfgs, states, batch.replicas):
         single = SoupSystem(c, st)
