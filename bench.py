@@ -525,6 +525,59 @@ def run_gradient(args, pkg, L, torch):
                         "Monte Carlo held off inside the window"}
 
 
+class CampaignSampler:
+    """The campaign's progress sample on the system (config 2: closure flood-fill and aggregate
+    labels every 200 steps): amphiphiles, aggregate labels at the nonbonded cutoff, the shapes of the
+    five largest aggregates and the closure (encapsulated water) of each, about its periodic centre."""
+
+    def __init__(self, pkg, cfgm, cfg, system):
+        import numpy as np
+        from protocell_genesis_b200 import observables
+        self.np, self.obs = np, observables
+        P = cfgm.load_params()
+        self.st = P["stageThresholds"]
+        self.alpha = P["circularAlpha"]
+        self.cutoff = float(cfg.rc_attr + cfg.wc)
+        self.box = list(cfg.box)
+        solvent = [k for k, m in enumerate(P["monomers"]) if m["solvent"]]
+        kinds = system.particles().reshape(-1, 4)[:, 3]
+        self.water = np.nonzero(np.isin(kinds, np.array(solvent, np.float32)))[0].astype(np.uint32)
+        self.times = []
+
+    def __call__(self, s):
+        np = self.np
+        t0 = time.perf_counter()
+        _, head_of = s.amphiphile_labels()
+        members = np.nonzero(head_of != 0xFFFFFFFF)[0].astype(np.uint32)
+        out = {"aggregates": 0, "largest": 0, "encapsulated": []}
+        if members.size:
+            ncomp, labels = s.aggregate_labels(members, self.cutoff)
+            _, shapes = s.aggregate_shapes(members, labels, int(self.st["detailAggregateCount"]))
+            pos = s.particles()
+            out["aggregates"], out["largest"] = int(ncomp), int(shapes[0]["size"]) if shapes else 0
+            for sh in shapes:
+                m = members[labels == sh["label"]]
+                c = self.obs.periodic_centre(pos, m, self.box, self.alpha)
+                if c is not None:
+                    r = s.closure(m, self.water, c, self.st["closureCell"], self.st["closureRadius"],
+                                  self.st["enclosedVolume"])
+                    out["encapsulated"].append(int(r["encapsulatedCount"]))
+        self.times.append(time.perf_counter() - t0)
+        return out
+
+
+def step_with_samples(s, steps, every, sampler):
+    """`steps` steps with the progress sample after every `every` of them."""
+    done, samples = 0, []
+    while done < steps:
+        k = min(every - done % every, steps - done)
+        s.step(k)
+        done += k
+        if sampler is not None and done % every == 0:
+            samples.append(sampler(s))
+    return samples
+
+
 def run_cuda(args):
     import ctypes as C
     import numpy as np
@@ -554,6 +607,10 @@ def run_cuda(args):
     tune = s.autotune(steps=20) if not args.no_tune else None   # untimed; the choice stays in effect
     s.step(args.warmup)
     s.prepare_graphs()   # every chunk graph of the schedule captured before the timed region
+    sampler = None if args.no_analysis else CampaignSampler(pkg, cfgm, cfg, s)
+    if sampler is not None:
+        sampler(s)       # untimed: the analysis scratch is allocated on first use
+        sampler.times.clear()
     stream = torch.cuda.ExternalStream(L.soup_stream(s._h))
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -565,7 +622,7 @@ def run_cuda(args):
     with ClockSampler(local) as clk:
         torch.cuda.nvtx.range_push("timed")
         e0.record(stream)
-        s.step(args.steps)
+        samples = step_with_samples(s, args.steps, args.analysis_every, sampler)
         e1.record(stream)
         torch.cuda.synchronize()
         torch.cuda.nvtx.range_pop()
@@ -638,6 +695,8 @@ def run_cuda(args):
         s2.step(c_)
         L.soup_read_pos(s2._h, out_pos.ctypes.data_as(C.c_void_p), out_pos.nbytes)
         done += c_
+        if sampler is not None and done % args.analysis_every == 0:
+            sampler(s2)
     torch.cuda.synchronize()
     e2e_s = time.perf_counter() - t0
     h2d = sum(v_.nbytes for v_ in pinned.values())
@@ -689,6 +748,12 @@ def run_cuda(args):
                        "rebuilds_in_timed_region": info1["rebuilds"] - info0["rebuilds"],
                        "sweeps_in_timed_region": info1["sweeps"] - info0["sweeps"],
                        "autotune": tune,
+                       "analysis": None if sampler is None else {
+                           "every": args.analysis_every, "samples_in_timed_region": len(samples),
+                           "ms_per_sample": 1e3 * sum(sampler.times[:len(samples)]) / max(len(samples), 1),
+                           "last": samples[-1] if samples else None,
+                           "what": "amphiphiles, aggregate labels at the nonbonded cutoff, shapes of the five "
+                                   "largest aggregates, closure flood-fill (0.5 sigma voxels) of each"},
                        "execution": "steps in captured CUDA graphs of 10 (one sweep period), the drift-triggered "
                                     "rebuild a conditional node",
                        "split": f"phases and the force roofline from a profiled segment of {args.prof_steps} steps "
@@ -721,6 +786,8 @@ def main():
     ap.add_argument("--replicas", type=int, default=64)
     ap.add_argument("--batched-steps", type=int, default=100)
     ap.add_argument("--no-tune", action="store_true", help="skip the autotuning (plain and batched)")
+    ap.add_argument("--no-analysis", action="store_true", help="leave the campaign's progress sample out of the timed steps")
+    ap.add_argument("--analysis-every", type=int, default=200)
     ap.add_argument("--no-gradient", action="store_true", help="skip the forward + adjoint window measurement")
     ap.add_argument("--prof-steps", type=int, default=100, help="steps of the profiled segment (per-kernel split)")
     ap.add_argument("--grad-steps", type=int, default=200)

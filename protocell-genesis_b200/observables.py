@@ -7,6 +7,7 @@ or on host arrays, written here in the reference's terms:
   area_per_lipid     engine/src/metrics.ts:8-10
   sum_profiles       engine/src/metrics.ts:52-69
   center_membrane_z  engine/src/metrics.ts:75-84
+  periodic_centre    soup/src/water-closure.ts:63-97 (periodicCentreOf, circularAxisStat)
   drop_escaped_z     engine/src/metrics.ts:91-110
   bilayer_peaks      engine/src/metrics.ts:118-146 (+ subBinPeak 148-157)
   bilayer_thickness  engine/src/metrics.ts:159-162
@@ -117,6 +118,28 @@ def apparent_pka(alpha, ph):
     return ph - math.log10(alpha / (1 - alpha))
 
 
+def periodic_centre(positions, idx, box, alpha):
+    """periodicCentreOf (soup/src/water-closure.ts:63-97): per axis the circular mean of the members'
+    wrapped coordinates (angle 2 pi x / L); None when the mean resultant length R falls below the
+    Rayleigh bound sqrt(-ln(alpha) / m) on any axis (no meaningful centre)."""
+    p = np.asarray(positions, np.float32).reshape(-1, 4)[np.asarray(idx, np.int64), :3].astype(np.float64)
+    m = len(p)
+    if m == 0:
+        return None
+    out = []
+    for a in range(3):
+        L = float(box[a])
+        x = p[:, a] - np.floor(p[:, a] / L) * L
+        th = 2.0 * math.pi * x / L
+        sc, ss = float(np.cos(th).mean()), float(np.sin(th).mean())
+        R = math.sqrt(sc * sc + ss * ss)
+        if not R >= math.sqrt(-math.log(alpha) / m):
+            return None
+        c = math.atan2(ss, sc) / (2.0 * math.pi) * L
+        out.append(c - math.floor(c / L) * L)
+    return out
+
+
 def symmetric_eigenvalues_3x3(sxx, syy, szz, sxy, sxz, syz):
     """Ascending eigenvalues of a real symmetric 3x3 matrix by Smith's closed form (O. K. Smith,
     "Eigenvalues of a symmetric 3x3 matrix", CACM 4(4):168, 1961): shift by the mean eigenvalue q,
@@ -202,6 +225,7 @@ def analyze_aggregates(system, cutoff, detail_count=5, min_amphiphiles_per_aggre
 areaPerLipid = area_per_lipid
 sumProfiles = sum_profiles
 centerMembraneZ = center_membrane_z
+periodicCentreOf = periodic_centre
 dropEscapedZ = drop_escaped_z
 bilayerPeaks = bilayer_peaks
 bilayerThickness = bilayer_thickness

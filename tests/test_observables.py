@@ -130,3 +130,25 @@ def test_oracle_shape_of_a_rod_across_the_boundary():
     assert m["principalMoments"][0] == pytest.approx(0.0, abs=1e-9)
     assert m["radiusOfGyration"] == pytest.approx(math.sqrt(80.0 / 12.0))
     assert m["flatnessRatio"] == pytest.approx(0.0, abs=1e-9)
+
+
+def test_periodic_centre_matches_the_oracle():
+    """periodicCentreOf against the oracle's restatement, on a cluster that straddles a box face and
+    on uniform points (no meaningful centre)."""
+    import oracle_binding as ob
+    from protocell_genesis_b200 import _abi
+    from protocell_genesis_b200 import observables as obs
+    rng = np.random.default_rng(4)
+    box = [20.0, 20.0, 20.0]
+    n = 400
+    pos = np.zeros((n, 4), np.float32)
+    pos[:200, :3] = np.mod(rng.normal(0.0, 1.5, (200, 3)) + [19.5, 10.0, 0.5], 20.0)
+    pos[200:, :3] = rng.uniform(0, 20, (200, 3))
+    flat = pos.reshape(-1)
+    for idx in (np.arange(200, dtype=np.uint32), np.arange(200, 400, dtype=np.uint32)):
+        c = obs.periodic_centre(flat, idx, box, 0.05)
+        co = ob.periodic_centre(_abi, flat, idx, box, 0.05)
+        if co is None:
+            assert c is None
+        else:
+            assert np.allclose(c, co, atol=1e-9)
