@@ -531,6 +531,7 @@ class CampaignSampler:
     five largest aggregates and the closure (encapsulated water) of each, about its periodic centre."""
 
     def __init__(self, pkg, cfgm, cfg, system):
+        import math
         import numpy as np
         from protocell_genesis_b200 import observables
         self.np, self.obs = np, observables
@@ -538,6 +539,7 @@ class CampaignSampler:
         self.st = P["stageThresholds"]
         self.alpha = P["circularAlpha"]
         self.cutoff = float(cfg.rc_attr + cfg.wc)
+        self.cells = int(np.prod([max(1, int(math.floor(b / self.cutoff))) for b in cfg.box]))
         self.box = list(cfg.box)
         solvent = [k for k, m in enumerate(P["monomers"]) if m["solvent"]]
         kinds = system.particles().reshape(-1, 4)[:, 3]
@@ -545,13 +547,17 @@ class CampaignSampler:
         self.times = []
 
     def __call__(self, s):
+        from protocell_genesis_b200 import _abi
         np = self.np
         t0 = time.perf_counter()
         _, head_of = s.amphiphile_labels()
         members = np.nonzero(head_of != 0xFFFFFFFF)[0].astype(np.uint32)
         out = {"aggregates": 0, "largest": 0, "encapsulated": []}
         if members.size:
-            ncomp, labels = s.aggregate_labels(members, self.cutoff)
+            if members.size <= _abi.NOALLOC_MAX_MEMBERS and self.cells <= _abi.NOALLOC_MAX_CELLS:
+                ncomp, labels = s.aggregate_labels_noalloc(members, self.cutoff)
+            else:
+                ncomp, labels = s.aggregate_labels(members, self.cutoff)
             _, shapes = s.aggregate_shapes(members, labels, int(self.st["detailAggregateCount"]))
             pos = s.particles()
             out["aggregates"], out["largest"] = int(ncomp), int(shapes[0]["size"]) if shapes else 0
@@ -564,6 +570,27 @@ class CampaignSampler:
                     out["encapsulated"].append(int(r["encapsulatedCount"]))
         self.times.append(time.perf_counter() - t0)
         return out
+
+
+def checkpoint_timing(s, cfg, reps=3):
+    """A checkpoint of the live system (soup/src/checkpoint.ts encodeCheckpoint): the one-call device
+    payload alone, and the whole CheckpointFile as JSON text (payload, base64, serialisation); the
+    median of `reps` each, wall clock."""
+    import json as _json
+    from protocell_genesis_b200 import checkpoint as ck
+    config = {"box": [float(x) for x in cfg.box], "seed": int(cfg.seed), "kT": float(cfg.kT)}
+    t_pay, t_file, size = [], [], 0
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        s.checkpoint_payload()
+        t_pay.append(time.perf_counter() - t0)
+        t0 = time.perf_counter()
+        size = len(_json.dumps(ck.encode_checkpoint(s, config)))
+        t_file.append(time.perf_counter() - t0)
+    return {"payload_ms": 1e3 * statistics.median(t_pay), "file_ms": 1e3 * statistics.median(t_file),
+            "file_bytes": size, "payload_bytes": 64 * s.n,
+            "what": "payload: soup_read_checkpoint (one device gather, one wait) into pageable host memory; "
+                    "file: payload + base64 + JSON text of the reference's CheckpointFile"}
 
 
 def step_with_samples(s, steps, every, sampler):
@@ -675,6 +702,8 @@ def run_cuda(args):
                 "algorithmic_bytes_per_launch": bytes_per_launch, "mean_list_entries": mean_list,
                 "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback 6.65 TB/s"}
 
+    ckpt = checkpoint_timing(s, cfg)
+
     # end to end through the public API with host buffers: create from pinned host arrays
     # (H2D of the whole state), step in chunks of 10 with the positions read back after each chunk
     state = {"positions": s.particles(), "velocities": s.velocities(), "charges": s.charges(),
@@ -748,6 +777,7 @@ def run_cuda(args):
                        "rebuilds_in_timed_region": info1["rebuilds"] - info0["rebuilds"],
                        "sweeps_in_timed_region": info1["sweeps"] - info0["sweeps"],
                        "autotune": tune,
+                       "checkpoint": ckpt,
                        "analysis": None if sampler is None else {
                            "every": args.analysis_every, "samples_in_timed_region": len(samples),
                            "ms_per_sample": 1e3 * sum(sampler.times[:len(samples)]) / max(len(samples), 1),

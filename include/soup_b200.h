@@ -226,6 +226,26 @@ int soup_read_verlet(SoupHandle* h, uint32_t* counts, uint32_t* lists, size_t li
 /* Protonation chain state (SoupSystem.protonationRngState). */
 int soup_read_protonation_rng(SoupHandle* h, uint32_t* out);
 
+/* ---- checkpoint payload (soup/src/checkpoint.ts:176-214 encodeCheckpoint) --------------------
+ * Every array encodeCheckpoint reads, in ONE call: the device gathers them into original particle
+ * order and the host waits once.  `dst` receives, back to back, in CheckpointFile's field order and
+ * the readback layouts above:
+ *   positions f32 x4 | velocities f32 x4 | bondSlots u32 x3 | centerLink u32 | centerHeldSteps u32 |
+ *   bondRng u32 | thermoRng u32 | charges f32
+ * = SOUP_CHECKPOINT_BYTES_PER_PARTICLE * n bytes (`bytes` must equal that).  `scalars` (may be NULL)
+ * receives the rest of the file's state.  A pure readback: the trajectory is unchanged. */
+#define SOUP_CHECKPOINT_BYTES_PER_PARTICLE 64
+typedef struct SoupCheckpointScalars {
+  uint64_t global_step;           /* globalStep */
+  uint32_t n;                     /* N */
+  uint32_t n_rules;               /* rules whose counters fill events[0 .. 2*n_rules) */
+  uint32_t protonation_rng;       /* protonationRng */
+  uint32_t desorb[2];             /* desorbEvents: stretch, timeout */
+  uint32_t events[2 * SOUP_MAX_RULES]; /* events: bond, break per rule */
+  double live_box[3];             /* liveBox */
+} SoupCheckpointScalars;
+int soup_read_checkpoint(SoupHandle* h, void* dst, size_t bytes, SoupCheckpointScalars* scalars);
+
 /* ---- writes --------------------------------------------------------------------------------- */
 /* writeBuffer(chargeBuf) (soup/src/soup-protonation.ts:60); marks forces stale. */
 int soup_write_charges(SoupHandle* h, const float* src, size_t bytes);

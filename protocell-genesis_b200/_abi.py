@@ -123,6 +123,19 @@ class SoupTuneResult(C.Structure):
     ]
 
 
+CHECKPOINT_BYTES_PER_PARTICLE = 64
+NOALLOC_MAX_MEMBERS = 1 << 18   # SOUP_NOALLOC_MAX_MEMBERS
+NOALLOC_MAX_CELLS = 1 << 18     # SOUP_NOALLOC_MAX_CELLS
+
+
+class SoupCheckpointScalars(C.Structure):
+    _fields_ = [
+        ("global_step", C.c_uint64), ("n", C.c_uint32), ("n_rules", C.c_uint32),
+        ("protonation_rng", C.c_uint32), ("desorb", C.c_uint32 * 2), ("events", C.c_uint32 * (2 * MAX_RULES)),
+        ("live_box", C.c_double * 3),
+    ]
+
+
 class SoupInfo(C.Structure):
     _fields_ = [
         ("n", C.c_uint32), ("global_step", C.c_uint64), ("list_capacity", C.c_uint32),
@@ -163,6 +176,7 @@ SIGNATURES = {
     "soup_nonfinite_count": (C.c_int, [_P, _U32P]),
     "soup_read_verlet": (C.c_int, [_P, _U32P, _U32P, _SZ]),
     "soup_read_protonation_rng": (C.c_int, [_P, _U32P]),
+    "soup_read_checkpoint": (C.c_int, [_P, _P, _SZ, C.POINTER(SoupCheckpointScalars)]),
     "soup_write_charges": (C.c_int, [_P, _P, _SZ]),
     "soup_set_box": (C.c_int, [_P, C.POINTER(C.c_double)]),
     "soup_autotune": (C.c_int, [_P, C.c_uint32, C.POINTER(SoupTuneResult)]),

@@ -1,0 +1,167 @@
+"""Checkpoint files of a soup run (soup/src/checkpoint.ts): encodeCheckpoint and
+decodeCheckpointResume over the reference's CheckpointFile format, so that a file written here
+resumes under the reference and the other way round.
+
+The format is the reference's (checkpoint.ts:118-172): a JSON object whose arrays are base64 strings
+of their little-endian bytes (standard alphabet with padding, what atob/btoa read and write), one
+string per array, in the readback layouts (positions f32 x4 with w = kind, bond slots u32 x3 with
+0xFFFFFFFF = none).  What differs is the read side: on a SoupSystem every array comes from ONE
+device gather and one host wait (soup_read_checkpoint) instead of ten concurrent readbacks.
+
+Writing the object to disk is the caller's job in the reference (soup/cli/campaign.ts);
+write_checkpoint / read_checkpoint are the plain JSON file I/O for callers in Python.
+"""
+import base64
+import datetime as _dt
+import json
+from typing import Optional
+
+import numpy as np
+
+from . import config as _config
+
+VERSION = 1
+
+# CheckpointFile's per-particle arrays: (file key, resume key, dtype, values per particle), in the
+# file's field order (checkpoint.ts:148-162).
+ARRAYS = (
+    ("positionsB64", "positions", np.float32, 4),
+    ("velocitiesB64", "velocities", np.float32, 4),
+    ("bondSlotsB64", "bondSlots", np.uint32, 3),
+    ("centerLinkB64", "centerLink", np.uint32, 1),
+    ("centerHeldStepsB64", "centerHeldSteps", np.uint32, 1),
+    ("bondRngB64", "bondRng", np.uint32, 1),
+    ("thermoRngB64", "thermoRng", np.uint32, 1),
+    ("chargesB64", "charges", np.float32, 1),
+)
+
+
+def _b64(a: np.ndarray, dtype) -> str:
+    """encodeTyped (checkpoint.ts:54-56): the array's little-endian bytes as one base64 string."""
+    return base64.b64encode(np.ascontiguousarray(a, np.dtype(dtype).newbyteorder("<")).tobytes()).decode("ascii")
+
+
+def _unb64(s: str, dtype) -> np.ndarray:
+    """decodeFloat32 / decodeUint32 (checkpoint.ts:58-66)."""
+    return np.frombuffer(base64.b64decode(s), np.dtype(dtype).newbyteorder("<")).astype(dtype)
+
+
+def census(positions: np.ndarray, P: Optional[dict] = None) -> dict:
+    """invariants().monomers (soup/src/soup-readback.ts:140-149): beads per monomer id, the kind read
+    from each position's w, rounded."""
+    monomers = (P or _config.load_params())["monomers"]
+    kinds = np.rint(np.asarray(positions, np.float32).reshape(-1, 4)[:, 3]).astype(np.int64)
+    c = np.bincount(kinds, minlength=len(monomers))
+    return {m["id"]: int(c[k]) for k, m in enumerate(monomers)}
+
+
+def _now() -> str:
+    t = _dt.datetime.now(_dt.timezone.utc)
+    return t.strftime("%Y-%m-%dT%H:%M:%S.") + f"{t.microsecond // 1000:03d}Z"
+
+
+def encode_checkpoint(sys, config: dict, created_at: Optional[str] = None) -> dict:
+    """encodeCheckpoint (checkpoint.ts:176-214): the CheckpointFile of `sys`'s current state.
+
+    `sys` is a SoupSystem (one soup_read_checkpoint call) or any object with the reference's
+    CheckpointableSystem readbacks (particles, velocities, bondSlots, centerLinks, centerHeldSteps,
+    desorbEvents, rngState, events, invariants, charges, protonationRngState, box, steps).  Like the
+    reference it only reads: the trajectory after it is the one without it."""
+    if hasattr(sys, "checkpoint_payload"):
+        arrays, sc = sys.checkpoint_payload()
+        active = census(arrays["positions"])
+        step, box, events, desorb, prot = (sc["globalStep"], sc["liveBox"], sc["events"], sc["desorbEvents"],
+                                           sc["protonationRng"])
+    else:
+        rng = sys.rngState()
+        arrays = dict(positions=sys.particles(), velocities=sys.velocities(), bondSlots=sys.bondSlots(),
+                      centerLink=sys.centerLinks(), centerHeldSteps=sys.centerHeldSteps(), bondRng=rng["bond"],
+                      thermoRng=rng["thermo"], charges=sys.charges())
+        active = sys.invariants()["monomers"]
+        step, box, events, desorb, prot = (sys.steps, sys.box, sys.events(), sys.desorbEvents(),
+                                           sys.protonationRngState())
+    out = {
+        "version": VERSION,
+        "createdAt": created_at or _now(),
+        "config": config,
+        "N": int(np.asarray(arrays["positions"]).size // 4),
+        "globalStep": int(step),
+        "liveBox": [float(x) for x in box],
+        "cyclePhase": getattr(sys, "cyclePhase", "none"),
+        "cycleIndex": int(getattr(sys, "cycleIndex", 0)),
+        "activeCounts": dict(active),
+        "events": {k: int(v) for k, v in events.items()},
+        "desorbEvents": {"stretch": int(desorb["stretch"]), "timeout": int(desorb["timeout"])},
+    }
+    for key, name, dt, _ in ARRAYS:
+        out[key] = _b64(arrays[name], dt)
+    out["protonationRng"] = int(prot)
+    return out
+
+
+def decode_checkpoint_resume(file: dict) -> dict:
+    """decodeCheckpointResume (checkpoint.ts:219-237): CreateSoupOpts.resume's shape, arrays as numpy.
+    A file without chargesB64 / protonationRng (written before electrostatics) gives None there."""
+    if file.get("version") != VERSION:
+        raise ValueError(f"checkpoint version {file.get('version')!r} is not {VERSION}")
+    r = {
+        "globalStep": int(file["globalStep"]),
+        "liveBox": [float(x) for x in file["liveBox"]],
+        "activeCounts": dict(file["activeCounts"]),
+        "desorbEvents": np.array([file["desorbEvents"]["stretch"], file["desorbEvents"]["timeout"]], np.uint32),
+        "events": dict(file["events"]),
+        "protonationRng": file.get("protonationRng"),
+    }
+    for key, name, dt, _ in ARRAYS:
+        r[name] = _unb64(file[key], dt) if file.get(key) is not None else None
+    return r
+
+
+def resume_options(file: dict, resume: Optional[dict] = None) -> _config.SoupOptions:
+    """createSoup({...file.config, resume}) (soup/cli/campaign.ts:118-125) as SoupOptions: the live box
+    and step of the file, its census as the composition (the MD step holds exactly the live beads),
+    the protonation chain's state, and a wall radius scaled to the live box (liveRadius,
+    soup/src/soup-confine.ts:76-78)."""
+    c = file["config"]
+    r = resume if resume is not None else decode_checkpoint_resume(file)
+    confine = None
+    if c.get("confine"):
+        confine = dict(c["confine"])
+        confine["radiusSigma"] = float(confine["radiusSigma"]) * (r["liveBox"][0] / float(c["box"][0]))
+    return _config.SoupOptions(box=r["liveBox"], seed=int(c["seed"]), kT=float(c["kT"]), start=dict(r["activeCounts"]),
+                               electrostatics=c.get("electrostatics"), confine=confine,
+                               global_step=r["globalStep"], protonation_rng=r["protonationRng"])
+
+
+def resume_state(resume: dict, rule_ids=None) -> dict:
+    """The resume arrays as SoupSystem's start state; the events record becomes the device's counter
+    array (bond, break per rule, in rule order)."""
+    ids = rule_ids or _config.rule_ids()
+    ev = np.zeros(2 * len(ids), np.uint32)
+    for k, (b, brk) in enumerate(ids):
+        ev[2 * k], ev[2 * k + 1] = resume["events"].get(b, 0), resume["events"].get(brk, 0)
+    st = {name: resume[name] for _, name, _, _ in ARRAYS if resume.get(name) is not None}
+    st["events"] = ev
+    st["desorbEvents"] = resume["desorbEvents"]
+    return st
+
+
+def create_from_checkpoint(file: dict):
+    """A SoupSystem resumed from `file`, at the file's global step."""
+    from .soup import SoupSystem
+    r = decode_checkpoint_resume(file)
+    return SoupSystem(_config.resolve(resume_options(file, r)), resume_state(r))
+
+
+def write_checkpoint(path: str, file: dict) -> None:
+    with open(path, "w") as fh:
+        json.dump(file, fh)
+
+
+def read_checkpoint(path: str) -> dict:
+    with open(path) as fh:
+        return json.load(fh)
+
+
+encodeCheckpoint = encode_checkpoint
+decodeCheckpointResume = decode_checkpoint_resume

@@ -271,7 +271,8 @@ __global__ void k_fill(uint32_t* __restrict__ a, uint32_t n, uint32_t v) {
   if (i < n) a[i] = v;
 }
 
-// scratch that lives for one analysis call
+// scratch that lives for one call of the aggregate labels (soup_aggregate_labels allocates and
+// frees per call, as its declaration states; the other analysis calls use the batch's scratch)
 struct Scratch {
   std::vector<void*> ptrs;
   ~Scratch() { for (void* p : ptrs) cudaFree(p); }
@@ -286,6 +287,19 @@ struct Scratch {
 }  // namespace
 
 void exclusive_scan(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* tmp, cudaStream_t st);
+
+char* analysis_scratch(Batch& b, size_t bytes) {
+  if (bytes > b.an_cap) {
+    SOUP_CUDA_TRY(cudaStreamSynchronize(b.stream));
+    if (b.an_buf) SOUP_CUDA_TRY(cudaFree(b.an_buf));
+    b.an_buf = nullptr;
+    b.an_cap = 0;
+    const size_t want = (bytes + (size_t(1) << 20) - 1) & ~((size_t(1) << 20) - 1);
+    SOUP_CUDA_TRY(cudaMalloc(&b.an_buf, want));
+    b.an_cap = want;
+  }
+  return b.an_buf;
+}
 
 int run_closure(Batch& b, uint32_t r, const uint32_t* mem, uint32_t nm, const uint32_t* wat, uint32_t nw,
                 const double centre[3], double cell, double radius, double vmin, SoupClosureResult* out,
@@ -303,15 +317,19 @@ int run_closure(Batch& b, uint32_t r, const uint32_t* mem, uint32_t nm, const ui
   const uint64_t nc = (uint64_t)g.nx * g.ny * g.nz;
   if (nc >= 0xFFFFFFF0ull) { err = "closure: grid too large"; return SOUP_E_ARG; }
   const int reach = std::max(1, (int)std::ceil(radius / cell));
-  Scratch S;
-  uint8_t* occ = S.get<uint8_t>(nc);
-  uint32_t* vis = S.get<uint32_t>(nc);
-  uint32_t* dmem = S.get<uint32_t>(nm);
-  uint32_t* dwat = S.get<uint32_t>(nw);
-  uint32_t* fa = S.get<uint32_t>(nc);
-  uint32_t* fb = S.get<uint32_t>(nc);
-  uint32_t* cnt = S.get<uint32_t>(2);
-  unsigned long long* u64 = S.get<unsigned long long>(8);
+  ScratchLayout L;
+  const size_t o_occ = L.add<uint8_t>(nc), o_vis = L.add<uint32_t>(nc), o_mem = L.add<uint32_t>(nm),
+               o_wat = L.add<uint32_t>(nw), o_fa = L.add<uint32_t>(nc), o_fb = L.add<uint32_t>(nc),
+               o_cnt = L.add<uint32_t>(2), o_u64 = L.add<unsigned long long>(8);
+  char* base = analysis_scratch(b, L.used);
+  uint8_t* occ = reinterpret_cast<uint8_t*>(base + o_occ);
+  uint32_t* vis = reinterpret_cast<uint32_t*>(base + o_vis);
+  uint32_t* dmem = reinterpret_cast<uint32_t*>(base + o_mem);
+  uint32_t* dwat = reinterpret_cast<uint32_t*>(base + o_wat);
+  uint32_t* fa = reinterpret_cast<uint32_t*>(base + o_fa);
+  uint32_t* fb = reinterpret_cast<uint32_t*>(base + o_fb);
+  uint32_t* cnt = reinterpret_cast<uint32_t*>(base + o_cnt);
+  unsigned long long* u64 = reinterpret_cast<unsigned long long*>(base + o_u64);
   cudaStream_t st = b.stream;
   SOUP_CUDA_TRY(cudaMemsetAsync(occ, 0, nc, st));
   SOUP_CUDA_TRY(cudaMemsetAsync(vis, 0, 4 * nc, st));
@@ -377,11 +395,14 @@ int run_closure(Batch& b, uint32_t r, const uint32_t* mem, uint32_t nm, const ui
 int run_amphiphiles(Batch& b, uint32_t r, uint32_t* head_of, uint32_t* n_out, std::string& err) {
   (void)err;
   const uint32_t n = b.cfg[r].n, off = b.hsp[r].slot_off;
-  Scratch S;
-  uint32_t* parent = S.get<uint32_t>(n);
-  uint32_t* acc = S.get<uint32_t>(5 * (size_t)n + 1);
-  uint32_t* dh = S.get<uint32_t>(n);
-  uint32_t* polar = S.get<uint32_t>(SOUP_KMAX);
+  ScratchLayout L;
+  const size_t o_parent = L.add<uint32_t>(n), o_acc = L.add<uint32_t>(5 * (size_t)n + 1), o_dh = L.add<uint32_t>(n),
+               o_polar = L.add<uint32_t>(SOUP_KMAX);
+  char* base = analysis_scratch(b, L.used);
+  uint32_t* parent = reinterpret_cast<uint32_t*>(base + o_parent);
+  uint32_t* acc = reinterpret_cast<uint32_t*>(base + o_acc);
+  uint32_t* dh = reinterpret_cast<uint32_t*>(base + o_dh);
+  uint32_t* polar = reinterpret_cast<uint32_t*>(base + o_polar);
   uint32_t hp[SOUP_KMAX];
   for (int k = 0; k < SOUP_KMAX; ++k) hp[k] = b.cfg[r].kind_class[k] == SOUP_CLASS_POLAR ? 1u : 0u;
   cudaStream_t st = b.stream;

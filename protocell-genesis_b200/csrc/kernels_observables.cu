@@ -98,14 +98,12 @@ int run_profile_z(Batch& b, uint32_t r, uint32_t bins, uint32_t head_mask, uint3
                   uint32_t* escaped, std::string& err) {
   const SoupConfig& c = b.cfg[r];
   std::vector<uint32_t> h(2 * (size_t)bins + 1, 0);
-  uint32_t* d = nullptr;
-  SOUP_CUDA_TRY(cudaMallocAsync(&d, 4 * h.size(), b.stream));
+  uint32_t* d = reinterpret_cast<uint32_t*>(analysis_scratch(b, 4 * h.size()));
   SOUP_CUDA_TRY(cudaMemsetAsync(d, 0, 4 * h.size(), b.stream));
   b.launches += 1;
   k_profile_z<<<nblocks(c.n), kBlock, 0, b.stream>>>(b.pos, b.hsp[r].slot_off, c.n, c.box[2], bins, head_mask, d);
   SOUP_CUDA_TRY(cudaGetLastError());
   SOUP_CUDA_TRY(cudaMemcpyAsync(h.data(), d, 4 * h.size(), cudaMemcpyDeviceToHost, b.stream));
-  SOUP_CUDA_TRY(cudaFreeAsync(d, b.stream));
   SOUP_CUDA_TRY(cudaStreamSynchronize(b.stream));
   const uint32_t esc = h[2 * (size_t)bins];
   if (esc && !escaped) {
@@ -131,8 +129,7 @@ int run_pairing(Batch& b, uint32_t r, double contact, uint32_t out5[5], std::str
     err = "pairingStats: the contact radius must be below the electrostatics cutoff (the head list's reach)";
     return SOUP_E_ARG;
   }
-  uint32_t* d = nullptr;
-  SOUP_CUDA_TRY(cudaMallocAsync(&d, 4 * 5, b.stream));
+  uint32_t* d = reinterpret_cast<uint32_t*>(analysis_scratch(b, 4 * 5));
   SOUP_CUDA_TRY(cudaMemsetAsync(d, 0, 4 * 5, b.stream));
   b.launches += 1;
   k_pairing<<<nblocks((uint64_t)P.nheads * 32, kBlock), kBlock, 0, b.stream>>>(
@@ -140,7 +137,6 @@ int run_pairing(Batch& b, uint32_t r, double contact, uint32_t out5[5], std::str
       contact, d);
   SOUP_CUDA_TRY(cudaGetLastError());
   SOUP_CUDA_TRY(cudaMemcpyAsync(out5, d, 4 * 5, cudaMemcpyDeviceToHost, b.stream));
-  SOUP_CUDA_TRY(cudaFreeAsync(d, b.stream));
   SOUP_CUDA_TRY(cudaStreamSynchronize(b.stream));
   return SOUP_OK;
 }
@@ -218,11 +214,12 @@ int run_shapes(Batch& b, uint32_t r, const uint32_t* members_csr, const uint32_t
   const uint32_t total = start[ncomp];
   for (uint32_t k = 0; k < total; ++k)
     if (members_csr[k] >= c.n) { err = "aggregate shapes: member index out of range"; return SOUP_E_ARG; }
-  uint32_t *dm = nullptr, *ds = nullptr;
-  double* dout = nullptr;
-  SOUP_CUDA_TRY(cudaMallocAsync(&dm, 4 * (size_t)std::max<uint32_t>(total, 1), b.stream));
-  SOUP_CUDA_TRY(cudaMallocAsync(&ds, 4 * ((size_t)ncomp + 1), b.stream));
-  SOUP_CUDA_TRY(cudaMallocAsync(&dout, 80 * (size_t)ncomp, b.stream));
+  ScratchLayout L;
+  const size_t o_m = L.add<uint32_t>(total), o_s = L.add<uint32_t>((size_t)ncomp + 1), o_out = L.add<double>(10 * (size_t)ncomp);
+  char* base = analysis_scratch(b, L.used);
+  uint32_t* dm = reinterpret_cast<uint32_t*>(base + o_m);
+  uint32_t* ds = reinterpret_cast<uint32_t*>(base + o_s);
+  double* dout = reinterpret_cast<double*>(base + o_out);
   SOUP_CUDA_TRY(cudaMemcpyAsync(dm, members_csr, 4 * (size_t)total, cudaMemcpyHostToDevice, b.stream));
   SOUP_CUDA_TRY(cudaMemcpyAsync(ds, start, 4 * ((size_t)ncomp + 1), cudaMemcpyHostToDevice, b.stream));
   b.launches += 1;
@@ -230,9 +227,6 @@ int run_shapes(Batch& b, uint32_t r, const uint32_t* members_csr, const uint32_t
                                                  c.box[2], dout);
   SOUP_CUDA_TRY(cudaGetLastError());
   SOUP_CUDA_TRY(cudaMemcpyAsync(out10, dout, 80 * (size_t)ncomp, cudaMemcpyDeviceToHost, b.stream));
-  SOUP_CUDA_TRY(cudaFreeAsync(dm, b.stream));
-  SOUP_CUDA_TRY(cudaFreeAsync(ds, b.stream));
-  SOUP_CUDA_TRY(cudaFreeAsync(dout, b.stream));
   SOUP_CUDA_TRY(cudaStreamSynchronize(b.stream));
   return SOUP_OK;
 }

@@ -443,8 +443,7 @@ void destroy_batch(Batch* b) {
                   b->cell_cursor, b->perm, b->scan_tmp, b->nl, b->nl_cnt, b->heads, b->head_sys, b->es_nl,
                   b->es_cnt, b->head_slot, b->head_e, b->head_pos, b->head_xq, b->head_d, b->head_flag, b->draw_site, b->sweep_band, b->hcell_count, b->hcell_start, b->hcell_cursor, b->hsorted, b->hcell_of, b->flags,
                   b->events, b->desorb, b->drift_bits, b->bond_items, b->bond_nitems, b->uf_parent, b->comp_min,
-                  b->item_done, b->has_item, b->sweep_out, b->prot_rng_dev, b->sp, b->shared, b->sysid, b->occ,
-                  b->vis, b->frontier};
+                  b->item_done, b->has_item, b->sweep_out, b->prot_rng_dev, b->sp, b->shared, b->sysid, b->an_buf};
   for (void* p : ptrs) if (p) cudaFree(p);
   for (void* p : {(void*)b->diff.frames, (void*)b->diff.A, (void*)b->diff.B, (void*)b->diff.g, (void*)b->diff.jg,
                   (void*)b->diff.frozen_o, (void*)b->diff.partial, (void*)b->diff.all})
@@ -1085,6 +1084,65 @@ int soup_nonfinite_count(SoupHandle* h, uint32_t* out2) {
 }
 int soup_read_protonation_rng(SoupHandle* h, uint32_t* out) {
   return guarded(h, [&](Batch& b, uint32_t r) { *out = b.prot_rng[r]; });
+}
+
+// ---- checkpoint payload (soup/src/checkpoint.ts:176-214) --------------------------------------
+// One pass over replica r's slots un-permutes all eight arrays of a checkpoint into the re-sort
+// gather's second buffers (free outside a rebuild); eight copies then land them back to back in the
+// caller's buffer behind a single wait.
+struct CkptArrays {
+  const float4 *pos, *vel;
+  const uint32_t *slots, *center, *held, *brng, *trng;
+  const float* q;
+  float4 *opos, *ovel;
+  uint32_t *oslots, *ocenter, *oheld, *obrng, *otrng;
+  float* oq;
+};
+__global__ void k_checkpoint_gather(CkptArrays a, const uint32_t* __restrict__ id, uint32_t off, uint32_t n) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= n) return;
+  const uint32_t s = off + k, i = id[s] - off;
+  auto local = [off](uint32_t v) { return v == NONE ? v : v - off; };
+  a.opos[i] = a.pos[s];
+  a.ovel[i] = a.vel[s];
+  for (int e = 0; e < 3; ++e) a.oslots[3 * (size_t)i + e] = local(a.slots[3 * (size_t)s + e]);
+  a.ocenter[i] = local(a.center[s]);
+  a.oheld[i] = a.held[s];
+  a.obrng[i] = a.brng[s];
+  a.otrng[i] = a.trng[s];
+  a.oq[i] = a.q[s];
+}
+
+int soup_read_checkpoint(SoupHandle* h, void* dst, size_t bytes, SoupCheckpointScalars* scalars) {
+  return guarded(h, [&](Batch& b, uint32_t r) {
+    if (!dst) fail(SOUP_E_ARG, "NULL destination");
+    const uint32_t n = b.cfg[r].n, off = b.hsp[r].slot_off;
+    need(bytes, (size_t)SOUP_CHECKPOINT_BYTES_PER_PARTICLE * n);
+    CkptArrays a{b.pos, b.vel, b.slots, b.center, b.held, b.brng, b.trng, b.charge,
+                 b.pos2, b.vel2, b.slots2, b.center2, b.held2, b.brng2, b.trng2, b.charge2};
+    if (n) k_checkpoint_gather<<<(n + 255) / 256, 256, 0, b.stream>>>(a, b.id, off, n);
+    SOUP_CUDA_TRY(cudaGetLastError());
+    char* o = static_cast<char*>(dst);
+    const struct { const void* src; size_t per; } parts[] = {
+        {b.pos2, 16}, {b.vel2, 16}, {b.slots2, 12}, {b.center2, 4}, {b.held2, 4}, {b.brng2, 4}, {b.trng2, 4}, {b.charge2, 4}};
+    for (const auto& p : parts) {
+      SOUP_CUDA_TRY(cudaMemcpyAsync(o, p.src, p.per * n, cudaMemcpyDeviceToHost, b.stream));
+      o += p.per * n;
+    }
+    SoupCheckpointScalars s{};
+    if (scalars) {
+      s.global_step = b.step[r];
+      s.n = n;
+      s.n_rules = b.cfg[r].n_rules;
+      s.protonation_rng = b.prot_rng[r];
+      for (int a3 = 0; a3 < 3; ++a3) s.live_box[a3] = b.cfg[r].box[a3];
+      SOUP_CUDA_TRY(cudaMemcpyAsync(s.desorb, b.desorb + 2 * r, 8, cudaMemcpyDeviceToHost, b.stream));
+      SOUP_CUDA_TRY(cudaMemcpyAsync(s.events, b.events + 2 * SOUP_MAX_RULES * r, sizeof s.events,
+                                    cudaMemcpyDeviceToHost, b.stream));
+    }
+    SOUP_CUDA_TRY(cudaStreamSynchronize(b.stream));
+    if (scalars) *scalars = s;
+  });
 }
 
 int soup_read_verlet(SoupHandle* h, uint32_t* counts, uint32_t* lists, size_t lists_cap) {

@@ -133,10 +133,11 @@ struct Batch {
   double* sweep_out = nullptr;       // per replica: attempts, accepted, dEsSum, dEsCount
   uint32_t* prot_rng_dev = nullptr;
 
-  // analysis scratch
-  uint8_t *occ = nullptr, *vis = nullptr;
-  size_t grid_cap = 0;
-  uint32_t* frontier = nullptr;
+  // analysis scratch: one buffer that grows to the largest request of the analysis calls and is
+  // reused after that (analysis_scratch), so a call makes no cudaMalloc / cudaFree once its sizes
+  // have been seen
+  char* an_buf = nullptr;
+  size_t an_cap = 0;
 
   // host-side schedule
   std::vector<uint64_t> step;        // per replica global step
@@ -226,6 +227,17 @@ int run_closure(Batch& b, uint32_t r, const uint32_t* mem, uint32_t nm, const ui
                 const double centre[3], double cell, double radius, double vmin, SoupClosureResult* out,
                 std::string& err);
 int run_amphiphiles(Batch& b, uint32_t r, uint32_t* head_of, uint32_t* n_out, std::string& err);
+// Offsets of the sub-buffers of one analysis call inside the batch's analysis scratch (256-byte
+// aligned), and the scratch itself, grown to `bytes` when it is smaller.
+struct ScratchLayout {
+  size_t used = 0;
+  template <class T> size_t add(size_t n) {
+    const size_t at = (used + 255) & ~size_t(255);
+    used = at + (n > 0 ? n : 1) * sizeof(T);
+    return at;
+  }
+};
+char* analysis_scratch(Batch& b, size_t bytes);
 int run_profile_z(Batch& b, uint32_t r, uint32_t bins, uint32_t head_mask, uint32_t* head, uint32_t* tail,
                   uint32_t* escaped, std::string& err);
 int run_pairing(Batch& b, uint32_t r, double contact, uint32_t out5[5], std::string& err);

@@ -197,6 +197,39 @@ class SoupSystem:
         _check(self._lib, self._h, self._lib.soup_read_protonation_rng(self._h, C.byref(v)))
         return v.value
 
+    def invariants(self) -> dict:
+        """invariants (soup/src/soup-readback.ts:136-152): the live census per monomer id (kind read
+        from the position's w, rounded), the bond count, and the summed monomer charge property
+        (absent from every monomer of the parameter tables, so 0)."""
+        monomers = _config.load_params()["monomers"]
+        kinds = np.rint(self.particles().reshape(-1, 4)[:, 3]).astype(np.int64)
+        census = np.bincount(kinds, minlength=len(monomers))
+        counts = {m["id"]: int(census[k]) for k, m in enumerate(monomers)}
+        charge = float(sum(census[k] * float(m.get("charge", 0) or 0) for k, m in enumerate(monomers)))
+        return dict(monomers=counts, bonds=int(self.bonds().size // 2), charge=charge)
+
+    def checkpoint_payload(self):
+        """Every array and scalar a checkpoint carries, from one soup_read_checkpoint call: a dict of
+        numpy arrays in the readback layouts (views of one host buffer) and a dict of scalars."""
+        buf = np.empty(_abi.CHECKPOINT_BYTES_PER_PARTICLE * self.n, np.uint8)
+        sc = _abi.SoupCheckpointScalars()
+        _check(self._lib, self._h, self._lib.soup_read_checkpoint(self._h, _ptr(buf), buf.nbytes, C.byref(sc)))
+        n, out, at = self.n, {}, 0
+        for name, dt, per in (("positions", np.float32, 4), ("velocities", np.float32, 4), ("bondSlots", np.uint32, 3),
+                              ("centerLink", np.uint32, 1), ("centerHeldSteps", np.uint32, 1), ("bondRng", np.uint32, 1),
+                              ("thermoRng", np.uint32, 1), ("charges", np.float32, 1)):
+            nb = 4 * per * n
+            out[name] = buf[at:at + nb].view(dt)
+            at += nb
+        ev = list(sc.events)[: 2 * sc.n_rules]
+        events = {}
+        for r, (b, k) in enumerate(self.rule_ids[: sc.n_rules]):
+            events[b], events[k] = int(ev[2 * r]), int(ev[2 * r + 1])
+        scalars = dict(globalStep=int(sc.global_step), N=int(sc.n), protonationRng=int(sc.protonation_rng),
+                       desorbEvents=dict(stretch=int(sc.desorb[0]), timeout=int(sc.desorb[1])), events=events,
+                       liveBox=[float(x) for x in sc.live_box])
+        return out, scalars
+
     def verlet_lists(self):
         counts = np.empty(self.n, np.uint32)
         _check(self._lib, self._h, self._lib.soup_read_verlet(self._h, counts.ctypes.data_as(_abi._U32P), None, 0))
