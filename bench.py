@@ -593,6 +593,27 @@ def checkpoint_timing(s, cfg, reps=3):
                     "file: payload + base64 + JSON text of the reference's CheckpointFile"}
 
 
+def box_scale_timing(s, cfg):
+    """One box change of the live system (soup/src/soup-box-scale.ts applyBoxScaleOnce) on the device:
+    rigid units of the covalent bonds, then with the amphiphiles' proximity cohesion at the nonbonded
+    cutoff; wall clock of each call (the map, the self-check, the re-grid, rebuild and force pass).
+    It runs after everything that is timed: the system is left in the slightly compressed box."""
+    import numpy as np
+    from protocell_genesis_b200 import _abi
+    box = [float(x) for x in s.box]
+    _, head_of = s.amphiphile_labels()
+    members = np.nonzero(head_of != _abi.NONE)[0].astype(np.uint32)
+    cut = float(cfg.rc_attr + cfg.wc)
+    out = {"beads": s.n, "bonds": int(s.bonds().size // 2), "cohesion_members": int(members.size)}
+    t0 = time.perf_counter()
+    s.scale_box_once([x * 0.995 for x in box])
+    out["bonds_only_ms"] = 1e3 * (time.perf_counter() - t0)
+    t0 = time.perf_counter()
+    s.scale_box_once([x * 0.99 for x in box], {"cutoff": cut, "memberIndices": members})
+    out["with_cohesion_ms"] = 1e3 * (time.perf_counter() - t0)
+    return out
+
+
 def step_with_samples(s, steps, every, sampler):
     """`steps` steps with the progress sample after every `every` of them."""
     done, samples = 0, []
@@ -735,6 +756,7 @@ def run_cuda(args):
                "h2d_bytes_per_step": h2d / e2e_steps, "d2h_bytes_per_step": 16 * n / 10,
                "note": "create from pinned host arrays + step(10) + particles() readback per 10 steps, wall clock"}
     s2.dispose()
+    box_scale = box_scale_timing(s, cfg)
 
     cpu = None
     if rank == 0 and ws == 1 and not args.no_cpu:
@@ -778,6 +800,7 @@ def run_cuda(args):
                        "sweeps_in_timed_region": info1["sweeps"] - info0["sweeps"],
                        "autotune": tune,
                        "checkpoint": ckpt,
+                       "box_scale": box_scale,
                        "analysis": None if sampler is None else {
                            "every": args.analysis_every, "samples_in_timed_region": len(samples),
                            "ms_per_sample": 1e3 * sum(sampler.times[:len(samples)]) / max(len(samples), 1),

@@ -246,10 +246,27 @@ typedef struct SoupCheckpointScalars {
 } SoupCheckpointScalars;
 int soup_read_checkpoint(SoupHandle* h, void* dst, size_t bytes, SoupCheckpointScalars* scalars);
 
+/* ---- box scale (soup/src/soup-box-scale.ts:81-165 applyBoxScaleOnce) -------------------------
+ * One box change of a live system: every rigid unit (a connected component of the covalent bonds,
+ * plus, when cohesion_cutoff > 0, of the proximity pairs within that cutoff among cohesion_members,
+ * or among all beads when that is NULL) keeps its internal offsets, and its centre of mass scales
+ * with the box (scaleMoleculesRigid, soup/src/soup-box-scale-math.ts:63-138).  Then the live box,
+ * grid and wall radius change, the lists are rebuilt and the force recomputed, and the finiteness
+ * and list guards run.  Refused (SOUP_E_STATE, state unchanged) with the reference's message when a
+ * rigid edge's length moves by more than 1e-3 or the system has immobile (mineral) beads.
+ * Velocities are not changed.  The ramp (scaleBoxTo, growBoxTo) is the caller's loop. */
+int soup_scale_box(SoupHandle* h, const double target_box[3], double cohesion_cutoff,
+                   const uint32_t* cohesion_members, uint32_t n_members);
+/* scaleMoleculesRigid alone, on h's device, over caller arrays: n positions (f32 x4), n_edges rigid
+ * edges as (i, j) pairs; out receives the positions in new_box (f32 x4, w copied). */
+int soup_scale_molecules_rigid(SoupHandle* h, const float* positions, uint32_t n, const uint32_t* edges,
+                               uint32_t n_edges, const double old_box[3], const double new_box[3], float* out);
+
 /* ---- writes --------------------------------------------------------------------------------- */
 /* writeBuffer(chargeBuf) (soup/src/soup-protonation.ts:60); marks forces stale. */
 int soup_write_charges(SoupHandle* h, const float* src, size_t bytes);
-/* Live box change (soup/src/soup-box-scale.ts resizeSoupGrid); positions are not moved. */
+/* Live box change (soup/src/soup-box-scale.ts resizeSoupGrid); positions are not moved, the wall
+ * radius follows the box (liveRadius, soup/src/soup-confine.ts:76-78). */
 int soup_set_box(SoupHandle* h, const double box[3]);
 
 /* ---- autotuning (no reference counterpart) ----------------------------------------------------

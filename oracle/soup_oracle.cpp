@@ -1614,4 +1614,101 @@ int oracle_relax(void* p, uint32_t iterations, double d0) {
   return SOUP_OK;
 }
 
+// scaleMoleculesRigid (soup/src/soup-box-scale-math.ts:63-138).  Adjacency lists in edge order
+// (each edge (i, j) appends j to i's list and i to j's); components discovered from the smallest
+// unvisited index; breadth-first walk with offsets accumulated edge by edge through mi1 (JavaScript
+// Math.round); FP64 centre of mass summed in visiting order; each bead rebuilt about the scaled,
+// wrapped centre from its unchanged offset and wrapped into the new box.  All double, no FMA
+// contraction (the Makefile's -ffp-contract=off), as the reference's JavaScript numbers.
+int oracle_scale_molecules_rigid(const float* pos, uint32_t n, const uint32_t* edges, uint32_t n_edges,
+                                 const double old_box[3], const double new_box[3], float* out) {
+  const double s[3] = {new_box[0] / old_box[0], new_box[1] / old_box[1], new_box[2] / old_box[2]};
+  std::vector<std::vector<uint32_t>> adj(n);
+  for (uint32_t k = 0; k < n_edges; ++k) {
+    const uint32_t i = edges[2 * k], j = edges[2 * k + 1];
+    if (i >= n || j >= n) { g_err = "scaleMoleculesRigid: edge names a particle outside the system"; return SOUP_E_ARG; }
+    adj[i].push_back(j);
+    adj[j].push_back(i);
+  }
+  std::vector<uint8_t> visited(n, 0);
+  std::vector<double> off(3 * (size_t)n, 0.0);
+  std::vector<uint32_t> members;
+  for (uint32_t root = 0; root < n; ++root) {
+    if (visited[root]) continue;
+    visited[root] = 1;
+    for (int a = 0; a < 3; ++a) off[3 * (size_t)root + a] = 0.0;
+    members.assign(1, root);
+    for (size_t qi = 0; qi < members.size(); ++qi) {
+      const uint32_t p = members[qi];
+      for (uint32_t c : adj[p]) {
+        if (visited[c]) continue;
+        visited[c] = 1;
+        for (int a = 0; a < 3; ++a)
+          off[3 * (size_t)c + a] = off[3 * (size_t)p + a] + mi1((double)pos[4 * (size_t)c + a] - (double)pos[4 * (size_t)p + a], old_box[a]);
+        members.push_back(c);
+      }
+    }
+    double cen[3], com[3];
+    for (int a = 0; a < 3; ++a) {
+      double sum = 0.0;
+      for (uint32_t b : members) sum += off[3 * (size_t)b + a];
+      cen[a] = sum / (double)members.size();
+      com[a] = wrap1((double)pos[4 * (size_t)root + a] + cen[a], old_box[a]) * s[a];
+    }
+    for (uint32_t b : members) {
+      for (int a = 0; a < 3; ++a) out[4 * (size_t)b + a] = (float)wrap1(com[a] + (off[3 * (size_t)b + a] - cen[a]), new_box[a]);
+      out[4 * (size_t)b + 3] = pos[4 * (size_t)b + 3];
+    }
+  }
+  return SOUP_OK;
+}
+
+// proximityPairs (soup/src/soup-box-scale-math.ts:162-221): pairs i < j among the eligible beads with
+// a minimum-image distance <= cutoff, from a cell list of floor(box / cutoff) cells per axis, every
+// axis periodic.  A pair is listed once per neighbouring-cell visit that reaches it, as the
+// reference's 27-cell loop does (fewer than three cells on an axis visits a cell more than once).
+// Writes up to `cap` pairs; returns the number found in *count.
+int oracle_proximity_pairs(const float* pos, uint32_t n, const double box[3], double cutoff, const uint8_t* eligible,
+                           uint32_t* pairs, size_t cap, size_t* count) {
+  int nc[3];
+  double w[3];
+  for (int a = 0; a < 3; ++a) { nc[a] = std::max(1, (int)std::floor(box[a] / cutoff)); w[a] = box[a] / nc[a]; }
+  std::vector<int> cx(n), cy(n), cz(n);
+  std::vector<std::vector<uint32_t>> bucket((size_t)nc[0] * nc[1] * nc[2]);
+  for (uint32_t i = 0; i < n; ++i) {
+    if (!eligible[i]) continue;
+    int c[3];
+    for (int a = 0; a < 3; ++a)
+      c[a] = std::min(nc[a] - 1, (int)std::floor(wrap1((double)pos[4 * (size_t)i + a], box[a]) / w[a]));
+    cx[i] = c[0]; cy[i] = c[1]; cz[i] = c[2];
+    bucket[((size_t)c[2] * nc[1] + c[1]) * nc[0] + c[0]].push_back(i);
+  }
+  const double c2 = cutoff * cutoff;
+  size_t k = 0;
+  for (uint32_t i = 0; i < n; ++i) {
+    if (!eligible[i]) continue;
+    for (int dx = -1; dx <= 1; ++dx) {
+      const int x = ((cx[i] + dx) % nc[0] + nc[0]) % nc[0];
+      for (int dy = -1; dy <= 1; ++dy) {
+        const int y = ((cy[i] + dy) % nc[1] + nc[1]) % nc[1];
+        for (int dz = -1; dz <= 1; ++dz) {
+          const int z = ((cz[i] + dz) % nc[2] + nc[2]) % nc[2];
+          for (uint32_t j : bucket[((size_t)z * nc[1] + y) * nc[0] + x]) {
+            if (j <= i) continue;
+            const double ddx = mi1((double)pos[4 * (size_t)i] - (double)pos[4 * (size_t)j], box[0]);
+            const double ddy = mi1((double)pos[4 * (size_t)i + 1] - (double)pos[4 * (size_t)j + 1], box[1]);
+            const double ddz = mi1((double)pos[4 * (size_t)i + 2] - (double)pos[4 * (size_t)j + 2], box[2]);
+            if (ddx * ddx + ddy * ddy + ddz * ddz <= c2) {
+              if (k < cap) { pairs[2 * k] = i; pairs[2 * k + 1] = j; }
+              ++k;
+            }
+          }
+        }
+      }
+    }
+  }
+  *count = k;
+  return SOUP_OK;
+}
+
 }  // extern "C"

@@ -288,17 +288,17 @@ struct Scratch {
 
 void exclusive_scan(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* tmp, cudaStream_t st);
 
-char* analysis_scratch(Batch& b, size_t bytes) {
-  if (bytes > b.an_cap) {
+char* analysis_scratch(Batch& b, size_t bytes, int which) {
+  if (bytes > b.an_cap[which]) {
     SOUP_CUDA_TRY(cudaStreamSynchronize(b.stream));
-    if (b.an_buf) SOUP_CUDA_TRY(cudaFree(b.an_buf));
-    b.an_buf = nullptr;
-    b.an_cap = 0;
+    if (b.an_buf[which]) SOUP_CUDA_TRY(cudaFree(b.an_buf[which]));
+    b.an_buf[which] = nullptr;
+    b.an_cap[which] = 0;
     const size_t want = (bytes + (size_t(1) << 20) - 1) & ~((size_t(1) << 20) - 1);
-    SOUP_CUDA_TRY(cudaMalloc(&b.an_buf, want));
-    b.an_cap = want;
+    SOUP_CUDA_TRY(cudaMalloc(&b.an_buf[which], want));
+    b.an_cap[which] = want;
   }
-  return b.an_buf;
+  return b.an_buf[which];
 }
 
 int run_closure(Batch& b, uint32_t r, const uint32_t* mem, uint32_t nm, const uint32_t* wat, uint32_t nw,
@@ -468,6 +468,423 @@ int run_aggregates(Batch& b, uint32_t r, const uint32_t* mem, uint32_t m, double
   SOUP_CUDA_TRY(cudaMemcpyAsync(&nco, cnt, 4, cudaMemcpyDeviceToHost, st));
   SOUP_CUDA_TRY(cudaStreamSynchronize(st));
   if (ncomp) *ncomp = nco;
+  return SOUP_OK;
+}
+
+// ---- box scale: scaleMoleculesRigid and proximityPairs (soup/src/soup-box-scale-math.ts:63-221) ----
+//
+// The rigid units are the connected components of the rigid edges (covalent bonds, plus proximity
+// pairs when cohesion is asked for).  Each component is walked breadth first from its smallest index,
+// one level per launch, each bead's offset accumulated from its parent's across one edge through mi1,
+// exactly the reference's per-edge construction.  Where a bead can be reached from several beads of
+// the previous level (a cycle), the smallest of them is its parent: on a component that does not
+// wrap the box every path gives the same offset up to FP64 rounding.  The centre of mass is an exact
+// integer sum (offsets in units of 2^-44 sigma, split in two 64-bit accumulators), so it does not
+// depend on the order the atomics land in.
+namespace {
+
+constexpr uint32_t kUnset = 0xFFFFFFFFu;
+constexpr double kOffScale = 17592186044416.0;        // 2^44
+constexpr double kOffLimit = 262144.0;                // 2^18 sigma: |offset| * 2^44 stays below 2^62
+
+struct PGrid {
+  int n[3];
+  double box[3], w[3];
+};
+
+__device__ __forceinline__ int pcell_axis(double x, const PGrid& g, int a) {
+  return min(g.n[a] - 1, (int)floor(__ddiv_rn(wrap1(x, g.box[a]), g.w[a])));
+}
+
+// the distinct cells among c-1, c, c+1 (periodic) on an axis of n cells
+__device__ __forceinline__ int near_cells(int c, int n, int out[3]) {
+  int k = 0;
+  for (int d = -1; d <= 1; ++d) {
+    const int v = ((c + d) % n + n) % n;
+    bool seen = false;
+    for (int q = 0; q < k; ++q) seen |= out[q] == v;
+    if (!seen) out[k++] = v;
+  }
+  return k;
+}
+
+__global__ void k_bs_bond_count(const uint32_t* __restrict__ slots, uint32_t n, uint32_t* __restrict__ cnt) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t c = 0;
+  for (int e = 0; e < 3; ++e) {
+    const uint32_t j = slots[3 * (size_t)i + e];
+    c += (j != NONE && j > i && j < n) ? 1u : 0u;
+  }
+  cnt[i] = c;
+}
+
+__global__ void k_bs_bin(const float4* __restrict__ pos, const uint8_t* __restrict__ elig, uint32_t n, PGrid g,
+                         uint32_t* __restrict__ cell, uint32_t* __restrict__ ccount) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  if (!elig[i]) { cell[i] = kUnset; return; }
+  const float4 p = pos[i];
+  const int cx = pcell_axis((double)p.x, g, 0), cy = pcell_axis((double)p.y, g, 1), cz = pcell_axis((double)p.z, g, 2);
+  const uint32_t c = (uint32_t)(((size_t)cz * g.n[1] + cy) * g.n[0] + cx);
+  cell[i] = c;
+  atomicAdd(&ccount[c], 1u);
+}
+
+__global__ void k_bs_cell_scatter(const uint32_t* __restrict__ cell, uint32_t n, const uint32_t* __restrict__ cstart,
+                                  uint32_t* __restrict__ ccursor, uint32_t* __restrict__ csorted) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || cell[i] == kUnset) return;
+  csorted[cstart[cell[i]] + atomicAdd(&ccursor[cell[i]], 1u)] = i;
+}
+
+// proximity pairs (i, j > i) of bead i: counted when `edges` is NULL, written from edges[2 * at] on
+template <bool FILL>
+__global__ void k_bs_prox(const float4* __restrict__ pos, const uint32_t* __restrict__ cell, uint32_t n, PGrid g,
+                          const uint32_t* __restrict__ cstart, const uint32_t* __restrict__ csorted, double c2,
+                          uint32_t* __restrict__ cnt, const uint32_t* __restrict__ at, uint32_t* __restrict__ edges) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n || cell[i] == kUnset) return;
+  const uint32_t ci = cell[i];
+  const int cx = (int)(ci % (uint32_t)g.n[0]), cy = (int)((ci / (uint32_t)g.n[0]) % (uint32_t)g.n[1]),
+            cz = (int)(ci / ((uint32_t)g.n[0] * (uint32_t)g.n[1]));
+  int xs[3], ys[3], zs[3];
+  const int nxs = near_cells(cx, g.n[0], xs), nys = near_cells(cy, g.n[1], ys), nzs = near_cells(cz, g.n[2], zs);
+  const float4 pi = pos[i];
+  uint32_t k = FILL ? at[i] : 0u;
+  for (int a = 0; a < nxs; ++a)
+    for (int b2 = 0; b2 < nys; ++b2)
+      for (int c = 0; c < nzs; ++c) {
+        const uint32_t cc = (uint32_t)(((size_t)zs[c] * g.n[1] + ys[b2]) * g.n[0] + xs[a]);
+        for (uint32_t q = cstart[cc]; q < cstart[cc + 1]; ++q) {
+          const uint32_t j = csorted[q];
+          if (j <= i) continue;
+          const float4 pj = pos[j];
+          const double dx = mi1(__dsub_rn((double)pi.x, (double)pj.x), g.box[0]);
+          const double dy = mi1(__dsub_rn((double)pi.y, (double)pj.y), g.box[1]);
+          const double dz = mi1(__dsub_rn((double)pi.z, (double)pj.z), g.box[2]);
+          if (sq3(dx, dy, dz) <= c2) {
+            if (FILL) { edges[2 * (size_t)k] = i; edges[2 * (size_t)k + 1] = j; }
+            ++k;
+          }
+        }
+      }
+  if (!FILL) cnt[i] += k;
+}
+
+__global__ void k_bs_bond_fill(const uint32_t* __restrict__ slots, uint32_t n, const uint32_t* __restrict__ at,
+                               uint32_t* __restrict__ next, uint32_t* __restrict__ edges) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  uint32_t k = at[i];
+  for (int e = 0; e < 3; ++e) {
+    const uint32_t j = slots[3 * (size_t)i + e];
+    if (j != NONE && j > i && j < n) { edges[2 * (size_t)k] = i; edges[2 * (size_t)k + 1] = j; ++k; }
+  }
+  next[i] = k;   // where this bead's proximity pairs start
+}
+
+__global__ void k_bs_degree(const uint32_t* __restrict__ edges, uint32_t ne, uint32_t n, uint32_t* __restrict__ deg,
+                            uint32_t* __restrict__ bad) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= ne) return;
+  const uint32_t i = edges[2 * (size_t)k], j = edges[2 * (size_t)k + 1];
+  if (i >= n || j >= n) { atomicExch(bad, 1u); return; }
+  atomicAdd(&deg[i], 1u);
+  atomicAdd(&deg[j], 1u);
+}
+
+__global__ void k_bs_adjacency(const uint32_t* __restrict__ edges, uint32_t ne, uint32_t n,
+                               const uint32_t* __restrict__ astart, uint32_t* __restrict__ acursor,
+                               uint32_t* __restrict__ adj) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= ne) return;
+  const uint32_t i = edges[2 * (size_t)k], j = edges[2 * (size_t)k + 1];
+  if (i >= n || j >= n) return;
+  adj[astart[i] + atomicAdd(&acursor[i], 1u)] = j;
+  adj[astart[j] + atomicAdd(&acursor[j], 1u)] = i;
+}
+
+__global__ void k_bs_union(const uint32_t* __restrict__ edges, uint32_t ne, uint32_t n, uint32_t* __restrict__ parent) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= ne) return;
+  const uint32_t i = edges[2 * (size_t)k], j = edges[2 * (size_t)k + 1];
+  if (i < n && j < n) uf_union(parent, i, j);
+}
+
+// roots (the smallest index of each component) start the walk at level 0 with a zero offset
+__global__ void k_bs_roots(uint32_t* __restrict__ parent, uint32_t n, uint32_t* __restrict__ level,
+                           uint32_t* __restrict__ cand, double* __restrict__ off, uint32_t* __restrict__ front,
+                           uint32_t* __restrict__ nfront) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t r = uf_find(parent, i);
+  cand[i] = kUnset;
+  if (r == i) {
+    level[i] = 0;
+    off[3 * (size_t)i] = 0.0; off[3 * (size_t)i + 1] = 0.0; off[3 * (size_t)i + 2] = 0.0;
+    front[atomicAdd(nfront, 1u)] = i;
+  } else {
+    level[i] = kUnset;
+  }
+}
+
+__global__ void k_bs_root_store(uint32_t* __restrict__ parent, uint32_t n, uint32_t* __restrict__ root) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) root[i] = uf_find(parent, i);
+}
+
+// one level: every unreached neighbour of the frontier takes the smallest frontier bead as parent
+__global__ void k_bs_claim(const uint32_t* __restrict__ front, const uint32_t* __restrict__ nfront,
+                           const uint32_t* __restrict__ astart, const uint32_t* __restrict__ adj,
+                           const uint32_t* __restrict__ level, uint32_t* __restrict__ cand, uint32_t* __restrict__ next,
+                           uint32_t* __restrict__ nnext) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= *nfront) return;
+  const uint32_t p = front[k];
+  for (uint32_t q = astart[p]; q < astart[p + 1]; ++q) {
+    const uint32_t c = adj[q];
+    if (level[c] != kUnset) continue;
+    if (atomicMin(&cand[c], p) == kUnset) next[atomicAdd(nnext, 1u)] = c;
+  }
+}
+
+__global__ void k_bs_settle(const uint32_t* __restrict__ next, const uint32_t* __restrict__ nnext, uint32_t lev,
+                            const float4* __restrict__ pos, const uint32_t* __restrict__ cand, Grid ob,
+                            uint32_t* __restrict__ level, double* __restrict__ off) {
+  const uint32_t m = *nnext;   // the size of the new level, known only on the device: grid-stride
+  for (uint32_t k = blockIdx.x * blockDim.x + threadIdx.x; k < m; k += gridDim.x * blockDim.x) {
+    const uint32_t c = next[k], p = cand[c];
+    const float4 pc = pos[c], pp = pos[p];
+    level[c] = lev;
+    off[3 * (size_t)c] = __dadd_rn(off[3 * (size_t)p], mi1(__dsub_rn((double)pc.x, (double)pp.x), ob.box[0]));
+    off[3 * (size_t)c + 1] = __dadd_rn(off[3 * (size_t)p + 1], mi1(__dsub_rn((double)pc.y, (double)pp.y), ob.box[1]));
+    off[3 * (size_t)c + 2] = __dadd_rn(off[3 * (size_t)p + 2], mi1(__dsub_rn((double)pc.z, (double)pp.z), ob.box[2]));
+  }
+}
+
+// exact per-component sums of the offsets: value * 2^44 rounded, high part (>> 24) and low 24 bits
+// accumulated separately so neither 64-bit sum can overflow
+__global__ void k_bs_accumulate(const uint32_t* __restrict__ root, const double* __restrict__ off, uint32_t n,
+                                unsigned long long* __restrict__ acc, uint32_t* __restrict__ cnt,
+                                uint32_t* __restrict__ bad) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t r = root[i];
+  for (int a = 0; a < 3; ++a) {
+    const double o = off[3 * (size_t)i + a];
+    if (!(fabs(o) < kOffLimit)) { atomicExch(bad, 2u); return; }
+    const long long t = __double2ll_rn(__dmul_rn(o, kOffScale));
+    const long long hi = t >> 24, lo = t & 0xFFFFFFll;
+    atomicAdd(&acc[6 * (size_t)r + a], (unsigned long long)hi);
+    atomicAdd(&acc[6 * (size_t)r + 3 + a], (unsigned long long)lo);
+  }
+  atomicAdd(&cnt[r], 1u);
+}
+
+// out = wrap1(wrap1(root + centre, old) * s + (offset - centre), new), the reference's expression order
+__global__ void k_bs_place(const float4* __restrict__ pos, const uint32_t* __restrict__ root,
+                           const double* __restrict__ off, const unsigned long long* __restrict__ acc,
+                           const uint32_t* __restrict__ cnt, uint32_t n, Grid ob, Grid nb, double sx, double sy,
+                           double sz, float4* __restrict__ out) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const uint32_t r = root[i];
+  const float4 pr = pos[r], pi = pos[i];
+  const double s[3] = {sx, sy, sz};
+  const double rp[3] = {(double)pr.x, (double)pr.y, (double)pr.z};
+  float o3[3];
+  for (int a = 0; a < 3; ++a) {
+    const double hi = (double)(long long)acc[6 * (size_t)r + a], lo = (double)(long long)acc[6 * (size_t)r + 3 + a];
+    const double sum = __dmul_rn(__dadd_rn(__dmul_rn(hi, 16777216.0), lo), 1.0 / kOffScale);
+    const double cen = __ddiv_rn(sum, (double)cnt[r]);
+    const double com = __dmul_rn(wrap1(__dadd_rn(rp[a], cen), ob.box[a]), s[a]);
+    o3[a] = __double2float_rn(wrap1(__dadd_rn(com, __dsub_rn(off[3 * (size_t)i + a], cen)), nb.box[a]));
+  }
+  out[i] = make_float4(o3[0], o3[1], o3[2], pi.w);
+}
+
+__device__ __forceinline__ double mi3_distance(float4 a, float4 b, const Grid& g) {
+  const double dx = mi1(__dsub_rn((double)a.x, (double)b.x), g.box[0]);
+  const double dy = mi1(__dsub_rn((double)a.y, (double)b.y), g.box[1]);
+  const double dz = mi1(__dsub_rn((double)a.z, (double)b.z), g.box[2]);
+  return __dsqrt_rn(sq3(dx, dy, dz));
+}
+
+// applyBoxScaleOnce's self-check (soup/src/soup-box-scale.ts:117-128): the smallest edge index whose
+// length moved by more than 1e-3
+__global__ void k_bs_check(const uint32_t* __restrict__ edges, uint32_t ne, const float4* __restrict__ before,
+                           const float4* __restrict__ after, Grid ob, Grid nb, uint32_t* __restrict__ first_bad) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= ne) return;
+  const uint32_t i = edges[2 * (size_t)k], j = edges[2 * (size_t)k + 1];
+  const double d0 = mi3_distance(before[i], before[j], ob), d1 = mi3_distance(after[i], after[j], nb);
+  if (fabs(d1 - d0) > 1e-3) atomicMin(first_bad, k);
+}
+
+}  // namespace
+
+int run_rigid_map(Batch& b, const float4* pos_o, const uint32_t* slots_o, uint32_t n, const uint32_t* edges_host,
+                  uint64_t n_edges_host, double cohesion, const uint8_t* eligible_host, const double old_box[3],
+                  const double new_box[3], float4* out_o, bool check, std::string& err) {
+  if (n == 0) return SOUP_OK;
+  cudaStream_t st = b.stream;
+  const bool prox = !edges_host && cohesion > 0;
+  PGrid pg{};
+  uint32_t ncell = 0;
+  if (prox) {
+    uint64_t nc = 1;
+    for (int a = 0; a < 3; ++a) {
+      pg.n[a] = std::max(1, (int)std::floor(old_box[a] / cohesion));
+      pg.box[a] = old_box[a];
+      pg.w[a] = old_box[a] / pg.n[a];
+      nc *= (uint64_t)pg.n[a];
+    }
+    if (nc >= 0xFFFFFFF0ull) { err = "scaleBoxTo: the cohesion cutoff gives too many cells"; return SOUP_E_ARG; }
+    ncell = (uint32_t)nc;
+  }
+  const uint32_t scan_words = std::max(4 * ((n + 1) / 4096 + 64) + 256, 4 * (ncell / 4096 + 64) + 256);
+  // per-bead buffers, known before the edges are counted
+  ScratchLayout L;
+  const size_t o_elig = L.add<uint8_t>(n), o_cell = L.add<uint32_t>(n), o_ccount = L.add<uint32_t>(ncell + 1),
+               o_cstart = L.add<uint32_t>(ncell + 1), o_ccur = L.add<uint32_t>(ncell + 1), o_csorted = L.add<uint32_t>(n),
+               o_ecnt = L.add<uint32_t>(n + 1), o_estart = L.add<uint32_t>(n + 1), o_enext = L.add<uint32_t>(n),
+               o_deg = L.add<uint32_t>(n + 1), o_astart = L.add<uint32_t>(n + 1), o_acur = L.add<uint32_t>(n),
+               o_parent = L.add<uint32_t>(n), o_root = L.add<uint32_t>(n), o_level = L.add<uint32_t>(n),
+               o_cand = L.add<uint32_t>(n), o_fa = L.add<uint32_t>(n), o_fb = L.add<uint32_t>(n),
+               o_off = L.add<double>(3 * (size_t)n), o_acc = L.add<unsigned long long>(6 * (size_t)n),
+               o_cnt = L.add<uint32_t>(n), o_misc = L.add<uint32_t>(8), o_tmp = L.add<uint32_t>(scan_words);
+  char* base = analysis_scratch(b, L.used, 0);
+  auto at = [base](size_t o) { return reinterpret_cast<uint32_t*>(base + o); };
+  uint8_t* elig = reinterpret_cast<uint8_t*>(base + o_elig);
+  uint32_t *cell = at(o_cell), *ccount = at(o_ccount), *cstart = at(o_cstart), *ccur = at(o_ccur), *csorted = at(o_csorted),
+           *ecnt = at(o_ecnt), *estart = at(o_estart), *enext = at(o_enext), *deg = at(o_deg), *astart = at(o_astart),
+           *acur = at(o_acur), *parent = at(o_parent), *root = at(o_root), *level = at(o_level), *cand = at(o_cand),
+           *fa = at(o_fa), *fb = at(o_fb), *cnt = at(o_cnt), *misc = at(o_misc), *tmp = at(o_tmp);
+  double* off = reinterpret_cast<double*>(base + o_off);
+  unsigned long long* acc = reinterpret_cast<unsigned long long*>(base + o_acc);
+  SOUP_CUDA_TRY(cudaMemsetAsync(misc, 0, 32, st));
+
+  // ---- the rigid edges ----
+  uint64_t ne64 = n_edges_host;
+  uint32_t* edges = nullptr;
+  if (edges_host) {
+    if (ne64 >= 0x7FFFFFFFull) { err = "scaleMoleculesRigid: too many edges"; return SOUP_E_ARG; }
+    edges = reinterpret_cast<uint32_t*>(analysis_scratch(b, 8 * std::max<uint64_t>(ne64, 1) * 2, 1));
+    if (ne64) SOUP_CUDA_TRY(cudaMemcpyAsync(edges, edges_host, 8 * ne64, cudaMemcpyHostToDevice, st));
+  } else {
+    k_bs_bond_count<<<nblocks(n), kBlock, 0, st>>>(slots_o, n, ecnt);
+    b.launches += 1;
+    if (prox) {
+      if (eligible_host) SOUP_CUDA_TRY(cudaMemcpyAsync(elig, eligible_host, n, cudaMemcpyHostToDevice, st));
+      else SOUP_CUDA_TRY(cudaMemsetAsync(elig, 1, n, st));
+      SOUP_CUDA_TRY(cudaMemsetAsync(ccount, 0, 4 * ((size_t)ncell + 1), st));
+      SOUP_CUDA_TRY(cudaMemsetAsync(ccur, 0, 4 * ((size_t)ncell + 1), st));
+      k_bs_bin<<<nblocks(n), kBlock, 0, st>>>(pos_o, elig, n, pg, cell, ccount);
+      exclusive_scan(ccount, cstart, ncell, tmp, st);
+      k_bs_cell_scatter<<<nblocks(n), kBlock, 0, st>>>(cell, n, cstart, ccur, csorted);
+      k_bs_prox<false><<<nblocks(n), kBlock, 0, st>>>(pos_o, cell, n, pg, cstart, csorted, cohesion * cohesion, ecnt,
+                                                      nullptr, nullptr);
+      b.launches += 4;
+    }
+    exclusive_scan(ecnt, estart, n, tmp, st);
+    uint32_t total = 0;
+    SOUP_CUDA_TRY(cudaMemcpyAsync(&total, estart + n, 4, cudaMemcpyDeviceToHost, st));
+    SOUP_CUDA_TRY(cudaStreamSynchronize(st));
+    ne64 = total;
+    edges = reinterpret_cast<uint32_t*>(analysis_scratch(b, 8 * std::max<uint64_t>(ne64, 1) * 2, 1));
+    k_bs_bond_fill<<<nblocks(n), kBlock, 0, st>>>(slots_o, n, estart, enext, edges);
+    b.launches += 1;
+    if (prox) {
+      k_bs_prox<true><<<nblocks(n), kBlock, 0, st>>>(pos_o, cell, n, pg, cstart, csorted, cohesion * cohesion, nullptr,
+                                                     enext, edges);
+      b.launches += 1;
+    }
+  }
+  const uint32_t ne = (uint32_t)ne64;
+  uint32_t* adj = edges + 2 * (size_t)std::max<uint32_t>(ne, 1);
+
+  // ---- adjacency and components ----
+  SOUP_CUDA_TRY(cudaMemsetAsync(deg, 0, 4 * ((size_t)n + 1), st));
+  SOUP_CUDA_TRY(cudaMemsetAsync(acur, 0, 4 * (size_t)n, st));
+  SOUP_CUDA_TRY(cudaMemsetAsync(acc, 0, 48 * (size_t)n, st));
+  SOUP_CUDA_TRY(cudaMemsetAsync(cnt, 0, 4 * (size_t)n, st));
+  k_iota<<<nblocks(n), kBlock, 0, st>>>(parent, n);
+  b.launches += 1;
+  if (ne) {
+    k_bs_degree<<<nblocks(ne), kBlock, 0, st>>>(edges, ne, n, deg, misc + 4);
+    exclusive_scan(deg, astart, n, tmp, st);
+    k_bs_adjacency<<<nblocks(ne), kBlock, 0, st>>>(edges, ne, n, astart, acur, adj);
+    k_bs_union<<<nblocks(ne), kBlock, 0, st>>>(edges, ne, n, parent);
+    b.launches += 3;
+  } else {
+    SOUP_CUDA_TRY(cudaMemsetAsync(astart, 0, 4 * ((size_t)n + 1), st));
+  }
+  k_bs_roots<<<nblocks(n), kBlock, 0, st>>>(parent, n, level, cand, off, fa, misc);
+  k_bs_root_store<<<nblocks(n), kBlock, 0, st>>>(parent, n, root);
+  b.launches += 2;
+  uint32_t h[2] = {0, 0};
+  SOUP_CUDA_TRY(cudaMemcpyAsync(h, misc + 4, 4, cudaMemcpyDeviceToHost, st));
+  SOUP_CUDA_TRY(cudaMemcpyAsync(h + 1, misc, 4, cudaMemcpyDeviceToHost, st));
+  SOUP_CUDA_TRY(cudaStreamSynchronize(st));
+  if (h[0]) { err = "scaleMoleculesRigid: an edge names a particle outside the system"; return SOUP_E_ARG; }
+
+  // ---- breadth-first walk, one level per launch pair ----
+  Grid ob{}, nb{};
+  for (int a = 0; a < 3; ++a) { ob.box[a] = old_box[a]; nb.box[a] = new_box[a]; }
+  uint32_t* front = fa; uint32_t* next = fb;
+  uint32_t* nfront = misc; uint32_t* nnext = misc + 1;
+  uint32_t level_size = h[1];
+  for (uint32_t lev = 1; level_size > 0 && ne; ++lev) {
+    if (lev > n) { err = "scaleMoleculesRigid: the walk did not finish"; return SOUP_E_STATE; }
+    SOUP_CUDA_TRY(cudaMemsetAsync(nnext, 0, 4, st));
+    k_bs_claim<<<nblocks(level_size), kBlock, 0, st>>>(front, nfront, astart, adj, level, cand, next, nnext);
+    k_bs_settle<<<std::min(nblocks(n), 148u * 8u), kBlock, 0, st>>>(next, nnext, lev, pos_o, cand, ob, level, off);
+    b.launches += 2;
+    SOUP_CUDA_TRY(cudaMemcpyAsync(&level_size, nnext, 4, cudaMemcpyDeviceToHost, st));
+    SOUP_CUDA_TRY(cudaStreamSynchronize(st));
+    std::swap(front, next);
+    std::swap(nfront, nnext);
+  }
+
+  // ---- centres, positions, self-check ----
+  k_bs_accumulate<<<nblocks(n), kBlock, 0, st>>>(root, off, n, acc, cnt, misc + 4);
+  k_bs_place<<<nblocks(n), kBlock, 0, st>>>(pos_o, root, off, acc, cnt, n, ob, nb, new_box[0] / old_box[0],
+                                            new_box[1] / old_box[1], new_box[2] / old_box[2], out_o);
+  const uint32_t none = kUnset;
+  SOUP_CUDA_TRY(cudaMemcpyAsync(misc + 5, &none, 4, cudaMemcpyHostToDevice, st));
+  b.launches += 2;
+  if (ne && check) {
+    k_bs_check<<<nblocks(ne), kBlock, 0, st>>>(edges, ne, pos_o, out_o, ob, nb, misc + 5);
+    b.launches += 1;
+  }
+  uint32_t res[2];
+  SOUP_CUDA_TRY(cudaMemcpyAsync(res, misc + 4, 8, cudaMemcpyDeviceToHost, st));
+  SOUP_CUDA_TRY(cudaStreamSynchronize(st));
+  SOUP_CUDA_TRY(cudaGetLastError());
+  if (res[0] == 2) { err = "scaleMoleculesRigid: a rigid unit extends beyond 262144 sigma from its first bead"; return SOUP_E_STATE; }
+  if (res[1] != kUnset) {
+    uint32_t e[2];
+    float4 p0[2], p1[2];
+    SOUP_CUDA_TRY(cudaMemcpy(e, edges + 2 * (size_t)res[1], 8, cudaMemcpyDeviceToHost));
+    for (int q = 0; q < 2; ++q) {
+      SOUP_CUDA_TRY(cudaMemcpy(&p0[q], pos_o + e[q], 16, cudaMemcpyDeviceToHost));
+      SOUP_CUDA_TRY(cudaMemcpy(&p1[q], out_o + e[q], 16, cudaMemcpyDeviceToHost));
+    }
+    auto dist = [](const float4& a, const float4& c, const double* L) {
+      auto m = [](double d, double l) { double x = d / l, r = std::floor(x); r = (x - r >= 0.5) ? r + 1 : r; return d - r * l; };
+      const double dx = m((double)a.x - c.x, L[0]), dy = m((double)a.y - c.y, L[1]), dz = m((double)a.z - c.z, L[2]);
+      return std::sqrt(dx * dx + dy * dy + dz * dz);
+    };
+    char m[400];
+    std::snprintf(m, sizeof m,
+                  "applyBoxScale: an intramolecular distance changed (%.6f -> %.6f) for bond %u-%u at box [%g,%g,%g] -> "
+                  "[%g,%g,%g] -- scaleMoleculesRigid is broken",
+                  dist(p0[0], p0[1], old_box), dist(p1[0], p1[1], new_box), e[0], e[1], old_box[0], old_box[1],
+                  old_box[2], new_box[0], new_box[1], new_box[2]);
+    err = m;
+    return SOUP_E_STATE;
+  }
   return SOUP_OK;
 }
 

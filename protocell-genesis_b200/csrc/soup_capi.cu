@@ -333,6 +333,10 @@ Batch* make_batch(const SoupConfig* cfgs, const SoupInitState* inits, uint32_t R
   b.N = (uint32_t)N;
   b.list_cap = (b.list_cap + 7u) & ~7u;
   b.prot_rng.assign(R, 0);
+  for (uint32_t r = 0; r < R; ++r) {
+    b.wall_r0.push_back(b.cfg[r].wall_radius);
+    b.wall_box0.push_back(b.cfg[r].box[0]);
+  }
   b.step.assign(R, 0);
   b.next_sweep.assign(R, UINT64_MAX);
   SOUP_CUDA_TRY(cudaStreamCreateWithFlags(&b.stream, cudaStreamNonBlocking));
@@ -443,7 +447,8 @@ void destroy_batch(Batch* b) {
                   b->cell_cursor, b->perm, b->scan_tmp, b->nl, b->nl_cnt, b->heads, b->head_sys, b->es_nl,
                   b->es_cnt, b->head_slot, b->head_e, b->head_pos, b->head_xq, b->head_d, b->head_flag, b->draw_site, b->sweep_band, b->hcell_count, b->hcell_start, b->hcell_cursor, b->hsorted, b->hcell_of, b->flags,
                   b->events, b->desorb, b->drift_bits, b->bond_items, b->bond_nitems, b->uf_parent, b->comp_min,
-                  b->item_done, b->has_item, b->sweep_out, b->prot_rng_dev, b->sp, b->shared, b->sysid, b->an_buf};
+                  b->item_done, b->has_item, b->sweep_out, b->prot_rng_dev, b->sp, b->shared, b->sysid, b->an_buf[0],
+                  b->an_buf[1]};
   for (void* p : ptrs) if (p) cudaFree(p);
   for (void* p : {(void*)b->diff.frames, (void*)b->diff.A, (void*)b->diff.B, (void*)b->diff.g, (void*)b->diff.jg,
                   (void*)b->diff.frozen_o, (void*)b->diff.partial, (void*)b->diff.all})
@@ -1225,20 +1230,98 @@ int soup_write_state(SoupHandle* h, const SoupInitState* st) {
   });
 }
 
+// resizeSoupGrid (soup/src/soup-buffers.ts:530-560): replica r's live box, its grid and the wall
+// radius that follows it (liveRadius, soup/src/soup-confine.ts:76-78), then the rebuild and force pass
+void apply_box(Batch& b, uint32_t r, const double box[3]) {
+  for (int a = 0; a < 3; ++a) if (!(box[a] > 0)) fail(SOUP_E_GEOMETRY, "box sides must be positive");
+  for (int a = 0; a < 3; ++a) b.cfg[r].box[a] = box[a];
+  if (b.wall_r0[r] > 0) b.cfg[r].wall_radius = b.wall_r0[r] * (box[0] / b.wall_box0[r]);
+  const SysParams old = b.hsp[r];
+  SysParams p = make_sys(b.cfg[r]);
+  p.slot_off = old.slot_off; p.n = old.n; p.head_off = old.head_off; p.nheads = old.nheads;
+  b.hsp[r] = p;
+  drop_graphs(b);
+  alloc_grids(b);
+  upload_params(b);
+  force_pass(b);
+  SOUP_CUDA_TRY(cudaStreamSynchronize(b.stream));
+}
+
 int soup_set_box(SoupHandle* h, const double box[3]) {
   return guarded(h, [&](Batch& b, uint32_t r) {
     if (!box) fail(SOUP_E_ARG, "NULL box");
-    for (int a = 0; a < 3; ++a) if (!(box[a] > 0)) fail(SOUP_E_GEOMETRY, "box sides must be positive");
-    for (int a = 0; a < 3; ++a) b.cfg[r].box[a] = box[a];
-    const SysParams old = b.hsp[r];
-    SysParams p = make_sys(b.cfg[r]);
-    p.slot_off = old.slot_off; p.n = old.n; p.head_off = old.head_off; p.nheads = old.nheads;
-    b.hsp[r] = p;
-    drop_graphs(b);
-    alloc_grids(b);
-    upload_params(b);
-    force_pass(b);
+    apply_box(b, r, box);
+  });
+}
+
+__global__ void k_place_replica(const float4* __restrict__ src, const uint32_t* __restrict__ slot_of, uint32_t off,
+                                uint32_t n, float4* __restrict__ pos) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) pos[slot_of[off + i]] = src[i];
+}
+
+int soup_scale_box(SoupHandle* h, const double target_box[3], double cohesion_cutoff, const uint32_t* cohesion_members,
+                   uint32_t n_members) {
+  return guarded(h, [&](Batch& b, uint32_t r) {
+    if (!target_box) fail(SOUP_E_ARG, "NULL box");
+    for (int a = 0; a < 3; ++a) if (!(target_box[a] > 0)) fail(SOUP_E_GEOMETRY, "box sides must be positive");
+    if (!(cohesion_cutoff >= 0)) fail(SOUP_E_ARG, "scaleBoxTo: the cohesion cutoff must be a non-negative number");
+    const uint32_t n = b.cfg[r].n, off = b.hsp[r].slot_off;
+    std::vector<uint8_t> fr(n);
+    if (n) SOUP_CUDA_TRY(cudaMemcpyAsync(fr.data(), b.frozen + off, n, cudaMemcpyDeviceToHost, b.stream));
     SOUP_CUDA_TRY(cudaStreamSynchronize(b.stream));
+    size_t nfrozen = 0;
+    for (uint8_t f : fr) nfrozen += f ? 1 : 0;
+    if (nfrozen)
+      fail(SOUP_E_STATE, "changing the box is impossible on a system with a mineral sheet: " + std::to_string(nfrozen) +
+                             " immobile beads (areaMove/scaleBoxTo/dryWetCycle require CreateSoupOpts.clay=false, see "
+                             "data/soup.json clay.basis §7)");
+    std::vector<uint8_t> elig;
+    if (cohesion_cutoff > 0 && cohesion_members) {
+      elig.assign(n, 0);
+      for (uint32_t k = 0; k < n_members; ++k) {
+        if (cohesion_members[k] >= n) fail(SOUP_E_ARG, "scaleBoxTo: a cohesion member index is out of range");
+        elig[cohesion_members[k]] = 1;
+      }
+    }
+    // original-order positions and bond partners into the re-sort's second buffers (free outside a
+    // rebuild); the new positions go to force2
+    CkptArrays a{b.pos, b.vel, b.slots, b.center, b.held, b.brng, b.trng, b.charge,
+                 b.pos2, b.vel2, b.slots2, b.center2, b.held2, b.brng2, b.trng2, b.charge2};
+    if (n) k_checkpoint_gather<<<(n + 255) / 256, 256, 0, b.stream>>>(a, b.id, off, n);
+    SOUP_CUDA_TRY(cudaGetLastError());
+    const double* old_box = b.cfg[r].box;
+    std::string err;
+    const int st = run_rigid_map(b, b.pos2, b.slots2, n, nullptr, 0, cohesion_cutoff, elig.empty() ? nullptr : elig.data(),
+                                 old_box, target_box, b.force2, true, err);
+    if (st) fail(st, err);
+    if (n) k_place_replica<<<(n + 255) / 256, 256, 0, b.stream>>>(b.force2, b.slot_of, off, n, b.pos);
+    SOUP_CUDA_TRY(cudaGetLastError());
+    b.launches += 2;
+    const double nb[3] = {target_box[0], target_box[1], target_box[2]};
+    apply_box(b, r, nb);
+    guards(b, b.step[r]);
+  });
+}
+
+int soup_scale_molecules_rigid(SoupHandle* h, const float* positions, uint32_t n, const uint32_t* edges,
+                               uint32_t n_edges, const double old_box[3], const double new_box[3], float* out) {
+  return guarded(h, [&](Batch& b, uint32_t) {
+    if ((n && (!positions || !out)) || (n_edges && !edges) || !old_box || !new_box) fail(SOUP_E_ARG, "NULL argument");
+    for (int a = 0; a < 3; ++a)
+      if (!(old_box[a] > 0 && new_box[a] > 0)) fail(SOUP_E_GEOMETRY, "box sides must be positive");
+    if (n == 0) return;
+    float4 *dp = nullptr, *dout = nullptr;
+    SOUP_CUDA_TRY(cudaMallocAsync(&dp, 16 * (size_t)n, b.stream));
+    SOUP_CUDA_TRY(cudaMallocAsync(&dout, 16 * (size_t)n, b.stream));
+    SOUP_CUDA_TRY(cudaMemcpyAsync(dp, positions, 16 * (size_t)n, cudaMemcpyHostToDevice, b.stream));
+    std::string err;
+    const int st = run_rigid_map(b, dp, nullptr, n, edges, n_edges, 0.0, nullptr, old_box, new_box, dout, false, err);
+    if (st == SOUP_OK) SOUP_CUDA_TRY(cudaMemcpyAsync(out, dout, 16 * (size_t)n, cudaMemcpyDeviceToHost, b.stream));
+    cudaFreeAsync(dp, b.stream);
+    cudaFreeAsync(dout, b.stream);
+    SOUP_CUDA_TRY(cudaStreamSynchronize(b.stream));
+    if (st) fail(st, err);
   });
 }
 

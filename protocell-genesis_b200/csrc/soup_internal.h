@@ -136,8 +136,10 @@ struct Batch {
   // analysis scratch: one buffer that grows to the largest request of the analysis calls and is
   // reused after that (analysis_scratch), so a call makes no cudaMalloc / cudaFree once its sizes
   // have been seen
-  char* an_buf = nullptr;
-  size_t an_cap = 0;
+  std::vector<double> wall_r0, wall_box0;   // per replica: the wall radius at creation and the box x it
+                                            // belongs to (the live radius scales with the box)
+  char* an_buf[2] = {nullptr, nullptr};   // [1]: a second buffer for sizes known only mid-call
+  size_t an_cap[2] = {0, 0};
 
   // host-side schedule
   std::vector<uint64_t> step;        // per replica global step
@@ -237,7 +239,17 @@ struct ScratchLayout {
     return at;
   }
 };
-char* analysis_scratch(Batch& b, size_t bytes);
+char* analysis_scratch(Batch& b, size_t bytes, int which = 0);
+// scaleMoleculesRigid (soup/src/soup-box-scale-math.ts:63-138) on the device over original-order
+// arrays: n positions pos_o (device), the rigid edges as flat (i, j) pairs (edges_host on the host, or
+// NULL with bond partners slots_o (device, u32 x3, NONE = empty) and, when cohesion > 0, the
+// proximity pairs within `cohesion` among the beads eligible_host marks (NULL: all)).  Writes out_o
+// (device).  With `check`, an edge whose minimum-image length moved by more than 1e-3 makes it return
+// SOUP_E_STATE with the reference's message in err (applyBoxScaleOnce's self-check), and out_o is not
+// to be used.
+int run_rigid_map(Batch& b, const float4* pos_o, const uint32_t* slots_o, uint32_t n, const uint32_t* edges_host,
+                  uint64_t n_edges_host, double cohesion, const uint8_t* eligible_host, const double old_box[3],
+                  const double new_box[3], float4* out_o, bool check, std::string& err);
 int run_profile_z(Batch& b, uint32_t r, uint32_t bins, uint32_t head_mask, uint32_t* head, uint32_t* tail,
                   uint32_t* escaped, std::string& err);
 int run_pairing(Batch& b, uint32_t r, double contact, uint32_t out5[5], std::string& err);

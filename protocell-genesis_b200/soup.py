@@ -5,6 +5,7 @@ particle order.  Method names follow the reference (camelCase aliases are provid
 soup/cli/campaign.ts and verify/ use).
 """
 import ctypes as C
+import math
 from typing import Dict, Optional
 
 import numpy as np
@@ -251,6 +252,49 @@ class SoupSystem:
         b = (C.c_double * 3)(*[float(x) for x in box])
         _check(self._lib, self._h, self._lib.soup_set_box(self._h, b))
 
+    def scale_box_once(self, target_box, cohesion=None):
+        """applyBoxScaleOnce (soup/src/soup-box-scale.ts:81-165) on the device: every rigid unit keeps its
+        shape while its centre of mass scales with the box.  cohesion: {"cutoff": c, "memberIndices":
+        optional indices} also holds beads within c of each other together (the reference's option)."""
+        b = (C.c_double * 3)(*[float(x) for x in target_box])
+        cut, mem = 0.0, None
+        if cohesion is not None:
+            cut = float(cohesion["cutoff"])
+            if cohesion.get("memberIndices") is not None:
+                mem = np.ascontiguousarray(cohesion["memberIndices"], np.uint32)
+        _check(self._lib, self._h, self._lib.soup_scale_box(
+            self._h, b, cut, mem.ctypes.data_as(_abi._U32P) if mem is not None else None,
+            0 if mem is None else mem.size))
+
+    def scale_box_to(self, target_box, ramp_steps: int, ramp_relax_steps: int, cohesion=None):
+        """scaleBoxTo (soup/src/soup-box-scale.ts:218-275): `ramp_steps` log-linear box increments, each
+        a scale_box_once, with `ramp_relax_steps` steps of dynamics between them (none after the last)."""
+        for box in _box_ramp(self.box, target_box, ramp_steps):
+            self.scale_box_once(box[0], cohesion)
+            if not box[1] and ramp_relax_steps > 0:
+                self.step(ramp_relax_steps)
+
+    def grow_box_to(self, target_box, ramp_steps: int, ramp_relax_steps: int):
+        """growBoxTo (soup/src/soup-box-scale.ts:318-360): the same ramp, moving no particle: only the
+        live box, the grid and the lists change.  The force is recomputed at each new box (the
+        reference keeps the previous force for the next half-kick)."""
+        for box in _box_ramp(self.box, target_box, ramp_steps):
+            self.set_box(box[0])
+            if not box[1] and ramp_relax_steps > 0:
+                self.step(ramp_relax_steps)
+
+    def scale_molecules_rigid(self, positions, edges, old_box, new_box):
+        """scaleMoleculesRigid (soup/src/soup-box-scale-math.ts:63-138) on this system's device over
+        caller arrays: positions f32 x4, edges flat (i, j) pairs; returns the positions in new_box."""
+        pos = np.ascontiguousarray(positions, np.float32)
+        e = np.ascontiguousarray(edges, np.uint32)
+        out = np.empty_like(pos)
+        ob = (C.c_double * 3)(*[float(x) for x in old_box])
+        nb = (C.c_double * 3)(*[float(x) for x in new_box])
+        _check(self._lib, self._h, self._lib.soup_scale_molecules_rigid(
+            self._h, _ptr(pos), pos.size // 4, e.ctypes.data_as(_abi._U32P), e.size // 2, ob, nb, _ptr(out)))
+        return out
+
     def prepare_graphs(self):
         """Capture the step graphs of the current schedule now (soup_step captures them on first use)."""
         _check(self._lib, self._h, self._lib.soup_prepare_graphs(self._h))
@@ -381,6 +425,8 @@ class SoupSystem:
         return int(nc.value), labels
 
     # reference-style aliases
+    scaleBoxTo = scale_box_to
+    growBoxTo = grow_box_to
     forcesBruteForce = forces_brute_force
     forcesNoRebuildDEBUG = forces_no_rebuild
     bondSlots = bond_slots
@@ -390,6 +436,19 @@ class SoupSystem:
     desorbEvents = desorb_events
     nonFiniteCount = nonfinite_count
     protonationRngState = protonation_rng_state
+
+
+def _box_ramp(from_box, target_box, ramp_steps: int):
+    """applyBoxScale's increments (soup/src/soup-box-scale.ts:228-250): from_box * exp(ln(target /
+    from) * s / ramp_steps) for s = 1 .. ramp_steps, the last exactly target; (box, is_last) pairs."""
+    fb = [float(x) for x in from_box]
+    tb = [float(x) for x in target_box]
+    ln = [math.log(tb[a] / fb[a]) for a in range(3)]
+    out = []
+    for s in range(1, int(ramp_steps) + 1):
+        last = s == ramp_steps
+        out.append((tb if last else [fb[a] * math.exp((ln[a] * s) / ramp_steps) for a in range(3)], last))
+    return out
 
 
 def _autotune(lib, h, steps):

@@ -66,6 +66,9 @@ def lib(abi):
         "oracle_density_profile_z": (C.c_int, [P, C.c_uint32, C.c_double, C.c_uint32, C.c_uint32, P, P, P]),
         "oracle_aggregate_shape": (C.c_int, [P, P, C.c_uint32, P, P]),
         "oracle_relax": (C.c_int, [P, C.c_uint32, C.c_double]),
+        "oracle_scale_molecules_rigid": (C.c_int, [P, C.c_uint32, P, C.c_uint32, P, P, P]),
+        "oracle_proximity_pairs": (C.c_int, [P, C.c_uint32, P, C.c_double, P, P, C.c_size_t,
+                                             C.POINTER(C.c_size_t)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -306,3 +309,32 @@ def aggregate_shape(abi, pos, members, box):
     out = np.zeros(10, np.float64)
     L.oracle_aggregate_shape(_ptr(pos), _ptr(members), len(members), _ptr(box), _ptr(out))
     return int(out[0]), out[1:4].copy(), out[4:10].copy()
+
+
+def scale_molecules_rigid(abi, pos, edges, old_box, new_box):
+    """scaleMoleculesRigid from the oracle: positions (f32 x4) in the new box; `edges` flat (i, j) pairs."""
+    L = lib(abi)
+    pos = np.ascontiguousarray(pos, np.float32)
+    edges = np.ascontiguousarray(edges, np.uint32)
+    out = np.zeros_like(pos)
+    ob_ = np.ascontiguousarray(old_box, np.float64)
+    nb_ = np.ascontiguousarray(new_box, np.float64)
+    st = L.oracle_scale_molecules_rigid(_ptr(pos), pos.size // 4, _ptr(edges), edges.size // 2, _ptr(ob_), _ptr(nb_),
+                                        _ptr(out))
+    if st != 0:
+        raise RuntimeError(L.oracle_last_error().decode())
+    return out
+
+
+def proximity_pairs(abi, pos, box, cutoff, eligible=None):
+    """proximityPairs from the oracle: flat (i, j) pairs, i < j, in the reference's visiting order."""
+    L = lib(abi)
+    pos = np.ascontiguousarray(pos, np.float32)
+    n = pos.size // 4
+    el = np.ones(n, np.uint8) if eligible is None else np.ascontiguousarray(eligible, np.uint8)
+    b = np.ascontiguousarray(box, np.float64)
+    cnt = C.c_size_t(0)
+    L.oracle_proximity_pairs(_ptr(pos), n, _ptr(b), float(cutoff), _ptr(el), None, 0, C.byref(cnt))
+    out = np.zeros(2 * max(cnt.value, 1), np.uint32)
+    L.oracle_proximity_pairs(_ptr(pos), n, _ptr(b), float(cutoff), _ptr(el), _ptr(out), cnt.value, C.byref(cnt))
+    return out[: 2 * cnt.value]
