@@ -361,6 +361,18 @@ typedef struct SoupAggregateShape {
 int soup_aggregate_shapes(SoupHandle* h, const uint32_t* member_idx, const uint32_t* labels, uint32_t n_members,
                           uint32_t max_shapes, SoupAggregateShape* out, uint32_t* n_components);
 
+/* unwrapAggregate (engine/src/aggregate.ts:245-262) of one aggregate: its members (original
+ * indices, the first one the reference) unwrapped on all three periodic axes, f32 x4 with w = kind,
+ * in the given order.  The frame shapeOfAggregate's head-shell profiles are measured in
+ * (soup/src/aggregates.ts:387-476). */
+int soup_aggregate_unwrap(SoupHandle* h, const uint32_t* members, uint32_t n_members, float* out);
+/* localCavityVolume (soup/src/aggregates.ts:350-385) on h's device: the vacuum cavity enclosed by n
+ * unwrapped positions (f32 x4) on a local grid of side `cell` around them (padded by 4 * radius),
+ * cells within `radius` of a bead occupied (engine/src/closure.ts:67-107 occupancy), the empty cells
+ * the open-boundary flood from the grid's faces does not reach (closure.ts:108-163), times cell^3. */
+int soup_local_cavity_volume(SoupHandle* h, const float* positions, uint32_t n, double cell, double radius,
+                             double* volume);
+
 /* densityProfileZ (engine/src/metrics.ts:21-47): histogram of the beads' z over [0, box_z) in
  * `bins` bins, split into heads (kinds whose bit is set in head_kind_mask) and tails (the rest).
  * The soup profiles polar kinds as heads (soup/src/aggregates.ts:95-109); the engine's own

@@ -1663,6 +1663,86 @@ int oracle_scale_molecules_rigid(const float* pos, uint32_t n, const uint32_t* e
   return SOUP_OK;
 }
 
+// unwrapAggregate (engine/src/aggregate.ts:245-262) on all three axes about members[0]; f32 out, w = kind
+int oracle_unwrap_aggregate(const float* pos, const uint32_t* members, uint32_t m, const double box[3], float* out) {
+  if (m == 0) return SOUP_OK;
+  const float* r = pos + 4 * (size_t)members[0];
+  for (uint32_t k = 0; k < m; ++k) {
+    const float* p = pos + 4 * (size_t)members[k];
+    for (int a = 0; a < 3; ++a) out[4 * (size_t)k + a] = (float)((double)r[a] + mi1((double)p[a] - (double)r[a], box[a]));
+    out[4 * (size_t)k + 3] = p[3];
+  }
+  return SOUP_OK;
+}
+
+// localCavityVolume (soup/src/aggregates.ts:350-385) over occupancy (engine/src/closure.ts:67-107: x
+// and y wrap, z open) and enclosedVolume/floodOutside (closure.ts:108-163: breadth-first from every
+// empty cell on the six faces, open boundary); unreached empty cells times cell^3
+double oracle_local_cavity_volume(const float* positions, uint32_t n, double cell, double radius) {
+  if (n == 0) return 0.0;
+  double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for (uint32_t i = 0; i < n; ++i)
+    for (int a = 0; a < 3; ++a) {
+      const double v = positions[4 * (size_t)i + a];
+      if (v < lo[a]) lo[a] = v;
+      if (v > hi[a]) hi[a] = v;
+    }
+  const double pad = radius * 4;
+  double box[3];
+  int dims[3];
+  std::vector<float> sh(4 * (size_t)n);
+  for (int a = 0; a < 3; ++a) {
+    box[a] = hi[a] - lo[a] + 2 * pad;
+    dims[a] = std::max(1, (int)std::ceil(box[a] / cell));
+  }
+  for (uint32_t i = 0; i < n; ++i)
+    for (int a = 0; a < 3; ++a) sh[4 * (size_t)i + a] = (float)((double)positions[4 * (size_t)i + a] + (pad - lo[a]));
+  const int nx = dims[0], ny = dims[1], nz = dims[2];
+  const size_t nc = (size_t)nx * ny * nz;
+  std::vector<uint8_t> occ(nc, 0), vis(nc, 0);
+  const int reach = std::max(1, (int)std::ceil(radius / cell));
+  const double r2 = radius * radius;
+  for (uint32_t i = 0; i < n; ++i) {
+    const double px = sh[4 * (size_t)i], py = sh[4 * (size_t)i + 1], pz = sh[4 * (size_t)i + 2];
+    const int cx = (int)std::floor(px / cell), cy = (int)std::floor(py / cell), cz = (int)std::floor(pz / cell);
+    for (int dz = -reach; dz <= reach; ++dz) {
+      const int gz = cz + dz;
+      if (gz < 0 || gz >= nz) continue;
+      const double ddz = (gz + 0.5) * cell - pz;
+      for (int dy = -reach; dy <= reach; ++dy) {
+        const int gy = ((cy + dy) % ny + ny) % ny;
+        double ddy = (gy + 0.5) * cell - py;
+        ddy -= js_round(ddy / box[1]) * box[1];
+        for (int dx = -reach; dx <= reach; ++dx) {
+          const int gx = ((cx + dx) % nx + nx) % nx;
+          double ddx = (gx + 0.5) * cell - px;
+          ddx -= js_round(ddx / box[0]) * box[0];
+          if (ddx * ddx + ddy * ddy + ddz * ddz <= r2) occ[gx + (size_t)nx * (gy + (size_t)ny * gz)] = 1;
+        }
+      }
+    }
+  }
+  std::vector<size_t> queue;
+  auto seed = [&](int x, int y, int z) {
+    if (x < 0 || x >= nx || y < 0 || y >= ny || z < 0 || z >= nz) return;
+    const size_t i = x + (size_t)nx * (y + (size_t)ny * z);
+    if (!occ[i] && !vis[i]) { vis[i] = 1; queue.push_back(i); }
+  };
+  for (int y = 0; y < ny; ++y) for (int z = 0; z < nz; ++z) { seed(0, y, z); seed(nx - 1, y, z); }
+  for (int x = 0; x < nx; ++x) for (int z = 0; z < nz; ++z) { seed(x, 0, z); seed(x, ny - 1, z); }
+  for (int x = 0; x < nx; ++x) for (int y = 0; y < ny; ++y) { seed(x, y, 0); seed(x, y, nz - 1); }
+  for (size_t h = 0; h < queue.size(); ++h) {
+    const size_t i = queue[h];
+    const int z = (int)(i / ((size_t)nx * ny));
+    const size_t rem = i - (size_t)z * nx * ny;
+    const int y = (int)(rem / nx), x = (int)(rem - (size_t)y * nx);
+    seed(x + 1, y, z); seed(x - 1, y, z); seed(x, y + 1, z); seed(x, y - 1, z); seed(x, y, z + 1); seed(x, y, z - 1);
+  }
+  size_t unreached = 0;
+  for (size_t i = 0; i < nc; ++i) unreached += (!occ[i] && !vis[i]) ? 1 : 0;
+  return (double)unreached * cell * cell * cell;
+}
+
 // proximityPairs (soup/src/soup-box-scale-math.ts:162-221): pairs i < j among the eligible beads with
 // a minimum-image distance <= cutoff, from a cell list of floor(box / cutoff) cells per axis, every
 // axis periodic.  A pair is listed once per neighbouring-cell visit that reaches it, as the

@@ -9,6 +9,10 @@
 // Both reduce to integer counts (atomics on integers), so the results do not depend on the order the
 // threads finish in.  Distances for pairingStats are FP64 with JavaScript rounding of the minimum
 // image (mi(d, L) = d - Math.round(d / L) * L), as the reference computes them.
+#include <algorithm>
+#include <cmath>
+#include <vector>
+
 #include "soup_internal.h"
 
 namespace soup {
@@ -228,6 +232,179 @@ int run_shapes(Batch& b, uint32_t r, const uint32_t* members_csr, const uint32_t
   SOUP_CUDA_TRY(cudaGetLastError());
   SOUP_CUDA_TRY(cudaMemcpyAsync(out10, dout, 80 * (size_t)ncomp, cudaMemcpyDeviceToHost, b.stream));
   SOUP_CUDA_TRY(cudaStreamSynchronize(b.stream));
+  return SOUP_OK;
+}
+
+// ---- per-aggregate detail (soup/src/aggregates.ts:350-476 shapeOfAggregate) -------------------
+namespace {
+
+// JavaScript's d - Math.round(d / L) * L with every operation rounded on its own (no FMA contraction)
+__device__ __forceinline__ double mi_rn(double d, double L) { return __dsub_rn(d, __dmul_rn(js_round(__ddiv_rn(d, L)), L)); }
+
+// unwrapAggregate (engine/src/aggregate.ts:245-262) on all three axes about the first member, each
+// coordinate rounded to f32 as the reference stores it; w = kind
+__global__ void k_unwrap_members(const float4* __restrict__ pos, const uint32_t* __restrict__ slot_of, uint32_t off,
+                                 const uint32_t* __restrict__ members, uint32_t m, double bx, double by, double bz,
+                                 float4* __restrict__ out) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= m) return;
+  const float4 r0 = pos[slot_of[off + members[0]]], p = pos[slot_of[off + members[k]]];
+  const double ref[3] = {(double)r0.x, (double)r0.y, (double)r0.z}, v[3] = {(double)p.x, (double)p.y, (double)p.z};
+  const double L[3] = {bx, by, bz};
+  float u[3];
+  for (int a = 0; a < 3; ++a) u[a] = __double2float_rn(__dadd_rn(ref[a], mi_rn(__dsub_rn(v[a], ref[a]), L[a])));
+  out[k] = make_float4(u[0], u[1], u[2], p.w);
+}
+
+// occupancy (engine/src/closure.ts:67-107) of a local grid: x and y wrap, z is open
+struct LGrid {
+  int n[3];
+  double box[3], cell;
+};
+__global__ void k_local_occupancy(const float4* __restrict__ p, uint32_t n, LGrid g, int reach, double r2,
+                                  uint8_t* __restrict__ occ) {
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double px = (double)p[i].x, py = (double)p[i].y, pz = (double)p[i].z;
+  const int cx = (int)floor(__ddiv_rn(px, g.cell)), cy = (int)floor(__ddiv_rn(py, g.cell)),
+            cz = (int)floor(__ddiv_rn(pz, g.cell));
+  for (int dz = -reach; dz <= reach; ++dz) {
+    const int gz = cz + dz;
+    if (gz < 0 || gz >= g.n[2]) continue;
+    const double ddz = __dsub_rn(__dmul_rn(gz + 0.5, g.cell), pz);
+    for (int dy = -reach; dy <= reach; ++dy) {
+      const int gy = ((cy + dy) % g.n[1] + g.n[1]) % g.n[1];
+      const double ddy = mi_rn(__dsub_rn(__dmul_rn(gy + 0.5, g.cell), py), g.box[1]);
+      for (int dx = -reach; dx <= reach; ++dx) {
+        const int gx = ((cx + dx) % g.n[0] + g.n[0]) % g.n[0];
+        const double ddx = mi_rn(__dsub_rn(__dmul_rn(gx + 0.5, g.cell), px), g.box[0]);
+        if (__dadd_rn(__dadd_rn(__dmul_rn(ddx, ddx), __dmul_rn(ddy, ddy)), __dmul_rn(ddz, ddz)) <= r2)
+          occ[(size_t)gx + (size_t)g.n[0] * ((size_t)gy + (size_t)g.n[1] * gz)] = 1;
+      }
+    }
+  }
+}
+
+// floodOutside (engine/src/closure.ts:108-150): every empty cell connected to a face of the grid
+// through empty cells, 6-neighbour, open boundary.  One pass marks an empty cell whose neighbour
+// is marked (or that lies on a face); passes repeat until one marks nothing.  The marked set is the
+// reachable set whatever order the passes run in.
+__global__ void k_local_flood(const uint8_t* __restrict__ occ, uint8_t* __restrict__ vis, LGrid g, uint64_t nc,
+                              uint32_t* __restrict__ changed) {
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nc; i += (uint64_t)gridDim.x * blockDim.x) {
+    if (occ[i] || vis[i]) continue;
+    const int x = (int)(i % (uint64_t)g.n[0]);
+    const int y = (int)((i / (uint64_t)g.n[0]) % (uint64_t)g.n[1]);
+    const int z = (int)(i / ((uint64_t)g.n[0] * g.n[1]));
+    bool reach = x == 0 || y == 0 || z == 0 || x == g.n[0] - 1 || y == g.n[1] - 1 || z == g.n[2] - 1;
+    if (!reach) {
+      const uint64_t sx = 1, sy = (uint64_t)g.n[0], sz = (uint64_t)g.n[0] * g.n[1];
+      reach = vis[i - sx] || vis[i + sx] || vis[i - sy] || vis[i + sy] || vis[i - sz] || vis[i + sz];
+    }
+    if (reach) {
+      vis[i] = 1;
+      *changed = 1u;
+    }
+  }
+}
+
+__global__ void k_local_unreached(const uint8_t* __restrict__ occ, const uint8_t* __restrict__ vis, uint64_t nc,
+                                  unsigned long long* __restrict__ count) {
+  unsigned long long c = 0;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < nc; i += (uint64_t)gridDim.x * blockDim.x)
+    c += (!occ[i] && !vis[i]) ? 1ull : 0ull;
+  for (int o = 16; o > 0; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+  if ((threadIdx.x & 31) == 0 && c) atomicAdd(count, c);
+}
+
+}  // namespace
+
+int run_unwrap(Batch& b, uint32_t r, const uint32_t* members, uint32_t m, float* out, std::string& err) {
+  const SoupConfig& c = b.cfg[r];
+  for (uint32_t k = 0; k < m; ++k)
+    if (members[k] >= c.n) { err = "unwrapAggregate: member index out of range"; return SOUP_E_ARG; }
+  if (m == 0) return SOUP_OK;
+  ScratchLayout L;
+  const size_t o_m = L.add<uint32_t>(m), o_out = L.add<float4>(m);
+  char* base = analysis_scratch(b, L.used);
+  uint32_t* dm = reinterpret_cast<uint32_t*>(base + o_m);
+  float4* dout = reinterpret_cast<float4*>(base + o_out);
+  SOUP_CUDA_TRY(cudaMemcpyAsync(dm, members, 4 * (size_t)m, cudaMemcpyHostToDevice, b.stream));
+  k_unwrap_members<<<nblocks(m), kBlock, 0, b.stream>>>(b.pos, b.slot_of, b.hsp[r].slot_off, dm, m, c.box[0], c.box[1],
+                                                       c.box[2], dout);
+  b.launches += 1;
+  SOUP_CUDA_TRY(cudaGetLastError());
+  SOUP_CUDA_TRY(cudaMemcpyAsync(out, dout, 16 * (size_t)m, cudaMemcpyDeviceToHost, b.stream));
+  SOUP_CUDA_TRY(cudaStreamSynchronize(b.stream));
+  return SOUP_OK;
+}
+
+// localCavityVolume (soup/src/aggregates.ts:350-385): the bounding region of the unwrapped beads,
+// padded by 4 radii, shifted to start at the pad (f32 positions, as the reference's Float32Array),
+// its occupancy and the empty cells the open-boundary flood does not reach, times cell^3
+int run_local_cavity(Batch& b, const float* positions, uint32_t n, double cell, double radius, double* volume,
+                     std::string& err) {
+  *volume = 0.0;
+  if (n == 0) return SOUP_OK;
+  if (!(cell > 0) || !(radius >= 0)) { err = "localCavityVolume: cell must be positive and radius non-negative"; return SOUP_E_ARG; }
+  double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  for (uint32_t i = 0; i < n; ++i)
+    for (int a = 0; a < 3; ++a) {
+      const double v = positions[4 * (size_t)i + a];
+      lo[a] = std::min(lo[a], v);
+      hi[a] = std::max(hi[a], v);
+    }
+  const double pad = radius * 4;
+  LGrid g{};
+  g.cell = cell;
+  uint64_t nc = 1;
+  double shift[3];
+  for (int a = 0; a < 3; ++a) {
+    if (!std::isfinite(lo[a]) || !std::isfinite(hi[a])) { err = "localCavityVolume: non-finite position"; return SOUP_E_ARG; }
+    shift[a] = pad - lo[a];
+    g.box[a] = hi[a] - lo[a] + 2 * pad;
+    g.n[a] = std::max(1, (int)std::ceil(g.box[a] / cell));
+    nc *= (uint64_t)g.n[a];
+  }
+  if (nc > (uint64_t)1 << 31) { err = "localCavityVolume: the local grid is too large"; return SOUP_E_ARG; }
+  std::vector<float> sh(4 * (size_t)n);
+  for (uint32_t i = 0; i < n; ++i) {
+    for (int a = 0; a < 3; ++a) sh[4 * (size_t)i + a] = (float)((double)positions[4 * (size_t)i + a] + shift[a]);
+    sh[4 * (size_t)i + 3] = positions[4 * (size_t)i + 3];
+  }
+  ScratchLayout L;
+  const size_t o_p = L.add<float4>(n), o_occ = L.add<uint8_t>(nc), o_vis = L.add<uint8_t>(nc),
+               o_cnt = L.add<unsigned long long>(2);
+  char* base = analysis_scratch(b, L.used);
+  float4* dp = reinterpret_cast<float4*>(base + o_p);
+  uint8_t* occ = reinterpret_cast<uint8_t*>(base + o_occ);
+  uint8_t* vis = reinterpret_cast<uint8_t*>(base + o_vis);
+  unsigned long long* cnt = reinterpret_cast<unsigned long long*>(base + o_cnt);
+  uint32_t* changed = reinterpret_cast<uint32_t*>(cnt + 1);
+  cudaStream_t st = b.stream;
+  SOUP_CUDA_TRY(cudaMemcpyAsync(dp, sh.data(), 16 * (size_t)n, cudaMemcpyHostToDevice, st));
+  SOUP_CUDA_TRY(cudaMemsetAsync(occ, 0, nc, st));
+  SOUP_CUDA_TRY(cudaMemsetAsync(vis, 0, nc, st));
+  SOUP_CUDA_TRY(cudaMemsetAsync(cnt, 0, 16, st));
+  const int reach = std::max(1, (int)std::ceil(radius / cell));
+  k_local_occupancy<<<nblocks(n), kBlock, 0, st>>>(dp, n, g, reach, radius * radius, occ);
+  const unsigned fgrid = (unsigned)std::min<uint64_t>(nblocks(nc), 148ull * 16ull);
+  uint32_t ch = 1;
+  uint64_t passes = 0;
+  while (ch) {
+    if (++passes > nc + 1) { err = "localCavityVolume: the flood did not finish"; return SOUP_E_STATE; }
+    SOUP_CUDA_TRY(cudaMemsetAsync(changed, 0, 4, st));
+    k_local_flood<<<fgrid, kBlock, 0, st>>>(occ, vis, g, nc, changed);
+    SOUP_CUDA_TRY(cudaMemcpyAsync(&ch, changed, 4, cudaMemcpyDeviceToHost, st));
+    SOUP_CUDA_TRY(cudaStreamSynchronize(st));
+  }
+  k_local_unreached<<<fgrid, kBlock, 0, st>>>(occ, vis, nc, cnt);
+  b.launches += 2 + passes;
+  unsigned long long unreached = 0;
+  SOUP_CUDA_TRY(cudaMemcpyAsync(&unreached, cnt, 8, cudaMemcpyDeviceToHost, st));
+  SOUP_CUDA_TRY(cudaStreamSynchronize(st));
+  SOUP_CUDA_TRY(cudaGetLastError());
+  *volume = (double)unreached * cell * cell * cell;
   return SOUP_OK;
 }
 

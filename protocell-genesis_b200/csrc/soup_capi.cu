@@ -1693,6 +1693,25 @@ int soup_aggregate_shapes(SoupHandle* h, const uint32_t* member_idx, const uint3
   });
 }
 
+int soup_aggregate_unwrap(SoupHandle* h, const uint32_t* members, uint32_t n_members, float* out) {
+  return guarded(h, [&](Batch& b, uint32_t r) {
+    if (n_members && (!members || !out)) fail(SOUP_E_ARG, "aggregate unwrap: NULL argument");
+    std::string err;
+    const int st = run_unwrap(b, r, members, n_members, out, err);
+    if (st) fail(st, err);
+  });
+}
+
+int soup_local_cavity_volume(SoupHandle* h, const float* positions, uint32_t n, double cell, double radius,
+                             double* volume) {
+  return guarded(h, [&](Batch& b, uint32_t) {
+    if ((n && !positions) || !volume) fail(SOUP_E_ARG, "local cavity volume: NULL argument");
+    std::string err;
+    const int st = run_local_cavity(b, positions, n, cell, radius, volume, err);
+    if (st) fail(st, err);
+  });
+}
+
 int soup_density_profile_z(SoupHandle* h, uint32_t bins, uint32_t head_kind_mask, uint32_t* head_counts,
                            uint32_t* tail_counts, uint32_t* escaped) {
   return guarded(h, [&](Batch& b, uint32_t r) {

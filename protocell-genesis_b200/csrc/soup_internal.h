@@ -253,6 +253,9 @@ int run_rigid_map(Batch& b, const float4* pos_o, const uint32_t* slots_o, uint32
 int run_profile_z(Batch& b, uint32_t r, uint32_t bins, uint32_t head_mask, uint32_t* head, uint32_t* tail,
                   uint32_t* escaped, std::string& err);
 int run_pairing(Batch& b, uint32_t r, double contact, uint32_t out5[5], std::string& err);
+int run_unwrap(Batch& b, uint32_t r, const uint32_t* members, uint32_t m, float* out, std::string& err);
+int run_local_cavity(Batch& b, const float* positions, uint32_t n, double cell, double radius, double* volume,
+                     std::string& err);
 int run_shapes(Batch& b, uint32_t r, const uint32_t* members_csr, const uint32_t* start, uint32_t ncomp,
                double* out10, std::string& err);
 int run_aggregates(Batch& b, uint32_t r, const uint32_t* mem, uint32_t nm, double cutoff, uint32_t* labels,

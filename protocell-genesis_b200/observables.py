@@ -192,21 +192,139 @@ def shape_metrics(shape):
             "flatnessRatio": l0 / l2 if l2 > 1e-12 else 1.0, "inPlaneSymmetry": l1 / l2 if l2 > 1e-12 else 1.0}
 
 
-def analyze_aggregates(system, cutoff, detail_count=5, min_amphiphiles_per_aggregate=1):
-    """The counting and shape parts of analyzeAggregates on a device system: amphiphiles
-    (findAmphiphiles), their members clustered by `cutoff` on all three periodic axes, amphiphiles
-    per aggregate (largest aggregate first), the qualifying aggregates, and shapeOf for the largest
-    `detail_count`.  The head-shell, cavity and closure detail of shapeOfAggregate (and the lamellar
-    / vesicle classification built on them) is not part of this."""
+HEAD_PEAKS_UNAVAILABLE = "unavailable"
+
+
+def density_profile_of(positions, box_z, bins):
+    """densityProfileZ (engine/src/metrics.ts:21-47) of f32 x4 positions whose w is 0 for a head:
+    z histogram over [0, box_z) in `bins` bins, heads and tails apart; a z outside raises."""
+    p = np.asarray(positions, np.float32).reshape(-1, 4)
+    z = p[:, 2].astype(np.float64)
+    bad = ~((z >= 0) & (z < box_z))
+    if bad.any():
+        raise ValueError(f"densityProfileZ: bead with z={z[bad][0]} outside [0, {box_z}): the z profile is undefined "
+                         f"for escaped beads (z is not periodic), and clamping them into the edge bin is not allowed: "
+                         f"it creates a false peak")
+    dz = box_z / bins
+    b = np.minimum(bins - 1, np.floor(z / dz)).astype(np.int64)
+    head = p[:, 3] == 0
+    return {"z": [(i + 0.5) * dz for i in range(bins)],
+            "head": np.bincount(b[head], minlength=bins).astype(np.int64).tolist(),
+            "tail": np.bincount(b[~head], minlength=bins).astype(np.int64).tolist()}
+
+
+def compute_head_peaks(particles, box, polar, bins, min_heads_per_bin, sep_min, sep_max):
+    """computeHeadPeaks (soup/src/aggregates.ts:83-120): 0 without polar beads; "unavailable" when
+    fewer than min_heads_per_bin heads per bin remain after dropping escaped z; 2 when the head profile
+    has two peaks min..max apart (bilayerThickness); 1 otherwise.  `polar[k]`: kind k is polar."""
+    p = np.asarray(particles, np.float32).reshape(-1, 4)
+    kinds = np.rint(p[:, 3]).astype(np.int64)
+    is_head = np.array([bool(polar[k]) if 0 <= k < len(polar) else False for k in kinds], bool)
+    if not is_head.any():
+        return 0
+    remapped = p.copy()
+    remapped[:, 3] = np.where(is_head, 0.0, 1.0)
+    kept, _ = drop_escaped_z(remapped.reshape(-1), box)
+    kept_heads = int((kept.reshape(-1, 4)[:, 3] == 0).sum())
+    if kept_heads == 0 or kept_heads / bins < min_heads_per_bin:
+        return HEAD_PEAKS_UNAVAILABLE
+    profile = density_profile_of(kept, box[2], bins)
+    try:
+        sep = bilayer_thickness(profile)
+    except ValueError:
+        return 1
+    return 2 if sep_min <= sep <= sep_max else 1
+
+
+def profile_along(coords, kinds):
+    """profileAlong (soup/src/aggregates.ts:324-347): a coordinate per bead packed into z (shifted to
+    start at 0, rounded to f32) with the bead's kind, in a [1, 1, span] box."""
+    c = np.asarray(coords, np.float64)
+    lo, hi = float(c.min()), float(c.max())
+    span = max(1e-6, (hi - lo) * 1.0001)
+    p = np.zeros((c.size, 4), np.float32)
+    p[:, 2] = (c - lo).astype(np.float32)
+    p[:, 3] = np.asarray(kinds, np.float32)
+    return p.reshape(-1), [1.0, 1.0, span]
+
+
+def is_lamellar_shape(shape, t):
+    """isLamellarShape (soup/src/aggregates.ts:273-282)."""
+    return shape["flatnessRatio"] <= t["lamellarFlatnessRatio"] and shape["inPlaneSymmetry"] >= t["lamellarInPlaneSymmetryMin"]
+
+
+def is_bilayer_shape(shape, t):
+    """isBilayerShape (soup/src/aggregates.ts:284-290)."""
+    return is_lamellar_shape(shape, t) and (shape["radialHeadShells"] == 2 or shape["transverseHeadShells"] == 2)
+
+
+def is_vesicle_shape(shape, t):
+    """isVesicleShape (soup/src/aggregates.ts:307-315): two radial head shells and a closed interior,
+    by encapsulated water when water was measured (None: the centre could not be trusted, not
+    closed), else by the vacuum cavity."""
+    if shape["radialHeadShells"] != 2:
+        return False
+    if "encapsulatedWater" in shape:
+        return shape["encapsulatedWater"] is not None and bool(shape["encapsulatedWater"]["closed"])
+    return shape["cavityVolume"] > t["enclosedVolume"]
+
+
+def shape_of_aggregate(system, members, amphiphile_count, device_shape, thresholds, positions=None, water=None):
+    """shapeOfAggregate (soup/src/aggregates.ts:387-476) of one aggregate (members ascending, the
+    first the unwrap reference) on a device system: shapeOf from the device gyration tensor, the
+    radial and (for a flat shape) transverse head-shell counts from the device-unwrapped members, the
+    vacuum cavity of the device local flood, and, when water indices are given, the encapsulated
+    water of the device periodic closure about the periodic centre."""
+    P = _config.load_params()
+    t = thresholds
+    polar = [bool(m["polar"]) for m in P["monomers"]]
+    sh = shape_metrics(device_shape)
+    unwrapped = system.aggregate_unwrap(members).reshape(-1, 4)
+    kinds = unwrapped[:, 3]
+    d = unwrapped[:, :3].astype(np.float64) - np.asarray(sh["centre"], np.float64)
+    hp = (t["aggregateHeadDensityBins"], t["aggregateMinHeadsPerBin"], t["headPeakSeparationMin"],
+          t["headPeakSeparationMax"])
+    rad, rbox = profile_along(np.sqrt((d * d).sum(axis=1)), kinds)
+    out = dict(sh)
+    out.update(particleCount=int(len(members)), amphiphileCount=int(amphiphile_count))
+    out["radialHeadShells"] = compute_head_peaks(rad, rbox, polar, *hp)
+    out["transverseHeadShells"] = 0
+    if is_lamellar_shape(out, t):
+        ax = np.asarray(sh["smallestAxis"], np.float64)
+        tr, tbox = profile_along(d[:, 0] * ax[0] + d[:, 1] * ax[1] + d[:, 2] * ax[2], kinds)
+        out["transverseHeadShells"] = compute_head_peaks(tr, tbox, polar, *hp)
+    out["cavityVolume"] = system.local_cavity_volume(unwrapped.reshape(-1), t["closureCell"], t["closureRadius"])
+    if water is not None and len(water) > 0:
+        pos = system.particles() if positions is None else positions
+        c = periodic_centre(pos, members, system.box, P["circularAlpha"])
+        out["encapsulatedWater"] = None if c is None else system.closure(
+            members, water, c, t["closureCell"], t["closureRadius"], t["enclosedVolume"])
+    return out
+
+
+def analyze_aggregates(system, cutoff, detail_count=None, min_amphiphiles_per_aggregate=None, thresholds=None,
+                       water=None):
+    """analyzeAggregates (soup/src/aggregates.ts:499-558) on a device system: amphiphiles
+    (findAmphiphiles), their members clustered by `cutoff` on all three periodic axes, amphiphiles per
+    aggregate (largest aggregate first), the qualifying aggregates, shapeOfAggregate for the largest
+    `detail_count`, and whether any of them reads as lamellar (bilayer) or as a vesicle.  Thresholds
+    default to the parameter tables' stage thresholds; `water`: the water indices, for the closure."""
+    t = dict(_config.load_params()["stageThresholds"])
+    t.update(thresholds or {})
+    if detail_count is not None:
+        t["detailAggregateCount"] = detail_count
+    if min_amphiphiles_per_aggregate is not None:
+        t["minAmphiphilesPerAggregate"] = min_amphiphiles_per_aggregate
     n_amph, head_of = system.amphiphile_labels()
     none = 0xFFFFFFFF
     members = np.nonzero(head_of != none)[0].astype(np.uint32)
     empty = {"aggregateCount": 0, "sizeHistogram": [], "aggregates": [], "qualifyingAggregateCount": 0,
-             "amphiphilesInQualifying": 0, "amphiphileShareInQualifying": 0.0}
+             "amphiphilesInQualifying": 0, "amphiphileShareInQualifying": 0.0, "hasLamellarAggregate": False,
+             "hasVesicleAggregate": False}
     if members.size == 0:
         return empty
     _, labels = system.aggregate_labels(members, cutoff)
-    ncomp, shapes = system.aggregate_shapes(members, labels, max(int(detail_count), 0))
+    ncomp, shapes = system.aggregate_shapes(members, labels, max(int(t["detailAggregateCount"]), 0))
     # amphiphiles per component: its members that are their amphiphile's head
     is_head = head_of[members] == members
     uniq, inv = np.unique(labels, return_inverse=True)
@@ -214,11 +332,18 @@ def analyze_aggregates(system, cutoff, detail_count=5, min_amphiphiles_per_aggre
     heads = np.bincount(inv, weights=is_head).astype(np.int64)
     order = sorted(range(len(uniq)), key=lambda c: (-int(size[c]), int(uniq[c])))
     hist = [int(heads[c]) for c in order]
-    qual = [h for h in hist if h >= min_amphiphiles_per_aggregate]
+    qual = [h for h in hist if h >= t["minAmphiphilesPerAggregate"]]
     total = int(n_amph)
-    return {"aggregateCount": int(ncomp), "sizeHistogram": hist, "aggregates": [shape_metrics(s) for s in shapes],
+    pos = system.particles() if water is not None else None
+    detail = []
+    for k, shp in enumerate(shapes):
+        c = order[k]
+        detail.append(shape_of_aggregate(system, members[inv == c], int(heads[c]), shp, t, pos, water))
+    return {"aggregateCount": int(ncomp), "sizeHistogram": hist, "aggregates": detail,
             "qualifyingAggregateCount": len(qual), "amphiphilesInQualifying": int(sum(qual)),
-            "amphiphileShareInQualifying": (sum(qual) / total) if total > 0 else 0.0}
+            "amphiphileShareInQualifying": (sum(qual) / total) if total > 0 else 0.0,
+            "hasLamellarAggregate": any(is_bilayer_shape(a, t) for a in detail),
+            "hasVesicleAggregate": any(is_vesicle_shape(a, t) for a in detail)}
 
 
 # reference-style names
@@ -233,3 +358,7 @@ hendersonAlpha = henderson_alpha
 apparentPKa = apparent_pka
 symmetricEigenvalues3x3 = symmetric_eigenvalues_3x3
 analyzeAggregates = analyze_aggregates
+computeHeadPeaks = compute_head_peaks
+isLamellarShape = is_lamellar_shape
+isBilayerShape = is_bilayer_shape
+isVesicleShape = is_vesicle_shape

@@ -388,6 +388,23 @@ class SoupSystem:
         return int(nc.value), [dict(size=out[c].size, label=out[c].label, centre=list(out[c].centre),
                                     gyration=list(out[c].gyration)) for c in range(k)]
 
+    def aggregate_unwrap(self, members):
+        """unwrapAggregate (engine/src/aggregate.ts:245-262) of one aggregate on the device: f32 x4 per
+        member (w = kind), in the given order, about the first member."""
+        m = np.ascontiguousarray(members, np.uint32)
+        out = np.empty(4 * m.size, np.float32)
+        _check(self._lib, self._h, self._lib.soup_aggregate_unwrap(self._h, m.ctypes.data_as(_abi._U32P), m.size,
+                                                                   _ptr(out)))
+        return out
+
+    def local_cavity_volume(self, unwrapped, cell, radius):
+        """localCavityVolume (soup/src/aggregates.ts:350-385) of unwrapped positions on the device."""
+        p = np.ascontiguousarray(unwrapped, np.float32)
+        v = C.c_double()
+        _check(self._lib, self._h, self._lib.soup_local_cavity_volume(self._h, _ptr(p), p.size // 4, float(cell),
+                                                                      float(radius), C.byref(v)))
+        return v.value
+
     # ---- differentiation (the adjoint of the step; no counterpart in the reference) ----
     def get_diff_params(self):
         t = (C.c_double * _abi.DIFF_NPARAM)()

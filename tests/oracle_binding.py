@@ -67,6 +67,8 @@ def lib(abi):
         "oracle_aggregate_shape": (C.c_int, [P, P, C.c_uint32, P, P]),
         "oracle_relax": (C.c_int, [P, C.c_uint32, C.c_double]),
         "oracle_scale_molecules_rigid": (C.c_int, [P, C.c_uint32, P, C.c_uint32, P, P, P]),
+        "oracle_unwrap_aggregate": (C.c_int, [P, P, C.c_uint32, P, P]),
+        "oracle_local_cavity_volume": (C.c_double, [P, C.c_uint32, C.c_double, C.c_double]),
         "oracle_proximity_pairs": (C.c_int, [P, C.c_uint32, P, C.c_double, P, P, C.c_size_t,
                                              C.POINTER(C.c_size_t)]),
     }
@@ -338,3 +340,19 @@ def proximity_pairs(abi, pos, box, cutoff, eligible=None):
     out = np.zeros(2 * max(cnt.value, 1), np.uint32)
     L.oracle_proximity_pairs(_ptr(pos), n, _ptr(b), float(cutoff), _ptr(el), _ptr(out), cnt.value, C.byref(cnt))
     return out[: 2 * cnt.value]
+
+
+def unwrap_aggregate(abi, pos, members, box):
+    """unwrapAggregate from the oracle: f32 x4 per member, about members[0]."""
+    L = lib(abi)
+    pos = np.ascontiguousarray(pos, np.float32)
+    m = np.ascontiguousarray(members, np.uint32)
+    out = np.zeros(4 * m.size, np.float32)
+    L.oracle_unwrap_aggregate(_ptr(pos), _ptr(m), m.size, _ptr(np.ascontiguousarray(box, np.float64)), _ptr(out))
+    return out
+
+
+def local_cavity_volume(abi, positions, cell, radius):
+    """localCavityVolume from the oracle, over unwrapped f32 x4 positions."""
+    p = np.ascontiguousarray(positions, np.float32)
+    return lib(abi).oracle_local_cavity_volume(_ptr(p), p.size // 4, float(cell), float(radius))
