@@ -300,6 +300,13 @@ int soup_protonation_sweep(SoupHandle* h, SoupSweepResult* out);
 int soup_closure(SoupHandle* h, const uint32_t* member_idx, uint32_t n_members,
                  const uint32_t* water_idx, uint32_t n_water, const double centre[3],
                  double cell, double radius, double enclosed_volume_min, SoupClosureResult* out);
+/* The same with encapsulatedWaterVolume's `parcel` (water-closure.ts:280-288, 323-337): for a finite
+ * parcel in a larger box, the reached empty cells the bulk water density is averaged over are the
+ * ones whose centre lies within parcel_radius of parcel_centre (no minimum image, as the reference). */
+int soup_closure_in_parcel(SoupHandle* h, const uint32_t* member_idx, uint32_t n_members,
+                           const uint32_t* water_idx, uint32_t n_water, const double centre[3], double cell,
+                           double radius, double enclosed_volume_min, const double parcel_centre[3],
+                           double parcel_radius, SoupClosureResult* out);
 
 /* findAmphiphiles (soup/src/amphiphile.ts:55-141) on the current bond graph: head_of[i] = the
  * head index of the amphiphile particle i belongs to, or SOUP_NONE.  n_out = amphiphile count. */

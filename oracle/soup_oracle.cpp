@@ -1135,10 +1135,11 @@ int periodic_centre(const float* pos, const uint32_t* idx, uint32_t m, const dou
 }
 
 // soup/src/water-closure.ts:109-363 occupancyPeriodic + farthestEmptyCellSeed + floodOutsidePeriodic
-// + encapsulatedWaterVolume (no parcel restriction)
+// + encapsulatedWaterVolume; with `parcel` (centre x y z, radius) the reached empty cells the bulk
+// density is taken over are those whose centre lies in the parcel (water-closure.ts:323-337)
 int closure(const float* pos, const uint32_t* mem, uint32_t nm, const uint32_t* wat, uint32_t nw, const double box[3],
             const double centre[3], double cell, double radius, double vmin, SoupClosureResult* res,
-            std::vector<uint8_t>* occ_out, std::vector<uint8_t>* vis_out) {
+            std::vector<uint8_t>* occ_out, std::vector<uint8_t>* vis_out, const double* parcel = nullptr) {
   int nx = std::max(1, (int)std::ceil(box[0] / cell)), ny = std::max(1, (int)std::ceil(box[1] / cell)),
       nz = std::max(1, (int)std::ceil(box[2] / cell));
   size_t NC = (size_t)nx * ny * nz;
@@ -1191,7 +1192,18 @@ int closure(const float* pos, const uint32_t* mem, uint32_t nm, const uint32_t* 
     }
   }
   uint32_t totalEmpty = 0, unreached = 0, reachedEmpty = 0;
-  for (size_t i = 0; i < NC; ++i) if (!occ[i]) { totalEmpty++; if (!vis[i]) unreached++; else reachedEmpty++; }
+  for (size_t i = 0; i < NC; ++i) if (!occ[i]) { totalEmpty++; if (!vis[i]) unreached++; }
+  for (size_t i = 0; i < NC; ++i) {
+    if (!(occ[i] == 0 && vis[i] != 0)) continue;
+    if (parcel) {
+      const int cz = (int)(i / ((size_t)nx * ny));
+      const size_t crem = i - (size_t)cz * nx * ny;
+      const int cy = (int)(crem / nx), cx = (int)(crem - (size_t)cy * nx);
+      const double ex = (cx + 0.5) * cell - parcel[0], ey = (cy + 0.5) * cell - parcel[1], ez = (cz + 0.5) * cell - parcel[2];
+      if (ex * ex + ey * ey + ez * ez > parcel[3] * parcel[3]) continue;
+    }
+    reachedEmpty++;
+  }
   uint32_t enc = 0, reachedWater = 0;
   for (uint32_t k = 0; k < nw; ++k) {
     uint32_t i = wat[k];
@@ -1515,6 +1527,12 @@ int oracle_closure(const float* pos, const uint32_t* mem, uint32_t nm, const uin
   if (occ) std::memcpy(occ, o.data(), o.size());
   if (vis) std::memcpy(vis, v.data(), v.size());
   return SOUP_OK;
+}
+int oracle_closure_in_parcel(const float* pos, const uint32_t* mem, uint32_t nm, const uint32_t* wat, uint32_t nw,
+                             const double box[3], const double centre[3], double cell, double radius, double vmin,
+                             const double parcel_centre[3], double parcel_radius, SoupClosureResult* res) {
+  const double parcel[4] = {parcel_centre[0], parcel_centre[1], parcel_centre[2], parcel_radius};
+  return closure(pos, mem, nm, wat, nw, box, centre, cell, radius, vmin, res, nullptr, nullptr, parcel);
 }
 uint32_t oracle_amphiphiles(const float* pos, const uint32_t* slots, uint32_t n, const uint32_t* polar_of_kind, uint32_t* head_of) {
   return amphiphiles(pos, slots, n, polar_of_kind, head_of);

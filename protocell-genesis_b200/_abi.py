@@ -190,6 +190,9 @@ SIGNATURES = {
     "soup_protonation_sweep": (C.c_int, [_P, C.POINTER(SoupSweepResult)]),
     "soup_closure": (C.c_int, [_P, _U32P, C.c_uint32, _U32P, C.c_uint32, C.POINTER(C.c_double),
                                C.c_double, C.c_double, C.c_double, C.POINTER(SoupClosureResult)]),
+    "soup_closure_in_parcel": (C.c_int, [_P, _U32P, C.c_uint32, _U32P, C.c_uint32, C.POINTER(C.c_double),
+                                         C.c_double, C.c_double, C.c_double, C.POINTER(C.c_double), C.c_double,
+                                         C.POINTER(SoupClosureResult)]),
     "soup_amphiphile_labels": (C.c_int, [_P, _U32P, _U32P]),
     "soup_aggregate_labels": (C.c_int, [_P, _U32P, C.c_uint32, C.c_double, _U32P, _U32P]),
     "soup_pairing_stats": (C.c_int, [_P, C.c_double, C.POINTER(SoupPairingStats)]),

@@ -113,11 +113,27 @@ __global__ void k_flood_level(const uint8_t* __restrict__ occ, uint32_t* __restr
 }
 
 // cell counts and water classification (water-closure.ts:297-327)
-__global__ void k_cell_counts(const uint8_t* __restrict__ occ, const uint32_t* __restrict__ vis, uint64_t nc,
+// reachedEmpty counts only cells whose centre lies in the parcel when pr2 >= 0 (water-closure.ts:323-337)
+__global__ void k_cell_counts(const uint8_t* __restrict__ occ, const uint32_t* __restrict__ vis, uint64_t nc, Grid g,
+                              double pcx, double pcy, double pcz, double pr2,
                               unsigned long long* __restrict__ out /* totalEmpty, unreached, reachedEmpty */) {
   const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
   uint32_t a = 0, b = 0, c = 0;
-  if (i < nc && !occ[i]) { a = 1; if (!vis[i]) b = 1; else c = 1; }
+  if (i < nc && !occ[i]) {
+    a = 1;
+    if (!vis[i]) {
+      b = 1;
+    } else if (pr2 < 0.0) {
+      c = 1;
+    } else {
+      const int cz = (int)(i / ((uint64_t)g.nx * g.ny));
+      const uint64_t rem = i - (uint64_t)cz * g.nx * g.ny;
+      const int cy = (int)(rem / (uint64_t)g.nx), cx = (int)(rem - (uint64_t)cy * g.nx);
+      const double ex = __dsub_rn(__dmul_rn(cx + 0.5, g.cell), pcx), ey = __dsub_rn(__dmul_rn(cy + 0.5, g.cell), pcy),
+                   ez = __dsub_rn(__dmul_rn(cz + 0.5, g.cell), pcz);
+      c = sq3(ex, ey, ez) > pr2 ? 0u : 1u;
+    }
+  }
   for (int o = 16; o > 0; o >>= 1) {
     a += __shfl_xor_sync(0xffffffffu, a, o); b += __shfl_xor_sync(0xffffffffu, b, o); c += __shfl_xor_sync(0xffffffffu, c, o);
   }
@@ -302,8 +318,8 @@ char* analysis_scratch(Batch& b, size_t bytes, int which) {
 }
 
 int run_closure(Batch& b, uint32_t r, const uint32_t* mem, uint32_t nm, const uint32_t* wat, uint32_t nw,
-                const double centre[3], double cell, double radius, double vmin, SoupClosureResult* out,
-                std::string& err) {
+                const double centre[3], double cell, double radius, double vmin, const double* parcel,
+                SoupClosureResult* out, std::string& err) {
   const SoupConfig& c = b.cfg[r];
   const uint32_t n = c.n, off = b.hsp[r].slot_off;
   for (uint32_t k = 0; k < nm; ++k) if (mem[k] >= n) { err = "closure: member index out of range"; return SOUP_E_ARG; }
@@ -363,7 +379,8 @@ int run_closure(Batch& b, uint32_t r, const uint32_t* mem, uint32_t nm, const ui
     std::swap(front, next);
     std::swap(nfront, nnext);
   }
-  k_cell_counts<<<nblocks(nc), kBlock, 0, st>>>(occ, vis, nc, u64 + 2);
+  k_cell_counts<<<nblocks(nc), kBlock, 0, st>>>(occ, vis, nc, g, parcel ? parcel[0] : 0.0, parcel ? parcel[1] : 0.0,
+                                                parcel ? parcel[2] : 0.0, parcel ? parcel[3] * parcel[3] : -1.0, u64 + 2);
   if (nw) k_water<<<nblocks(nw), kBlock, 0, st>>>(b.pos, b.slot_of, off, dwat, nw, g, occ, vis, u64 + 5);
   unsigned long long res[8];
   SOUP_CUDA_TRY(cudaMemcpyAsync(res, u64, 64, cudaMemcpyDeviceToHost, st));

@@ -1433,7 +1433,22 @@ int soup_closure(SoupHandle* h, const uint32_t* member_idx, uint32_t n_members, 
     if (!out || !centre || (n_members && !member_idx) || (n_water && !water_idx)) fail(SOUP_E_ARG, "NULL argument");
     if (!(cell > 0) || !(radius > 0)) fail(SOUP_E_ARG, "cell and radius must be positive");
     std::string err;
-    int st = run_closure(b, r, member_idx, n_members, water_idx, n_water, centre, cell, radius, vmin, out, err);
+    int st = run_closure(b, r, member_idx, n_members, water_idx, n_water, centre, cell, radius, vmin, nullptr, out, err);
+    if (st) fail(st, err);
+  });
+}
+
+int soup_closure_in_parcel(SoupHandle* h, const uint32_t* member_idx, uint32_t n_members, const uint32_t* water_idx,
+                           uint32_t n_water, const double centre[3], double cell, double radius, double vmin,
+                           const double parcel_centre[3], double parcel_radius, SoupClosureResult* out) {
+  return guarded(h, [&](Batch& b, uint32_t r) {
+    if (!out || !centre || !parcel_centre || (n_members && !member_idx) || (n_water && !water_idx))
+      fail(SOUP_E_ARG, "NULL argument");
+    if (!(cell > 0) || !(radius > 0)) fail(SOUP_E_ARG, "cell and radius must be positive");
+    if (!(parcel_radius >= 0)) fail(SOUP_E_ARG, "the parcel radius must be a non-negative number");
+    const double parcel[4] = {parcel_centre[0], parcel_centre[1], parcel_centre[2], parcel_radius};
+    std::string err;
+    int st = run_closure(b, r, member_idx, n_members, water_idx, n_water, centre, cell, radius, vmin, parcel, out, err);
     if (st) fail(st, err);
   });
 }

@@ -226,8 +226,8 @@ void sweep_prepare(Batch& b);
 void launch_rebuild_check(Batch& b);
 // analysis
 int run_closure(Batch& b, uint32_t r, const uint32_t* mem, uint32_t nm, const uint32_t* wat, uint32_t nw,
-                const double centre[3], double cell, double radius, double vmin, SoupClosureResult* out,
-                std::string& err);
+                const double centre[3], double cell, double radius, double vmin, const double* parcel,
+                SoupClosureResult* out, std::string& err);
 int run_amphiphiles(Batch& b, uint32_t r, uint32_t* head_of, uint32_t* n_out, std::string& err);
 // Offsets of the sub-buffers of one analysis call inside the batch's analysis scratch (256-byte
 // aligned), and the scratch itself, grown to `bytes` when it is smaller.

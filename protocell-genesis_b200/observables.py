@@ -269,7 +269,8 @@ def is_vesicle_shape(shape, t):
     return shape["cavityVolume"] > t["enclosedVolume"]
 
 
-def shape_of_aggregate(system, members, amphiphile_count, device_shape, thresholds, positions=None, water=None):
+def shape_of_aggregate(system, members, amphiphile_count, device_shape, thresholds, positions=None, water=None,
+                       parcel=None):
     """shapeOfAggregate (soup/src/aggregates.ts:387-476) of one aggregate (members ascending, the
     first the unwrap reference) on a device system: shapeOf from the device gyration tensor, the
     radial and (for a flat shape) transverse head-shell counts from the device-unwrapped members, the
@@ -298,17 +299,18 @@ def shape_of_aggregate(system, members, amphiphile_count, device_shape, threshol
         pos = system.particles() if positions is None else positions
         c = periodic_centre(pos, members, system.box, P["circularAlpha"])
         out["encapsulatedWater"] = None if c is None else system.closure(
-            members, water, c, t["closureCell"], t["closureRadius"], t["enclosedVolume"])
+            members, water, c, t["closureCell"], t["closureRadius"], t["enclosedVolume"], parcel)
     return out
 
 
 def analyze_aggregates(system, cutoff, detail_count=None, min_amphiphiles_per_aggregate=None, thresholds=None,
-                       water=None):
+                       water=None, parcel=None):
     """analyzeAggregates (soup/src/aggregates.ts:499-558) on a device system: amphiphiles
     (findAmphiphiles), their members clustered by `cutoff` on all three periodic axes, amphiphiles per
     aggregate (largest aggregate first), the qualifying aggregates, shapeOfAggregate for the largest
     `detail_count`, and whether any of them reads as lamellar (bilayer) or as a vesicle.  Thresholds
-    default to the parameter tables' stage thresholds; `water`: the water indices, for the closure."""
+    default to the parameter tables' stage thresholds; `water`: the water indices, for the closure;
+    `parcel`: {"centre", "radius"} of a confined run, for the closure's bulk density."""
     t = dict(_config.load_params()["stageThresholds"])
     t.update(thresholds or {})
     if detail_count is not None:
@@ -338,7 +340,7 @@ def analyze_aggregates(system, cutoff, detail_count=None, min_amphiphiles_per_ag
     detail = []
     for k, shp in enumerate(shapes):
         c = order[k]
-        detail.append(shape_of_aggregate(system, members[inv == c], int(heads[c]), shp, t, pos, water))
+        detail.append(shape_of_aggregate(system, members[inv == c], int(heads[c]), shp, t, pos, water, parcel))
     return {"aggregateCount": int(ncomp), "sizeHistogram": hist, "aggregates": detail,
             "qualifyingAggregateCount": len(qual), "amphiphilesInQualifying": int(sum(qual)),
             "amphiphileShareInQualifying": (sum(qual) / total) if total > 0 else 0.0,

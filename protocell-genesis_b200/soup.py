@@ -314,14 +314,22 @@ class SoupSystem:
 
     protonationSweepDEBUG = protonation_sweep
 
-    def closure(self, members, water, centre, cell, radius, enclosed_volume_min):
+    def closure(self, members, water, centre, cell, radius, enclosed_volume_min, parcel=None):
+        """encapsulatedWaterVolume (soup/src/water-closure.ts:271-363); parcel: {"centre": [x, y, z],
+        "radius": R} restricts the bulk-density cells to a finite parcel (config 5's confined runs)."""
         m = np.ascontiguousarray(members, np.uint32)
         w = np.ascontiguousarray(water, np.uint32)
         c = (C.c_double * 3)(*[float(x) for x in centre])
         r = _abi.SoupClosureResult()
-        _check(self._lib, self._h, self._lib.soup_closure(
-            self._h, m.ctypes.data_as(_abi._U32P), m.size, w.ctypes.data_as(_abi._U32P), w.size, c,
-            float(cell), float(radius), float(enclosed_volume_min), C.byref(r)))
+        if parcel is None:
+            st = self._lib.soup_closure(self._h, m.ctypes.data_as(_abi._U32P), m.size, w.ctypes.data_as(_abi._U32P),
+                                        w.size, c, float(cell), float(radius), float(enclosed_volume_min), C.byref(r))
+        else:
+            pc = (C.c_double * 3)(*[float(x) for x in parcel["centre"]])
+            st = self._lib.soup_closure_in_parcel(self._h, m.ctypes.data_as(_abi._U32P), m.size,
+                                                  w.ctypes.data_as(_abi._U32P), w.size, c, float(cell), float(radius),
+                                                  float(enclosed_volume_min), pc, float(parcel["radius"]), C.byref(r))
+        _check(self._lib, self._h, st)
         return dict(encapsulatedCount=r.encapsulated_count, totalWater=r.total_water,
                     bulkWaterDensity=r.bulk_water_density, encapsulationThresholdCount=r.threshold_count,
                     closed=bool(r.closed), totalEmptyCells=r.total_empty_cells, unreachedCells=r.unreached_cells,

@@ -68,6 +68,8 @@ def lib(abi):
         "oracle_relax": (C.c_int, [P, C.c_uint32, C.c_double]),
         "oracle_scale_molecules_rigid": (C.c_int, [P, C.c_uint32, P, C.c_uint32, P, P, P]),
         "oracle_unwrap_aggregate": (C.c_int, [P, P, C.c_uint32, P, P]),
+        "oracle_closure_in_parcel": (C.c_int, [P, P, C.c_uint32, P, C.c_uint32, P, P, C.c_double, C.c_double,
+                                               C.c_double, P, C.c_double, C.POINTER(abi.SoupClosureResult)]),
         "oracle_local_cavity_volume": (C.c_double, [P, C.c_uint32, C.c_double, C.c_double]),
         "oracle_proximity_pairs": (C.c_int, [P, C.c_uint32, P, C.c_double, P, P, C.c_size_t,
                                              C.POINTER(C.c_size_t)]),
@@ -356,3 +358,18 @@ def local_cavity_volume(abi, positions, cell, radius):
     """localCavityVolume from the oracle, over unwrapped f32 x4 positions."""
     p = np.ascontiguousarray(positions, np.float32)
     return lib(abi).oracle_local_cavity_volume(_ptr(p), p.size // 4, float(cell), float(radius))
+
+
+def closure_in_parcel(abi, pos, members, water, box, centre, cell, radius, vmin, parcel_centre, parcel_radius):
+    """encapsulatedWaterVolume with the parcel restriction, from the oracle."""
+    L = lib(abi)
+    pos = np.ascontiguousarray(pos, np.float32)
+    m = np.ascontiguousarray(members, np.uint32)
+    w = np.ascontiguousarray(water, np.uint32)
+    r = abi.SoupClosureResult()
+    st = L.oracle_closure_in_parcel(_ptr(pos), _ptr(m), m.size, _ptr(w), w.size, _ptr(np.ascontiguousarray(box, np.float64)),
+                                    _ptr(np.ascontiguousarray(centre, np.float64)), float(cell), float(radius), float(vmin),
+                                    _ptr(np.ascontiguousarray(parcel_centre, np.float64)), float(parcel_radius), C.byref(r))
+    if st != 0:
+        raise RuntimeError(L.oracle_last_error().decode())
+    return r

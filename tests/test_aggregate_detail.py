@@ -66,3 +66,26 @@ def test_unwrap_about_the_first_member():
     assert u[1, 0] == pytest.approx(20.3, abs=1e-5) and u[2, 1] == pytest.approx(-0.2, abs=1e-5)
     assert u[2, 2] == np.float32(0.1) and u[0, 0] == np.float32(19.5)
     assert u[:, 3].tolist() == [0, 1, 0]
+
+
+def test_parcel_restricts_the_bulk_density_to_the_parcel():
+    """encapsulatedWaterVolume's parcel (soup/src/water-closure.ts:280-288, 323-337): water only within
+    18 sigma of the shell's centre and vacuum beyond; the bulk density over the parcel's reached cells
+    is the water's own density, over the whole box it is diluted by the vacuum."""
+    from test_oracle_pins import SYN_BOX, _assemble, _shell
+    rng = np.random.default_rng(5)
+    centre = np.array([25.0, 25.0, 25.0])
+    members = _shell(rng, centre)
+    d = rng.normal(size=(6000, 3))
+    d /= np.linalg.norm(d, axis=1)[:, None]
+    water = centre + d * rng.uniform(13.0, 18.0, 6000)[:, None]
+    pos, mem, wat = _assemble(members, water)
+    c = ob.periodic_centre(_abi, pos, mem, SYN_BOX, P["circularAlpha"])
+    plain = ob.closure(_abi, pos, mem, wat, SYN_BOX, c, ST["closureCell"], ST["closureRadius"], ST["enclosedVolume"])
+    parcel = ob.closure_in_parcel(_abi, pos, mem, wat, SYN_BOX, c, ST["closureCell"], ST["closureRadius"],
+                                  ST["enclosedVolume"], centre, 18.0)
+    shell_vol = 4 / 3 * np.pi * (18.0 ** 3 - 12.6 ** 3)
+    assert parcel.bulk_water_density == pytest.approx(6000 / shell_vol, rel=0.1)
+    assert parcel.bulk_water_density > 3 * plain.bulk_water_density
+    assert parcel.encapsulated_count == plain.encapsulated_count == 0
+    assert parcel.total_empty_cells == plain.total_empty_cells and parcel.unreached_cells == plain.unreached_cells

@@ -61,3 +61,24 @@ def test_amphiphiles_and_aggregates_match_oracle():
     nc_g, lab_g = g.aggregate_labels(members, cut)
     assert nc_g == nc_o and np.array_equal(lab_g, lab_o)
     g.dispose()
+
+
+def test_closure_in_a_parcel_matches_oracle():
+    rng = np.random.default_rng(5)
+    centre = np.array([25.0, 25.0, 25.0])
+    members = _shell(rng, centre)
+    d = rng.normal(size=(6000, 3))
+    d /= np.linalg.norm(d, axis=1)[:, None]
+    e = rng.normal(size=(800, 3))
+    inside = centre + e / np.linalg.norm(e, axis=1)[:, None] * (rng.uniform(0, 1, 800) ** (1 / 3) * 7.0)[:, None]
+    water = np.concatenate([inside, centre + d * rng.uniform(13.0, 18.0, 6000)[:, None]])
+    pos, mem, wat = _assemble(members, water)
+    g = _system_for(pos, len(mem))
+    c = ob.periodic_centre(_abi, pos, mem, SYN_BOX, P["circularAlpha"])
+    args = (ST["closureCell"], ST["closureRadius"], ST["enclosedVolume"])
+    ro = ob.closure_in_parcel(_abi, pos, mem, wat, SYN_BOX, c, *args, centre, 18.0)
+    rg = g.closure(mem, wat, c, *args, parcel={"centre": list(centre), "radius": 18.0})
+    assert rg["encapsulatedCount"] == ro.encapsulated_count > 0
+    assert rg["bulkWaterDensity"] == pytest.approx(ro.bulk_water_density, rel=1e-12)
+    assert rg["closed"] == bool(ro.closed) and rg["seedCell"] == ro.seed_cell
+    g.dispose()
