@@ -171,6 +171,22 @@ __device__ __forceinline__ double pcg_out(uint32_t v) {
 }
 
 constexpr int kWalkThreads = 512;
+constexpr uint32_t kEndOfSweep = 0xFFFFFFFFu;   // s_cflag once the sweep is over
+constexpr uint32_t kSpinLimit = 1u << 25;       // polls of a handoff flag before the walk gives up
+
+// cluster-scope release / acquire on 32-bit words in shared memory (own or a peer CTA's, by generic
+// address): the handoffs between the walking warp and the CTAs that scatter its flips
+__device__ __forceinline__ uint32_t ld_acquire_cluster(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.acquire.cluster.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
+__device__ __forceinline__ void st_release_cluster(uint32_t* p, uint32_t v) {
+  asm volatile("st.release.cluster.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+__device__ __forceinline__ void red_add_release_cluster(uint32_t* p, uint32_t v) {
+  asm volatile("red.release.cluster.add.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
 constexpr int kUpd = 8;
 constexpr uint32_t kBand = 64;    // a band row: one draw's changes on the sites of the next 63 draws
 constexpr uint32_t kRing = 64;    // band rows the walk keeps in shared memory
@@ -381,6 +397,8 @@ __global__ void __launch_bounds__(kWalkThreads) k_sweep_walk(const SysParams* __
   __shared__ Flips F[2];
   __shared__ Flips Fh;                 // a helper CTA's copy of the flips it scatters
   __shared__ uint32_t s_dep, s_done, s_base;
+  __shared__ uint32_t s_cflag, s_scat, s_timeout;   // CTA 0: the handoffs with the helper CTAs
+  __shared__ uint32_t s_hv;                         // a helper CTA: the signal its thread 0 read
   cg::cluster_group cluster = cg::this_cluster();
   const uint32_t crank = cluster.block_rank(), csize = cluster.num_blocks();
   const bool lead = crank == 0;
@@ -406,13 +424,17 @@ __global__ void __launch_bounds__(kWalkThreads) k_sweep_walk(const SysParams* __
     if (threadIdx.x < 32) {
       F[0].start[lane + 1] = 0xFFFFFFFFu;
       F[1].start[lane + 1] = 0xFFFFFFFFu;
-      if (lane == 0) { F[0].n = F[1].n = 0; F[0].start[0] = F[1].start[0] = 0; s_done = 0; s_base = 0; s_dep = 0; }
+      if (lane == 0) {
+        F[0].n = F[1].n = 0; F[0].start[0] = F[1].start[0] = 0; s_done = 0; s_base = 0; s_dep = 0;
+        s_cflag = 0; s_scat = 0; s_timeout = 0;
+      }
     }
   }
   // the lead CTA's window state, read by every CTA of the cluster
   const Flips* lead_F = cluster.map_shared_rank(&F[0], 0);
-  const uint32_t* lead_done = cluster.map_shared_rank(&s_done, 0);
-  const uint32_t* lead_base = cluster.map_shared_rank(&s_base, 0);
+  uint32_t* lead_cflag = cluster.map_shared_rank(&s_cflag, 0);
+  uint32_t* lead_scat = cluster.map_shared_rank(&s_scat, 0);
+  uint32_t* lead_timeout = cluster.map_shared_rank(&s_timeout, 0);
   // scatter threads: every thread of the other CTAs, or CTA 0's warps 1.. when the cluster is one CTA
   // (then they also fetch the band rows, which is all they do otherwise)
   const bool lead_scatters = csize == 1u;
@@ -441,14 +463,9 @@ __global__ void __launch_bounds__(kWalkThreads) k_sweep_walk(const SysParams* __
   }
   cluster.sync();
 
-  for (uint32_t wnd = 0;; ++wnd) {
-    Flips& Fc = F[wnd & 1];               // this window's flips (lead CTA)
-    const Flips& Fp = F[(wnd + 1) & 1];   // the previous window's
-    // written by warp 0 of CTA 0 during the previous R, read by everyone before this window's barrier
-    if (*lead_done) break;
-    const uint32_t base = *lead_base;
-    // ---- C ----
-    if (chain) {
+  // ---- the chain's two phases of a window (warp 0 of CTA 0) ----
+  // C: E and the charge states of this window's sites, with the previous window's flips added
+  auto chain_C = [&](const Flips& Fp) {
       e = (long long)__ldcg(reinterpret_cast<const unsigned long long*>(E + A.site));
       f = flag[A.site];
       // the previous window's flips, accumulated for this window's draws while they were taken; a
@@ -462,10 +479,9 @@ __global__ void __launch_bounds__(kWalkThreads) k_sweep_walk(const SysParams* __
       // this lane's flip would change a later lane of the window: its band row's nonzero mask
       const unsigned long long nz = (unsigned long long)ring[(consumed + (uint32_t)lane) & (kRing - 1)][0];
       inter_m = __ballot_sync(0xffffffffu, ((nz >> 1) & ((1ull << (31 - lane)) - 1ull)) != 0);
-    }
-    cluster.sync();
-    // ---- R ----
-    if (chain) {
+  };
+  // R: resolve the window, record its flips, slide the draws
+  auto chain_R = [&](Flips& Fc) {
       const double u_acc = __shfl_down_sync(0xffffffffu, A.u, 1);   // lane l: draw consumed+l+1 (l < 31)
       int res = decide(e, f, u_acc, kT, inv_kT, lane);
       uint32_t acc_m = __ballot_sync(0xffffffffu, res & 1), need_m = __ballot_sync(0xffffffffu, res & 2);
@@ -595,16 +611,79 @@ __global__ void __launch_bounds__(kWalkThreads) k_sweep_walk(const SysParams* __
         A = b1;
         draw_from(B, j32.a * b1.st + j32.c, H, off, es_cnt);
       }
-    } else {
-      if (!lead) {                        // a copy of the flips this CTA scatters
-        const uint32_t* src = reinterpret_cast<const uint32_t*>(lead_F + ((wnd + 1) & 1));
-        for (uint32_t i = threadIdx.x; i < sizeof(Flips) / 4; i += kWalkThreads) reinterpret_cast<uint32_t*>(&Fh)[i] = src[i];
-        __syncthreads();
+  };
+
+  if (csize == 1u) {
+    // one CTA: its other warps scatter the previous window's flips and fetch band rows while warp 0
+    // resolves, between two CTA barriers a window
+    for (uint32_t wnd = 0;; ++wnd) {
+      Flips& Fc = F[wnd & 1];
+      const Flips& Fp = F[(wnd + 1) & 1];
+      if (s_done) break;
+      const uint32_t base = s_base;
+      if (chain) chain_C(Fp);
+      __syncthreads();
+      if (chain) {
+        chain_R(Fc);
+      } else {
+        scatter_flips(Fp, P, off, cap, es_nl, D, hpos, E, cut2, reach2, tscat, nscat);
+        fetch_rows(ring, brow, base + 32u, threadIdx.x - 32u, kWalkThreads - 32u);
       }
-      if (!lead || lead_scatters) scatter_flips(lead ? Fp : Fh, P, off, cap, es_nl, D, hpos, E, cut2, reach2, tscat, nscat);
-      if (lead) fetch_rows(ring, brow, base + 32u, threadIdx.x - 32u, kWalkThreads - 32u);
+      __syncthreads();
     }
-    cluster.sync();
+  } else if (lead) {
+    // CTA 0 of a cluster.  Warp 0 signals (s_cflag, a release at cluster scope) once its E reads of
+    // window w are done, so the helper CTAs may add window w-1's flips to E, and before window w+1
+    // reads E it waits (s_scat) until every helper has.  The other warps fetch the band rows.  No
+    // cluster barrier inside the loop.
+    for (uint32_t wnd = 0;; ++wnd) {
+      Flips& Fc = F[wnd & 1];
+      const Flips& Fp = F[(wnd + 1) & 1];
+      if (s_done) {
+        if (threadIdx.x == 0) st_release_cluster(&s_cflag, kEndOfSweep);
+        break;
+      }
+      const uint32_t base = s_base;
+      if (chain) {
+        chain_C(Fp);
+        __syncwarp();
+        if (lane == 0) st_release_cluster(&s_cflag, wnd + 1u);
+        chain_R(Fc);
+        if (lane == 0) {
+          const uint32_t want = (csize - 1u) * (wnd + 1u);
+          uint32_t spins = 0;
+          while (ld_acquire_cluster(&s_scat) < want) {
+            if (++spins > kSpinLimit) { s_timeout = 1u; s_done = 1u; break; }
+          }
+        }
+        __syncwarp();
+      } else {
+        fetch_rows(ring, brow, base + 32u, threadIdx.x - 32u, kWalkThreads - 32u);
+      }
+      __syncthreads();
+    }
+  } else {
+    // a helper CTA: wait for window w's signal, copy window w-1's flips from CTA 0, add them to E,
+    // report
+    for (uint32_t wnd = 0;; ++wnd) {
+      if (threadIdx.x == 0) {
+        uint32_t v, spins = 0;
+        for (;;) {
+          v = ld_acquire_cluster(lead_cflag);
+          if (v == kEndOfSweep || v >= wnd + 1u) break;
+          if (++spins > kSpinLimit) { v = kEndOfSweep; atomicExch(lead_timeout, 1u); break; }
+        }
+        s_hv = v;
+      }
+      __syncthreads();
+      if (s_hv == kEndOfSweep) break;
+      const uint32_t* src = reinterpret_cast<const uint32_t*>(lead_F + ((wnd + 1) & 1));
+      for (uint32_t i = threadIdx.x; i < sizeof(Flips) / 4; i += kWalkThreads) reinterpret_cast<uint32_t*>(&Fh)[i] = src[i];
+      __syncthreads();
+      scatter_flips(Fh, P, off, cap, es_nl, D, hpos, E, cut2, reach2, tscat, nscat);
+      __syncthreads();
+      if (threadIdx.x == 0) red_add_release_cluster(lead_scat, 1u);
+    }
   }
   if (!lead) {
     cluster.sync();                       // CTA 0's shared memory stays up until every helper is done
@@ -631,7 +710,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_sweep_walk(const SysParams* __
   if (threadIdx.x == 0) {
     const Lcg j = lcg_pow(consumed);
     rng_io[r] = j.a * s0 + j.c;
-    out[4 * r + 0] = (double)H;
+    out[4 * r + 0] = s_timeout ? -1.0 : (double)H;   // -1: a handoff gave up (the host reports it)
     out[4 * r + 1] = (double)accepted;
     out[4 * r + 2] = dcount > 0 ? dsum / kT / dcount : 0.0;
     out[4 * r + 3] = (double)s_dep;

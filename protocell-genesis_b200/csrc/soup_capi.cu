@@ -540,6 +540,10 @@ void sweep_all(Batch& b, std::vector<SoupSweepResult>* out) {
   }
   else force_pass(b);
   SOUP_CUDA_TRY(cudaStreamSynchronize(b.stream));
+  for (uint32_t r = 0; r < b.R; ++r)
+    if (so[4 * r] < 0)
+      fail(SOUP_E_TIMEOUT, "constant-pH sweep: a handoff between the cluster's CTAs did not arrive within its "
+                           "poll limit; the charges of this sweep are not valid");
   b.sweeps++;
   if (out) {
     out->resize(b.R);
@@ -1400,6 +1404,9 @@ int soup_protonation_sweep(SoupHandle* h, SoupSweepResult* out) {
     SOUP_CUDA_TRY(cudaMemcpyAsync(&b.prot_rng[r], b.prot_rng_dev + r, 4, cudaMemcpyDeviceToHost, b.stream));
     force_pass(b);
     SOUP_CUDA_TRY(cudaStreamSynchronize(b.stream));
+    if (so[0] < 0)
+      fail(SOUP_E_TIMEOUT, "constant-pH sweep: a handoff between the cluster's CTAs did not arrive within its "
+                           "poll limit; the charges of this sweep are not valid");
     b.sweeps++;
     b.next_sweep[r] = b.step[r] + b.cfg[r].sweep_every;
     if (out) {
