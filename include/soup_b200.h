@@ -284,6 +284,11 @@ typedef struct SoupTuneResult {
   double ms_per_step_before, ms_per_step_after;
 } SoupTuneResult;
 int soup_autotune(SoupHandle* h, uint32_t steps, SoupTuneResult* out);
+/* Apply a tuning found before (by soup_autotune on a system of the same shape) without timing
+ * anything: lanes per particle, list-walk radius, and the current skin scaled by skin_scale (at most
+ * 1: the list capacity was sized for it; drift-triggered rebuilds only).  The lists are rebuilt and
+ * the force recomputed.  Only tpp, walk and skin_scale are read. */
+int soup_apply_tuning(SoupHandle* h, const SoupTuneResult* tuning);
 /* soup_step runs chunks of chunkSteps steps (at least 4) as captured CUDA graphs, captured on first
  * use; this captures every chunk graph of the current schedule now, without stepping. */
 int soup_prepare_graphs(SoupHandle* h);

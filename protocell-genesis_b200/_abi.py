@@ -185,6 +185,7 @@ SIGNATURES = {
     "soup_write_charges": (C.c_int, [_P, _P, _SZ]),
     "soup_set_box": (C.c_int, [_P, C.POINTER(C.c_double)]),
     "soup_autotune": (C.c_int, [_P, C.c_uint32, C.POINTER(SoupTuneResult)]),
+    "soup_apply_tuning": (C.c_int, [_P, C.POINTER(SoupTuneResult)]),
     "soup_prepare_graphs": (C.c_int, [_P]),
     "soup_write_state": (C.c_int, [_P, C.POINTER(SoupInitState)]),
     "soup_protonation_sweep": (C.c_int, [_P, C.POINTER(SoupSweepResult)]),

@@ -229,7 +229,10 @@ void upload_replica(Batch& b, uint32_t r, const SoupInitState* init, bool fresh_
   const uint32_t n = c.n, off = b.hsp[r].slot_off;
   std::vector<float> pos(4 * (size_t)n), vel(4 * (size_t)n), charge(n);
   std::vector<uint32_t> slots(3 * (size_t)n, NONE), center(n, NONE), held(n, 0), brng(n), trng(n), frozen32(n, 0);
-  if (fresh_allowed) host_fresh_state(c, pos.data(), vel.data(), frozen32.data(), brng.data(), trng.data());
+  // the fresh lattice (a few tens of ms at 483k beads) only when the given state leaves one of its
+  // arrays to it; its frozen flags are all zero in this build, as frozen32 already is
+  const bool complete = init && init->positions && init->velocities && init->bond_rng && init->thermo_rng;
+  if (fresh_allowed && !complete) host_fresh_state(c, pos.data(), vel.data(), frozen32.data(), brng.data(), trng.data());
   if (init) {
     if (init->positions) std::memcpy(pos.data(), init->positions, 16 * (size_t)n);
     if (init->velocities) std::memcpy(vel.data(), init->velocities, 16 * (size_t)n);
@@ -1392,6 +1395,23 @@ int soup_autotune(SoupHandle* h, uint32_t steps, SoupTuneResult* out) {
     res.tpp_before = (uint32_t)tpp0;
     res.walk_before = (uint32_t)walk0;
     if (out) *out = res;
+  });
+}
+
+int soup_apply_tuning(SoupHandle* h, const SoupTuneResult* t) {
+  return guarded(h, [&](Batch& b, uint32_t) {
+    if (!t) fail(SOUP_E_ARG, "NULL tuning");
+    if (t->tpp != 1 && t->tpp != 2 && t->tpp != 4 && t->tpp != 8) fail(SOUP_E_ARG, "tuning: tpp must be 1, 2, 4 or 8");
+    if (t->walk != 2 && t->walk != 3) fail(SOUP_E_ARG, "tuning: walk must be 2 or 3");
+    if (!(t->skin_scale > 0.0 && t->skin_scale <= 1.0)) fail(SOUP_E_ARG, "tuning: skin_scale must be in (0, 1]");
+    if (t->skin_scale != 1.0 && !b.cfg[0].rebuild_on_drift)
+      fail(SOUP_E_ARG, "tuning: the skin can only be scaled with drift-triggered rebuilds");
+    b.tpp = (int)t->tpp;
+    std::vector<double> sk(b.R);
+    for (uint32_t r = 0; r < b.R; ++r) sk[r] = b.cfg[r].skin * t->skin_scale;
+    tune_plan(b, sk, (int)t->walk);
+    force_pass(b);
+    SOUP_CUDA_TRY(cudaStreamSynchronize(b.stream));
   });
 }
 

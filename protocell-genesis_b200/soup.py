@@ -305,6 +305,11 @@ class SoupSystem:
         the state (see soup_autotune in include/soup_b200.h)."""
         return _autotune(self._lib, self._h, steps)
 
+    def apply_tuning(self, tuning: dict):
+        """Apply a result of autotune (tpp, walk, skin_scale) found on a system of the same shape,
+        without timing anything (soup_apply_tuning)."""
+        _apply_tuning(self._lib, self._h, tuning)
+
     # ---- Monte Carlo and analysis ----
     def protonation_sweep(self):
         r = _abi.SoupSweepResult()
@@ -476,6 +481,12 @@ def _box_ramp(from_box, target_box, ramp_steps: int):
     return out
 
 
+def _apply_tuning(lib, h, tuning):
+    r = _abi.SoupTuneResult()
+    r.tpp, r.walk, r.skin_scale = int(tuning["tpp"]), int(tuning["walk"]), float(tuning["skin_scale"])
+    _check(lib, h, lib.soup_apply_tuning(h, C.byref(r)))
+
+
 def _autotune(lib, h, steps):
     r = _abi.SoupTuneResult()
     _check(lib, h, lib.soup_autotune(h, int(steps), C.byref(r)))
@@ -539,6 +550,10 @@ class SoupBatch:
     def autotune(self, steps: int = 20) -> dict:
         """soup_autotune for the whole batch (through replica 0's handle, which addresses the batch)."""
         return _autotune(self._lib, self.replicas[0]._h, steps)
+
+    def apply_tuning(self, tuning: dict):
+        """soup_apply_tuning for the whole batch."""
+        _apply_tuning(self._lib, self.replicas[0]._h, tuning)
 
     def dispose(self):
         if getattr(self, "_h", None):

@@ -86,3 +86,25 @@ def test_tuned_batch_steps_like_its_replicas():
         assert np.abs(d).max() < 1e-2
         single.dispose()
     batch.dispose()
+
+
+def test_apply_tuning_reproduces_the_tuned_shape():
+    """soup_apply_tuning puts a fresh system in the shape a tuning found: from the tuned system's
+    state it then follows the tuned system's trajectory bit for bit."""
+    from helpers import charged_opts
+    opts = charged_opts(rebuild_on_drift=True)
+    a = SoupSystem(cfgm.resolve(opts, P))
+    a.relax_cold_start()
+    tune = a.autotune(steps=10)
+    arrays, sc = a.checkpoint_payload()
+    cfg_b = cfgm.resolve(opts, P)
+    cfg_b.protonation_rng = sc["protonationRng"]
+    b = SoupSystem(cfg_b, {k: v.copy() for k, v in arrays.items()})
+    b.apply_tuning(tune)
+    a.step(40)
+    b.step(40)
+    assert np.array_equal(a.particles().view(np.uint32), b.particles().view(np.uint32))
+    with pytest.raises(_abi.SoupError):
+        b.apply_tuning(dict(tune, tpp=3))
+    a.dispose()
+    b.dispose()
