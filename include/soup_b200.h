@@ -122,7 +122,10 @@ typedef struct SoupConfig {
   /* Schedule (soup/src/soup-integrate.ts:136-175) */
   uint64_t global_step;            /* starting step (resume.globalStep) */
   uint32_t chunk_steps;            /* steps per submission chunk; the reference uses 1000 */
-  uint32_t reserved[7];
+  uint32_t cell_divisor;            /* neighborGrid.cellDivisor: the plan's cell = interaction_range /
+                                      this (0 reads as 1); a live box change is refused, as
+                                      planSoupGrid refuses it, when the plan's grid is too small */
+  uint32_t reserved[6];
 } SoupConfig;
 
 /* Initial state: the resume arrays of CreateSoupOpts.resume (soup/src/soup-types.ts:145-178) plus

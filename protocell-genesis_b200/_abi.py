@@ -73,7 +73,7 @@ class SoupConfig(C.Structure):
         ("wall_radius", C.c_double), ("wall_k", C.c_double),
         ("global_step", C.c_uint64),
         ("chunk_steps", C.c_uint32),
-        ("reserved", C.c_uint32 * 7),
+        ("cell_divisor", C.c_uint32), ("reserved", C.c_uint32 * 6),
     ]
 
 

@@ -373,6 +373,7 @@ def resolve(opts: SoupOptions, P: Optional[dict] = None) -> _abi.SoupConfig:
             cfg.attr_scale[ci][cj] = table[ci][cj]
     cfg.acid_soap_scale = acid_soap_scale(P, opts.acid_soap_scale_override, opts.solvent_attraction_scale_override)
     cfg.interaction_range = plan.interaction_range
+    cfg.cell_divisor = int(P["neighborGrid"]["cellDivisor"])
     cfg.skin = skin
     cfg.list_range = plan.list_range
     cfg.rebuild_every = rebuild_every

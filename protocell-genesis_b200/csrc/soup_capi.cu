@@ -1239,8 +1239,28 @@ int soup_write_state(SoupHandle* h, const SoupInitState* st) {
 
 // resizeSoupGrid (soup/src/soup-buffers.ts:530-560): replica r's live box, its grid and the wall
 // radius that follows it (liveRadius, soup/src/soup-confine.ts:76-78), then the rebuild and force pass
-void apply_box(Batch& b, uint32_t r, const double box[3]) {
+// planSoupGrid's refusal (soup/src/soup-plan.ts:133-146): the grid of cells of side
+// interaction_range / cell_divisor needs 2 * ceil(list_range / cell) + 1 cells on every axis, and
+// the box twice the bend rest length
+void check_box(const SoupConfig& c, const double box[3]) {
   for (int a = 0; a < 3; ++a) if (!(box[a] > 0)) fail(SOUP_E_GEOMETRY, "box sides must be positive");
+  const double cell = c.interaction_range / (c.cell_divisor ? c.cell_divisor : 1u);
+  const int lwalk = (int)std::ceil(c.list_range / cell), min_cells = 2 * lwalk + 1;
+  int dims[3];
+  for (int a = 0; a < 3; ++a) dims[a] = std::max(1, (int)std::floor(box[a] / cell));
+  const double half = std::min(box[0], std::min(box[1], box[2])) / 2;
+  if (dims[0] < min_cells || dims[1] < min_cells || dims[2] < min_cells || !(half > c.r_bend)) {
+    char m[400];
+    std::snprintf(m, sizeof m,
+                  "neighbour grid: box=[%g,%g,%g] gives cellSize=%.4f, dims=[%d,%d,%d] and min(box)/2=%.4f; it needs "
+                  "dims>=%d (2*effectiveWalkRadius+1) on all three axes and min(box)/2 > bend.r0=%g",
+                  box[0], box[1], box[2], cell, dims[0], dims[1], dims[2], half, min_cells, c.r_bend);
+    fail(SOUP_E_GEOMETRY, m);
+  }
+}
+
+void apply_box(Batch& b, uint32_t r, const double box[3]) {
+  check_box(b.cfg[r], box);
   for (int a = 0; a < 3; ++a) b.cfg[r].box[a] = box[a];
   if (b.wall_r0[r] > 0) b.cfg[r].wall_radius = b.wall_r0[r] * (box[0] / b.wall_box0[r]);
   const SysParams old = b.hsp[r];
@@ -1302,6 +1322,9 @@ int soup_scale_box(SoupHandle* h, const double target_box[3], double cohesion_cu
     const int st = run_rigid_map(b, b.pos2, b.slots2, n, nullptr, 0, cohesion_cutoff, elig.empty() ? nullptr : elig.data(),
                                  old_box, target_box, b.force2, true, err);
     if (st) fail(st, err);
+    // planSoupGrid's refusal comes after the self-check, as in the reference (which throws it from
+    // resizeSoupGrid), but before any position moves
+    check_box(b.cfg[r], target_box);
     if (n) k_place_replica<<<(n + 255) / 256, 256, 0, b.stream>>>(b.force2, b.slot_of, off, n, b.pos);
     SOUP_CUDA_TRY(cudaGetLastError());
     b.launches += 2;

@@ -79,8 +79,9 @@ def test_device_map_equals_the_oracle(case):
 
 
 def _amphiphile_system():
-    """A bonded soup (the oracle run of tests/test_gpu_analysis.py) on the device."""
-    opts = plain_opts(box=[15, 15, 15], start={"C": 900, "O": 260, "H": 0, "M": 160, "W": 0})
+    """A bonded soup (the oracle's boosted bond chemistry, 400 steps) on the device, in a box that
+    leaves the grid room to shrink by 10% (planSoupGrid needs 5 cells of 2.947 sigma a side)."""
+    opts = plain_opts(box=[18, 18, 18], start={"C": 900, "O": 260, "H": 0, "M": 160, "W": 0})
     cfg = boosted(cfgm.resolve(opts, P), attempt=0.9, accept=1.0, brk=0.02)
     o = ob.OracleSystem(_abi, cfg)
     o.relax(30, 0.1)
@@ -169,4 +170,16 @@ def test_ramps_reach_the_target_box():
     g.grow_box_to(box, 2, 5)
     assert list(g.box) == box and g.steps == 25
     assert g.nonfinite_count() == dict(pos=0, vel=0)
+    g.dispose()
+
+
+def test_a_box_too_small_for_the_grid_is_refused_before_anything_moves():
+    """planSoupGrid's refusal (soup/src/soup-plan.ts:133-146) on a live box change: the same message,
+    and the positions and the box as they were (set_box and scale_box_once alike)."""
+    g = SoupSystem(cfgm.resolve(plain_opts(), P))   # box 16: 5 cells of 2.947 sigma, the minimum
+    p0, box = g.particles(), list(g.box)
+    for change in (lambda: g.set_box([14.0, 16.0, 16.0]), lambda: g.scale_box_once([14.0, 16.0, 16.0])):
+        with pytest.raises(_abi.SoupError, match=r"neighbour grid: box=\[14,16,16\] .* it needs dims>=5"):
+            change()
+        assert np.array_equal(g.particles(), p0) and list(g.box) == box
     g.dispose()
