@@ -82,3 +82,63 @@ def oracle_bilayer_start(lx=15.0, lz=16.0, per_side=10, seed=3, relax=200, steps
                  thermo_rng=o.read(ob.F_THERMO_RNG), charges=o.read(ob.F_CHARGES), frozen=o.read(ob.F_FROZEN))
     o.close()
     return cfg, start
+
+
+def config1_start(seed=0):
+    """The plain small case (16 sigma cube, 3,277 beads): 200 five-bead amphiphiles (head + 4 carbon,
+    straight along x, 0.95 sigma apart) on a 4 x 5 x 10 lattice, 2,277 water beads placed uniformly at
+    random at least 0.8 sigma from every bead, every head charged -1 and no constant-pH sweep
+    (lambda_D = 6.5 sigma, so I = (0.304 / (6.5 * 0.8))^2 M and rc_es = 0.45 L = 7.2 sigma), seed 0,
+    kT 1.  Slots as tests/water-bilayer.test.ts:113-118: head[0] = c1; c1[2] = head, c1[0] = c2;
+    c2 = (c1, c3); c3 = (c2, c4); c4[0] = c3.  Returns (options, start state)."""
+    L = 16.0
+    ion = (0.304 / (6.5 * 0.8)) ** 2
+    opts = cfgm.SoupOptions(box=[L, L, L], seed=seed, kT=1.0, start={"C": 800, "O": 200, "H": 0, "M": 0, "W": 2277},
+                            electrostatics={"enabled": True, "pH": 7.0, "ionicStrengthMolar": ion},
+                            sweep_every=10 ** 9)
+    P = cfgm.load_params()
+    kind = {m["id"]: k for k, m in enumerate(P["monomers"])}
+    pts, kinds = [], []
+    slots = []
+    for ix in range(4):
+        for iy in range(5):
+            for iz in range(10):
+                h = len(pts)
+                base = np.array([0.3 + ix * 4.0, 1.6 + iy * 3.2, 0.8 + iz * 1.6])
+                pts.append(base)
+                kinds.append(kind["O"])
+                for c in range(1, 5):
+                    pts.append(base + np.array([0.95 * c, 0.0, 0.0]))
+                    kinds.append(kind["C"])
+                s = [[h + 1, _abi.NONE, _abi.NONE], [h + 2, _abi.NONE, h], [h + 1, h + 3, _abi.NONE], [h + 2, h + 4, _abi.NONE],
+                     [h + 3, _abi.NONE, _abi.NONE]]
+                slots += s
+    rng = np.random.default_rng(seed)
+    cell = {}
+    def key(p):
+        return tuple((np.floor(p / 1.0).astype(int)) % 16)
+    for i, p in enumerate(pts):
+        cell.setdefault(key(p), []).append(i)
+    placed = [np.asarray(p) for p in pts]
+    while len(placed) < 3277:
+        p = rng.uniform(0, L, 3)
+        k = key(p)
+        ok = True
+        for dx in (-1, 0, 1):
+            for dy in (-1, 0, 1):
+                for dz in (-1, 0, 1):
+                    for j in cell.get(((k[0] + dx) % 16, (k[1] + dy) % 16, (k[2] + dz) % 16), []):
+                        d = placed[j] - p
+                        d -= np.round(d / L) * L
+                        if d @ d < 0.64:
+                            ok = False
+        if ok:
+            cell.setdefault(k, []).append(len(placed))
+            placed.append(p)
+            kinds.append(kind["W"])
+            slots.append([_abi.NONE, _abi.NONE, _abi.NONE])
+    pos = np.zeros((3277, 4), np.float32)
+    pos[:, :3] = np.mod(np.array(placed), L)
+    pos[:, 3] = kinds
+    q = np.where(pos[:, 3] == kind["O"], -1.0, 0.0).astype(np.float32)
+    return opts, {"positions": pos.reshape(-1), "bond_slots": np.array(slots, np.uint32).reshape(-1), "charges": q}

@@ -209,3 +209,31 @@ def test_sweep_head_force_recompute_is_exact(monkeypatch):
     assert np.array_equal(out["0"][1], out["1"][1])
     assert np.array_equal(out["0"][2], out["1"][2])
     assert not np.array_equal(st["charges"], out["0"][1])   # the sweeps flipped charges
+
+
+def test_plain_small_case_lists_forces_and_trajectory():
+    """The plain small case (3,277 beads, 200 charged amphiphiles, no sweep): lists equal the oracle's
+    sets, forces within 1e-5 relative RMS of FP64 on the thermalised state, and 100 steps follow the
+    oracle's trajectory.  (Right after the relax the forces nearly cancel: there the oracle's own FP32
+    restatement of the reference's arithmetic is 1.1e-5 from FP64; after 100 steps 1.6e-6.)"""
+    from helpers import config1_start
+    opts, st = config1_start()
+    cfg = cfgm.resolve(opts, P)
+    o = ob.OracleSystem(_abi, cfg, st)
+    o.relax(100, 0.1)
+    g = SoupSystem(cfg, oracle_state(o))     # both lists built from the relaxed positions
+    gc, gl = g.verlet_lists()
+    oc, ol = o.verlet()
+    assert np.array_equal(gc, oc) and np.array_equal(gl, ol)
+    o.step(100)                              # the oracle runs on from the relaxed state
+    t = SoupSystem(cfg, oracle_state(o))
+    assert rel_rms(t.forces(), o.forces64()) < 1e-5
+    t.dispose()
+    g.step(100)                              # the device from the same relaxed state
+    assert np.array_equal(g.rng_state()["thermo"], o.read(ob.F_THERMO_RNG))
+    pg_, po = g.particles().reshape(-1, 4), o.read(ob.F_POS).reshape(-1, 4)
+    d = pg_[:, :3] - po[:, :3]
+    d -= np.rint(d / cfg.box[0]) * cfg.box[0]
+    assert np.abs(d).max() < 1e-2
+    assert np.array_equal(g.charges(), o.read(ob.F_CHARGES))
+    g.dispose()
