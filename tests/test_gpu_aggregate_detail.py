@@ -78,3 +78,31 @@ def test_unwrap_and_cavity_equal_the_oracle(scenario):
     cell, radius = ST["closureCell"], ST["closureRadius"]
     assert g.local_cavity_volume(dev, cell, radius) == ob.local_cavity_volume(_abi, ref, cell, radius)
     g.dispose()
+
+
+def test_hollow_shell_with_water_is_closed_by_its_encapsulated_water():
+    """With water indices given, the vesicle flag follows the encapsulated water (isVesicleShape,
+    soup/src/aggregates.ts:307-315): water inside the shell is unreached by the flood from outside."""
+    pos, bonds, box = sc.hollow_shell()
+    rng = np.random.default_rng(3)
+    c = np.array([30.0, 30.0, 30.0])
+    d = rng.normal(size=(4000, 3))
+    d /= np.linalg.norm(d, axis=1)[:, None]
+    inside = c + d[:600] * (rng.uniform(0, 1, 600) ** (1 / 3) * 6.5)[:, None]
+    outside = c + d[600:] * rng.uniform(14.0, 28.0, 3400)[:, None]
+    w = np.zeros((4000, 4), np.float32)
+    w[:, :3] = np.concatenate([inside, outside])
+    w[:, 3] = next(k for k, m in enumerate(P["monomers"]) if m["solvent"])
+    allpos = np.concatenate([pos.reshape(-1, 4), w]).reshape(-1)
+    n = allpos.size // 4
+    kinds = allpos.reshape(-1, 4)[:, 3]
+    start = {"C": int((kinds == sc.KIND_C).sum()), "O": int((kinds == sc.KIND_O).sum()), "H": 0, "M": 0, "W": 4000}
+    opts = cfgm.SoupOptions(box=box, seed=1, kT=1.1, start=start, electrostatics={"enabled": False},
+                            verlet_override={"listCapacity": 2048})
+    g = SoupSystem(cfgm.resolve(opts, P), {"positions": allpos, "bond_slots": sc.slots_of(n, bonds)})
+    water = np.arange(pos.size // 4, n, dtype=np.uint32)
+    a = obs.analyze_aggregates(g, sc.cutoff(), water=water)
+    ew = a["aggregates"][0]["encapsulatedWater"]
+    assert ew is not None and ew["encapsulatedCount"] == 600 and ew["closed"]
+    assert a["hasVesicleAggregate"]
+    g.dispose()
