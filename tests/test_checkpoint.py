@@ -4,6 +4,7 @@ encoding, and an exact encode -> JSON -> decode round trip of a stepped oracle s
 import json
 
 import numpy as np
+import pytest
 
 import oracle_binding as ob
 from helpers import boosted
@@ -134,3 +135,23 @@ def test_resume_options_scale_the_wall_to_the_live_box():
     o = ck.resume_options(f)
     assert o.box == [30.0, 30.0, 30.0] and o.global_step == 7 and o.protonation_rng == 11
     assert o.confine["radiusSigma"] == 7.5 and o.start == {"C": 5, "W": 9}
+
+
+def test_a_file_from_before_the_charges_resumes_with_fresh_charges():
+    """A CheckpointFile written before chargesB64 / protonationRng existed (checkpoint.ts:163-171:
+    both optional): decoding gives None for them, and the resumed system takes its charges and
+    protonation chain from the fresh-start rule (initialCharges)."""
+    o, cfg = _stepped_oracle()
+    f = ck.encode_checkpoint(OracleCheckpointable(o, cfg), CONFIG)
+    del f["chargesB64"], f["protonationRng"]
+    r = ck.decode_checkpoint_resume(json.loads(json.dumps(f)))
+    assert r["charges"] is None and r["protonationRng"] is None
+    st = ck.resume_state(r)
+    assert "charges" not in st
+    opts = ck.resume_options(f, r)
+    assert opts.protonation_rng is None
+
+
+def test_unknown_version_is_refused():
+    with pytest.raises(ValueError, match="version"):
+        ck.decode_checkpoint_resume({"version": 2})
