@@ -183,3 +183,23 @@ def test_a_box_too_small_for_the_grid_is_refused_before_anything_moves():
             change()
         assert np.array_equal(g.particles(), p0) and list(g.box) == box
     g.dispose()
+
+
+def test_wall_radius_follows_the_live_box():
+    """resizeSoupGrid rewrites the wall with liveRadius (soup/src/soup-buffers.ts:551,
+    soup/src/soup-confine.ts:76-78): after set_box the force equals the oracle's for a system created
+    in that box with the wall radius scaled the same way."""
+    from helpers import confined_opts, rel_rms
+    cfg = cfgm.resolve(confined_opts(), P)
+    o = ob.OracleSystem(_abi, cfg)
+    o.relax(20, 0.1)
+    st = dict(positions=o.read(ob.F_POS), velocities=o.read(ob.F_VEL), charges=o.read(ob.F_CHARGES))
+    g = SoupSystem(cfg, st)
+    g.set_box([88.0, 88.0, 88.0])
+    cfg2 = cfgm.resolve(confined_opts(box=[88, 88, 88], confine={"radiusSigma": 16 * 1.1, "stiffness": 100}), P)
+    o2 = ob.OracleSystem(_abi, cfg2, st)
+    assert rel_rms(g.forces(), o2.forces64()) < 1e-5
+    # the wall acts: beads beyond the scaled radius from the new centre feel it
+    p = st["positions"].reshape(-1, 4)[:, :3].astype(np.float64)
+    assert (np.linalg.norm(p - 44.0, axis=1) > 17.6).any()
+    g.dispose()
