@@ -388,6 +388,22 @@ int soup_aggregate_unwrap(SoupHandle* h, const uint32_t* members, uint32_t n_mem
 int soup_local_cavity_volume(SoupHandle* h, const float* positions, uint32_t n, double cell, double radius,
                              double* volume);
 
+/* enclosedVolume (engine/src/closure.ts:51-163: dimsFor, occupancy, floodOutside, enclosedVolume)
+ * on the grid of this system's live box: cells of side `cell`, x and y periodic, z open; cells
+ * within `radius` of a bead occupied; the empty cells the flood from the grid's faces does not reach,
+ * times cell^3.  The positions (f32 x4) are taken as given; enclosedVolumeFromPositions
+ * (closure.ts:315-323) recentres them on the largest cluster first, which the caller does with
+ * soup_cluster_labels. */
+int soup_box_cavity_volume(SoupHandle* h, const float* positions, uint32_t n, double cell, double radius,
+                           double* volume);
+
+/* buildClusterUnionFind (engine/src/aggregate.ts:65-130) with its periodicZ switch: labels as
+ * soup_aggregate_labels (the minimum original index of each component), x and y periodic, z periodic
+ * only when periodic_z is non-zero (largestClusterCenter, aggregate.ts:157-190, clusters with z open).
+ * soup_aggregate_labels is this call with periodic_z = 1. */
+int soup_cluster_labels(SoupHandle* h, const uint32_t* member_idx, uint32_t n_members, double cutoff, int periodic_z,
+                        uint32_t* labels, uint32_t* n_components);
+
 /* densityProfileZ (engine/src/metrics.ts:21-47): histogram of the beads' z over [0, box_z) in
  * `bins` bins, split into heads (kinds whose bit is set in head_kind_mask) and tails (the rest).
  * The soup profiles polar kinds as heads (soup/src/aggregates.ts:95-109); the engine's own

@@ -26,8 +26,10 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <map>
 #include <numeric>
 #include <string>
+#include <tuple>
 #include <type_traits>
 #include <vector>
 #ifdef _OPENMP
@@ -1696,6 +1698,9 @@ int oracle_unwrap_aggregate(const float* pos, const uint32_t* members, uint32_t 
 // localCavityVolume (soup/src/aggregates.ts:350-385) over occupancy (engine/src/closure.ts:67-107: x
 // and y wrap, z open) and enclosedVolume/floodOutside (closure.ts:108-163: breadth-first from every
 // empty cell on the six faces, open boundary); unreached empty cells times cell^3
+static double cavity_on_grid(const float* sh, uint32_t n, const double box[3], const int dims[3], double cell,
+                             double radius);
+
 double oracle_local_cavity_volume(const float* positions, uint32_t n, double cell, double radius) {
   if (n == 0) return 0.0;
   double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
@@ -1715,6 +1720,13 @@ double oracle_local_cavity_volume(const float* positions, uint32_t n, double cel
   }
   for (uint32_t i = 0; i < n; ++i)
     for (int a = 0; a < 3; ++a) sh[4 * (size_t)i + a] = (float)((double)positions[4 * (size_t)i + a] + (pad - lo[a]));
+  return cavity_on_grid(sh.data(), n, box, dims, cell, radius);
+}
+
+// engine/src/closure.ts:51-163 occupancy (x, y periodic, z open) + floodOutside + enclosedVolume on
+// the grid `dims` of `box`, positions as given
+static double cavity_on_grid(const float* sh, uint32_t n, const double box[3], const int dims[3], double cell,
+                             double radius) {
   const int nx = dims[0], ny = dims[1], nz = dims[2];
   const size_t nc = (size_t)nx * ny * nz;
   std::vector<uint8_t> occ(nc, 0), vis(nc, 0);
@@ -1759,6 +1771,68 @@ double oracle_local_cavity_volume(const float* positions, uint32_t n, double cel
   size_t unreached = 0;
   for (size_t i = 0; i < nc; ++i) unreached += (!occ[i] && !vis[i]) ? 1 : 0;
   return (double)unreached * cell * cell * cell;
+}
+
+// engine/src/closure.ts:315-323 enclosedVolumeFromPositions after its recentring: the grid of the
+// periodic box (dimsFor, closure.ts:51-57), positions as given
+double oracle_box_cavity_volume(const float* positions, uint32_t n, const double box[3], double cell, double radius) {
+  if (n == 0) return 0.0;
+  int dims[3];
+  for (int a = 0; a < 3; ++a) dims[a] = std::max(1, (int)std::ceil(box[a] / cell));
+  return cavity_on_grid(positions, n, box, dims, cell, radius);
+}
+
+// engine/src/aggregate.ts:65-130 buildClusterUnionFind with its periodicZ switch, binned as the
+// reference bins: with z open the z cell is floor(z / cutoff), unwrapped and unbounded, and the z
+// neighbours are not wrapped.  Labels: the minimum original index of each component.
+uint32_t oracle_cluster_labels(const float* pos, const uint32_t* mem, uint32_t m, const double box[3], double cutoff,
+                               int periodic_z, uint32_t* labels) {
+  if (periodic_z) return aggregates(pos, mem, m, box, cutoff, labels);
+  std::vector<uint32_t> parent(m);
+  std::iota(parent.begin(), parent.end(), 0u);
+  auto find = [&](uint32_t x) { while (parent[x] != x) { parent[x] = parent[parent[x]]; x = parent[x]; } return x; };
+  const int nx = std::max(1, (int)std::floor(box[0] / cutoff)), ny = std::max(1, (int)std::floor(box[1] / cutoff));
+  const double wx = box[0] / nx, wy = box[1] / ny, wz = cutoff;
+  std::vector<int> cx(m), cy(m);
+  std::vector<long long> cz(m);
+  std::map<std::tuple<int, int, long long>, std::vector<uint32_t>> buckets;
+  for (uint32_t k = 0; k < m; ++k) {
+    const uint32_t i = mem[k];
+    cx[k] = std::min(nx - 1, (int)std::floor(wrap1(pos[i * 4], box[0]) / wx));
+    cy[k] = std::min(ny - 1, (int)std::floor(wrap1(pos[i * 4 + 1], box[1]) / wy));
+    cz[k] = (long long)std::floor((double)pos[i * 4 + 2] / wz);
+    buckets[std::make_tuple(cx[k], cy[k], cz[k])].push_back(k);
+  }
+  const double c2 = cutoff * cutoff;
+  for (uint32_t k = 0; k < m; ++k) {
+    const uint32_t i = mem[k];
+    for (int dx = -1; dx <= 1; ++dx) {
+      const int ax = ((cx[k] + dx) % nx + nx) % nx;
+      for (int dy = -1; dy <= 1; ++dy) {
+        const int ay = ((cy[k] + dy) % ny + ny) % ny;
+        for (int dz = -1; dz <= 1; ++dz) {
+          auto it = buckets.find(std::make_tuple(ax, ay, cz[k] + dz));
+          if (it == buckets.end()) continue;
+          for (uint32_t l : it->second) {
+            if (l <= k) continue;
+            const uint32_t j = mem[l];
+            const double ddx = mi1((double)pos[i * 4] - pos[j * 4], box[0]);
+            const double ddy = mi1((double)pos[i * 4 + 1] - pos[j * 4 + 1], box[1]);
+            const double ddz = (double)pos[i * 4 + 2] - pos[j * 4 + 2];
+            if (ddx * ddx + ddy * ddy + ddz * ddz <= c2) {
+              const uint32_t ra = find(k), rb = find(l);
+              if (ra != rb) parent[ra] = rb;
+            }
+          }
+        }
+      }
+    }
+  }
+  std::vector<uint32_t> minIdx(m, NONE);
+  for (uint32_t k = 0; k < m; ++k) { const uint32_t r = find(k); minIdx[r] = std::min(minIdx[r], mem[k]); }
+  uint32_t ncomp = 0;
+  for (uint32_t k = 0; k < m; ++k) { labels[k] = minIdx[find(k)]; if (find(k) == k) ncomp++; }
+  return ncomp;
 }
 
 // proximityPairs (soup/src/soup-box-scale-math.ts:162-221): pairs i < j among the eligible beads with

@@ -180,6 +180,8 @@ SIGNATURES = {
     "soup_scale_box": (C.c_int, [_P, C.POINTER(C.c_double), C.c_double, _U32P, C.c_uint32]),
     "soup_aggregate_unwrap": (C.c_int, [_P, _U32P, C.c_uint32, _P]),
     "soup_local_cavity_volume": (C.c_int, [_P, _P, C.c_uint32, C.c_double, C.c_double, C.POINTER(C.c_double)]),
+    "soup_box_cavity_volume": (C.c_int, [_P, _P, C.c_uint32, C.c_double, C.c_double, C.POINTER(C.c_double)]),
+    "soup_cluster_labels": (C.c_int, [_P, _U32P, C.c_uint32, C.c_double, C.c_int, _U32P, C.POINTER(C.c_uint32)]),
     "soup_scale_molecules_rigid": (C.c_int, [_P, _P, C.c_uint32, _U32P, C.c_uint32, C.POINTER(C.c_double),
                                              C.POINTER(C.c_double), _P]),
     "soup_write_charges": (C.c_int, [_P, _P, _SZ]),

@@ -214,7 +214,10 @@ __global__ void k_amph_label(uint32_t n, uint32_t* __restrict__ parent, const ui
   if (ok && r == i) atomicAdd(count, 1u);
 }
 
-// buildClusterUnionFind (aggregate.ts:65-130), periodic on all three axes; one thread per member
+// buildClusterUnionFind (aggregate.ts:65-130); one thread per member.  With periodic_z = 0 the z
+// separation is the raw difference (the reference's periodicZ = false).  The binning stays the
+// wrapped periodic grid: cells are at least `cutoff` wide, so a pair within the cutoff in raw z lies
+// in neighbouring wrapped cells, and the raw difference rejects the pairs the wrap brings together.
 __global__ void k_agg_bin(const float4* __restrict__ pos, const uint32_t* __restrict__ slot_of, uint32_t off,
                           const uint32_t* __restrict__ mem, uint32_t m, Grid g, double wx, double wy, double wz,
                           uint32_t* __restrict__ cell, uint32_t* __restrict__ count) {
@@ -238,7 +241,7 @@ __global__ void k_agg_scatter(const uint32_t* __restrict__ cell, uint32_t m, con
 __global__ void k_agg_union(const float4* __restrict__ pos, const uint32_t* __restrict__ slot_of, uint32_t off,
                             const uint32_t* __restrict__ mem, uint32_t m, Grid g, const uint32_t* __restrict__ cell,
                             const uint32_t* __restrict__ start, const uint32_t* __restrict__ sorted, double c2,
-                            uint32_t* __restrict__ parent) {
+                            int periodic_z, uint32_t* __restrict__ parent) {
   const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= m) return;
   const float4 pi = pos[slot_of[off + mem[k]]];
@@ -257,7 +260,8 @@ __global__ void k_agg_union(const float4* __restrict__ pos, const uint32_t* __re
           const float4 pj = pos[slot_of[off + mem[l]]];
           const double ddx = mi1(__dsub_rn((double)pi.x, (double)pj.x), g.box[0]);
           const double ddy = mi1(__dsub_rn((double)pi.y, (double)pj.y), g.box[1]);
-          const double ddz = mi1(__dsub_rn((double)pi.z, (double)pj.z), g.box[2]);
+          const double rz = __dsub_rn((double)pi.z, (double)pj.z);
+          const double ddz = periodic_z ? mi1(rz, g.box[2]) : rz;
           if (sq3(ddx, ddy, ddz) <= c2) uf_union(parent, k, l);
         }
       }
@@ -441,7 +445,7 @@ int run_amphiphiles(Batch& b, uint32_t r, uint32_t* head_of, uint32_t* n_out, st
 }
 
 int run_aggregates(Batch& b, uint32_t r, const uint32_t* mem, uint32_t m, double cutoff, uint32_t* labels,
-                   uint32_t* ncomp, std::string& err) {
+                   uint32_t* ncomp, std::string& err, bool periodic_z) {
   const SoupConfig& c = b.cfg[r];
   const uint32_t n = c.n, off = b.hsp[r].slot_off;
   for (uint32_t k = 0; k < m; ++k) if (mem[k] >= n) { err = "aggregates: member index out of range"; return SOUP_E_ARG; }
@@ -477,7 +481,8 @@ int run_aggregates(Batch& b, uint32_t r, const uint32_t* mem, uint32_t m, double
   k_agg_scatter<<<nblocks(m), kBlock, 0, st>>>(cell, m, start, cursor, sorted);
   k_iota<<<nblocks(m), kBlock, 0, st>>>(parent, m);
   k_fill<<<nblocks(m), kBlock, 0, st>>>(minidx, m, NONE);
-  k_agg_union<<<nblocks(m), kBlock, 0, st>>>(b.pos, b.slot_of, off, dmem, m, g, cell, start, sorted, cutoff * cutoff, parent);
+  k_agg_union<<<nblocks(m), kBlock, 0, st>>>(b.pos, b.slot_of, off, dmem, m, g, cell, start, sorted, cutoff * cutoff,
+                                             periodic_z ? 1 : 0, parent);
   k_agg_min<<<nblocks(m), kBlock, 0, st>>>(dmem, m, parent, minidx, cnt);
   k_agg_label<<<nblocks(m), kBlock, 0, st>>>(dmem, m, parent, minidx, dl);
   SOUP_CUDA_TRY(cudaMemcpyAsync(labels, dl, 4 * (size_t)m, cudaMemcpyDeviceToHost, st));

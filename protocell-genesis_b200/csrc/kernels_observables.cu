@@ -343,10 +343,11 @@ int run_unwrap(Batch& b, uint32_t r, const uint32_t* members, uint32_t m, float*
 // padded by 4 radii, shifted to start at the pad (f32 positions, as the reference's Float32Array),
 // its occupancy and the empty cells the open-boundary flood does not reach, times cell^3
 int run_local_cavity(Batch& b, const float* positions, uint32_t n, double cell, double radius, double* volume,
-                     std::string& err) {
+                     std::string& err, const double* frame_box) {
+  const std::string who = frame_box ? "enclosedVolume: " : "localCavityVolume: ";
   *volume = 0.0;
-  if (n == 0) return SOUP_OK;
-  if (!(cell > 0) || !(radius >= 0)) { err = "localCavityVolume: cell must be positive and radius non-negative"; return SOUP_E_ARG; }
+  if (n == 0) return SOUP_OK;   // nothing occupied: every empty cell is reached
+  if (!(cell > 0) || !(radius >= 0)) { err = who + "cell must be positive and radius non-negative"; return SOUP_E_ARG; }
   double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
   for (uint32_t i = 0; i < n; ++i)
     for (int a = 0; a < 3; ++a) {
@@ -360,13 +361,19 @@ int run_local_cavity(Batch& b, const float* positions, uint32_t n, double cell, 
   uint64_t nc = 1;
   double shift[3];
   for (int a = 0; a < 3; ++a) {
-    if (!std::isfinite(lo[a]) || !std::isfinite(hi[a])) { err = "localCavityVolume: non-finite position"; return SOUP_E_ARG; }
-    shift[a] = pad - lo[a];
-    g.box[a] = hi[a] - lo[a] + 2 * pad;
+    if (!std::isfinite(lo[a]) || !std::isfinite(hi[a])) { err = who + "non-finite position"; return SOUP_E_ARG; }
+    if (frame_box) {   // closure.ts:51-57 dimsFor over the periodic box, no shift
+      if (!(frame_box[a] > 0)) { err = who + "the box must be positive"; return SOUP_E_ARG; }
+      shift[a] = 0.0;
+      g.box[a] = frame_box[a];
+    } else {
+      shift[a] = pad - lo[a];
+      g.box[a] = hi[a] - lo[a] + 2 * pad;
+    }
     g.n[a] = std::max(1, (int)std::ceil(g.box[a] / cell));
     nc *= (uint64_t)g.n[a];
   }
-  if (nc > (uint64_t)1 << 31) { err = "localCavityVolume: the local grid is too large"; return SOUP_E_ARG; }
+  if (nc > (uint64_t)1 << 31) { err = who + "the grid is too large"; return SOUP_E_ARG; }
   std::vector<float> sh(4 * (size_t)n);
   for (uint32_t i = 0; i < n; ++i) {
     for (int a = 0; a < 3; ++a) sh[4 * (size_t)i + a] = (float)((double)positions[4 * (size_t)i + a] + shift[a]);
@@ -392,7 +399,7 @@ int run_local_cavity(Batch& b, const float* positions, uint32_t n, double cell, 
   uint32_t ch = 1;
   uint64_t passes = 0;
   while (ch) {
-    if (++passes > nc + 1) { err = "localCavityVolume: the flood did not finish"; return SOUP_E_STATE; }
+    if (++passes > nc + 1) { err = who + "the flood did not finish"; return SOUP_E_STATE; }
     SOUP_CUDA_TRY(cudaMemsetAsync(changed, 0, 4, st));
     k_local_flood<<<fgrid, kBlock, 0, st>>>(occ, vis, g, nc, changed);
     SOUP_CUDA_TRY(cudaMemcpyAsync(&ch, changed, 4, cudaMemcpyDeviceToHost, st));

@@ -1777,6 +1777,26 @@ int soup_local_cavity_volume(SoupHandle* h, const float* positions, uint32_t n, 
   });
 }
 
+int soup_box_cavity_volume(SoupHandle* h, const float* positions, uint32_t n, double cell, double radius,
+                           double* volume) {
+  return guarded(h, [&](Batch& b, uint32_t r) {
+    if ((n && !positions) || !volume) fail(SOUP_E_ARG, "enclosedVolume: NULL argument");
+    std::string err;
+    const int st = run_local_cavity(b, positions, n, cell, radius, volume, err, b.cfg[r].box);
+    if (st) fail(st, err);
+  });
+}
+
+int soup_cluster_labels(SoupHandle* h, const uint32_t* member_idx, uint32_t n_members, double cutoff, int periodic_z,
+                        uint32_t* labels, uint32_t* n_components) {
+  return guarded(h, [&](Batch& b, uint32_t r) {
+    if ((n_members && (!member_idx || !labels)) || !(cutoff > 0)) fail(SOUP_E_ARG, "bad argument");
+    std::string err;
+    int st = run_aggregates(b, r, member_idx, n_members, cutoff, labels, n_components, err, periodic_z != 0);
+    if (st) fail(st, err);
+  });
+}
+
 int soup_density_profile_z(SoupHandle* h, uint32_t bins, uint32_t head_kind_mask, uint32_t* head_counts,
                            uint32_t* tail_counts, uint32_t* escaped) {
   return guarded(h, [&](Batch& b, uint32_t r) {

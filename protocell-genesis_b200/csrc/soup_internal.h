@@ -254,12 +254,14 @@ int run_profile_z(Batch& b, uint32_t r, uint32_t bins, uint32_t head_mask, uint3
                   uint32_t* escaped, std::string& err);
 int run_pairing(Batch& b, uint32_t r, double contact, uint32_t out5[5], std::string& err);
 int run_unwrap(Batch& b, uint32_t r, const uint32_t* members, uint32_t m, float* out, std::string& err);
+// frame_box null: localCavityVolume's padded frame around the positions; otherwise the grid of
+// that box (closure.ts dimsFor + occupancy + enclosedVolume), positions taken as given
 int run_local_cavity(Batch& b, const float* positions, uint32_t n, double cell, double radius, double* volume,
-                     std::string& err);
+                     std::string& err, const double* frame_box = nullptr);
 int run_shapes(Batch& b, uint32_t r, const uint32_t* members_csr, const uint32_t* start, uint32_t ncomp,
                double* out10, std::string& err);
 int run_aggregates(Batch& b, uint32_t r, const uint32_t* mem, uint32_t nm, double cutoff, uint32_t* labels,
-                   uint32_t* ncomp, std::string& err);
+                   uint32_t* ncomp, std::string& err, bool periodic_z = true);
 // host
 void host_fresh_state(const SoupConfig& c, float* pos, float* vel, uint32_t* frozen, uint32_t* brng, uint32_t* trng);
 void host_initial_charges(const SoupConfig& c, const float* pos, float* charges, uint32_t* prot_rng);

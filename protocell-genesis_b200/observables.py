@@ -348,7 +348,156 @@ def analyze_aggregates(system, cutoff, detail_count=None, min_amphiphiles_per_ag
             "hasVesicleAggregate": any(is_vesicle_shape(a, t) for a in detail)}
 
 
+STAGES = ("monomers", "amphiphiles", "micelles", "bilayer", "vesicle")
+
+
+def _js_round(x):
+    """JavaScript Math.round on float64: to the nearest integer, halves toward +infinity."""
+    f = np.floor(x)
+    return f + ((x - f) >= 0.5)
+
+
+def _wrap1(v, box):
+    return v - np.floor(v / box) * box
+
+
+def largest_cluster_shift(positions, labels, box):
+    """largestClusterShift + largestClusterCenter (engine/src/closure.ts:291-296,
+    engine/src/aggregate.ts:157-190) from the members' component labels, in the members' order: the
+    largest component (ties to the one met first), its x, y centre as minimum-image offsets from its
+    first member summed in order, its plain z mean; the shift that puts that centre at the box's
+    middle.  positions: f32 x4 of the members in that order."""
+    p = np.asarray(positions, np.float32).reshape(-1, 4).astype(np.float64)
+    lab = np.asarray(labels)
+    if lab.size == 0:
+        raise ValueError("largestClusterCenter: empty set of beads")
+    uniq, first, size = np.unique(lab, return_index=True, return_counts=True)
+    best = uniq[min(range(uniq.size), key=lambda c: (-int(size[c]), int(first[c])))]
+    idx = np.nonzero(lab == best)[0]
+    box = [float(b) for b in box]
+    ref_x, ref_y = p[idx[0], 0], p[idx[0], 1]
+    dx = p[idx, 0] - ref_x
+    dy = p[idx, 1] - ref_y
+    sx = np.cumsum(dx - _js_round(dx / box[0]) * box[0])[-1]   # sequential, as the reference sums
+    sy = np.cumsum(dy - _js_round(dy / box[1]) * box[1])[-1]
+    sz = np.cumsum(p[idx, 2])[-1]
+    n = float(idx.size)
+    com = (_wrap1(ref_x + sx / n, box[0]), _wrap1(ref_y + sy / n, box[1]), sz / n)
+    return (box[0] / 2 - com[0], box[1] / 2 - com[1], box[2] / 2 - com[2])
+
+
+def recenter_positions(positions, shift, box):
+    """recenterOnLargestCluster's translation (engine/src/closure.ts:298-309): x, y shifted and wrapped,
+    z shifted only, in float64 and stored as f32."""
+    p = np.asarray(positions, np.float32).reshape(-1, 4)
+    out = p.copy()
+    for a in range(2):
+        out[:, a] = _wrap1(p[:, a].astype(np.float64) + shift[a], float(box[a])).astype(np.float32)
+    out[:, 2] = (p[:, 2].astype(np.float64) + shift[2]).astype(np.float32)
+    return out.reshape(-1)
+
+
+def enclosed_volume_from_positions(system, members, particles, cell, radius):
+    """enclosedVolumeFromPositions (engine/src/closure.ts:315-323) over the given member beads of a
+    device system: clustered with z open at the tail-tail attraction range (closure.ts:291-296) on the
+    device, recentred on the largest cluster, then the box-grid occupancy and flood on the device."""
+    P = _config.load_params()
+    m = np.ascontiguousarray(members, np.uint32)
+    if m.size == 0:
+        return 0.0
+    cutoff = _config.wca_cutoff(P["params"]["beadSizes"]["tail_tail"]) + P["params"]["wc"]
+    _, labels = system.cluster_labels(m, cutoff, periodic_z=False)
+    pos = np.asarray(particles, np.float32).reshape(-1, 4)[m]
+    box = system.box
+    shift = largest_cluster_shift(pos, labels, box)
+    return system.box_cavity_volume(recenter_positions(pos, shift, box), cell, radius)
+
+
+def load_stage_thresholds():
+    """loadStageThresholds (soup/src/stages.ts:130-170): the stage thresholds of the parameter
+    tables.  The tables are generated from the reference's data files, so the two cross-checks the
+    reference makes there (the closure minimum against the literature table, and the minimum
+    amphiphiles per aggregate against its formula) held when they were written."""
+    return dict(_config.load_params()["stageThresholds"])
+
+
+def stage_from_evidence(evidence, thresholds):
+    """stageFromEvidence (soup/src/stages.ts:184-202): every stage above monomers needs the amphiphile
+    fraction; vesicle, bilayer and micelles are then checked in that order on the per-aggregate
+    analysis."""
+    a = evidence["aggregateAnalysis"]
+    amphiphile_ok = evidence["amphiphileFraction"] >= thresholds["amphiphileFraction"]
+    micelle_ok = (amphiphile_ok and a["qualifyingAggregateCount"] >= thresholds["minMicelleAggregates"]
+                  and a["amphiphileShareInQualifying"] >= thresholds["minAmphiphileShareInAggregates"])
+    if amphiphile_ok and a["hasVesicleAggregate"]:
+        return "vesicle"
+    if amphiphile_ok and a["hasLamellarAggregate"]:
+        return "bilayer"
+    if micelle_ok:
+        return "micelles"
+    if amphiphile_ok:
+        return "amphiphiles"
+    return "monomers"
+
+
+def _member_order(head_of, members):
+    """memberIndicesOf (soup/src/aggregates.ts:122-129) order: amphiphiles by the smallest index of
+    their component (findAmphiphiles' order), each as its head then its other members.  The reference
+    lists a chain in walk order; ascending order here changes only the rounding of the recentring's
+    centre sum, whose first member (the head) is the same."""
+    heads = head_of[members]
+    uh, first = np.unique(heads, return_index=True)
+    rank = np.empty(uh.size, np.int64)
+    rank[np.argsort(first)] = np.arange(uh.size)
+    group = rank[np.searchsorted(uh, heads)]
+    not_head = (heads != members).astype(np.int64)
+    return members[np.lexsort((members, not_head, group))]
+
+
+def detect_stage(system, thresholds=None, parcel=None):
+    """detectStage (soup/src/stages.ts:204-289) on a device system: {"stage", "evidence"} with the
+    amphiphile fraction (carbon beads in a recognised chain over all carbon beads), the largest
+    aggregate's share of the amphiphile members (z periodic), the box-wide head-peak count and
+    enclosed volume (diagnostics), and analyzeAggregates with the water beads.  `parcel`: {"centre",
+    "radius"} of a confined run (stages.ts:274-279 reads it off the system's live confinement)."""
+    P = _config.load_params()
+    t = load_stage_thresholds()
+    t.update(thresholds or {})
+    mon = P["monomers"]
+    particles = system.particles()
+    kinds = np.rint(np.asarray(particles, np.float32).reshape(-1, 4)[:, 3]).astype(np.int64)
+    n_amph, head_of = system.amphiphile_labels()
+    members = np.nonzero(head_of != 0xFFFFFFFF)[0].astype(np.uint32)
+    carbon = [k for k, m in enumerate(mon) if m["kind"] == "carbon"]
+    total_carbon = int(np.isin(kinds, carbon).sum())
+    in_chains = int(members.size) - int(n_amph)
+    radii = [m["radiusSigma"] for m in mon if m["kind"] in ("carbon", "head")]
+    cutoff = _config.wca_cutoff(P["params"]["sigma"] * max(radii)) + P["params"]["wc"]
+    largest = 0.0
+    enclosed = 0.0
+    if members.size:
+        _, lab = system.aggregate_labels(members, cutoff)
+        largest = float(np.unique(lab, return_counts=True)[1].max()) / members.size
+        enclosed = enclosed_volume_from_positions(system, _member_order(head_of, members), particles,
+                                                  t["closureCell"], t["closureRadius"])
+    polar = [bool(m["polar"]) for m in mon]
+    peaks = compute_head_peaks(particles, system.box, polar, t["headDensityBins"], t["minHeadsPerBin"],
+                               t["headPeakSeparationMin"], t["headPeakSeparationMax"])
+    water_kind = next((k for k, m in enumerate(mon) if m.get("solvent")), None)
+    water = None if water_kind is None else np.nonzero(kinds == water_kind)[0].astype(np.uint32)
+    analysis = analyze_aggregates(system, cutoff, thresholds=t,
+                                  water=water if water is not None and water.size else None, parcel=parcel)
+    evidence = {"amphiphileFraction": in_chains / total_carbon if total_carbon > 0 else 0.0,
+                "largestAggregateFraction": largest, "headPeaks": peaks, "enclosedVolume": enclosed,
+                "aggregateAnalysis": analysis}
+    return {"stage": stage_from_evidence(evidence, t), "evidence": evidence}
+
+
 # reference-style names
+loadStageThresholds = load_stage_thresholds
+stageFromEvidence = stage_from_evidence
+detectStage = detect_stage
+enclosedVolumeFromPositions = enclosed_volume_from_positions
 areaPerLipid = area_per_lipid
 sumProfiles = sum_profiles
 centerMembraneZ = center_membrane_z

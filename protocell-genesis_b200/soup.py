@@ -418,6 +418,26 @@ class SoupSystem:
                                                                       float(radius), C.byref(v)))
         return v.value
 
+    def box_cavity_volume(self, positions, cell, radius):
+        """enclosedVolume (engine/src/closure.ts:51-163) of f32 x4 positions on the grid of the live box
+        (x, y periodic, z open), on the device; the positions are taken as given."""
+        p = np.ascontiguousarray(positions, np.float32)
+        v = C.c_double()
+        _check(self._lib, self._h, self._lib.soup_box_cavity_volume(self._h, _ptr(p), p.size // 4, float(cell),
+                                                                    float(radius), C.byref(v)))
+        return v.value
+
+    def cluster_labels(self, members, cutoff, periodic_z=True):
+        """buildClusterUnionFind (engine/src/aggregate.ts:65-130) over the members on the device, z
+        periodic or open: (components, labels = the minimum original index of each component)."""
+        m = np.ascontiguousarray(members, np.uint32)
+        labels = np.empty(m.size, np.uint32)
+        nc = C.c_uint32()
+        _check(self._lib, self._h, self._lib.soup_cluster_labels(
+            self._h, m.ctypes.data_as(_abi._U32P), m.size, float(cutoff), int(bool(periodic_z)),
+            labels.ctypes.data_as(_abi._U32P), C.byref(nc)))
+        return int(nc.value), labels
+
     # ---- differentiation (the adjoint of the step; no counterpart in the reference) ----
     def get_diff_params(self):
         t = (C.c_double * _abi.DIFF_NPARAM)()

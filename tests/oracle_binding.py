@@ -71,6 +71,8 @@ def lib(abi):
         "oracle_closure_in_parcel": (C.c_int, [P, P, C.c_uint32, P, C.c_uint32, P, P, C.c_double, C.c_double,
                                                C.c_double, P, C.c_double, C.POINTER(abi.SoupClosureResult)]),
         "oracle_local_cavity_volume": (C.c_double, [P, C.c_uint32, C.c_double, C.c_double]),
+        "oracle_box_cavity_volume": (C.c_double, [P, C.c_uint32, P, C.c_double, C.c_double]),
+        "oracle_cluster_labels": (C.c_uint32, [P, P, C.c_uint32, P, C.c_double, C.c_int, P]),
         "oracle_proximity_pairs": (C.c_int, [P, C.c_uint32, P, C.c_double, P, P, C.c_size_t,
                                              C.POINTER(C.c_size_t)]),
     }
@@ -373,3 +375,20 @@ def closure_in_parcel(abi, pos, members, water, box, centre, cell, radius, vmin,
     if st != 0:
         raise RuntimeError(L.oracle_last_error().decode())
     return r
+
+
+def box_cavity_volume(abi, positions, box, cell, radius):
+    """enclosedVolume on the periodic box's grid (closure.ts:51-163), positions as given."""
+    p = np.ascontiguousarray(positions, np.float32)
+    return lib(abi).oracle_box_cavity_volume(_ptr(p), p.size // 4, _ptr(np.ascontiguousarray(box, np.float64)),
+                                             float(cell), float(radius))
+
+
+def cluster_labels(abi, pos, members, box, cutoff, periodic_z):
+    """buildClusterUnionFind with its periodicZ switch (aggregate.ts:65-130): (components, labels)."""
+    pos = np.ascontiguousarray(pos, np.float32)
+    m = np.ascontiguousarray(members, np.uint32)
+    labels = np.zeros(m.size, np.uint32)
+    n = lib(abi).oracle_cluster_labels(_ptr(pos), _ptr(m), m.size, _ptr(np.ascontiguousarray(box, np.float64)),
+                                       float(cutoff), int(bool(periodic_z)), _ptr(labels))
+    return int(n), labels
