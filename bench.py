@@ -593,6 +593,27 @@ def checkpoint_timing(s, cfg, reps=3):
                     "file: payload + base64 + JSON text of the reference's CheckpointFile"}
 
 
+def stage_timing(s, reps=3):
+    """detectStage (soup/src/stages.ts:204-289) of the live system through observables.detect_stage:
+    the particle read-back, amphiphiles, aggregate labels, the box-wide head peaks and enclosed
+    volume, and analyzeAggregates with the water beads; median wall clock of `reps` after one warm
+    call."""
+    from protocell_genesis_b200 import observables as obs
+    r = obs.detect_stage(s)
+    t = []
+    for _ in range(reps):
+        t0 = time.perf_counter()
+        r = obs.detect_stage(s)
+        t.append(time.perf_counter() - t0)
+    e = r["evidence"]
+    a = e["aggregateAnalysis"]
+    return {"ms": 1e3 * statistics.median(t), "stage": r["stage"],
+            "amphiphile_fraction": e["amphiphileFraction"], "aggregates": a["aggregateCount"],
+            "enclosed_volume": e["enclosedVolume"], "head_peaks": e["headPeaks"],
+            "what": "one detect_stage call per sample, wall clock (the reference quotes 1.5-1.9 s per sample at "
+                    "this size)"}
+
+
 def box_scale_timing(s, cfg):
     """One box change of the live system (soup/src/soup-box-scale.ts applyBoxScaleOnce) on the device:
     rigid units of the covalent bonds, then with the amphiphiles' proximity cohesion at the nonbonded
@@ -724,6 +745,7 @@ def run_cuda(args):
                 "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback 6.65 TB/s"}
 
     ckpt = checkpoint_timing(s, cfg)
+    stage = stage_timing(s)
 
     # end to end through the public API with host buffers: create from pinned host arrays
     # (H2D of the whole state), step in chunks of 10 with the positions read back after each chunk
@@ -802,6 +824,7 @@ def run_cuda(args):
                        "sweeps_in_timed_region": info1["sweeps"] - info0["sweeps"],
                        "autotune": tune,
                        "checkpoint": ckpt,
+                       "stage_detection": stage,
                        "box_scale": box_scale,
                        "analysis": None if sampler is None else {
                            "every": args.analysis_every, "samples_in_timed_region": len(samples),
