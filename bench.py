@@ -579,18 +579,25 @@ def checkpoint_timing(s, cfg, reps=3):
     import json as _json
     from protocell_genesis_b200 import checkpoint as ck
     config = {"box": [float(x) for x in cfg.box], "seed": int(cfg.seed), "kT": float(cfg.kT)}
-    t_pay, t_file, size = [], [], 0
-    for _ in range(reps):
-        t0 = time.perf_counter()
-        s.checkpoint_payload()
-        t_pay.append(time.perf_counter() - t0)
-        t0 = time.perf_counter()
-        size = len(_json.dumps(ck.encode_checkpoint(s, config)))
-        t_file.append(time.perf_counter() - t0)
+    import tempfile
+    t_pay, t_file, t_bin, size, bsize = [], [], [], 0, 0
+    with tempfile.TemporaryDirectory() as tmp:
+        for _ in range(reps):
+            t0 = time.perf_counter()
+            s.checkpoint_payload()
+            t_pay.append(time.perf_counter() - t0)
+            t0 = time.perf_counter()
+            size = len(_json.dumps(ck.encode_checkpoint(s, config)))
+            t_file.append(time.perf_counter() - t0)
+            t0 = time.perf_counter()
+            bsize = ck.write_checkpoint_binary(os.path.join(tmp, "c.bin"), s, config)
+            t_bin.append(time.perf_counter() - t0)
     return {"payload_ms": 1e3 * statistics.median(t_pay), "file_ms": 1e3 * statistics.median(t_file),
+            "binary_file_ms": 1e3 * statistics.median(t_bin), "binary_file_bytes": bsize,
             "file_bytes": size, "payload_bytes": 64 * s.n,
             "what": "payload: soup_read_checkpoint (one device gather, one wait) into pageable host memory; "
-                    "file: payload + base64 + JSON text of the reference's CheckpointFile"}
+                    "file: payload + base64 + JSON text of the reference's CheckpointFile; binary_file: payload "
+                    "+ the binary form written to a local file"}
 
 
 def stage_timing(s, reps=3):

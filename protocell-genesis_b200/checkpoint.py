@@ -41,8 +41,11 @@ def _b64(a: np.ndarray, dtype) -> str:
     return base64.b64encode(np.ascontiguousarray(a, np.dtype(dtype).newbyteorder("<")).tobytes()).decode("ascii")
 
 
-def _unb64(s: str, dtype) -> np.ndarray:
-    """decodeFloat32 / decodeUint32 (checkpoint.ts:58-66)."""
+def _unb64(s, dtype) -> np.ndarray:
+    """decodeFloat32 / decodeUint32 (checkpoint.ts:58-66).  An array read from a binary checkpoint
+    passes through as it is."""
+    if isinstance(s, np.ndarray):
+        return s.astype(dtype)
     return np.frombuffer(base64.b64decode(s), np.dtype(dtype).newbyteorder("<")).astype(dtype)
 
 
@@ -61,7 +64,17 @@ def _now() -> str:
 
 
 def encode_checkpoint(sys, config: dict, created_at: Optional[str] = None) -> dict:
-    """encodeCheckpoint (checkpoint.ts:176-214): the CheckpointFile of `sys`'s current state.
+    """encodeCheckpoint (checkpoint.ts:176-214): the CheckpointFile of `sys`'s current state."""
+    out, arrays = _checkpoint_fields(sys, config, created_at)
+    prot = out.pop("protonationRng")   # the reference's field order: the arrays, then protonationRng
+    for key, name, dt, _ in ARRAYS:
+        out[key] = _b64(arrays[name], dt)
+    out["protonationRng"] = prot
+    return out
+
+
+def _checkpoint_fields(sys, config: dict, created_at: Optional[str] = None):
+    """The CheckpointFile's scalar fields and its eight arrays (by name), unencoded.
 
     `sys` is a SoupSystem (one soup_read_checkpoint call) or any object with the reference's
     CheckpointableSystem readbacks (particles, velocities, bondSlots, centerLinks, centerHeldSteps,
@@ -92,11 +105,9 @@ def encode_checkpoint(sys, config: dict, created_at: Optional[str] = None) -> di
         "activeCounts": dict(active),
         "events": {k: int(v) for k, v in events.items()},
         "desorbEvents": {"stretch": int(desorb["stretch"]), "timeout": int(desorb["timeout"])},
+        "protonationRng": int(prot),
     }
-    for key, name, dt, _ in ARRAYS:
-        out[key] = _b64(arrays[name], dt)
-    out["protonationRng"] = int(prot)
-    return out
+    return out, arrays
 
 
 def decode_checkpoint_resume(file: dict) -> dict:
@@ -154,8 +165,69 @@ def create_from_checkpoint(file: dict):
 
 
 def write_checkpoint(path: str, file: dict) -> None:
+    """The CheckpointFile as the reference's JSON text; arrays read from a binary checkpoint are
+    encoded to base64 here, so a binary file converts to the reference's format."""
+    out = dict(file)
+    for key, _, dt, _ in ARRAYS:
+        if isinstance(out.get(key), np.ndarray):
+            out[key] = _b64(out[key], dt)
     with open(path, "w") as fh:
-        json.dump(file, fh)
+        json.dump(out, fh)
+
+
+BINARY_MAGIC = b"SOUPCKB1"
+_ALIGN = 64
+
+
+def write_checkpoint_binary(path: str, sys, config: dict, created_at: Optional[str] = None) -> int:
+    """The checkpoint of `sys` without the base64 round trip: an 8-byte magic, the header length
+    (u64 little-endian), the CheckpointFile's fields as JSON with an "arrays" table (key, dtype,
+    offset, bytes), then the eight arrays' little-endian bytes, each at a 64-byte aligned offset.
+    Returns the file's size in bytes."""
+    out, arrays = _checkpoint_fields(sys, config, created_at)
+    table, blobs, at = [], [], 0
+    for key, name, dt, _ in ARRAYS:
+        b = np.ascontiguousarray(arrays[name], np.dtype(dt).newbyteorder("<"))
+        table.append({"key": key, "dtype": np.dtype(dt).str.lstrip("<>|="), "offset": at, "bytes": b.nbytes})
+        blobs.append((at, b))
+        at += -(-b.nbytes // _ALIGN) * _ALIGN
+    out["arrays"] = table
+    head = json.dumps(out).encode()
+    start = -(-(16 + len(head)) // _ALIGN) * _ALIGN
+    with open(path, "wb") as fh:
+        fh.write(BINARY_MAGIC + len(head).to_bytes(8, "little") + head)
+        fh.write(b"\0" * (start - 16 - len(head)))
+        pos = 0
+        for off, b in blobs:
+            if off > pos:
+                fh.write(b"\0" * (off - pos))
+            fh.write(memoryview(b).cast("B"))
+            pos = off + b.nbytes
+        if at > pos:
+            fh.write(b"\0" * (at - pos))
+    return start + at
+
+
+def read_checkpoint_binary(path: str) -> dict:
+    """A binary checkpoint as a CheckpointFile whose array fields are numpy arrays (accepted by
+    decode_checkpoint_resume, create_from_checkpoint and write_checkpoint)."""
+    with open(path, "rb") as fh:
+        data = fh.read()
+    if data[:8] != BINARY_MAGIC:
+        raise ValueError("not a binary soup checkpoint")
+    n = int.from_bytes(data[8:16], "little")
+    file = json.loads(data[16:16 + n].decode())
+    start = -(-(16 + n) // _ALIGN) * _ALIGN
+    dts = {key: dt for key, _, dt, _ in ARRAYS}
+    for a in file.pop("arrays"):
+        dt = np.dtype(a["dtype"]).newbyteorder("<")
+        if a["key"] not in dts or np.dtype(a["dtype"]) != np.dtype(dts[a["key"]]):
+            raise ValueError(f"binary checkpoint: unexpected array {a['key']!r} of {a['dtype']}")
+        lo = start + int(a["offset"])
+        if lo + int(a["bytes"]) > len(data):
+            raise ValueError(f"binary checkpoint: {a['key']} runs past the end of the file")
+        file[a["key"]] = np.frombuffer(data, dt, int(a["bytes"]) // dt.itemsize, lo).astype(dts[a["key"]])
+    return file
 
 
 def read_checkpoint(path: str) -> dict:
@@ -164,4 +236,6 @@ def read_checkpoint(path: str) -> dict:
 
 
 encodeCheckpoint = encode_checkpoint
+writeCheckpointBinary = write_checkpoint_binary
+readCheckpointBinary = read_checkpoint_binary
 decodeCheckpointResume = decode_checkpoint_resume

@@ -155,3 +155,26 @@ def test_a_file_from_before_the_charges_resumes_with_fresh_charges():
 def test_unknown_version_is_refused():
     with pytest.raises(ValueError, match="version"):
         ck.decode_checkpoint_resume({"version": 2})
+
+
+def test_binary_checkpoint_holds_the_same_file(tmp_path):
+    """The binary form: the same fields and the same array bytes as the JSON CheckpointFile; read back
+    it decodes to the same resume state, and written as JSON it is the reference's file."""
+    o, cfg = _stepped_oracle()
+    sysA = OracleCheckpointable(o, cfg)
+    when = "2026-01-01T00:00:00.000Z"
+    f = ck.encode_checkpoint(sysA, CONFIG, created_at=when)
+    size = ck.write_checkpoint_binary(str(tmp_path / "c.bin"), sysA, CONFIG, created_at=when)
+    assert size == (tmp_path / "c.bin").stat().st_size and size % 64 == 0
+    fb = ck.read_checkpoint_binary(str(tmp_path / "c.bin"))
+    r, rb = ck.decode_checkpoint_resume(f), ck.decode_checkpoint_resume(fb)
+    for k, v in r.items():
+        if isinstance(v, np.ndarray):
+            assert rb[k].dtype == v.dtype and np.array_equal(rb[k].view(np.uint32), v.view(np.uint32)), k
+        else:
+            assert rb[k] == v, k
+    ck.write_checkpoint(str(tmp_path / "c.json"), fb)
+    assert ck.read_checkpoint(str(tmp_path / "c.json")) == json.loads(json.dumps(f))
+    (tmp_path / "bad.bin").write_bytes(b"NOTSOUP!" + bytes(8))
+    with pytest.raises(ValueError, match="not a binary"):
+        ck.read_checkpoint_binary(str(tmp_path / "bad.bin"))

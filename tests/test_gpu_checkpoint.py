@@ -117,3 +117,20 @@ def test_resumed_system_continues_the_run():
     assert a.steps == b.steps == STEPS + 20
     a.dispose()
     b.dispose()
+
+
+def test_binary_checkpoint_resumes_as_the_json_one(tmp_path):
+    """A system resumed from the binary checkpoint and one resumed from the JSON CheckpointFile of the
+    same state are the same system: equal fields, and bit-identical steps after."""
+    a = _system()
+    a.step(300)
+    when = "2026-01-01T00:00:00.000Z"
+    f = ck.encode_checkpoint(a, CONFIG, created_at=when)
+    ck.write_checkpoint_binary(str(tmp_path / "c.bin"), a, CONFIG, created_at=when)
+    b, c = _resume(f), _resume(ck.read_checkpoint_binary(str(tmp_path / "c.bin")))
+    _same(_fields(b), _fields(c))
+    b.step(50)
+    c.step(50)
+    assert np.array_equal(b.particles().view(np.uint32), c.particles().view(np.uint32))
+    for s in (a, b, c):
+        s.dispose()
