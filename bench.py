@@ -2,7 +2,7 @@
 """Benchmark: particle-steps/s of the soup MD step at 483,268 beads on B200.
 
 Workload (the reference's full-campaign shape, box 76 sigma, its B76 census C 55,988 / O 18,659 /
-H 55,988 / M 1,452 / W 351,181): seeded fresh lattice + 200-iteration cold-start relax (untimed),
+H 55,988 / M 1,452 / W 351,181): seeded fresh lattice + 50-iteration cold-start relax (untimed),
 pH 7 constant-pH Monte Carlo every 10 steps, I = 0.01 M long-range Debye-Hueckel (rc_es 15.2 sigma),
 Verlet rebuild on half-skin drift, bond Monte Carlo every 20 steps.  Inputs (state + lists,
 > 400 MB) are larger than the 126 MB L2, so no flush is needed between steps.
@@ -27,9 +27,13 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "tests"))
 
 METRIC = "particle-steps/s at 483k beads, plain vs batched, at <=1e-5 force err"
+SKIN = 0.8                 # the Verlet skin of the plain workload, both arms (rebuilt on half-skin drift)
+RELAX_ITERATIONS = 50      # cold-start relax of the fresh lattice, both arms (untimed)
+E2E_MIN_STEPS = 200        # the end-to-end sample covers at least one analysis period
 UNIT = "particle-steps/s"
 # the reference's published full-campaign rate at this size (87.2 ms/step, Apple GPU via WebGPU)
 PUBLISHED = 483268 / 0.0872
+FORCE_KERNEL = "k_force (list pair force + bonded terms)"
 CENSUS = {"C": 55988, "O": 18659, "H": 55988, "M": 1452, "W": 351181}
 
 
@@ -42,9 +46,16 @@ def workload_opts(cfgm, seed=19, skin=1.0, sweep_every=10, scale=1.0):
                             skin=skin, rebuild_on_drift=True, sweep_every=sweep_every, chunk_steps=sweep_every)
 
 
+def workload_config(skin, relax, n):
+    """The `config` of both arms' lines: the same keys and values for the same workload."""
+    return {"workload": workload_name(skin), "beads": int(n), "skin": float(skin), "relax_iterations": int(relax),
+            "l2": "inputs larger than L2 (state + lists ~2.5 GB vs 126 MB), no flush"}
+
+
 def workload_name(skin):
     return (f"campaign shape: 483,268 beads, 76 sigma box, pH 7 MC every 10 steps, I 0.01 M (rc_es 15.2), "
-            f"bonds every 20, Verlet skin planned {skin} (scaled by the autotuner) rebuilt on half-skin drift")
+            f"bonds every 20, Verlet skin {skin} rebuilt on half-skin drift, fresh lattice relaxed "
+            f"{RELAX_ITERATIONS} iterations")
 
 
 class ClockSampler:
@@ -108,8 +119,21 @@ def dist_init():
 
 
 def rank_seeds(rank):
-    """Replicas only: every rank runs its own copy of the workload, seeded apart (plain, batched)."""
-    return 19 + rank, 7 + rank
+    """Replicas only: every rank runs its own copy of the plain workload, seeded apart; the batched
+    replica set is one set (seed 7) split across the ranks (replica_share)."""
+    return 19 + rank, 7
+
+
+def replica_share(sizes, ws, rank):
+    """Whole replicas to ranks, balanced by beads: largest first, each to the least loaded rank (ties
+    to the lower rank).  Returns the replica indices of `rank`, ascending."""
+    load = [0] * ws
+    own = [[] for _ in range(ws)]
+    for i in sorted(range(len(sizes)), key=lambda k: (-sizes[k], k)):
+        r = min(range(ws), key=lambda q: (load[q], q))
+        load[r] += sizes[i]
+        own[r].append(i)
+    return sorted(own[rank])
 
 
 def max_over_ranks(x, dist, device):
@@ -166,7 +190,7 @@ def run_reference(args):
     from protocell_genesis_b200 import _abi, config as cfgm
     cfg = cfgm.resolve(workload_opts(cfgm, skin=args.skin))
     o = ob.OracleSystem(_abi, cfg)
-    o.relax(args.ref_relax, 0.1)
+    o.relax(args.relax, 0.1)
     threads = ob.lib(_abi).oracle_threads()
     o.step(max(1, min(args.warmup, 2)))
     t0 = time.perf_counter()
@@ -180,7 +204,7 @@ def run_reference(args):
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": ws, "steps": k,
             "warmup": args.warmup, "ms_per_step": 1e3 * dt / k, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": v / PUBLISHED, "dtype": "f32", "data": "synthetic",
-            "config": {"workload": workload_name(args.skin), "relax_iterations": args.ref_relax},
+            "config": workload_config(args.skin, args.relax, cfg.n),
             "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
                              "sample": f"{k} of the requested {args.steps} steps (bounded to ~{args.ref_budget:.0f} s), "
                                        f"C++ restatement of the reference step, OpenMP {threads} threads"},
@@ -363,7 +387,7 @@ def run_gradient_batched(args, pkg, L, torch):
     for cfg, na, sd, radius in items:
         st = parcel_state(L, cfg, na, sd, radius)
         s_ = pkg.SoupSystem(cfg, st)
-        s_.relax_cold_start(args.relax, 0.1)
+        s_.relax_cold_start(args.aux_relax, 0.1)
         st["positions"] = s_.particles()
         s_.dispose()
         cfgs.append(cfg)
@@ -425,15 +449,18 @@ def run_gradient_batched(args, pkg, L, torch):
                         f"and charge Monte Carlo held off; seeded synthetic, relaxed untimed"}
 
 
-def run_batched(args, pkg, L, cfgm, rank, torch):
-    """The batched form: many uneven replicas stepped together, one launch per kernel per step."""
+def run_batched(args, pkg, L, cfgm, rank, torch, ws=1):
+    """The batched form: many uneven replicas stepped together, one launch per kernel per step.  With
+    several ranks the one replica set is split across them, balanced by beads (replica_share)."""
     import ctypes as C
     items = batched_configs(cfgm, seed=rank_seeds(rank)[1], replicas=args.replicas)
+    mine = replica_share([int(c.n) for c, _, _ in items], ws, rank)
+    items = [items[i] for i in mine]
     cfgs, states = [], []
     for cfg, na, sd in items:
         st = amphiphile_state(L, cfg, na, sd)
         s = pkg.SoupSystem(cfg, st)
-        s.relax_cold_start(args.relax, 0.1)
+        s.relax_cold_start(args.aux_relax, 0.1)
         st["positions"] = s.particles()
         s.dispose()
         cfgs.append(cfg)
@@ -472,7 +499,7 @@ def run_gradient(args, pkg, L, torch):
     from protocell_genesis_b200 import adjoint, config as cfgm
     cfg, st = bilayer_patch(L, cfgm)
     s = pkg.SoupSystem(cfg, st)
-    s.relax_cold_start(args.relax, 0.05)
+    s.relax_cold_start(args.aux_relax, 0.05)
     s.step(200)
     p = s.particles().reshape(-1, 4)
     slots = s.bond_slots().reshape(-1, 3)
@@ -680,7 +707,9 @@ def run_cuda(args):
     L.soup_fresh_state(C.byref(cfg), p(host["positions"]), p(host["velocities"]), p(fr), p(br), p(tr))
     s = pkg.SoupSystem(cfg)
     relax = s.relax_cold_start(args.relax, 0.1)
-    tune = s.autotune(steps=20) if not args.no_tune else None   # untimed; the choice stays in effect
+    # untimed; the choice (lanes per particle, cell size) stays in effect; the skin stays as planned,
+    # the same as the reference arm's
+    tune = s.autotune(steps=0) if not args.no_tune else None
     s.step(args.warmup)
     s.prepare_graphs()   # every chunk graph of the schedule captured before the timed region
     sampler = None if args.no_analysis else CampaignSampler(pkg, cfgm, cfg, s)
@@ -730,26 +759,34 @@ def run_cuda(args):
     bytes_per_launch = n * (4.0 * mean_list + 56.0)
     achieved = bytes_per_launch / (f_ms / max(f_n, 1) / 1e3) / 1e9 if f_n else None
     peak, peak_kind = peaks()
-    # DRAM bytes per launch of the force kernel from the committed ncu summary (captured on the
-    # quarter-size case and scaled there to 483,268 beads at its mean list length); scaled again by
-    # particles x list entries, which the traffic follows
+    # DRAM bytes per launch of the force kernel from the committed ncu capture's numbers
+    # (profiles/roofline_traffic.json: measured on a smaller case of the same workload and scaled to
+    # 483,268 beads there); scaled again by particles x list entries, which the traffic follows
     traffic = None
-    tf = os.path.join(ROOT, "profiles", "k_force_campaign121k.md")
+    tf = os.path.join(ROOT, "profiles", "roofline_traffic.json")
     if os.path.exists(tf):
-        t483 = l483 = None
         with open(tf) as fh:
-            for line in fh:
-                if line.startswith("traffic_bytes_per_launch_483k:"):
-                    t483 = float(line.split(":", 1)[1])
-                if line.startswith("mean_list_entries_483k:"):
-                    l483 = float(line.split(":", 1)[1])
-        if t483 is not None:
-            traffic = t483 * (n * mean_list) / (483268.0 * (l483 or mean_list))
+            tj = json.load(fh)
+        if tj.get("kernel") == FORCE_KERNEL:
+            traffic = float(tj["traffic_bytes_per_launch_483k"]) * (n * mean_list) / (
+                483268.0 * float(tj["mean_list_entries_483k"]))
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                 "frac": (achieved / peak) if achieved else None, "traffic": traffic,
-                "kernel": "k_force (list pair force + bonded terms)",
+                "kernel": FORCE_KERNEL,
                 "algorithmic_bytes_per_launch": bytes_per_launch, "mean_list_entries": mean_list,
                 "peak_source": f"{peak_kind} (MEASURED_PEAKS.json hbm_gbs)" if peak_kind == "measured" else "fallback 6.65 TB/s"}
+
+    # the force error of the timed state (untimed): the list force + far half against the oracle's
+    # FP64 force at the same positions
+    force_err = None
+    if not args.no_force_check:
+        import oracle_binding as ob
+        from helpers import rel_rms
+        st_now = {"positions": s.particles(), "charges": s.charges(), "bond_slots": s.bond_slots(),
+                  "center_link": s.center_links()}
+        o_ = ob.OracleSystem(_abi, cfg, st_now)
+        force_err = rel_rms(s.forces_no_rebuild(), o_.forces64())
+        o_.close()
 
     ckpt = checkpoint_timing(s, cfg)
     stage = stage_timing(s)
@@ -764,7 +801,7 @@ def run_cuda(args):
         t_ = torch.from_numpy(np.ascontiguousarray(v_)).pin_memory()
         pinned[k_] = t_.numpy()
     out_pos = torch.empty(4 * n, dtype=torch.float32).pin_memory().numpy()
-    e2e_steps = args.steps if not args.no_e2e else 0
+    e2e_steps = max(args.steps, E2E_MIN_STEPS) if not args.no_e2e else 0
     torch.cuda.synchronize()
     t0 = time.perf_counter()
     s2 = pkg.SoupSystem(cfg, pinned)
@@ -785,7 +822,9 @@ def run_cuda(args):
     if e2e_steps:
         e2e = {"value": ws * n * e2e_steps / e2e_s, "unit": UNIT,
                "h2d_bytes_per_step": h2d / e2e_steps, "d2h_bytes_per_step": 16 * n / 10,
-               "note": "create from pinned host arrays + apply the autotuned shape + step(10) + particles() readback per 10 steps, wall clock"}
+               "steps": e2e_steps,
+               "note": "create from pinned host arrays + apply the autotuned shape + step(10) + particles() readback "
+                       "per 10 steps + the analysis sample every 200 steps, wall clock"}
     s2.dispose()
     box_scale = box_scale_timing(s, cfg)
 
@@ -796,9 +835,9 @@ def run_cuda(args):
 
     batched = None
     if not args.no_batched:
-        batched = run_batched(args, pkg, L, cfgm, rank, torch)
+        batched = run_batched(args, pkg, L, cfgm, rank, torch, ws)
         if dist:
-            # ranks draw different replica sets: all their beads over the slowest rank's step
+            # the replica set is split across the ranks: all their beads over the slowest rank's step
             batched["ms_per_step"] = max_over_ranks(batched["ms_per_step"], dist, "cuda")
             batched["beads"] = int(sum_over_ranks(batched["beads"], dist, "cuda"))
             batched["value"] = aggregate_rate(1, batched["beads"], 1, batched["ms_per_step"])
@@ -821,11 +860,15 @@ def run_cuda(args):
                                                gradient["ms_per_window"])
 
     phases = {name: {"ms_total": t, "launches": c, "ms_per_step": t / args.prof_steps} for name, (t, c) in ktime.items() if c}
+    # diagnostic: the rate with the constant-pH sweep's share of the profiled segment taken out
+    seg_ms = sum(t for t, c in ktime.values())
+    sweep_ms = ktime.get("sweep", (0.0, 0))[0]
+    value_ex_sweep = value * seg_ms / (seg_ms - sweep_ms) if seg_ms > sweep_ms > 0 else None
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": value / (ws * PUBLISHED), "dtype": "f32", "data": "synthetic",
-            "config": {"workload": workload_name(args.skin), "beads": n, "replicas_per_gpu": 1,
-                       "l2": "inputs larger than L2 (state + lists ~3 GB vs 126 MB), no flush",
+            "config": workload_config(args.skin, args.relax, n),
+            "details": {"replicas_per_gpu": 1,
                        "relax": {"iterations": args.relax, "max_force_after": relax["maxForceAfter"]},
                        "rebuilds_in_timed_region": info1["rebuilds"] - info0["rebuilds"],
                        "sweeps_in_timed_region": info1["sweeps"] - info0["sweeps"],
@@ -843,6 +886,8 @@ def run_cuda(args):
                                     "rebuild a conditional node",
                        "split": f"phases and the force roofline from a profiled segment of {args.prof_steps} steps "
                                 "right after the timed region"},
+            "force_rel_rms": force_err,
+            "value_excluding_sweep": value_ex_sweep,
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
             "clocks": clk.summary(), "phases": phases, "batched": batched, "gradient": gradient,
             "gradient_batched": gradient_batched}
@@ -859,13 +904,14 @@ def main():
     ap.add_argument("--steps", type=int, default=500)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="cuda", choices=["cuda", "reference"])
-    ap.add_argument("--skin", type=float, default=1.0)
-    ap.add_argument("--relax", type=int, default=200)
-    ap.add_argument("--ref-relax", type=int, default=10)
+    ap.add_argument("--skin", type=float, default=SKIN)
+    ap.add_argument("--relax", type=int, default=RELAX_ITERATIONS, help="cold-start relax of the plain workload (both arms)")
+    ap.add_argument("--aux-relax", type=int, default=200, help="cold-start relax of the batched and gradient workloads")
     ap.add_argument("--ref-budget", type=float, default=60.0)
     ap.add_argument("--cpu-budget", type=float, default=12.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-force-check", action="store_true", help="skip the FP64 force check of the timed state")
     ap.add_argument("--scale", type=float, default=1.0, help="census and box-volume factor (profiling captures)")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched-replica measurement")
     ap.add_argument("--replicas", type=int, default=64)

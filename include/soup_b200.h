@@ -226,6 +226,11 @@ int soup_nonfinite_count(SoupHandle* h, uint32_t* out2);
  * NULL, each particle's neighbours sorted ascending in a CSR layout (offsets = prefix of counts).
  * `lists_cap` is the element capacity of `lists`.  Diagnostic/parity access. */
 int soup_read_verlet(SoupHandle* h, uint32_t* counts, uint32_t* lists, size_t lists_cap);
+/* The long-range (head) list of every titratable head, the heads in ascending original index: counts
+ * u32[heads] and, when `lists` is not NULL, each head's neighbours as ORIGINAL particle indices sorted
+ * ascending in a CSR layout (soup/wgsl/electrostatics-long.wgsl:31-56 esList, read back as sets).
+ * `lists_cap` is the element capacity of `lists`.  Diagnostic/parity access. */
+int soup_read_es_list(SoupHandle* h, uint32_t* counts, uint32_t* lists, size_t lists_cap);
 /* Protonation chain state (SoupSystem.protonationRngState). */
 int soup_read_protonation_rng(SoupHandle* h, uint32_t* out);
 
@@ -279,7 +284,8 @@ int soup_set_box(SoupHandle* h, const double box[3]);
  * skin, which sized the list capacity; timed on `steps` whole steps).  The choice stays in effect.
  * The state is restored afterwards: positions, velocities, charges, bonds, RNG states, event
  * counters and the step schedule are as they were, and the particles are re-sorted, so later forces
- * agree with an untuned run to FP32 rounding. */
+ * agree with an untuned run to FP32 rounding.  steps = 0 tunes the block shape and the cell size
+ * only: the skin stays as planned and the ms_per_step fields are 0. */
 typedef struct SoupTuneResult {
   uint32_t tpp, walk;             /* chosen lanes per particle, list-walk radius */
   uint32_t tpp_before, walk_before;
@@ -297,6 +303,12 @@ int soup_apply_tuning(SoupHandle* h, const SoupTuneResult* tuning);
 int soup_prepare_graphs(SoupHandle* h);
 /* Replace the whole state (CreateSoupOpts.resume semantics); NULL members keep current values. */
 int soup_write_state(SoupHandle* h, const SoupInitState* st);
+
+/* Polls a bounded device-side handoff (the constant-pH walk's flags between the CTAs of its cluster)
+ * makes before it gives up and the call returns SOUP_E_TIMEOUT; 0 restores the default (2^25).  It has
+ * no counterpart in the reference, whose sweep runs on the host; a small limit makes the failure path
+ * testable without faulting the device.  Applies to the handle's whole batch. */
+int soup_set_wait_limit(SoupHandle* h, uint32_t polls);
 
 /* ---- Monte Carlo and analysis -------------------------------------------------------------- */
 /* protonationSweepDEBUG (soup/src/sim.ts): one constant-pH sweep now on the device, then the

@@ -1475,6 +1475,21 @@ int oracle_verlet(void* p, uint32_t* counts, uint32_t* lists, size_t cap) {
   }
   return SOUP_OK;
 }
+// head (long-range) list as sorted CSR over the heads in ascending index (counts[heads]; lists may be
+// NULL); rows hold particle indices
+int oracle_es_list(void* p, uint32_t* counts, uint32_t* lists, size_t cap) {
+  System& s = *static_cast<System*>(p);
+  const size_t H = s.heads.size();
+  for (size_t h = 0; h < H; ++h) counts[h] = (uint32_t)(s.es_off[h + 1] - s.es_off[h]);
+  if (lists) {
+    if (cap < s.es.size()) return SOUP_E_ARG;
+    for (size_t h = 0; h < H; ++h) {
+      std::copy(s.es.begin() + s.es_off[h], s.es.begin() + s.es_off[h + 1], lists + s.es_off[h]);
+      std::sort(lists + s.es_off[h], lists + s.es_off[h + 1]);
+    }
+  }
+  return SOUP_OK;
+}
 int oracle_info(void* p, uint64_t* out6) {
   System& s = *static_cast<System*>(p);
   out6[0] = s.step; out6[1] = s.rebuilds; out6[2] = s.sweeps; out6[3] = s.vl.size();

@@ -175,6 +175,8 @@ SIGNATURES = {
     "soup_read_desorb": (C.c_int, [_P, _P, _SZ]),
     "soup_nonfinite_count": (C.c_int, [_P, _U32P]),
     "soup_read_verlet": (C.c_int, [_P, _U32P, _U32P, _SZ]),
+    "soup_read_es_list": (C.c_int, [_P, _U32P, _U32P, _SZ]),
+    "soup_set_wait_limit": (C.c_int, [_P, C.c_uint32]),
     "soup_read_protonation_rng": (C.c_int, [_P, _U32P]),
     "soup_read_checkpoint": (C.c_int, [_P, _P, _SZ, C.POINTER(SoupCheckpointScalars)]),
     "soup_scale_box": (C.c_int, [_P, C.POINTER(C.c_double), C.c_double, _U32P, C.c_uint32]),

@@ -112,7 +112,10 @@ def _checkpoint_fields(sys, config: dict, created_at: Optional[str] = None):
 
 def decode_checkpoint_resume(file: dict) -> dict:
     """decodeCheckpointResume (checkpoint.ts:219-237): CreateSoupOpts.resume's shape, arrays as numpy.
-    A file without chargesB64 / protonationRng (written before electrostatics) gives None there."""
+    A file without chargesB64 / protonationRng (written before electrostatics) gives None there; the
+    other seven arrays are required (the reference's decodeFloat32 / decodeUint32 throw on a missing
+    string), and every array must hold exactly N x its values per particle, N being the live census
+    sum(activeCounts) (checkpoint.ts:113-126), or ValueError is raised before anything reads it."""
     if file.get("version") != VERSION:
         raise ValueError(f"checkpoint version {file.get('version')!r} is not {VERSION}")
     r = {
@@ -123,8 +126,19 @@ def decode_checkpoint_resume(file: dict) -> dict:
         "events": dict(file["events"]),
         "protonationRng": file.get("protonationRng"),
     }
-    for key, name, dt, _ in ARRAYS:
-        r[name] = _unb64(file[key], dt) if file.get(key) is not None else None
+    n = int(sum(int(v) for v in r["activeCounts"].values()))
+    if "N" in file and int(file["N"]) != n:
+        raise ValueError(f"checkpoint: N={file['N']} does not equal the census sum {n} of activeCounts")
+    for key, name, dt, per in ARRAYS:
+        if file.get(key) is None:
+            if name == "charges":
+                r[name] = None
+                continue
+            raise ValueError(f"checkpoint: the required array {key} is missing")
+        a = _unb64(file[key], dt)
+        if a.size != n * per:
+            raise ValueError(f"checkpoint: {key} holds {a.size} values, expected N x {per} = {n * per}")
+        r[name] = a
     return r
 
 
@@ -224,7 +238,11 @@ def read_checkpoint_binary(path: str) -> dict:
         if a["key"] not in dts or np.dtype(a["dtype"]) != np.dtype(dts[a["key"]]):
             raise ValueError(f"binary checkpoint: unexpected array {a['key']!r} of {a['dtype']}")
         lo = start + int(a["offset"])
-        if lo + int(a["bytes"]) > len(data):
+        nb = int(a["bytes"])
+        if int(a["offset"]) < 0 or nb < 0 or nb % dt.itemsize:
+            raise ValueError(f"binary checkpoint: {a['key']} has offset {a['offset']} and {nb} bytes, "
+                             f"not a whole number of {dt.itemsize}-byte values at a non-negative offset")
+        if lo + nb > len(data):
             raise ValueError(f"binary checkpoint: {a['key']} runs past the end of the file")
         file[a["key"]] = np.frombuffer(data, dt, int(a["bytes"]) // dt.itemsize, lo).astype(dts[a["key"]])
     return file

@@ -306,7 +306,7 @@ struct Scratch {
 
 }  // namespace
 
-void exclusive_scan(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* tmp, cudaStream_t st);
+uint64_t exclusive_scan(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* tmp, cudaStream_t st);
 
 char* analysis_scratch(Batch& b, size_t bytes, int which) {
   if (bytes > b.an_cap[which]) {

@@ -76,11 +76,11 @@ __global__ void k_set_total(uint32_t* __restrict__ start, const uint32_t* __rest
 
 }  // namespace
 
-// exclusive scan of in[0..n) into out[0..n), out[n] = total; tmp must hold >= 2*ceil(n/4096)+2 words
-uint64_t g_scan_launches = 0;
-void exclusive_scan(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* tmp, cudaStream_t st) {
-  if (n == 0) return;
-  g_scan_launches += 2;
+// exclusive scan of in[0..n) into out[0..n), out[n] = total; tmp must hold >= 2*ceil(n/4096)+2 words.
+// Returns the kernels it launched (no shared counter: calls from several host threads do not race).
+uint64_t exclusive_scan(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* tmp, cudaStream_t st) {
+  if (n == 0) return 0;
+  uint64_t launches = 2;
   uint32_t nb = (n + 4095) / 4096;
   if (nb == 1) {
     k_scan_block<<<1, 1024, 0, st>>>(in, out, n, nullptr);
@@ -88,10 +88,11 @@ void exclusive_scan(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* tmp
     uint32_t* sums = tmp;
     uint32_t* offs = tmp + nb + 1;
     k_scan_block<<<nb, 1024, 0, st>>>(in, out, n, sums);
-    exclusive_scan(sums, offs, nb, offs + nb + 1, st);
+    launches += exclusive_scan(sums, offs, nb, offs + nb + 1, st) + 1;
     k_scan_add<<<nblocks(n), kBlock, 0, st>>>(out, n, offs);
   }
   k_set_total<<<1, 1, 0, st>>>(out, in, n);
+  return launches;
 }
 
 namespace {
@@ -440,8 +441,7 @@ void launch_cell_index(Batch& b) {
 
 void launch_sort_and_gather(Batch& b) {
   prof_begin(b, SOUP_K_SORT);
-  g_scan_launches = 0;
-  exclusive_scan(b.cell_count, b.cell_start, b.ncells, b.scan_tmp, b.stream);
+  const uint64_t scans = exclusive_scan(b.cell_count, b.cell_start, b.ncells, b.scan_tmp, b.stream);
   cudaMemsetAsync(b.cell_cursor, 0, sizeof(uint32_t) * b.ncells, b.stream);
   k_scatter<<<nblocks(b.N), kBlock, 0, b.stream>>>(b.cell_of_slot, b.cell_start, b.N, b.cell_cursor, b.perm);
   k_sort_cells<<<nblocks(b.ncells), kBlock, 0, b.stream>>>(b.cell_start, b.ncells, b.id, b.perm);
@@ -456,7 +456,7 @@ void launch_sort_and_gather(Batch& b) {
   // the cell of every new slot: cell_start is monotone, so recompute from the sorted positions
   cudaMemsetAsync(b.cell_count, 0, sizeof(uint32_t) * (b.ncells + 1), b.stream);
   k_cell_index<<<nblocks(b.N), kBlock, 0, b.stream>>>(b.pos, b.sysid, b.sp, b.N, b.cell_of_slot, b.cell_count);
-  b.launches += 6 + g_scan_launches;
+  b.launches += 6 + scans;
   prof_end(b);
 }
 
@@ -470,19 +470,18 @@ void launch_build_lists(Batch& b) {
 
 void launch_build_es_lists(Batch& b) {
   if (b.H == 0) return;
-  g_scan_launches = 0;
   prof_begin(b, SOUP_K_LIST);
   cudaMemsetAsync(b.hcell_count, 0, sizeof(uint32_t) * (b.nhcells + 1), b.stream);
   k_head_index<<<nblocks(b.H), kBlock, 0, b.stream>>>(b.heads, b.head_sys, b.H, b.slot_of, b.pos, b.sp, b.hcell_of,
                                                        b.hcell_count, b.head_slot);
-  exclusive_scan(b.hcell_count, b.hcell_start, b.nhcells, b.scan_tmp, b.stream);
+  const uint64_t scans = exclusive_scan(b.hcell_count, b.hcell_start, b.nhcells, b.scan_tmp, b.stream);
   cudaMemsetAsync(b.hcell_cursor, 0, sizeof(uint32_t) * b.nhcells, b.stream);
   k_head_scatter<<<nblocks(b.H), kBlock, 0, b.stream>>>(b.hcell_of, b.hcell_start, b.H, b.hcell_cursor, b.hsorted);
   k_head_sort_cells<<<nblocks(b.nhcells), kBlock, 0, b.stream>>>(b.hcell_start, b.nhcells, b.hsorted);
   k_build_es_list<<<nblocks((uint64_t)b.H * 32, 256), 256, 0, b.stream>>>(b.head_sys, b.H, b.head_slot, b.pos, b.sp,
                                                                          b.hcell_of, b.hcell_start, b.hsorted, b.es_cap,
                                                                          b.es_nl, b.es_cnt, b.flags);
-  b.launches += 5 + g_scan_launches;
+  b.launches += 5 + scans;
   prof_end(b);
 }
 

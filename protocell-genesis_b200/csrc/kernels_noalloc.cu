@@ -18,8 +18,7 @@
 #include "soup_internal.h"
 
 namespace soup {
-void exclusive_scan(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* tmp, cudaStream_t st);
-extern uint64_t g_scan_launches;
+uint64_t exclusive_scan(const uint32_t* in, uint32_t* out, uint32_t n, uint32_t* tmp, cudaStream_t st);
 }
 
 namespace {
@@ -183,6 +182,13 @@ extern "C" int soup_aggregate_labels_noalloc(SoupHandle* h, const uint32_t* memb
   if (nc > kMaxCells)
     return bad(SOUP_E_ARG, "aggregate labels (no-alloc): the grid of " + std::to_string(nc) + " cells exceeds the maximum of " +
                                std::to_string(kMaxCells) + " (box / cutoff too large)");
+  // the calling thread's current device is put back on every return below
+  int prev = -1;
+  if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+  struct Restore {
+    int d;
+    ~Restore() { if (d >= 0) cudaSetDevice(d); }
+  } restore{prev};
   if (cudaSetDevice(b.device) != cudaSuccess) return bad(SOUP_E_CUDA, "cudaSetDevice failed");
   std::string err;
   uint32_t* s = scratch_for(b.device, err);
@@ -197,14 +203,13 @@ extern "C" int soup_aggregate_labels_noalloc(SoupHandle* h, const uint32_t* memb
   ok(cudaMemsetAsync(s + kOffCount, 0, 4 * ((size_t)nc + 1), st));
   ok(cudaMemsetAsync(s + kOffCursor, 0, 4 * ((size_t)nc + 1), st));
   ok(cudaMemsetAsync(s + kOffCnt, 0, 4, st));
-  const uint64_t scans0 = soup::g_scan_launches;
   k_nf_bin<<<nblocks(m), kBlock, 0, st>>>(b.pos, b.slot_of, off, m, g, s);
-  soup::exclusive_scan(s + kOffCount, s + kOffStart, (uint32_t)nc, s + kOffTmp, st);
+  const uint64_t scans = soup::exclusive_scan(s + kOffCount, s + kOffStart, (uint32_t)nc, s + kOffTmp, st);
   k_nf_scatter<<<nblocks(m), kBlock, 0, st>>>(m, s);
   k_nf_union<<<nblocks(m), kBlock, 0, st>>>(b.pos, b.slot_of, off, m, g, cutoff * cutoff, s);
   k_nf_min<<<nblocks(m), kBlock, 0, st>>>(m, s);
   k_nf_label<<<nblocks(m), kBlock, 0, st>>>(m, s);
-  b.launches += 5 + (soup::g_scan_launches - scans0);
+  b.launches += 5 + scans;
   ok(cudaGetLastError());
   uint32_t ncomp = 0;
   ok(cudaMemcpyAsync(labels, s + kOffLabels, 4 * (size_t)m, cudaMemcpyDeviceToHost, st));

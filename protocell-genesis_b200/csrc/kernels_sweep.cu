@@ -172,7 +172,7 @@ __device__ __forceinline__ double pcg_out(uint32_t v) {
 
 constexpr int kWalkThreads = 512;
 constexpr uint32_t kEndOfSweep = 0xFFFFFFFFu;   // s_cflag once the sweep is over
-constexpr uint32_t kSpinLimit = 1u << 25;       // polls of a handoff flag before the walk gives up
+constexpr uint32_t kSpinLimit = 1u << 25;       // default polls of a handoff flag before the walk gives up
 
 // cluster-scope release / acquire on 32-bit words in shared memory (own or a peer CTA's, by generic
 // address): the handoffs between the walking warp and the CTAs that scatter its flips
@@ -392,7 +392,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_sweep_walk(const SysParams* __
                                                              long long* __restrict__ Eg,
                                                              const long long* __restrict__ band,
                                                              uint32_t* __restrict__ rng_io, double* __restrict__ out,
-                                                             uint32_t only) {
+                                                             uint32_t only, uint32_t spin_limit) {
   extern __shared__ __align__(16) unsigned char smem[];
   __shared__ Flips F[2];
   __shared__ Flips Fh;                 // a helper CTA's copy of the flips it scatters
@@ -653,7 +653,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_sweep_walk(const SysParams* __
           const uint32_t want = (csize - 1u) * (wnd + 1u);
           uint32_t spins = 0;
           while (ld_acquire_cluster(&s_scat) < want) {
-            if (++spins > kSpinLimit) { s_timeout = 1u; s_done = 1u; break; }
+            if (++spins > spin_limit) { s_timeout = 1u; s_done = 1u; break; }
           }
         }
         __syncwarp();
@@ -671,7 +671,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_sweep_walk(const SysParams* __
         for (;;) {
           v = ld_acquire_cluster(lead_cflag);
           if (v == kEndOfSweep || v >= wnd + 1u) break;
-          if (++spins > kSpinLimit) { v = kEndOfSweep; atomicExch(lead_timeout, 1u); break; }
+          if (++spins > spin_limit) { v = kEndOfSweep; atomicExch(lead_timeout, 1u); break; }
         }
         s_hv = v;
       }
@@ -761,7 +761,8 @@ void launch_sweep(Batch& b, uint32_t replica) {
   SOUP_CUDA_TRY(cudaLaunchKernelEx(&lc, k_sweep_walk, (const SysParams*)b.sp, (const uint32_t*)b.head_slot,
                                    (const float4*)b.head_pos, b.charge, (const uint32_t*)b.es_nl,
                                    (const uint32_t*)b.es_cnt, (const long long*)b.head_d, b.es_cap, b.head_e,
-                                   (const long long*)b.sweep_band, b.prot_rng_dev, b.sweep_out, replica));
+                                   (const long long*)b.sweep_band, b.prot_rng_dev, b.sweep_out, replica,
+                                   b.wait_limit ? b.wait_limit : kSpinLimit));
   prof_end(b);
 }
 

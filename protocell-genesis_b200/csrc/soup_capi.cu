@@ -491,8 +491,14 @@ void guards(Batch& b, uint64_t chunk_start) {
                                    "holds (data may have been silently dropped)");
   }
   if (fl[1]) {
-    fail(SOUP_E_ES_OVERFLOW, "long-range electrostatics list: longRangeListCapacity=" + std::to_string(b.es_cap) +
-                                 " was insufficient -- data may have been silently dropped");
+    uint32_t r = 0;
+    while (r + 1 < b.R && !b.cfg[r].es_enabled) ++r;
+    char m[400];
+    std::snprintf(m, sizeof m,
+                  "long-range electrostatics list: longRangeListCapacity=%u or the headIdx size (%u) was insufficient "
+                  "at rc_es=%.4f (heads found=%u) -- data may have been silently dropped",
+                  b.cfg[r].es_list_capacity, b.hsp[r].nheads, b.cfg[r].es_cutoff, b.hsp[r].nheads);
+    fail(SOUP_E_ES_OVERFLOW, m);
   }
   if (fl[6]) fail(SOUP_E_STATE, "bond pass: item buffer overflow");
   for (uint32_t r = 0; r < b.R; ++r) {
@@ -500,7 +506,8 @@ void guards(Batch& b, uint64_t chunk_start) {
     std::memcpy(&d2, &drift[r], 4);
     const double d = std::sqrt(std::max(0.0, (double)d2));
     if (!std::isfinite(d))
-      fail(SOUP_E_NONFINITE, "Verlet list: the measured drift is not a number -- the state is already non-finite");
+      fail(SOUP_E_NONFINITE, "Verlet list: the measured drift is not a number (NaN) -- the state is already non-finite, "
+                             "see soup/src/soup-health.ts's assertStateFinite");
     if (d > b.cfg[r].skin / 2 + 1e-6) {
       char m[320];
       std::snprintf(m, sizeof m,
@@ -1182,6 +1189,35 @@ int soup_read_verlet(SoupHandle* h, uint32_t* counts, uint32_t* lists, size_t li
   });
 }
 
+int soup_read_es_list(SoupHandle* h, uint32_t* counts, uint32_t* lists, size_t lists_cap) {
+  return guarded(h, [&](Batch& b, uint32_t r) {
+    const SysParams& P = b.hsp[r];
+    const uint32_t nh = P.nheads, hoff = P.head_off, off = P.slot_off;
+    if (nh == 0) return;
+    std::vector<uint32_t> cnt(nh), heads(b.H), rows((size_t)nh * b.es_cap);
+    SOUP_CUDA_TRY(cudaMemcpyAsync(cnt.data(), b.es_cnt + hoff, 4 * (size_t)nh, cudaMemcpyDeviceToHost, b.stream));
+    SOUP_CUDA_TRY(cudaMemcpyAsync(heads.data(), b.heads, 4 * (size_t)b.H, cudaMemcpyDeviceToHost, b.stream));
+    SOUP_CUDA_TRY(cudaMemcpyAsync(rows.data(), b.es_nl + (size_t)hoff * b.es_cap, 4 * rows.size(), cudaMemcpyDeviceToHost,
+                                  b.stream));
+    SOUP_CUDA_TRY(cudaStreamSynchronize(b.stream));
+    uint64_t total = 0;
+    for (uint32_t h = 0; h < nh; ++h) { counts[h] = cnt[h]; total += cnt[h]; }
+    if (!lists) return;
+    if (lists_cap < total) fail(SOUP_E_ARG, "lists buffer too small");
+    uint64_t at = 0;
+    for (uint32_t h = 0; h < nh; ++h) {
+      uint32_t* o = lists + at;
+      for (uint32_t s = 0; s < cnt[h]; ++s) o[s] = heads[rows[(size_t)h * b.es_cap + s]] - off;
+      std::sort(o, o + cnt[h]);
+      at += cnt[h];
+    }
+  });
+}
+
+int soup_set_wait_limit(SoupHandle* h, uint32_t polls) {
+  return guarded(h, [&](Batch& b, uint32_t) { b.wait_limit = polls; });
+}
+
 int soup_write_charges(SoupHandle* h, const float* src, size_t bytes) {
   return guarded(h, [&](Batch& b, uint32_t r) {
     const uint32_t n = b.cfg[r].n, off = b.hsp[r].slot_off;
@@ -1364,7 +1400,7 @@ int soup_prepare_graphs(SoupHandle* h) {
 
 int soup_autotune(SoupHandle* h, uint32_t steps, SoupTuneResult* out) {
   return guarded(h, [&](Batch& b, uint32_t) {
-    if (steps < 10) fail(SOUP_E_ARG, "autotune: at least 10 steps per candidate");
+    if (steps != 0 && steps < 10) fail(SOUP_E_ARG, "autotune: at least 10 steps per candidate (0: shape only)");
     const TuneSnapshot snap = tune_snapshot(b);
     const bool prof = b.prof;
     b.prof = false;
@@ -1374,8 +1410,10 @@ int soup_autotune(SoupHandle* h, uint32_t steps, SoupTuneResult* out) {
     const int tpp0 = b.tpp;
     auto steps_ms = [&]() { return tune_time(b, 1, [&] { step_batch(b, steps); }) / steps; };
     SoupTuneResult res{};
-    res.ms_per_step_before = steps_ms();
-    tune_restore(b, snap);
+    if (steps) {
+      res.ms_per_step_before = steps_ms();
+      tune_restore(b, snap);
+    }
     // block shape: lanes per particle of the list force, timed on the force alone
     const int tpps[4] = {1, 2, 4, 8};
     double best = 1e30;
@@ -1397,7 +1435,7 @@ int soup_autotune(SoupHandle* h, uint32_t steps, SoupTuneResult* out) {
     // skin (drift-triggered rebuilds only): at most the planned one, which sized the list capacity;
     // timed on whole steps, rebuilds and sweeps included
     res.skin_scale = 1.0;
-    if (b.cfg[0].rebuild_on_drift) {
+    if (steps && b.cfg[0].rebuild_on_drift) {
       best = 1e30;
       for (double f : {0.6, 0.8, 1.0}) {
         std::vector<double> sk(b.R);
@@ -1412,8 +1450,10 @@ int soup_autotune(SoupHandle* h, uint32_t steps, SoupTuneResult* out) {
     for (uint32_t r = 0; r < b.R; ++r) sk[r] = planned[r] * res.skin_scale;
     tune_plan(b, sk, (int)res.walk);
     tune_restore(b, snap);
-    res.ms_per_step_after = steps_ms();
-    tune_restore(b, snap);
+    if (steps) {
+      res.ms_per_step_after = steps_ms();
+      tune_restore(b, snap);
+    }
     b.prof = prof;
     res.tpp_before = (uint32_t)tpp0;
     res.walk_before = (uint32_t)walk0;

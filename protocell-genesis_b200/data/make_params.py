@@ -100,4 +100,6 @@ def main(ref_root: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: python make_params.py <path of a protocell-genesis checkout (its data/ is read)>")
+    main(sys.argv[1])

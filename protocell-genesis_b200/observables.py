@@ -459,7 +459,13 @@ def detect_stage(system, thresholds=None, parcel=None):
     amphiphile fraction (carbon beads in a recognised chain over all carbon beads), the largest
     aggregate's share of the amphiphile members (z periodic), the box-wide head-peak count and
     enclosed volume (diagnostics), and analyzeAggregates with the water beads.  `parcel`: {"centre",
-    "radius"} of a confined run (stages.ts:274-279 reads it off the system's live confinement)."""
+    "radius"} of a confined run; when it is not given, it is read off the system's live confinement
+    as stages.ts:274-279 does (the box centre and the live wall radius; None on a periodic system)."""
+    if parcel is None and hasattr(system, "confinement"):
+        cf = system.confinement()
+        if cf is not None:
+            b = cf["boxLive"]
+            parcel = {"centre": [b[0] / 2, b[1] / 2, b[2] / 2], "radius": float(cf["radiusLive"])}
     P = _config.load_params()
     t = load_stage_thresholds()
     t.update(thresholds or {})

@@ -23,8 +23,16 @@ def _check(lib, h, st):
         raise _abi.SoupError(st, lib.soup_last_error(h).decode())
 
 
-def init_state(st: Optional[dict]):
-    """SoupInitState from a dict of numpy arrays (CreateSoupOpts.resume field names accepted)."""
+# values per particle of each SoupInitState array (events and desorb_events are per system)
+_PER = {"positions": 4, "velocities": 4, "bond_slots": 3, "center_link": 1, "center_held": 1, "bond_rng": 1,
+        "thermo_rng": 1, "charges": 1, "frozen": 1, "desorb_events": None, "events": None}
+
+
+def init_state(st: Optional[dict], cfg=None):
+    """SoupInitState from a dict of numpy arrays (CreateSoupOpts.resume field names accepted).  With
+    the system's SoupConfig `cfg`, every per-particle array must hold exactly n x its values per
+    particle, events 2 x n_rules values and desorb_events two (ValueError otherwise): the library
+    reads that many from each pointer."""
     alias = {"positions": "positions", "velocities": "velocities", "bondSlots": "bond_slots",
              "bond_slots": "bond_slots", "centerLink": "center_link", "center_link": "center_link",
              "centerHeldSteps": "center_held", "center_held": "center_held", "bondRng": "bond_rng",
@@ -39,6 +47,13 @@ def init_state(st: Optional[dict]):
             continue
         name = alias[k]
         a = np.ascontiguousarray(v, dtype=dtypes.get(name, np.uint32))
+        if cfg is not None:
+            per = _PER[name]
+            want = {"desorb_events": 2, "events": 2 * int(cfg.n_rules)}.get(name)
+            if per is not None:
+                want = int(cfg.n) * per
+            if a.size != want:
+                raise ValueError(f"state array {k!r} holds {a.size} values, expected {want}")
         keep.append(a)
         setattr(s, name, a.ctypes.data)
     s._keep = keep
@@ -54,7 +69,7 @@ class SoupSystem:
         self.n = int(cfg.n)
         self.rule_ids = rule_ids or _config.rule_ids()
         h = C.c_void_p()
-        st = init_state(state) if state is not None else None
+        st = init_state(state, cfg) if state is not None else None
         rc = self._lib.soup_create(C.byref(cfg), C.byref(st) if st is not None else None, C.byref(h))
         if rc != 0:
             raise _abi.SoupError(rc, self._lib.soup_last_error(None).decode())
@@ -98,6 +113,20 @@ class SoupSystem:
     @property
     def box(self):
         return self.info()["box"]
+
+    def confinement(self) -> Optional[dict]:
+        """confinement() (soup/src/sim.ts:542-556): the parcel derived from the LIVE box (the radius
+        scales with box x, soup/src/soup-confine.ts:76-78 liveRadius), or None on a periodic system."""
+        r0 = float(self.cfg.wall_radius)
+        if not r0 > 0:
+            return None
+        box = [float(x) for x in self.box]
+        box0 = [float(x) for x in self.cfg.box]
+        live = r0 * (box[0] / box0[0])
+        return {"radiusWet": r0, "radiusLive": live, "stiffness": float(self.cfg.wall_k), "boxWet": box0,
+                "boxLive": box, "parcelVolumeLive": 4.0 / 3.0 * math.pi * live ** 3,
+                "boxVolumeLive": box[0] * box[1] * box[2], "cutMax": float(self.cfg.interaction_range),
+                "clearanceLive": box[0] / 2 - live, "strongNoWrapLive": 2 * live < box[0] / 2}
 
     # ---- stepping ----
     def step(self, n: int):
@@ -239,13 +268,30 @@ class SoupSystem:
             self._h, counts.ctypes.data_as(_abi._U32P), lists.ctypes.data_as(_abi._U32P), lists.size))
         return counts, lists
 
+    def es_lists(self):
+        """The long-range head list as sets: (counts per head, CSR of sorted original indices), the
+        heads in ascending original index."""
+        nh = int(self.info()["heads"])
+        counts = np.empty(nh, np.uint32)
+        if nh == 0:
+            return counts, np.empty(0, np.uint32)
+        _check(self._lib, self._h, self._lib.soup_read_es_list(self._h, counts.ctypes.data_as(_abi._U32P), None, 0))
+        lists = np.empty(int(counts.sum(dtype=np.uint64)), np.uint32)
+        _check(self._lib, self._h, self._lib.soup_read_es_list(
+            self._h, counts.ctypes.data_as(_abi._U32P), lists.ctypes.data_as(_abi._U32P), lists.size))
+        return counts, lists
+
+    def set_wait_limit(self, polls: int = 0):
+        """Polls of the constant-pH walk's bounded handoffs before SOUP_E_TIMEOUT (0: the default)."""
+        _check(self._lib, self._h, self._lib.soup_set_wait_limit(self._h, int(polls)))
+
     # ---- writes ----
     def write_charges(self, q):
         q = np.ascontiguousarray(q, np.float32)
         _check(self._lib, self._h, self._lib.soup_write_charges(self._h, _ptr(q), q.nbytes))
 
     def write_state(self, state: dict):
-        st = init_state(state)
+        st = init_state(state, self.cfg)
         _check(self._lib, self._h, self._lib.soup_write_state(self._h, C.byref(st)))
 
     def set_box(self, box):
@@ -302,7 +348,8 @@ class SoupSystem:
     def autotune(self, steps: int = 20) -> dict:
         """Pick the list force's lanes per particle, the neighbour-cell size and (with drift-triggered
         rebuilds) the skin for this system's whole batch by timing them, keep the choice, and restore
-        the state (see soup_autotune in include/soup_b200.h)."""
+        the state (see soup_autotune in include/soup_b200.h).  steps = 0: the lanes and the cell size
+        only, the skin stays as planned."""
         return _autotune(self._lib, self._h, steps)
 
     def apply_tuning(self, tuning: dict):
@@ -528,7 +575,7 @@ class SoupBatch:
         if states is not None:
             sts = (_abi.SoupInitState * R)()
             for r, st in enumerate(states):
-                s = init_state(st)
+                s = init_state(st, cfgs[r])
                 self._keep.append(s)
                 sts[r] = s
         h = C.c_void_p()

@@ -49,6 +49,7 @@ def lib(abi):
         "oracle_forces_brute64": (C.c_int, [P, P]),
         "oracle_forces_brute32": (C.c_int, [P, P]),
         "oracle_verlet": (C.c_int, [P, P, P, C.c_size_t]),
+        "oracle_es_list": (C.c_int, [P, P, P, C.c_size_t]),
         "oracle_info": (C.c_int, [P, P]),
         "oracle_max_drift_sq": (C.c_double, [P]),
         "oracle_nonfinite": (C.c_int, [P, P]),
@@ -179,6 +180,16 @@ class OracleSystem:
         self._check(self.L.oracle_verlet(self.h, _ptr(counts), None, 0))
         lists = np.zeros(int(counts.sum(dtype=np.uint64)), np.uint32)
         self._check(self.L.oracle_verlet(self.h, _ptr(counts), _ptr(lists), lists.size))
+        return counts, lists
+
+    def es_lists(self):
+        nh = self.info()["heads"]
+        counts = np.zeros(nh, np.uint32)
+        if nh == 0:
+            return counts, np.zeros(0, np.uint32)
+        self._check(self.L.oracle_es_list(self.h, _ptr(counts), None, 0))
+        lists = np.zeros(int(counts.sum(dtype=np.uint64)), np.uint32)
+        self._check(self.L.oracle_es_list(self.h, _ptr(counts), _ptr(lists), lists.size))
         return counts, lists
 
     def info(self):

@@ -178,3 +178,58 @@ def test_binary_checkpoint_holds_the_same_file(tmp_path):
     (tmp_path / "bad.bin").write_bytes(b"NOTSOUP!" + bytes(8))
     with pytest.raises(ValueError, match="not a binary"):
         ck.read_checkpoint_binary(str(tmp_path / "bad.bin"))
+
+
+def _small_file(n_c=5, n_w=9):
+    f = {"version": 1, "config": {"box": [20, 20, 20], "seed": 3, "kT": 1.0}, "N": n_c + n_w,
+         "globalStep": 0, "liveBox": [20, 20, 20], "activeCounts": {"C": n_c, "W": n_w},
+         "desorbEvents": {"stretch": 0, "timeout": 0}, "events": {}, "protonationRng": 1}
+    for key, _, dt, per in ck.ARRAYS:
+        f[key] = ck._b64(np.zeros((n_c + n_w) * per, dt), dt)
+    return f
+
+
+def test_truncated_or_missing_arrays_are_refused(tmp_path):
+    """Every array must hold N x its values per particle, N the census sum; a required array that is
+    missing fails as the reference's decodeFloat32(undefined) does, and nothing reaches the library."""
+    ck.decode_checkpoint_resume(_small_file())
+    f = _small_file()
+    f["velocitiesB64"] = ck._b64(np.zeros(13 * 4, np.float32), np.float32)   # one particle short
+    with pytest.raises(ValueError, match="velocitiesB64"):
+        ck.decode_checkpoint_resume(f)
+    f = _small_file()
+    del f["thermoRngB64"]
+    with pytest.raises(ValueError, match="thermoRngB64"):
+        ck.decode_checkpoint_resume(f)
+    f = _small_file()
+    f["N"] = 15
+    with pytest.raises(ValueError, match="census"):
+        ck.decode_checkpoint_resume(f)
+    # the binary form: a table entry with a negative offset or a ragged byte count
+    o, cfg = _stepped_oracle()
+    ck.write_checkpoint_binary(str(tmp_path / "c.bin"), OracleCheckpointable(o, cfg), CONFIG)
+    data = bytearray((tmp_path / "c.bin").read_bytes())
+    n = int.from_bytes(data[8:16], "little")
+    head = json.loads(data[16:16 + n].decode())
+    for field, value, what in (("offset", -64, "non-negative"), ("bytes", 6, "whole number")):
+        h2 = json.loads(json.dumps(head))
+        h2["arrays"][1][field] = value
+        enc = json.dumps(h2).encode()
+        assert len(enc) <= n
+        bad = bytes(data[:8]) + n.to_bytes(8, "little") + enc + b" " * (n - len(enc)) + bytes(data[16 + n:])
+        (tmp_path / "bad.bin").write_bytes(bad)
+        with pytest.raises(ValueError, match=what):
+            ck.read_checkpoint_binary(str(tmp_path / "bad.bin"))
+
+
+def test_state_arrays_of_the_wrong_size_are_refused_before_the_library():
+    """SoupInitState takes plain pointers: init_state checks every array's size against the config."""
+    from protocell_genesis_b200 import soup as soupm
+    cfg = cfgm.resolve(cfgm.SoupOptions(box=[16, 16, 16], seed=1, kT=1.0, start={"C": 10, "W": 20}), P)
+    good = {"positions": np.zeros(4 * cfg.n, np.float32), "bondSlots": np.zeros(3 * cfg.n, np.uint32),
+            "desorbEvents": np.zeros(2, np.uint32), "events": np.zeros(2 * cfg.n_rules, np.uint32)}
+    soupm.init_state(good, cfg)
+    for k, bad in (("positions", np.zeros(4 * cfg.n - 4, np.float32)), ("bondSlots", np.zeros(cfg.n, np.uint32)),
+                   ("events", np.zeros(1, np.uint32))):
+        with pytest.raises(ValueError, match=k):
+            soupm.init_state(dict(good, **{k: bad}), cfg)

@@ -237,3 +237,32 @@ def test_plain_small_case_lists_forces_and_trajectory():
     assert np.abs(d).max() < 1e-2
     assert np.array_equal(g.charges(), o.read(ob.F_CHARGES))
     g.dispose()
+
+
+@pytest.mark.parametrize("maker", [plain_opts, charged_opts])
+def test_cold_start_relax_tracks_the_oracle(maker):
+    """relaxColdStart (soup/src/soup-relax.ts:87-185, relax.wgsl:50-72) on the device against the
+    oracle's relax from the same fresh lattice: every bead steps d (shrinking linearly over the
+    iterations) along its own force direction, so the two agree to the rounding of the force
+    direction; the largest force before and after agrees to 1e-3 relative."""
+    cfg = cfgm.resolve(maker(), P)
+    o = ob.OracleSystem(_abi, cfg)
+    start = oracle_state(o)
+    g = SoupSystem(cfg, start)
+    r = g.relax_cold_start(60, 0.1)
+    o.relax(60, 0.1)
+    pg_, po = g.particles().reshape(-1, 4), o.read(ob.F_POS).reshape(-1, 4)
+    d = pg_[:, :3].astype(np.float64) - po[:, :3]
+    d -= np.rint(d / cfg.box[0]) * cfg.box[0]
+    moved = pg_[:, :3].astype(np.float64) - start["positions"].reshape(-1, 4)[:, :3]
+    moved -= np.rint(moved / cfg.box[0]) * cfg.box[0]
+    err = np.sqrt((d ** 2).sum(axis=1))
+    print(f"relax: RMS difference {np.sqrt((err ** 2).mean()):.2e} sigma over RMS displacement "
+          f"{np.sqrt((moved ** 2).sum(axis=1).mean()):.2e}, max {err.max():.2e}")
+    assert np.sqrt((moved ** 2).sum(axis=1).mean()) > 0.05          # the relax moved the beads
+    assert np.sqrt((err ** 2).mean()) < 1e-4
+    assert (err > 1e-3).mean() < 0.01
+    fo = o.read(ob.F_FORCE).reshape(-1, 4)[:, :3]
+    assert r["maxForceAfter"] == pytest.approx(float(np.abs(fo).max()), rel=1e-3)
+    assert np.array_equal(pg_[:, 3], po[:, 3])
+    g.dispose()

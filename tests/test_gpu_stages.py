@@ -2,6 +2,8 @@
 the box-grid enclosed volume equal the oracle's, and the reference's four synthetic arrangements
 read as their stages (tests/soup-aggregates.test.ts:80-234: micelles, bilayer, vesicle, and the dense
 ball as none of the three)."""
+import json
+
 import numpy as np
 import pytest
 
@@ -72,4 +74,25 @@ def test_detect_stage_on_the_reference_arrangements(scenario, stage):
     assert n_agg == (3 if stage == "micelles" else 1)
     if stage == "vesicle":
         assert e["enclosedVolume"] > ST["enclosedVolume"]
+    g.dispose()
+
+
+def test_detect_stage_reads_the_parcel_off_a_confined_system():
+    """stages.ts:274-279: a confined system's parcel comes from its live confinement (box centre,
+    live wall radius) when the caller gives none; after a box change the radius follows the box."""
+    from helpers import confined_opts
+    g = SoupSystem(cfgm.resolve(confined_opts(), P))
+    g.relax_cold_start(30, 0.1)
+    g.step(20)
+    cf = g.confinement()
+    assert cf["radiusLive"] == pytest.approx(16.0) and cf["boxLive"] == [80.0, 80.0, 80.0]
+    for box in ([80.0, 80.0, 80.0], [78.0, 78.0, 78.0]):
+        g.set_box(box)
+        live = 16.0 * box[0] / 80.0
+        assert g.confinement()["radiusLive"] == pytest.approx(live)
+        implicit = obs.detect_stage(g)
+        explicit = obs.detect_stage(g, parcel={"centre": [b / 2 for b in box], "radius": live})
+        assert implicit["stage"] == explicit["stage"]
+        same = lambda e: json.dumps(e["evidence"], default=str, sort_keys=True)
+        assert same(implicit) == same(explicit)
     g.dispose()

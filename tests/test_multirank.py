@@ -1,6 +1,7 @@
-"""The multi-GPU form is replicas only: every rank runs its own seeded copy of the workload and the
-reported rate is all ranks' particle-steps over the slowest rank's time.  These tests run that host
-logic (the rank seeds, the max/sum reductions and the aggregate) on two gloo ranks on the CPU."""
+"""The multi-GPU form is replicas only: every rank runs its own seeded copy of the plain workload, the
+batched replica set is split across the ranks by beads, and the reported rate is all ranks'
+particle-steps over the slowest rank's time.  These tests run that host logic (the rank seeds, the
+replica split, the max/sum reductions and the aggregate) on two gloo ranks on the CPU."""
 import os
 import socket
 
@@ -32,8 +33,12 @@ def _rank(rank, ws, port, q):
         total = bench.sum_over_ranks(beads, dist, "cpu")
         plain_seed, batch_seed = bench.rank_seeds(r)
         cfg = cfgm.resolve(bench.workload_opts(cfgm, seed=plain_seed, scale=0.02))
+        items = bench.batched_configs(cfgm, seed=batch_seed, replicas=16)
+        share = bench.replica_share([int(c.n) for c, _, _ in items], w, r)
+        mine = int(sum(int(items[i][0].n) for i in share))
+        all_beads = bench.sum_over_ranks(mine, dist, "cpu")
         q.put((r, w, ms_max, total, bench.aggregate_rate(w, 500, 100, ms_max), plain_seed, batch_seed,
-               int(cfg.seed), tuple(cfg.box)))
+               int(cfg.seed), tuple(cfg.box), tuple(share), mine, all_beads, sum(int(c.n) for c, _, _ in items)))
     finally:
         dist.destroy_process_group()
 
@@ -49,10 +54,14 @@ def test_two_gloo_ranks_reduce_time_and_units():
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
-    for r, (rr, w, ms_max, total, rate, ps, bs, seed, box) in enumerate(out):
+    for r, (rr, w, ms_max, total, rate, ps, bs, seed, box, share, mine, all_beads, set_beads) in enumerate(out):
         assert rr == r and w == ws
         assert ms_max == 15.0                         # max over ranks
         assert total == 3000                          # sum over ranks
         assert rate == pytest.approx(2 * 500 * 100 / 0.015)
-    assert out[0][5] != out[1][5] and out[0][6] != out[1][6]   # ranks are seeded apart
+        assert all_beads == set_beads                 # the ranks' shares make up the one replica set
+    assert out[0][5] != out[1][5]                     # plain replicas are seeded apart
+    assert out[0][6] == out[1][6]                     # one batched replica set, split
     assert out[0][7] != out[1][7] and out[0][8] == out[1][8]   # same geometry, different seed
+    assert not set(out[0][9]) & set(out[1][9]) and len(out[0][9]) + len(out[1][9]) == 16
+    assert abs(out[0][10] - out[1][10]) < 0.1 * out[0][12]     # balanced by beads

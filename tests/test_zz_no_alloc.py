@@ -60,3 +60,24 @@ def test_noalloc_limits_are_refused():
     nc_ref, lab_ref = g.aggregate_labels(np.arange(100, dtype=np.uint32), 1.5)
     assert g.aggregate_labels_noalloc(np.arange(100, dtype=np.uint32), 1.5)[0] == nc_ref
     g.dispose()
+
+
+def test_noalloc_calls_allocate_nothing():
+    """The entry point's contract: after one warm call on the device, calls of different sizes leave
+    the device's free memory exactly where it was (cudaMemGetInfo, device-wide)."""
+    import torch
+    cfg, g = _system()
+    n = cfg.n
+    cut = cfgm.wca_cutoff(P["params"]["sigma"] * 1.0) + P["params"]["wc"]
+    torch.cuda.mem_get_info()                        # the runtime's own context first
+    g.aggregate_labels_noalloc(np.arange(n, dtype=np.uint32), cut)
+    torch.cuda.synchronize()
+    free0, _ = torch.cuda.mem_get_info()
+    rng = np.random.default_rng(3)
+    for frac, c in ((1.0, cut), (0.25, 2 * cut), (0.6, 0.7 * cut), (1.0, 3 * cut)):
+        members = np.sort(rng.choice(n, int(frac * n), replace=False)).astype(np.uint32)
+        g.aggregate_labels_noalloc(members, c)
+    torch.cuda.synchronize()
+    free1, _ = torch.cuda.mem_get_info()
+    assert free1 == free0
+    g.dispose()
