@@ -279,7 +279,7 @@ int soup_set_box(SoupHandle* h, const double box[3]);
 
 /* ---- autotuning (no reference counterpart) ----------------------------------------------------
  * Picks, for the handle's whole batch, the block shape of the list force (1, 2, 4 or 8 lanes per
- * particle, timed on the force), the neighbour-cell size (list-walk radius 2 or 3, timed on the
+ * particle, with the pair maths in the screening loop or the in-range pairs queued; timed on the force), the neighbour-cell size (list-walk radius 2 or 3, timed on the
  * list build) and, with drift-triggered rebuilds, the Verlet skin (0.6, 0.8 or 1.0 of the planned
  * skin, which sized the list capacity; timed on `steps` whole steps).  The choice stays in effect.
  * The state is restored afterwards: positions, velocities, charges, bonds, RNG states, event
@@ -291,12 +291,14 @@ typedef struct SoupTuneResult {
   uint32_t tpp_before, walk_before;
   double skin_scale;              /* chosen skin / planned skin */
   double ms_per_step_before, ms_per_step_after;
+  uint32_t queued, queued_before; /* list-force variant: 0 pair maths in the screening loop, 1 in-range
+                                     pairs queued per lane and evaluated together (same result bits) */
 } SoupTuneResult;
 int soup_autotune(SoupHandle* h, uint32_t steps, SoupTuneResult* out);
 /* Apply a tuning found before (by soup_autotune on a system of the same shape) without timing
- * anything: lanes per particle, list-walk radius, and the current skin scaled by skin_scale (at most
- * 1: the list capacity was sized for it; drift-triggered rebuilds only).  The lists are rebuilt and
- * the force recomputed.  Only tpp, walk and skin_scale are read. */
+ * anything: lanes per particle, the list-force variant, list-walk radius, and the current skin scaled
+ * by skin_scale (at most 1: the list capacity was sized for it; drift-triggered rebuilds only).  The
+ * lists are rebuilt and the force recomputed.  Only tpp, queued, walk and skin_scale are read. */
 int soup_apply_tuning(SoupHandle* h, const SoupTuneResult* tuning);
 /* soup_step runs chunks of chunkSteps steps (at least 4) as captured CUDA graphs, captured on first
  * use; this captures every chunk graph of the current schedule now, without stepping. */

@@ -134,6 +134,128 @@ __global__ void __launch_bounds__(256, SOUP_FORCE_MINB) k_force(
   }
 }
 
+// The same list force with the pair maths taken off the screening path.  In k_force a warp runs the
+// pair maths whenever any of its lanes holds an in-range entry, which at a skin of 0.8 is nearly
+// every chunk, so the out-of-range half of the list pays for it too.  Here each lane screens its
+// entries (index, gather, minimum image, squared distance) and pushes the in-range ones -- their
+// separation, the neighbour's charge and kind -- onto its own ring in shared memory; the warp then
+// evaluates the rings' heads together, every lane on a pair of its own particle.  A ring is first in,
+// first out in list order, so every lane accumulates exactly the terms k_force's lane does, in the
+// same order, and the force is bit-identical to k_force's.
+//
+// Ring layout: entry s of lane l at [s][l], 16 bytes (dx, dy, dz, qj) plus one byte (kj), so a row of
+// the warp's pushes or pops touches each bank once.  After each chunk of 4 entries a lane holds at
+// most kQD - 4 + 4 entries: the warp evaluates min(count) rounds with every lane busy, and more
+// rounds (lanes with empty rings idle) only when some ring could not take the next chunk.
+constexpr int kQD = 16;
+constexpr int kQBlock = 256;
+constexpr size_t kQSmem = (size_t)(kQBlock / 32) * kQD * 32 * (sizeof(float4) + 1);
+
+template <int TPP, bool SEL>
+__global__ void __launch_bounds__(kQBlock, 3) k_force_q(
+    const Shared* __restrict__ Sg, const SysParams* __restrict__ sp, const uint8_t* __restrict__ sysid, uint32_t N,
+    const float4* __restrict__ pos, const float* __restrict__ charge, const uint32_t* __restrict__ slots,
+    const uint32_t* __restrict__ center, const uint32_t* __restrict__ id, const uint32_t* __restrict__ slot_of,
+    const uint32_t* __restrict__ nl, const uint32_t* __restrict__ nl_cnt, uint32_t cap, float4* __restrict__ force,
+    const uint32_t* __restrict__ sel, uint32_t nsel) {
+  __shared__ Shared S;
+  extern __shared__ float4 qbuf[];
+  for (int w = threadIdx.x; w < (int)(sizeof(Shared) / 4); w += blockDim.x)
+    reinterpret_cast<uint32_t*>(&S)[w] = reinterpret_cast<const uint32_t*>(Sg)[w];
+  __syncthreads();
+  const int wib = threadIdx.x >> 5, l32 = threadIdx.x & 31;
+  float4* qv = qbuf + (size_t)wib * kQD * 32 + l32;
+  uint8_t* qk = reinterpret_cast<uint8_t*>(qbuf + (size_t)(kQBlock / 32) * kQD * 32) + (size_t)wib * kQD * 32 + l32;
+  const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
+  const uint32_t g = gtid / TPP;
+  const int lane = (int)(gtid % TPP);
+  const bool active = SEL ? g < nsel : g < N;
+  const uint32_t k = SEL ? (active ? sel[g] : 0u) : (active ? g : 0u);
+  const SysParams& Pg = sp[sysid[k]];
+  const PairP P = PairP::of(Pg);
+  const float4 xi = pos[k];
+  const int ki = (int)xi.w;
+  const float qi = charge[k];
+  const bool needq = (qi != 0.f) || (S.cls[ki] == 1u && P.acid > 0.f);
+  const float rmax2 = S.rmax2;
+  const uint32_t cnt = active ? nl_cnt[k] : 0u;
+  const uint32_t* row = nl + (size_t)k * cap;
+  const PairConst* prow = &S.pair[ki * SOUP_KMAX];
+  float fx = 0.f, fy = 0.f, fz = 0.f;
+  uint32_t head = 0, tail = 0;
+  auto pop = [&]() {
+    const uint32_t s = head & (kQD - 1);
+    const float4 e = qv[s * 32];
+    const int kj = qk[s * 32];
+    ++head;
+    const float r2 = e.x * e.x + e.y * e.y + e.z * e.z;
+    const float sc = pair_scalar(S, P, prow[kj], r2, ki, kj, qi, e.w);
+    fx += sc * e.x; fy += sc * e.y; fz += sc * e.z;
+  };
+  constexpr uint32_t CH = 4 * TPP;
+  uint32_t base = 4u * (uint32_t)lane;
+  uint4 nxt = base < cnt ? __ldg(reinterpret_cast<const uint4*>(row + base)) : make_uint4(k, k, k, k);
+  for (;; base += CH) {
+    const bool more = base < cnt;
+    if (!__any_sync(0xffffffffu, more)) break;
+    if (more) {
+      const uint4 jj = nxt;
+      if (base + CH < cnt) nxt = __ldg(reinterpret_cast<const uint4*>(row + base + CH));
+      const uint32_t jv[4] = {jj.x, base + 1 < cnt ? jj.y : k, base + 2 < cnt ? jj.z : k, base + 3 < cnt ? jj.w : k};
+      float4 xj[4];
+#pragma unroll
+      for (int e = 0; e < 4; ++e) xj[e] = __ldg(pos + jv[e]);
+#pragma unroll
+      for (int e = 0; e < 4; ++e) {
+        const float dx = fast_mi(xi.x - xj[e].x, P.box[0], P.inv_box[0]);
+        const float dy = fast_mi(xi.y - xj[e].y, P.box[1], P.inv_box[1]);
+        const float dz = fast_mi(xi.z - xj[e].z, P.box[2], P.inv_box[2]);
+        const float r2 = dx * dx + dy * dy + dz * dz;
+        if (r2 < rmax2 && r2 >= 1e-12f) {
+          const uint32_t s = tail & (kQD - 1);
+          qv[s * 32] = make_float4(dx, dy, dz, needq ? __ldg(charge + jv[e]) : 0.f);
+          qk[s * 32] = (uint8_t)xj[e].w;
+          ++tail;
+        }
+      }
+    }
+    // every lane busy for min(count) rounds; more only when a ring could not take the next chunk
+    const uint32_t c = tail - head;
+    const uint32_t mn = __reduce_min_sync(0xffffffffu, c), mx = __reduce_max_sync(0xffffffffu, c);
+    const uint32_t rounds = max(mn, mx > (uint32_t)(kQD - 4) ? mx - (uint32_t)(kQD - 4) : 0u);
+    for (uint32_t t = 0; t < rounds; ++t)
+      if (tail != head) pop();
+  }
+  while (__any_sync(0xffffffffu, tail != head))
+    if (tail != head) pop();
+  if (active) {
+    // bonded terms (bondedForce), spread over the group
+    uint32_t sl[3] = {slots[3 * k], slots[3 * k + 1], slots[3 * k + 2]};
+    uint32_t owner = center[k];
+    if ((sl[0] & sl[1] & sl[2] & owner) != SOUP_NONE_U32) {
+      const uint32_t gi = id[k];
+      for (int t = lane; t < 13; t += TPP) bonded_term(S, Pg, t, gi, xi, sl, owner, slots, slot_of, pos, fx, fy, fz);
+    }
+  }
+#pragma unroll
+  for (int o = TPP / 2; o > 0; o >>= 1) {
+    fx += __shfl_xor_sync(0xffffffffu, fx, o);
+    fy += __shfl_xor_sync(0xffffffffu, fy, o);
+    fz += __shfl_xor_sync(0xffffffffu, fz, o);
+  }
+  if (active && lane == 0) {
+    if (Pg.wall_r > 0.f) {   // wall.wgsl:42-56
+      float d0 = xi.x - Pg.box[0] * 0.5f, d1 = xi.y - Pg.box[1] * 0.5f, d2 = xi.z - Pg.box[2] * 0.5f;
+      float r = sqrtf(d0 * d0 + d1 * d1 + d2 * d2);
+      if (r > Pg.wall_r) {
+        float w = -Pg.wall_k * (r - Pg.wall_r) / fmaxf(r, 1e-6f);
+        fx += w * d0; fy += w * d1; fz += w * d2;
+      }
+    }
+    force[k] = make_float4(fx, fy, fz, 0.f);
+  }
+}
+
 // soup/wgsl/electrostatics-long.wgsl:63-82 soup_es_force_far_main, a warp per head.
 // positions and charges of the heads by head index (x, y, z, q): the far half reads one 16-byte
 // record per list entry instead of a slot lookup followed by two gathers
@@ -245,6 +367,26 @@ __global__ void __launch_bounds__(128) k_force_brute(
 }
 
 template <int TPP>
+void launch_force_q(Batch& b, bool heads) {
+  static bool attr = false;   // once per process: the rings are dynamic shared memory above 48 KB
+  if (!attr) {
+    SOUP_CUDA_TRY(cudaFuncSetAttribute(k_force_q<TPP, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kQSmem));
+    SOUP_CUDA_TRY(cudaFuncSetAttribute(k_force_q<TPP, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kQSmem));
+    attr = true;
+  }
+  if (heads) {
+    if (b.H == 0) return;
+    k_force_q<TPP, true><<<nblocks((uint64_t)b.H * TPP, kQBlock), kQBlock, kQSmem, b.stream>>>(
+        b.shared, b.sp, b.sysid, b.N, b.pos, b.charge, b.slots, b.center, b.id, b.slot_of, b.nl, b.nl_cnt, b.list_cap,
+        b.force, b.head_slot, b.H);
+    return;
+  }
+  k_force_q<TPP, false><<<nblocks((uint64_t)b.N * TPP, kQBlock), kQBlock, kQSmem, b.stream>>>(
+      b.shared, b.sp, b.sysid, b.N, b.pos, b.charge, b.slots, b.center, b.id, b.slot_of, b.nl, b.nl_cnt, b.list_cap,
+      b.force, nullptr, 0u);
+}
+
+template <int TPP>
 void launch_force_tpp(Batch& b, bool heads) {
   if (heads) {
     if (b.H == 0) return;
@@ -273,6 +415,14 @@ void launch_force(Batch& b) {
 
 void launch_force_list(Batch& b, bool heads) {
   b.launches += 1;
+  if (b.queued) {
+    switch (b.tpp) {
+      case 1: launch_force_q<1>(b, heads); break;
+      case 2: launch_force_q<2>(b, heads); break;
+      default: launch_force_q<4>(b, heads); break;
+    }
+    return;
+  }
   switch (b.tpp) {
     case 1: launch_force_tpp<1>(b, heads); break;
     case 2: launch_force_tpp<2>(b, heads); break;

@@ -425,6 +425,7 @@ Batch* make_batch(const SoupConfig* cfgs, const SoupInitState* inits, uint32_t R
   // 16: +16%); SOUP_TPP in the environment overrides it for tuning (1, 2, 4, 8, 16 or 32)
   b.tpp = 4;
   if (const char* e = std::getenv("SOUP_TPP")) b.tpp = std::atoi(e);
+  if (const char* e = std::getenv("SOUP_FORCE_QUEUED")) b.queued = std::atoi(e) != 0;
   force_pass(b);   // priming pass (soup/src/sim.ts:396-408)
   SOUP_CUDA_TRY(cudaStreamSynchronize(b.stream));
   SOUP_CUDA_TRY(cudaGetLastError());
@@ -1416,13 +1417,18 @@ int soup_autotune(SoupHandle* h, uint32_t steps, SoupTuneResult* out) {
     }
     // block shape: lanes per particle of the list force, timed on the force alone
     const int tpps[4] = {1, 2, 4, 8};
+    const bool queued0 = b.queued;
     double best = 1e30;
-    for (int t : tpps) {
-      b.tpp = t;
-      const double ms = tune_time(b, 5, [&] { launch_force_list(b); });
-      if (ms < best) { best = ms; res.tpp = (uint32_t)t; }
-    }
+    for (int q = 0; q < 2; ++q)
+      for (int t : tpps) {
+        if (q && t == 8) continue;
+        b.tpp = t;
+        b.queued = q != 0;
+        const double ms = tune_time(b, 5, [&] { launch_force_list(b); });
+        if (ms < best) { best = ms; res.tpp = (uint32_t)t; res.queued = (uint32_t)q; }
+      }
     b.tpp = (int)res.tpp;
+    b.queued = res.queued != 0;
     drop_graphs(b);
     // cell size: the list-walk radius (cell = list range / walk), timed on the list build
     best = 1e30;
@@ -1456,6 +1462,7 @@ int soup_autotune(SoupHandle* h, uint32_t steps, SoupTuneResult* out) {
     }
     b.prof = prof;
     res.tpp_before = (uint32_t)tpp0;
+    res.queued_before = queued0 ? 1u : 0u;
     res.walk_before = (uint32_t)walk0;
     if (out) *out = res;
   });
@@ -1470,6 +1477,7 @@ int soup_apply_tuning(SoupHandle* h, const SoupTuneResult* t) {
     if (t->skin_scale != 1.0 && !b.cfg[0].rebuild_on_drift)
       fail(SOUP_E_ARG, "tuning: the skin can only be scaled with drift-triggered rebuilds");
     b.tpp = (int)t->tpp;
+    b.queued = t->queued != 0;
     std::vector<double> sk(b.R);
     for (uint32_t r = 0; r < b.R; ++r) sk[r] = b.cfg[r].skin * t->skin_scale;
     tune_plan(b, sk, (int)t->walk);

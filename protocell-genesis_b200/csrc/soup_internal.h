@@ -147,6 +147,7 @@ struct Batch {
   uint64_t rebuilds = 0, sweeps = 0;
   bool force_fresh = false;          // force array matches positions+charges+lists
   int tpp = 4;                       // threads per particle in the list force
+  bool queued = false;               // list force with the in-range pairs queued per lane (k_force_q)
   uint32_t wait_limit = 0;           // polls of a bounded device-side handoff before it gives up (0: default)
   DiffWindow diff;
   // captured step chunks (CUDA graphs), keyed by length and schedule phase; the drift-triggered

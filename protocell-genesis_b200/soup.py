@@ -551,6 +551,7 @@ def _box_ramp(from_box, target_box, ramp_steps: int):
 def _apply_tuning(lib, h, tuning):
     r = _abi.SoupTuneResult()
     r.tpp, r.walk, r.skin_scale = int(tuning["tpp"]), int(tuning["walk"]), float(tuning["skin_scale"])
+    r.queued = int(tuning.get("queued", 0))
     _check(lib, h, lib.soup_apply_tuning(h, C.byref(r)))
 
 
@@ -559,7 +560,7 @@ def _autotune(lib, h, steps):
     _check(lib, h, lib.soup_autotune(h, int(steps), C.byref(r)))
     return dict(tpp=r.tpp, walk=r.walk, tpp_before=r.tpp_before, walk_before=r.walk_before,
                 skin_scale=r.skin_scale, ms_per_step_before=r.ms_per_step_before,
-                ms_per_step_after=r.ms_per_step_after)
+                ms_per_step_after=r.ms_per_step_after, queued=r.queued, queued_before=r.queued_before)
 
 
 class SoupBatch:

@@ -108,3 +108,30 @@ def test_apply_tuning_reproduces_the_tuned_shape():
         b.apply_tuning(dict(tune, tpp=3))
     a.dispose()
     b.dispose()
+
+
+@pytest.mark.parametrize("tpp", [1, 2, 4])
+def test_queued_force_is_bit_identical_to_the_plain_one(tpp):
+    """The list force with the in-range pairs queued per lane (k_force_q) accumulates every lane's
+    terms in k_force's order: the forces are the same bits, for all particles and for the heads-only
+    recompute after a sweep, on compositions with charges, catalysts and a confining wall."""
+    from helpers import charged_opts, confined_opts
+    for opts in (charged_opts(rebuild_on_drift=True, sweep_every=10, chunk_steps=10),
+                 confined_opts(rebuild_on_drift=True, sweep_every=10, chunk_steps=10)):
+        cfg = cfgm.resolve(opts, P)
+        o = ob.OracleSystem(_abi, cfg)
+        o.relax(20, 0.1)
+        o.step(20)
+        st = dict(positions=o.read(ob.F_POS), velocities=o.read(ob.F_VEL), bond_slots=o.read(ob.F_SLOTS),
+                  center_link=o.read(ob.F_CENTER), charges=o.read(ob.F_CHARGES))
+        out = []
+        for q in (0, 1):
+            g = SoupSystem(cfg, st)
+            g.apply_tuning(dict(tpp=tpp, walk=2, skin_scale=1.0, queued=q))
+            f = g.forces_no_rebuild()
+            g.step(30)                          # sweeps every 10 steps recompute the heads' forces only
+            out.append((f, g.forces_no_rebuild(), g.charges()))
+            g.dispose()
+        assert np.array_equal(out[0][0].view(np.uint32), out[1][0].view(np.uint32))
+        assert np.array_equal(out[0][2], out[1][2])
+        assert np.array_equal(out[0][1].view(np.uint32), out[1][1].view(np.uint32))
