@@ -87,7 +87,7 @@ def test_a_long_range_list_overflow_is_refused_with_the_references_message():
     assert e.value.code == "SOUP_E_ES_OVERFLOW"
     msg = str(e.value)
     heads = g.info()["heads"]
-    assert msg.startswith("long-range electrostatics list: longRangeListCapacity=4 or the headIdx size "
+    assert msg.startswith("SOUP_E_ES_OVERFLOW: long-range electrostatics list: longRangeListCapacity=4 or the headIdx size "
                           f"({heads}) was insufficient at rc_es=")
     assert "-- data may have been silently dropped" in msg
     g.dispose()

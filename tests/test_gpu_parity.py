@@ -242,27 +242,54 @@ def test_plain_small_case_lists_forces_and_trajectory():
 @pytest.mark.parametrize("maker", [plain_opts, charged_opts])
 def test_cold_start_relax_tracks_the_oracle(maker):
     """relaxColdStart (soup/src/soup-relax.ts:87-185, relax.wgsl:50-72) on the device against the
-    oracle's relax from the same fresh lattice: every bead steps d (shrinking linearly over the
-    iterations) along its own force direction, so the two agree to the rounding of the force
-    direction; the largest force before and after agrees to 1e-3 relative."""
+    oracle's relax from the same fresh lattice.  Every bead steps d along its own force direction
+    f/|f|, whatever |f| is, so a bead whose force is near zero turns with the last bits of its force:
+    two correct relaxes part after a few tens of iterations, and the map itself is what is compared.
+    - one iteration from the same positions, at four points along the oracle's 60-iteration path
+      (d = d0 (1 - k/60)): the device moves the beads where the oracle moves them, to the rounding of
+      the force direction (99% of the beads within 1e-4 d; fewer than 0.2% turned by more than 1e-2 d);
+    - the whole 60 iterations: the two relaxes move the beads as far (RMS displacement within 5%) and
+      leave forces of the same size (largest force within a factor of 2, both below the start's)."""
     cfg = cfgm.resolve(maker(), P)
     o = ob.OracleSystem(_abi, cfg)
     start = oracle_state(o)
+    its, d0 = 60, 0.1
+    checked = 0
+    for k in range(its):
+        d = d0 * (1.0 - k / its)
+        if k in (0, 15, 40, 59):
+            before = o.read(ob.F_POS).reshape(-1, 4).copy()
+            g = SoupSystem(cfg, dict(oracle_state(o), positions=before.ravel()))
+            g.relax_cold_start(1, d / cfg.sigma)
+            o.relax(1, d)
+            pg_, po = g.particles().reshape(-1, 4), o.read(ob.F_POS).reshape(-1, 4)
+            e = pg_[:, :3].astype(np.float64) - po[:, :3]
+            e -= np.rint(e / cfg.box[0]) * cfg.box[0]
+            err = np.sqrt((e ** 2).sum(axis=1)) / d
+            print(f"relax iteration {k}: RMS {np.sqrt((err ** 2).mean()):.2e} d, max {err.max():.2e} d, "
+                  f"{(err > 1e-2).sum()} of {err.size} beads beyond 1e-2 d")
+            assert np.quantile(err, 0.99) < 1e-4
+            assert (err > 1e-2).mean() < 2e-3
+            assert np.array_equal(pg_[:, 3], po[:, 3])
+            g.dispose()
+            checked += 1
+        else:
+            o.relax(1, d)
+    assert checked == 4
+    o_end = o.read(ob.F_POS).reshape(-1, 4)
+    fo = np.abs(o.read(ob.F_FORCE).reshape(-1, 4)[:, :3]).max()
     g = SoupSystem(cfg, start)
-    r = g.relax_cold_start(60, 0.1)
-    o.relax(60, 0.1)
-    pg_, po = g.particles().reshape(-1, 4), o.read(ob.F_POS).reshape(-1, 4)
-    d = pg_[:, :3].astype(np.float64) - po[:, :3]
-    d -= np.rint(d / cfg.box[0]) * cfg.box[0]
-    moved = pg_[:, :3].astype(np.float64) - start["positions"].reshape(-1, 4)[:, :3]
-    moved -= np.rint(moved / cfg.box[0]) * cfg.box[0]
-    err = np.sqrt((d ** 2).sum(axis=1))
-    print(f"relax: RMS difference {np.sqrt((err ** 2).mean()):.2e} sigma over RMS displacement "
-          f"{np.sqrt((moved ** 2).sum(axis=1).mean()):.2e}, max {err.max():.2e}")
-    assert np.sqrt((moved ** 2).sum(axis=1).mean()) > 0.05          # the relax moved the beads
-    assert np.sqrt((err ** 2).mean()) < 1e-4
-    assert (err > 1e-3).mean() < 0.01
-    fo = o.read(ob.F_FORCE).reshape(-1, 4)[:, :3]
-    assert r["maxForceAfter"] == pytest.approx(float(np.abs(fo).max()), rel=1e-3)
-    assert np.array_equal(pg_[:, 3], po[:, 3])
+    r = g.relax_cold_start(its, d0)
+    s0 = start["positions"].reshape(-1, 4)[:, :3].astype(np.float64)
+
+    def rms_moved(p):
+        m = p[:, :3].astype(np.float64) - s0
+        m -= np.rint(m / cfg.box[0]) * cfg.box[0]
+        return float(np.sqrt((m ** 2).sum(axis=1).mean()))
+    mg, mo = rms_moved(g.particles().reshape(-1, 4)), rms_moved(o_end)
+    print(f"relax {its} iterations: RMS displacement {mg:.4f} vs oracle {mo:.4f}; largest force "
+          f"{r['maxForceAfter']:.3e} vs {fo:.3e} (start {r['maxForceBefore']:.3e})")
+    assert mo > 0.05 and abs(mg / mo - 1) < 0.05
+    assert 0.5 < r["maxForceAfter"] / fo < 2.0
+    assert r["maxForceAfter"] < r["maxForceBefore"] and fo < r["maxForceBefore"]
     g.dispose()
