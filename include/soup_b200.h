@@ -447,8 +447,16 @@ int soup_set_diff_params(SoupHandle* h, const double* theta);
  * replay a segment bit for bit from it).  traj_device (may be NULL): device memory for steps + 1
  * frames of n float4 positions in original order (frame 0 the start), 16-byte aligned. */
 int soup_diff_forward(SoupHandle* h, uint32_t steps, uint32_t checkpoint_every, float* traj_device);
-/* The reverse pass of the last soup_diff_forward.  dldx_device: dJ/dx_t for t = 0..steps as steps + 1
- * frames of n float4 in original order (w ignored), device memory.  theta_grad receives dJ/dtheta
+/* soup_diff_forward keeping only every frame_stride-th frame for the caller: traj_device holds
+ * steps / frame_stride + 1 frames (steps 0, frame_stride, 2 frame_stride, ..), and the reverse pass
+ * takes dJ/dx at those frames alone (the loss depends on no other step).  frame_stride must divide
+ * steps; 1 is soup_diff_forward.  This is what lets a long window of a large batch fit: the
+ * internal replay does not depend on it. */
+int soup_diff_forward_strided(SoupHandle* h, uint32_t steps, uint32_t checkpoint_every, uint32_t frame_stride,
+                              float* traj_device);
+/* The reverse pass of the last soup_diff_forward(_strided).  dldx_device: dJ/dx_t for the kept frames
+ * (t = 0, frame_stride, .., steps: steps / frame_stride + 1 frames) of n float4 in original order
+ * (w ignored), device memory.  theta_grad receives dJ/dtheta
  * (SOUP_DIFF_NPARAM doubles, host); dx0_device / dv0_device (device, n float4, may be NULL) receive
  * dJ/dx_0 and dJ/dv_0.  The Langevin noise is fixed by the window's seeds (the adjoint does not depend
  * on it).  The system is left at the window's end state. */

@@ -206,6 +206,7 @@ SIGNATURES = {
     "soup_get_diff_params": (C.c_int, [_P, C.POINTER(C.c_double)]),
     "soup_set_diff_params": (C.c_int, [_P, C.POINTER(C.c_double)]),
     "soup_diff_forward": (C.c_int, [_P, C.c_uint32, C.c_uint32, _P]),
+    "soup_diff_forward_strided": (C.c_int, [_P, C.c_uint32, C.c_uint32, C.c_uint32, _P]),
     "soup_diff_backward": (C.c_int, [_P, _P, C.POINTER(C.c_double), _P, _P]),
     "soup_aggregate_shapes": (C.c_int, [_P, _U32P, _U32P, C.c_uint32, C.c_uint32, C.POINTER(SoupAggregateShape),
                                         _U32P]),

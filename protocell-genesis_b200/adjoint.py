@@ -28,14 +28,18 @@ PARAM_NAMES = ["A_apolar_apolar", "A_apolar_polar", "A_apolar_solvent", "A_polar
 
 
 class SoupWindow(torch.autograd.Function):
+    """apply(theta, system, steps, checkpoint_every, frame_stride=1): the trajectory's frames at steps
+    0, frame_stride, .., steps (steps / frame_stride + 1 of them)."""
     @staticmethod
-    def forward(ctx, theta, system, steps, checkpoint_every):
+    def forward(ctx, theta, system, steps, checkpoint_every, frame_stride=1):
+        if int(frame_stride) < 1 or int(steps) % int(frame_stride):
+            raise ValueError("frame_stride must be positive and divide steps")
         th = theta.detach().cpu().double().numpy()
         if not np.array_equal(th, system.get_diff_params()):
             system.set_diff_params(th)
-        traj = torch.empty((int(steps) + 1, system.n, 4), dtype=torch.float32, device="cuda")
+        traj = torch.empty((int(steps) // int(frame_stride) + 1, system.n, 4), dtype=torch.float32, device="cuda")
         torch.cuda.synchronize()
-        system.diff_forward(steps, checkpoint_every, traj.data_ptr())
+        system.diff_forward(steps, checkpoint_every, traj.data_ptr(), frame_stride)
         torch.cuda.synchronize()
         ctx.system = system
         ctx.theta_dtype, ctx.theta_device = theta.dtype, theta.device
@@ -47,12 +51,12 @@ class SoupWindow(torch.autograd.Function):
         torch.cuda.synchronize()
         grad = ctx.system.diff_backward(g.data_ptr())
         torch.cuda.synchronize()
-        return torch.as_tensor(grad, dtype=ctx.theta_dtype, device=ctx.theta_device), None, None, None
+        return torch.as_tensor(grad, dtype=ctx.theta_dtype, device=ctx.theta_device), None, None, None, None
 
 
-def window(system, theta, steps, checkpoint_every):
-    """traj = SoupWindow.apply(theta, system, steps, checkpoint_every)."""
-    return SoupWindow.apply(theta, system, steps, checkpoint_every)
+def window(system, theta, steps, checkpoint_every, frame_stride=1):
+    """traj = SoupWindow.apply(theta, system, steps, checkpoint_every, frame_stride)."""
+    return SoupWindow.apply(theta, system, steps, checkpoint_every, frame_stride)
 
 
 def thickness_proxy(traj, heads, tails, box_z):

@@ -1614,9 +1614,16 @@ int soup_set_diff_params(SoupHandle* h, const double* theta) {
 }
 
 int soup_diff_forward(SoupHandle* h, uint32_t steps, uint32_t checkpoint_every, float* traj_device) {
+  return soup_diff_forward_strided(h, steps, checkpoint_every, 1, traj_device);
+}
+
+int soup_diff_forward_strided(SoupHandle* h, uint32_t steps, uint32_t checkpoint_every, uint32_t frame_stride,
+                              float* traj_device) {
   return guarded(h, [&](Batch& b, uint32_t) {
     diff_check_batch(b);
     if (steps == 0 || checkpoint_every == 0) fail(SOUP_E_ARG, "steps and checkpoint_every must be positive");
+    if (frame_stride == 0 || steps % frame_stride != 0)
+      fail(SOUP_E_ARG, "frame_stride must be positive and divide steps");
     if (traj_device && (reinterpret_cast<uintptr_t>(traj_device) & 15u)) fail(SOUP_E_ARG, "traj_device must be 16-byte aligned");
     DiffWindow& w = b.diff;
     const uint32_t N = b.N, R = b.R;
@@ -1635,9 +1642,13 @@ int soup_diff_forward(SoupHandle* h, uint32_t steps, uint32_t checkpoint_every, 
       read_replica<uint8_t>(b, r, b.frozen, 1, fr.data(), false);
       w.frozen[r].assign(fr.begin(), fr.end());
     }
-    w.steps = steps; w.every = checkpoint_every; w.step0 = b.step[0]; w.prot_rng = b.prot_rng;
+    w.steps = steps; w.every = checkpoint_every; w.stride = frame_stride; w.step0 = b.step[0]; w.prot_rng = b.prot_rng;
+    // the caller's frame of step t (t a multiple of the stride), or NULL
+    auto out_frame = [&](uint32_t t) -> float4* {
+      return (traj_device && t % frame_stride == 0) ? reinterpret_cast<float4*>(traj_device) + (size_t)(t / frame_stride) * N
+                                                    : nullptr;
+    };
     w.ck_pos.clear(); w.ck_vel.clear(); w.ck_trng.clear();
-    float4* traj = reinterpret_cast<float4*>(traj_device);
     const size_t frame_bytes = 16 * (size_t)N * (steps + 1);
     w.stored = frame_bytes <= frame_budget();
     if (w.stored) {   // keep every frame: the reverse pass reads them instead of replaying segments
@@ -1648,17 +1659,19 @@ int soup_diff_forward(SoupHandle* h, uint32_t steps, uint32_t checkpoint_every, 
         diff_step(b);
         adj_unpermute(b, w.all + (size_t)(t + 1) * N);
       }
-      if (traj) SOUP_CUDA_TRY(cudaMemcpyAsync(traj, w.all, frame_bytes, cudaMemcpyDeviceToDevice, b.stream));
+      for (uint32_t t = 0; t <= steps && traj_device; t += frame_stride)
+        SOUP_CUDA_TRY(cudaMemcpyAsync(out_frame(t), w.all + (size_t)t * N, 16 * (size_t)N, cudaMemcpyDeviceToDevice,
+                                      b.stream));
     }
     for (uint32_t t = 0; t < steps && !w.stored; ++t) {
       if (t % checkpoint_every == 0) {
         w.ck_pos.emplace_back(); w.ck_vel.emplace_back(); w.ck_trng.emplace_back();
         diff_read(b, w.ck_pos.back(), w.ck_vel.back(), w.ck_trng.back());
         diff_restore(b, w.ck_pos.back(), w.ck_vel.back(), w.ck_trng.back());
-        if (t == 0 && traj) adj_unpermute(b, traj);
+        if (t == 0 && traj_device) adj_unpermute(b, out_frame(0));
       }
       diff_step(b);
-      if (traj) adj_unpermute(b, traj + (size_t)(t + 1) * N);
+      if (float4* f = out_frame(t + 1)) adj_unpermute(b, f);
     }
     diff_read(b, w.end_pos, w.end_vel, w.end_trng);
     w.end_step = b.step[0];
@@ -1673,8 +1686,11 @@ int soup_diff_backward(SoupHandle* h, const float* dldx_device, double* theta_gr
     DiffWindow& w = b.diff;
     if (!w.ready) fail(SOUP_E_STATE, "no differentiable window: call soup_diff_forward first");
     if (!dldx_device || !theta_grad) fail(SOUP_E_ARG, "NULL argument");
-    const uint32_t N = b.N, T = w.steps, K = w.every;
-    const float4* dldx = reinterpret_cast<const float4*>(dldx_device);
+    const uint32_t N = b.N, T = w.steps, K = w.every, S = w.stride;
+    // dJ/dx_t: the caller gave it for the kept frames (every S-th step); the others are zero
+    auto dldx_at = [&](uint32_t t) -> const float4* {
+      return t % S == 0 ? reinterpret_cast<const float4*>(dldx_device) + (size_t)(t / S) * N : nullptr;
+    };
     // scratch
     size_t cap1 = w.frames_cap;
     w.frames = dgrow(w.frames, cap1, (size_t)(K + 1) * N);
@@ -1692,7 +1708,7 @@ int soup_diff_backward(SoupHandle* h, const float* dldx_device, double* theta_gr
     for (uint32_t r = 0; r < b.R; ++r)
       for (uint32_t i = 0; i < b.cfg[r].n; ++i) fo[b.hsp[r].slot_off + i] = (uint8_t)w.frozen[r][i];
     SOUP_CUDA_TRY(cudaMemcpyAsync(w.frozen_o, fo.data(), N, cudaMemcpyHostToDevice, b.stream));
-    SOUP_CUDA_TRY(cudaMemcpyAsync(w.A, dldx + (size_t)T * N, 16 * (size_t)N, cudaMemcpyDeviceToDevice, b.stream));
+    SOUP_CUDA_TRY(cudaMemcpyAsync(w.A, dldx_at(T), 16 * (size_t)N, cudaMemcpyDeviceToDevice, b.stream));
     SOUP_CUDA_TRY(cudaMemsetAsync(w.B, 0, 16 * (size_t)N, b.stream));
     SOUP_CUDA_TRY(cudaMemsetAsync(w.g, 0, 16 * (size_t)N, b.stream));
     const SysParams& P = b.hsp[0];
@@ -1705,7 +1721,7 @@ int soup_diff_backward(SoupHandle* h, const float* dldx_device, double* theta_gr
         refresh_lists(b);
         adj_hvp(b, w.g, w.jg, w.partial);
         const float coef = (t - 1 == 0) ? hh : hh * (1.0f + a);
-        adj_update(b, N, w.A, w.B, w.jg, dldx + (size_t)(t - 1) * N, w.frozen_o, a, dt, coef, w.g, nullptr);
+        adj_update(b, N, w.A, w.B, w.jg, dldx_at(t - 1), w.frozen_o, a, dt, coef, w.g, nullptr);
       }
       if (dv0_device) SOUP_CUDA_TRY(cudaMemcpyAsync(dv0_device, w.B, 16 * (size_t)N, cudaMemcpyDeviceToDevice, b.stream));
       adj_scatter_pos(b, w.all);
@@ -1728,7 +1744,7 @@ int soup_diff_backward(SoupHandle* h, const float* dldx_device, double* theta_gr
         refresh_lists(b);
         adj_hvp(b, w.g, w.jg, w.partial);
         const float coef = (t - 1 == 0) ? hh : hh * (1.0f + a);
-        adj_update(b, N, w.A, w.B, w.jg, dldx + (size_t)(t - 1) * N, w.frozen_o, a, dt, coef, w.g, nullptr);
+        adj_update(b, N, w.A, w.B, w.jg, dldx_at(t - 1), w.frozen_o, a, dt, coef, w.g, nullptr);
       }
       if (seg == 0) {   // time 0: the force at x_0 only feeds the first half kick
         if (dv0_device) SOUP_CUDA_TRY(cudaMemcpyAsync(dv0_device, w.B, 16 * (size_t)N, cudaMemcpyDeviceToDevice, b.stream));

@@ -39,6 +39,7 @@ template <class T> struct DevBuf {
 // original order, the arrays that stay constant inside the window, and the reverse-pass scratch.
 struct DiffWindow {
   uint32_t steps = 0, every = 0;
+  uint32_t stride = 1;                   // the caller's frames: every stride-th step (0, stride, ..)
   uint64_t step0 = 0;
   bool ready = false;
   // per checkpoint, per replica: positions, velocities, thermostat states in original order

@@ -495,10 +495,11 @@ class SoupSystem:
         t = (C.c_double * _abi.DIFF_NPARAM)(*[float(v) for v in theta])
         _check(self._lib, self._h, self._lib.soup_set_diff_params(self._h, t))
 
-    def diff_forward(self, steps, checkpoint_every, traj_ptr=None):
-        """Differentiable window from the current state; traj_ptr: device pointer for steps + 1 frames."""
-        _check(self._lib, self._h, self._lib.soup_diff_forward(self._h, int(steps), int(checkpoint_every),
-                                                               C.c_void_p(traj_ptr) if traj_ptr else None))
+    def diff_forward(self, steps, checkpoint_every, traj_ptr=None, frame_stride=1):
+        """Differentiable window from the current state; traj_ptr: device pointer for
+        steps / frame_stride + 1 frames (every frame_stride-th step)."""
+        _check(self._lib, self._h, self._lib.soup_diff_forward_strided(
+            self._h, int(steps), int(checkpoint_every), int(frame_stride), C.c_void_p(traj_ptr) if traj_ptr else None))
 
     def diff_backward(self, dldx_ptr, dx0_ptr=None, dv0_ptr=None):
         t = (C.c_double * _abi.DIFF_NPARAM)()
@@ -605,8 +606,8 @@ class SoupBatch:
     def set_diff_params(self, theta):
         self.replicas[0].set_diff_params(theta)
 
-    def diff_forward(self, steps, checkpoint_every, traj_ptr=None):
-        self.replicas[0].diff_forward(steps, checkpoint_every, traj_ptr)
+    def diff_forward(self, steps, checkpoint_every, traj_ptr=None, frame_stride=1):
+        self.replicas[0].diff_forward(steps, checkpoint_every, traj_ptr, frame_stride)
 
     def diff_backward(self, dldx_ptr, dx0_ptr=None, dv0_ptr=None):
         return self.replicas[0].diff_backward(dldx_ptr, dx0_ptr, dv0_ptr)

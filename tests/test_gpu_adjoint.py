@@ -265,3 +265,32 @@ def test_batched_window_equals_its_replicas(monkeypatch):
     assert np.array_equal(tb[:, :n1], parts[0][2]) and np.array_equal(tb[:, n1:], parts[1][2])
     assert lb == pytest.approx(parts[0][0] + parts[1][0], rel=1e-12)
     assert np.allclose(gb, parts[0][1] + parts[1][1], rtol=1e-9, atol=1e-12)
+
+
+def test_frame_stride_gives_the_gradient_of_the_kept_frames(patch):
+    """A window that hands back every 5th frame (soup_diff_forward_strided) differentiates a loss on
+    those frames exactly as the full window does when the loss reads the same frames: the reverse
+    pass adds dJ/dx only at the kept steps, and the others are zero either way."""
+    cfg, start, w = patch
+    stride = 5
+    box = torch.tensor(list(cfg.box) + [1.0], dtype=torch.float64, device="cuda")
+    ws = w[::stride].cuda()
+
+    def run(g, frames_of):
+        g.write_state(start)
+        th = torch.tensor(g.get_diff_params(), dtype=torch.float64, requires_grad=True)
+        traj = frames_of(th)
+        loss = _displacement_loss(traj, ws, box)
+        loss.backward()
+        return traj.detach(), float(loss.detach()), th.grad.numpy().copy()
+
+    g = SoupSystem(cfg, start)
+    t_full, l_full, g_full = run(g, lambda th: adjoint.SoupWindow.apply(th, g, STEPS, EVERY)[::stride])
+    t_str, l_str, g_str = run(g, lambda th: adjoint.SoupWindow.apply(th, g, STEPS, EVERY, stride))
+    g.dispose()
+    assert t_str.shape[0] == STEPS // stride + 1
+    assert torch.equal(t_full, t_str)
+    assert l_full == l_str
+    assert np.array_equal(g_full, g_str), (g_full, g_str)
+    with pytest.raises(ValueError):
+        adjoint.SoupWindow.apply(torch.zeros(_abi.DIFF_NPARAM, dtype=torch.float64), g, STEPS, EVERY, 3)
