@@ -413,16 +413,18 @@ def run_gradient_batched(args, pkg, L, torch):
         inside = torch.sigmoid((shell[:, rep_t[water]] - rad[:, water]) / 0.5)
         return inside.sum(dim=1).mean()
 
-    steps, every = args.parcel_steps, 20
+    # config 5's window: 2,000 steps, checkpoints every 100 (the replay segments), the loss on every
+    # 20th frame (the frame stride keeps 101 frames of the batch instead of 2,001)
+    steps, every, stride = args.parcel_steps, args.parcel_checkpoint, args.parcel_stride
     stream = torch.cuda.ExternalStream(L.soup_stream(batch.replicas[0]._h))
     theta0 = batch.get_diff_params()
 
-    def window():
+    def window(n_steps):
         th = torch.tensor(theta0, dtype=torch.float64, requires_grad=True)
         e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
         torch.cuda.synchronize()
         e0.record(stream)
-        traj = adjoint.SoupWindow.apply(th, batch, steps, every)
+        traj = adjoint.SoupWindow.apply(th, batch, n_steps, every, stride)
         e1.record(stream)
         loss = encapsulated(traj)
         loss.backward()
@@ -430,23 +432,25 @@ def run_gradient_batched(args, pkg, L, torch):
         torch.cuda.synchronize()
         return float(loss.detach()), th.grad.numpy(), e0.elapsed_time(e1), e1.elapsed_time(e2)
 
-    window()
+    window(every)     # untimed: scratch allocated on first use
     fwd, bwd = [], []
-    for _ in range(args.grad_windows):
-        loss, grad, f_ms, b_ms = window()
+    for _ in range(args.parcel_windows):
+        loss, grad, f_ms, b_ms = window(steps)
         fwd.append(f_ms)
         bwd.append(b_ms)
     batch.dispose()
     total = (sum(fwd) + sum(bwd)) / len(fwd)
     return {"value": N * steps / (total / 1e3), "unit": "particle-steps/s (forward + adjoint)", "replicas": R,
-            "beads": N, "window_steps": steps, "checkpoint_every": every, "windows": len(fwd),
+            "beads": N, "window_steps": steps, "checkpoint_every": every, "frame_stride": stride,
+            "frames_kept": steps // stride + 1, "windows": len(fwd),
             "ms_per_window": total, "forward_ms": sum(fwd) / len(fwd), "backward_ms": sum(bwd) / len(bwd),
             "loss": "encapsulated-water proxy", "value_of_loss": loss,
             "theta": list(adjoint.PARAM_NAMES), "grad": [float(x) for x in grad],
             "workload": f"{R} spherical water parcels of {cfgs[0].n} beads (radius {items[0][3]:.1f} sigma, "
                         f"density 1.1 as the reference's confined composition) behind a neutral wall, 12% "
                         f"beads in five-bead amphiphiles, pH U[6,8], I 0.01 M; a {steps}-step window with bond "
-                        f"and charge Monte Carlo held off; seeded synthetic, relaxed untimed"}
+                        f"and charge Monte Carlo held off, checkpoints every {every} steps, the loss on every "
+                        f"{stride}th frame; seeded synthetic, relaxed untimed"}
 
 
 def run_batched(args, pkg, L, cfgm, rank, torch, ws=1):
@@ -490,6 +494,29 @@ def run_batched(args, pkg, L, cfgm, rank, torch, ws=1):
                         "amphiphiles, rest water, pH U[5,9], I log-U[0.001,0.1] M, sweep every 10, bonds every "
                         "20, skin planned 1.0 with drift rebuilds, lanes per particle, cell size and skin "
                         "autotuned (untimed); steps in captured CUDA graphs; seeded synthetic, relaxed untimed"}
+
+
+def run_physics_pin(pkg):
+    """The trajectory-level pin against the reference's published run (untimed): its bilayer patch
+    (tests/water-bilayer-broth.test.ts:68-181, 400 three-bead lipids + 4,500 water, seed 31), equilibrated
+    2,000 steps at 1.3 sigma^2 per lipid, taken to the area its area move settled at (1.1734 sigma^2, fixed
+    volume), settled 20,000 steps, then the head-peak thickness every 500 steps over 80 snapshots against
+    its 4.4689 sigma (verify/out/water-bilayer-area-move.json)."""
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import bilayer_broth as bb
+    import test_gpu_bilayer_pin as pin
+    t0 = time.perf_counter()
+    th, amph, box, events = pin.run_patch()
+    blocks = th.reshape(pin.BLOCKS, -1).mean(axis=1)
+    mean, sd = float(th.mean()), float(th.std(ddof=1))
+    se = float(blocks.std(ddof=1) / np.sqrt(pin.BLOCKS))
+    return {"observable": "bilayer thickness (head-density peaks, 200 bins)", "value": mean, "unit": "sigma",
+            "snapshot_sd": sd, "block_se": se, "snapshots": int(th.size), "reference": bb.THICKNESS_REFERENCE,
+            "z": (bb.THICKNESS_REFERENCE - mean) / float(np.hypot(sd, se)),
+            "area_per_lipid": box[0] * box[1] / (bb.N_LIPIDS / 2), "amphiphiles_min": int(amph.min()),
+            "events": events, "wall_s": time.perf_counter() - t0,
+            "reference_source": "verify/out/water-bilayer-area-move.json (one snapshot of its settled run)"}
 
 
 def run_gradient(args, pkg, L, torch):
@@ -859,6 +886,8 @@ def run_cuda(args):
             gradient["value"] = aggregate_rate(ws, gradient["beads"], gradient["window_steps"],
                                                gradient["ms_per_window"])
 
+    physics = run_physics_pin(pkg) if (rank == 0 and not args.no_physics) else None
+
     phases = {name: {"ms_total": t, "launches": c, "ms_per_step": t / args.prof_steps} for name, (t, c) in ktime.items() if c}
     # diagnostic: the rate with the constant-pH sweep's share of the profiled segment taken out
     seg_ms = sum(t for t, c in ktime.values())
@@ -890,7 +919,7 @@ def run_cuda(args):
             "value_excluding_sweep": value_ex_sweep,
             "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "gpu_launches": int(launches),
             "clocks": clk.summary(), "phases": phases, "batched": batched, "gradient": gradient,
-            "gradient_batched": gradient_batched}
+            "gradient_batched": gradient_batched, "physics_pin": physics}
     if rank == 0:
         print(json.dumps(line), flush=True)
     s.dispose()
@@ -920,11 +949,15 @@ def main():
     ap.add_argument("--no-analysis", action="store_true", help="leave the campaign's progress sample out of the timed steps")
     ap.add_argument("--analysis-every", type=int, default=200)
     ap.add_argument("--no-gradient", action="store_true", help="skip the forward + adjoint window measurement")
+    ap.add_argument("--no-physics", action="store_true", help="skip the bilayer-thickness pin (untimed)")
     ap.add_argument("--prof-steps", type=int, default=100, help="steps of the profiled segment (per-kernel split)")
     ap.add_argument("--grad-steps", type=int, default=200)
     ap.add_argument("--grad-windows", type=int, default=3)
     ap.add_argument("--parcel-replicas", type=int, default=16)
-    ap.add_argument("--parcel-steps", type=int, default=200)
+    ap.add_argument("--parcel-steps", type=int, default=2000)
+    ap.add_argument("--parcel-checkpoint", type=int, default=100)
+    ap.add_argument("--parcel-stride", type=int, default=20)
+    ap.add_argument("--parcel-windows", type=int, default=1)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

@@ -291,14 +291,18 @@ typedef struct SoupTuneResult {
   uint32_t tpp_before, walk_before;
   double skin_scale;              /* chosen skin / planned skin */
   double ms_per_step_before, ms_per_step_after;
-  uint32_t queued, queued_before; /* list-force variant: 0 pair maths in the screening loop, 1 in-range
-                                     pairs queued per lane and evaluated together (same result bits) */
+  uint32_t queued, queued_before; /* list-force variant: 0 pair maths in the screening loop (tpp lanes per
+                                     particle), 1 each warp's in-range pairs compacted and evaluated with
+                                     every lane busy (one lane per particle; the same result bits as
+                                     variant 0 with tpp 1) */
+  uint32_t list_cells;            /* list build: 0 a thread per particle, 1 a group of lanes per cell */
 } SoupTuneResult;
 int soup_autotune(SoupHandle* h, uint32_t steps, SoupTuneResult* out);
 /* Apply a tuning found before (by soup_autotune on a system of the same shape) without timing
  * anything: lanes per particle, the list-force variant, list-walk radius, and the current skin scaled
  * by skin_scale (at most 1: the list capacity was sized for it; drift-triggered rebuilds only).  The
- * lists are rebuilt and the force recomputed.  Only tpp, queued, walk and skin_scale are read. */
+ * lists are rebuilt and the force recomputed.  Only tpp, queued, walk, skin_scale and list_cells are
+ * read. */
 int soup_apply_tuning(SoupHandle* h, const SoupTuneResult* tuning);
 /* soup_step runs chunks of chunkSteps steps (at least 4) as captured CUDA graphs, captured on first
  * use; this captures every chunk graph of the current schedule now, without stepping. */

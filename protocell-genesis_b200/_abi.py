@@ -120,7 +120,7 @@ class SoupTuneResult(C.Structure):
     _fields_ = [
         ("tpp", C.c_uint32), ("walk", C.c_uint32), ("tpp_before", C.c_uint32), ("walk_before", C.c_uint32),
         ("skin_scale", C.c_double), ("ms_per_step_before", C.c_double), ("ms_per_step_after", C.c_double),
-        ("queued", C.c_uint32), ("queued_before", C.c_uint32),
+        ("queued", C.c_uint32), ("queued_before", C.c_uint32), ("list_cells", C.c_uint32),
     ]
 
 

@@ -51,10 +51,15 @@ __global__ void __launch_bounds__(128) k_bond_walk(
   __syncthreads();
   const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= N) return;
-  const SysParams& P = sp[sysid[k]];
-  const float box[3] = {P.box[0], P.box[1], P.box[2]};
   const float4 xi = pos[k];
   const float ti = xi.w;
+  // a bead whose kind is in no rule has no candidate, draws nothing and, unless it is a catalyst or
+  // tethered to one, leaves no item: its walk would change nothing (water, most of a campaign's beads)
+  bool in_rule = false;
+  for (int r = 0; r < 2; ++r) in_rule = in_rule || ti == S.kindA[r] || ti == S.kindB[r];
+  if (!in_rule && ti != S.cat_kind && center[k] == NONE) return;
+  const SysParams& P = sp[sysid[k]];
+  const float box[3] = {P.box[0], P.box[1], P.box[2]};
   const uint32_t gi = id[k];
   const uint32_t s0 = slots[3 * k], s1 = slots[3 * k + 1], s2 = slots[3 * k + 2];
   const float cat_reach = ex_wcut(S, ex_pairB(S, ti, S.cat_kind));

@@ -51,13 +51,32 @@ __device__ __forceinline__ void bonded_term(const Shared& S, const SysParams& P,
   fx += s * dx; fy += s * dy; fz += s * dz;
 }
 
+// The end of the part of particle k's row a force pass must read.  The row is grouped by build
+// distance (k_group_rows): shell 0 within the force's reach r0 = sqrt(rmax2), shells 1..4 the rest of the
+// list range in four widths w.  No bead has moved more than dm since the build (the replica's largest
+// drift), so a pair of shell s is at least r0 + (s - 1) w - 2 dm apart now, and shell s can hold an
+// in-range pair only if (s - 1) w < 2 dm (a margin of 1e-3 sigma covers rounding).  Skipped entries are
+// beyond the reach, so the force is the same bits as over the whole row.
+__device__ __forceinline__ uint32_t list_force_end(uint32_t k, const uint32_t* __restrict__ nl_cnt,
+                                                   const uint4* __restrict__ nl_shell, float drift2, float rmax2,
+                                                   float list_range) {
+  const uint32_t cnt = nl_cnt[k];
+  const float r0 = sqrtf(rmax2), w = (list_range - r0) * 0.25f;
+  if (!nl_shell || !(drift2 >= 0.f && drift2 < 1e30f) || !(w > 0.f)) return cnt;
+  const float x = (2.0f * sqrtf(drift2) + 1e-3f) / w;
+  if (x >= 3.0f) return cnt;
+  const uint4 e = nl_shell[k];
+  return x < 1.0f ? e.y : (x < 2.0f ? e.z : e.w);
+}
+
 // SEL: the particles are the nsel slots sel[] (the heads, after a charge sweep) instead of all N
 template <int TPP, bool SEL>
 __global__ void __launch_bounds__(256, SOUP_FORCE_MINB) k_force(
     const Shared* __restrict__ Sg, const SysParams* __restrict__ sp, const uint8_t* __restrict__ sysid, uint32_t N,
     const float4* __restrict__ pos, const float* __restrict__ charge, const uint32_t* __restrict__ slots,
     const uint32_t* __restrict__ center, const uint32_t* __restrict__ id, const uint32_t* __restrict__ slot_of,
-    const uint32_t* __restrict__ nl, const uint32_t* __restrict__ nl_cnt, uint32_t cap, float4* __restrict__ force,
+    const uint32_t* __restrict__ nl, const uint32_t* __restrict__ nl_cnt, const uint4* __restrict__ nl_shell,
+    const uint32_t* __restrict__ drift_bits, uint32_t cap, float4* __restrict__ force,
     const uint32_t* __restrict__ sel, uint32_t nsel) {
   __shared__ Shared S;
   for (int w = threadIdx.x; w < (int)(sizeof(Shared) / 4); w += blockDim.x)
@@ -70,16 +89,26 @@ __global__ void __launch_bounds__(256, SOUP_FORCE_MINB) k_force(
   const uint32_t k = SEL ? (active ? sel[g] : 0u) : g;
   float fx = 0.f, fy = 0.f, fz = 0.f;
   if (active) {
-    const SysParams& Pg = sp[sysid[k]];
+    const uint32_t rs = sysid[k];
+    const SysParams& Pg = sp[rs];
     const PairP P = PairP::of(Pg);
+    const PairLean L = PairLean::of(S, Pg);
     const float4 xi = pos[k];
     const int ki = (int)xi.w;
     const float qi = charge[k];
-    const bool needq = (qi != 0.f) || (S.cls[ki] == 1u && P.acid > 0.f);
+    const bool qi_nz = qi != 0.f;
+    const bool needq = qi_nz || (S.cls[ki] == 1u && P.acid > 0.f);
     const float rmax2 = S.rmax2;
-    const uint32_t cnt = nl_cnt[k];
+    const uint32_t cnt = list_force_end(k, nl_cnt, nl_shell, __uint_as_float(drift_bits[rs]), rmax2, Pg.list_range);
     const uint32_t* row = nl + (size_t)k * cap;
-    const PairConst* prow = &S.pair[ki * SOUP_KMAX];
+    const PairW* prow = &S.pw[ki * SOUP_KMAX];
+    // a particle at least the interaction reach inside every face has its in-range neighbours at
+    // their stored (wrapped) coordinates: the minimum image is the plain difference there (fast_mi
+    // returns it unchanged), and an entry beyond the reach by the plain difference is beyond it by the
+    // minimum image too.  Decided per warp, so that whole warps skip the image.
+    const float reach = sqrtf(rmax2) + 1e-3f;
+    const bool inside = __all_sync(__activemask(), xi.x >= reach && xi.x <= P.box[0] - reach && xi.y >= reach &&
+                                                   xi.y <= P.box[1] - reach && xi.z >= reach && xi.z <= P.box[2] - reach);
     // lane takes entries [c*4*TPP + 4*lane, +4): one 16-byte load (rows are 32-byte aligned); the
     // next chunk's load is issued before the current chunk is evaluated
     constexpr uint32_t CH = 4 * TPP;
@@ -94,14 +123,17 @@ __global__ void __launch_bounds__(256, SOUP_FORCE_MINB) k_force(
       for (int e = 0; e < 4; ++e) xj[e] = __ldg(pos + jv[e]);
 #pragma unroll
       for (int e = 0; e < 4; ++e) {
-        const float dx = fast_mi(xi.x - xj[e].x, P.box[0], P.inv_box[0]);
-        const float dy = fast_mi(xi.y - xj[e].y, P.box[1], P.inv_box[1]);
-        const float dz = fast_mi(xi.z - xj[e].z, P.box[2], P.inv_box[2]);
+        float dx = xi.x - xj[e].x, dy = xi.y - xj[e].y, dz = xi.z - xj[e].z;
+        if (!inside) {
+          dx = fast_mi(dx, P.box[0], P.inv_box[0]);
+          dy = fast_mi(dy, P.box[1], P.inv_box[1]);
+          dz = fast_mi(dz, P.box[2], P.inv_box[2]);
+        }
         const float r2 = dx * dx + dy * dy + dz * dz;
         if (r2 >= rmax2 || r2 < 1e-12f) continue;
         const int kj = (int)xj[e].w;
         const float qj = needq ? __ldg(charge + jv[e]) : 0.f;
-        const float sc = pair_scalar(S, P, prow[kj], r2, ki, kj, qi, qj);
+        const float sc = pair_lean(prow[kj], L, r2, qi_nz, qi, qj);
         fx += sc * dx; fy += sc * dy; fz += sc * dz;
       }
     }
@@ -134,116 +166,155 @@ __global__ void __launch_bounds__(256, SOUP_FORCE_MINB) k_force(
   }
 }
 
-// The same list force with the pair maths taken off the screening path.  In k_force a warp runs the
-// pair maths whenever any of its lanes holds an in-range entry, which at a skin of 0.8 is nearly
-// every chunk, so the out-of-range half of the list pays for it too.  Here each lane screens its
-// entries (index, gather, minimum image, squared distance) and pushes the in-range ones -- their
-// separation, the neighbour's charge and kind -- onto its own ring in shared memory; the warp then
-// evaluates the rings' heads together, every lane on a pair of its own particle.  A ring is first in,
-// first out in list order, so every lane accumulates exactly the terms k_force's lane does, in the
-// same order, and the force is bit-identical to k_force's.
+// The list force with the pair maths evaluated only on in-range entries, every lane busy.  In k_force
+// a warp runs the pair maths whenever any of its lanes holds an in-range entry, which at the skins in
+// use is nearly every entry, with about half the lanes idle.  Here each lane owns one particle (its
+// list row) and works in rounds: it screens its next four entries (index, gather, minimum image,
+// squared distance), the warp compacts the in-range ones owner-major (lane 0's first, each lane's in
+// list order) into shared memory, every lane evaluates pairs lane, lane + 32, .. of the compacted
+// set, and each owner then adds sc * d for its own pairs in list order with its own separations.  So
+// every particle accumulates exactly the terms k_force<1>'s lane does, in the same order and with the
+// same arithmetic, and the force is bit-identical to k_force<1>'s.
 //
-// Ring layout: entry s of lane l at [s][l], 16 bytes (dx, dy, dz, qj) plus one byte (kj), so a row of
-// the warp's pushes or pops touches each bank once.  After each chunk of 4 entries a lane holds at
-// most kQD - 4 + 4 entries: the warp evaluates min(count) rounds with every lane busy, and more
-// rounds (lanes with empty rings idle) only when some ring could not take the next chunk.
-constexpr int kQD = 16;
-constexpr int kQBlock = 256;
-constexpr size_t kQSmem = (size_t)(kQBlock / 32) * kQD * 32 * (sizeof(float4) + 1);
+// A warp whose particles all lie at least the interaction reach inside every face of one replica's box
+// skips the minimum image: for such a particle every neighbour within the reach has its stored
+// (wrapped) coordinates within the reach too, and an entry whose direct separation is beyond the
+// reach is beyond it under the minimum image as well.  Per-pair numbers that depend on the replica are
+// the owner's: a warp whose particles span replicas evaluates each owner's pairs on the owner's lane.
+constexpr int kWBlock = 128;
+constexpr int kWRound = 4;                      // entries a lane screens per round
+constexpr int kWPairs = 32 * kWRound;           // in-range pairs of one warp round, at most
+struct WarpPairs {
+  float r2[kWPairs];
+  float qj[kWPairs];
+  uint32_t ko[kWPairs];                         // neighbour kind | owner lane << 8
+  float sc[kWPairs];
+  float oq[32];                                 // owner charge
+  uint32_t okind[32];                           // owner kind | owner charge nonzero << 8
+};
 
-template <int TPP, bool SEL>
-__global__ void __launch_bounds__(kQBlock, 3) k_force_q(
+// six 128-thread blocks per SM: 80 registers, no spills (64 registers spill the round's arrays)
+#ifndef SOUP_FORCE_W_MINB
+#define SOUP_FORCE_W_MINB 6
+#endif
+template <bool SEL>
+__global__ void __launch_bounds__(kWBlock, SOUP_FORCE_W_MINB) k_force_w(
     const Shared* __restrict__ Sg, const SysParams* __restrict__ sp, const uint8_t* __restrict__ sysid, uint32_t N,
     const float4* __restrict__ pos, const float* __restrict__ charge, const uint32_t* __restrict__ slots,
     const uint32_t* __restrict__ center, const uint32_t* __restrict__ id, const uint32_t* __restrict__ slot_of,
-    const uint32_t* __restrict__ nl, const uint32_t* __restrict__ nl_cnt, uint32_t cap, float4* __restrict__ force,
+    const uint32_t* __restrict__ nl, const uint32_t* __restrict__ nl_cnt, const uint4* __restrict__ nl_shell,
+    const uint32_t* __restrict__ drift_bits, uint32_t cap, float4* __restrict__ force,
     const uint32_t* __restrict__ sel, uint32_t nsel) {
   __shared__ Shared S;
-  extern __shared__ float4 qbuf[];
+  __shared__ WarpPairs W[kWBlock / 32];
   for (int w = threadIdx.x; w < (int)(sizeof(Shared) / 4); w += blockDim.x)
     reinterpret_cast<uint32_t*>(&S)[w] = reinterpret_cast<const uint32_t*>(Sg)[w];
   __syncthreads();
-  const int wib = threadIdx.x >> 5, l32 = threadIdx.x & 31;
-  float4* qv = qbuf + (size_t)wib * kQD * 32 + l32;
-  uint8_t* qk = reinterpret_cast<uint8_t*>(qbuf + (size_t)(kQBlock / 32) * kQD * 32) + (size_t)wib * kQD * 32 + l32;
-  const uint32_t gtid = blockIdx.x * blockDim.x + threadIdx.x;
-  const uint32_t g = gtid / TPP;
-  const int lane = (int)(gtid % TPP);
+  WarpPairs& wp = W[threadIdx.x >> 5];
+  const uint32_t lane = threadIdx.x & 31u;
+  const uint32_t lt = (1u << lane) - 1u;
+  const uint32_t g = blockIdx.x * blockDim.x + threadIdx.x;
   const bool active = SEL ? g < nsel : g < N;
   const uint32_t k = SEL ? (active ? sel[g] : 0u) : (active ? g : 0u);
-  const SysParams& Pg = sp[sysid[k]];
+  const uint32_t rs = sysid[k];
+  const SysParams& Pg = sp[rs];
   const PairP P = PairP::of(Pg);
+  const PairLean L = PairLean::of(S, Pg);
   const float4 xi = pos[k];
   const int ki = (int)xi.w;
   const float qi = charge[k];
-  const bool needq = (qi != 0.f) || (S.cls[ki] == 1u && P.acid > 0.f);
+  const bool qi_nz = qi != 0.f;
+  const bool needq = qi_nz || (S.cls[ki] == 1u && P.acid > 0.f);
   const float rmax2 = S.rmax2;
-  const uint32_t cnt = active ? nl_cnt[k] : 0u;
+  const uint32_t cnt =
+      active ? list_force_end(k, nl_cnt, nl_shell, __uint_as_float(drift_bits[rs]), rmax2, Pg.list_range) : 0u;
   const uint32_t* row = nl + (size_t)k * cap;
-  const PairConst* prow = &S.pair[ki * SOUP_KMAX];
+  wp.oq[lane] = qi;
+  wp.okind[lane] = (uint32_t)ki | (qi_nz ? 0x100u : 0u);
+  const bool uni = __all_sync(0xffffffffu, rs == __shfl_sync(0xffffffffu, rs, 0));
+  const float reach = sqrtf(rmax2) + 1e-3f;
+  const bool inside = !active || (xi.x >= reach && xi.x <= P.box[0] - reach && xi.y >= reach &&
+                                  xi.y <= P.box[1] - reach && xi.z >= reach && xi.z <= P.box[2] - reach);
+  const bool direct = uni && __all_sync(0xffffffffu, inside);
   float fx = 0.f, fy = 0.f, fz = 0.f;
-  uint32_t head = 0, tail = 0;
-  auto pop = [&]() {
-    const uint32_t s = head & (kQD - 1);
-    const float4 e = qv[s * 32];
-    const int kj = qk[s * 32];
-    ++head;
-    const float r2 = e.x * e.x + e.y * e.y + e.z * e.z;
-    const float sc = pair_scalar(S, P, prow[kj], r2, ki, kj, qi, e.w);
-    fx += sc * e.x; fy += sc * e.y; fz += sc * e.z;
-  };
-  constexpr uint32_t CH = 4 * TPP;
-  uint32_t base = 4u * (uint32_t)lane;
-  uint4 nxt = base < cnt ? __ldg(reinterpret_cast<const uint4*>(row + base)) : make_uint4(k, k, k, k);
-  for (;; base += CH) {
-    const bool more = base < cnt;
-    if (!__any_sync(0xffffffffu, more)) break;
-    if (more) {
-      const uint4 jj = nxt;
-      if (base + CH < cnt) nxt = __ldg(reinterpret_cast<const uint4*>(row + base + CH));
-      const uint32_t jv[4] = {jj.x, base + 1 < cnt ? jj.y : k, base + 2 < cnt ? jj.z : k, base + 3 < cnt ? jj.w : k};
-      float4 xj[4];
+  uint4 nxt = cnt > 0 ? __ldg(reinterpret_cast<const uint4*>(row)) : make_uint4(k, k, k, k);
+  for (uint32_t base = 0;; base += kWRound) {
+    if (!__any_sync(0xffffffffu, base < cnt)) break;
+    const uint4 jj = nxt;
+    if (base + kWRound < cnt) nxt = __ldg(reinterpret_cast<const uint4*>(row + base + kWRound));
+    const uint32_t jv[4] = {base < cnt ? jj.x : k, base + 1 < cnt ? jj.y : k, base + 2 < cnt ? jj.z : k,
+                            base + 3 < cnt ? jj.w : k};
+    float4 xj[4];
 #pragma unroll
-      for (int e = 0; e < 4; ++e) xj[e] = __ldg(pos + jv[e]);
+    for (int e = 0; e < 4; ++e) xj[e] = __ldg(pos + jv[e]);
+    float dx[4], dy[4], dz[4], r2[4];
+    bool in[4];
+    uint32_t c = 0;
 #pragma unroll
-      for (int e = 0; e < 4; ++e) {
-        const float dx = fast_mi(xi.x - xj[e].x, P.box[0], P.inv_box[0]);
-        const float dy = fast_mi(xi.y - xj[e].y, P.box[1], P.inv_box[1]);
-        const float dz = fast_mi(xi.z - xj[e].z, P.box[2], P.inv_box[2]);
-        const float r2 = dx * dx + dy * dy + dz * dz;
-        if (r2 < rmax2 && r2 >= 1e-12f) {
-          const uint32_t s = tail & (kQD - 1);
-          qv[s * 32] = make_float4(dx, dy, dz, needq ? __ldg(charge + jv[e]) : 0.f);
-          qk[s * 32] = (uint8_t)xj[e].w;
-          ++tail;
-        }
+    for (int e = 0; e < 4; ++e) {
+      if (direct) {
+        dx[e] = xi.x - xj[e].x; dy[e] = xi.y - xj[e].y; dz[e] = xi.z - xj[e].z;
+      } else {
+        dx[e] = fast_mi(xi.x - xj[e].x, P.box[0], P.inv_box[0]);
+        dy[e] = fast_mi(xi.y - xj[e].y, P.box[1], P.inv_box[1]);
+        dz[e] = fast_mi(xi.z - xj[e].z, P.box[2], P.inv_box[2]);
+      }
+      r2[e] = dx[e] * dx[e] + dy[e] * dy[e] + dz[e] * dz[e];
+      in[e] = base + e < cnt && r2[e] < rmax2 && r2[e] >= 1e-12f;
+      c += in[e] ? 1u : 0u;
+    }
+    // owner-major offsets of this round's in-range pairs
+    uint32_t incl = c;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= (uint32_t)o) incl += t;
+    }
+    const uint32_t first = incl - c;
+    const uint32_t total = __shfl_sync(0xffffffffu, incl, 31);
+    uint32_t p = first;
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      if (in[e]) {
+        wp.r2[p] = r2[e];
+        wp.qj[p] = needq ? __ldg(charge + jv[e]) : 0.f;
+        wp.ko[p] = (uint32_t)xj[e].w | (lane << 8);
+        ++p;
       }
     }
-    // every lane busy for min(count) rounds; more only when a ring could not take the next chunk
-    const uint32_t c = tail - head;
-    const uint32_t mn = __reduce_min_sync(0xffffffffu, c), mx = __reduce_max_sync(0xffffffffu, c);
-    const uint32_t rounds = max(mn, mx > (uint32_t)(kQD - 4) ? mx - (uint32_t)(kQD - 4) : 0u);
-    for (uint32_t t = 0; t < rounds; ++t)
-      if (tail != head) pop();
+    __syncwarp();
+    if (uni) {
+      for (uint32_t q = lane; q < total; q += 32u) {
+        const uint32_t ko = wp.ko[q];
+        const uint32_t o = ko >> 8, kj = ko & 0xffu;
+        const uint32_t ok = wp.okind[o];
+        const uint32_t kio = ok & 0xffu;
+        wp.sc[q] = pair_lean(S.pw[kio * SOUP_KMAX + kj], L, wp.r2[q], (ok >> 8) != 0u, wp.oq[o], wp.qj[q]);
+      }
+    } else {
+      const PairW* prow = &S.pw[ki * SOUP_KMAX];
+      for (uint32_t q = first; q < incl; ++q)
+        wp.sc[q] = pair_lean(prow[wp.ko[q] & 0xffu], L, wp.r2[q], qi_nz, qi, wp.qj[q]);
+    }
+    __syncwarp();
+    p = first;
+#pragma unroll
+    for (int e = 0; e < 4; ++e) {
+      if (in[e]) {
+        const float sc = wp.sc[p++];
+        fx += sc * dx[e]; fy += sc * dy[e]; fz += sc * dz[e];
+      }
+    }
+    __syncwarp();
   }
-  while (__any_sync(0xffffffffu, tail != head))
-    if (tail != head) pop();
   if (active) {
-    // bonded terms (bondedForce), spread over the group
+    // bonded terms (bondedForce), all on the particle's lane
     uint32_t sl[3] = {slots[3 * k], slots[3 * k + 1], slots[3 * k + 2]};
     uint32_t owner = center[k];
     if ((sl[0] & sl[1] & sl[2] & owner) != SOUP_NONE_U32) {
       const uint32_t gi = id[k];
-      for (int t = lane; t < 13; t += TPP) bonded_term(S, Pg, t, gi, xi, sl, owner, slots, slot_of, pos, fx, fy, fz);
+      for (int t = 0; t < 13; ++t) bonded_term(S, Pg, t, gi, xi, sl, owner, slots, slot_of, pos, fx, fy, fz);
     }
-  }
-#pragma unroll
-  for (int o = TPP / 2; o > 0; o >>= 1) {
-    fx += __shfl_xor_sync(0xffffffffu, fx, o);
-    fy += __shfl_xor_sync(0xffffffffu, fy, o);
-    fz += __shfl_xor_sync(0xffffffffu, fz, o);
-  }
-  if (active && lane == 0) {
     if (Pg.wall_r > 0.f) {   // wall.wgsl:42-56
       float d0 = xi.x - Pg.box[0] * 0.5f, d1 = xi.y - Pg.box[1] * 0.5f, d2 = xi.z - Pg.box[2] * 0.5f;
       float r = sqrtf(d0 * d0 + d1 * d1 + d2 * d2);
@@ -283,21 +354,29 @@ __global__ void __launch_bounds__(256) k_es_far(const SysParams* __restrict__ sp
   float fx = 0.f, fy = 0.f, fz = 0.f;
   const uint32_t cnt = es_cnt[h];
   const uint32_t* row = es_nl + (size_t)h * cap;
-  for (uint32_t s = lane; s < cnt; s += 32) {
-    const float4 xj = __ldg(xq + __ldg(row + s));
+  auto add = [&](const float4& xj) {
     const float qj = xj.w;
-    if (qj == 0.f) continue;
+    if (qj == 0.f) return;
     const float dx = fast_mi(xi.x - xj.x, P.box[0], P.inv_box[0]);
     const float dy = fast_mi(xi.y - xj.y, P.box[1], P.inv_box[1]);
     const float dz = fast_mi(xi.z - xj.z, P.box[2], P.inv_box[2]);
     const float r2 = dx * dx + dy * dy + dz * dz;
     const float rinv = rsqrtf(r2);
     const float r = r2 * rinv;
-    if (r < P.es_split || r >= P.es_rc) continue;   // esForceFar (electrostatics.wgsl:87-90)
+    if (r < P.es_split || r >= P.es_rc) return;   // esForceFar (electrostatics.wgsl:87-90)
     const float u = P.es_A * __expf(-P.es_kappa * r) * rinv;
     const float sc = qi * qj * (u * (rinv + P.es_kappa) - P.es_fc) * rinv;
     fx += sc * dx; fy += sc * dy; fz += sc * dz;
+  };
+  // lane takes entries lane, lane + 32, ... in order; four of them per pass have every index and
+  // every gather in flight before the first is evaluated
+  uint32_t s = (uint32_t)lane;
+  for (; s + 96u < cnt; s += 128u) {
+    const uint32_t i0 = __ldg(row + s), i1 = __ldg(row + s + 32u), i2 = __ldg(row + s + 64u), i3 = __ldg(row + s + 96u);
+    const float4 x0 = __ldg(xq + i0), x1 = __ldg(xq + i1), x2 = __ldg(xq + i2), x3 = __ldg(xq + i3);
+    add(x0); add(x1); add(x2); add(x3);
   }
+  for (; s < cnt; s += 32u) add(__ldg(xq + __ldg(row + s)));
   for (int o = 16; o > 0; o >>= 1) {
     fx += __shfl_xor_sync(0xffffffffu, fx, o);
     fy += __shfl_xor_sync(0xffffffffu, fy, o);
@@ -323,6 +402,7 @@ __global__ void __launch_bounds__(128) k_force_brute(
   const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= N) return;
   const SysParams& P = sp[sysid[k]];
+  const PairLean L = PairLean::of(S, P);
   const float4 xi = pos[k];
   const int ki = (int)xi.w;
   const float qi = charge[k];
@@ -338,7 +418,7 @@ __global__ void __launch_bounds__(128) k_force_brute(
     const int kj = (int)xj.w;
     const float qj = charge[j];
     if (r2 < S.rmax2) {
-      const float sc = pair_scalar(S, P, S.pair[ki * SOUP_KMAX + kj], r2, ki, kj, qi, qj);
+      const float sc = pair_lean(S.pw[ki * SOUP_KMAX + kj], L, r2, qi != 0.f, qi, qj);
       fx += sc * dx; fy += sc * dy; fz += sc * dz;
     }
     const float qq = qi * qj;
@@ -366,23 +446,16 @@ __global__ void __launch_bounds__(128) k_force_brute(
   force[k] = make_float4(fx, fy, fz, 0.f);
 }
 
-template <int TPP>
-void launch_force_q(Batch& b, bool heads) {
-  static bool attr = false;   // once per process: the rings are dynamic shared memory above 48 KB
-  if (!attr) {
-    SOUP_CUDA_TRY(cudaFuncSetAttribute(k_force_q<TPP, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kQSmem));
-    SOUP_CUDA_TRY(cudaFuncSetAttribute(k_force_q<TPP, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)kQSmem));
-    attr = true;
-  }
+void launch_force_w(Batch& b, bool heads) {
   if (heads) {
     if (b.H == 0) return;
-    k_force_q<TPP, true><<<nblocks((uint64_t)b.H * TPP, kQBlock), kQBlock, kQSmem, b.stream>>>(
-        b.shared, b.sp, b.sysid, b.N, b.pos, b.charge, b.slots, b.center, b.id, b.slot_of, b.nl, b.nl_cnt, b.list_cap,
+    k_force_w<true><<<nblocks(b.H, kWBlock), kWBlock, 0, b.stream>>>(
+        b.shared, b.sp, b.sysid, b.N, b.pos, b.charge, b.slots, b.center, b.id, b.slot_of, b.nl, b.nl_cnt, b.prune ? b.nl_shell : nullptr, b.drift_bits, b.list_cap,
         b.force, b.head_slot, b.H);
     return;
   }
-  k_force_q<TPP, false><<<nblocks((uint64_t)b.N * TPP, kQBlock), kQBlock, kQSmem, b.stream>>>(
-      b.shared, b.sp, b.sysid, b.N, b.pos, b.charge, b.slots, b.center, b.id, b.slot_of, b.nl, b.nl_cnt, b.list_cap,
+  k_force_w<false><<<nblocks(b.N, kWBlock), kWBlock, 0, b.stream>>>(
+      b.shared, b.sp, b.sysid, b.N, b.pos, b.charge, b.slots, b.center, b.id, b.slot_of, b.nl, b.nl_cnt, b.prune ? b.nl_shell : nullptr, b.drift_bits, b.list_cap,
       b.force, nullptr, 0u);
 }
 
@@ -391,12 +464,12 @@ void launch_force_tpp(Batch& b, bool heads) {
   if (heads) {
     if (b.H == 0) return;
     k_force<TPP, true><<<nblocks((uint64_t)b.H * TPP, 256), 256, 0, b.stream>>>(
-        b.shared, b.sp, b.sysid, b.N, b.pos, b.charge, b.slots, b.center, b.id, b.slot_of, b.nl, b.nl_cnt, b.list_cap,
+        b.shared, b.sp, b.sysid, b.N, b.pos, b.charge, b.slots, b.center, b.id, b.slot_of, b.nl, b.nl_cnt, b.prune ? b.nl_shell : nullptr, b.drift_bits, b.list_cap,
         b.force, b.head_slot, b.H);
     return;
   }
   k_force<TPP, false><<<nblocks((uint64_t)b.N * TPP, 256), 256, 0, b.stream>>>(
-      b.shared, b.sp, b.sysid, b.N, b.pos, b.charge, b.slots, b.center, b.id, b.slot_of, b.nl, b.nl_cnt, b.list_cap,
+      b.shared, b.sp, b.sysid, b.N, b.pos, b.charge, b.slots, b.center, b.id, b.slot_of, b.nl, b.nl_cnt, b.prune ? b.nl_shell : nullptr, b.drift_bits, b.list_cap,
       b.force, nullptr, 0u);
 }
 
@@ -415,12 +488,8 @@ void launch_force(Batch& b) {
 
 void launch_force_list(Batch& b, bool heads) {
   b.launches += 1;
-  if (b.queued) {
-    switch (b.tpp) {
-      case 1: launch_force_q<1>(b, heads); break;
-      case 2: launch_force_q<2>(b, heads); break;
-      default: launch_force_q<4>(b, heads); break;
-    }
+  if (b.queued) {   // the warp-compacted kernel: one lane per particle whatever tpp says
+    launch_force_w(b, heads);
     return;
   }
   switch (b.tpp) {

@@ -203,6 +203,25 @@ __device__ __forceinline__ float gap_to_cell(float p, int c, float cs) {
   return fmaxf(0.f, fmaxf(lo, -hi) - 1e-4f);
 }
 
+// The build-distance shell of a list entry, carried in its top three bits until k_group_rows groups
+// the row: 0 inside the force's reach (sqrt(rmax2)), 1..4 the rest of the list range in four equal
+// widths.  A force pass needs shell k > 0 only once the largest displacement since the build can have
+// closed (k - 1) widths (list_force_end).
+struct Shells {
+  float reach2, e1, e2, e3;
+  __device__ __forceinline__ static Shells of(float rmax2, float list_range) {
+    Shells s;
+    const float r0 = sqrtf(rmax2), w = fmaxf(list_range - r0, 0.f) * 0.25f;
+    s.reach2 = rmax2;
+    s.e1 = (r0 + w) * (r0 + w); s.e2 = (r0 + 2.f * w) * (r0 + 2.f * w); s.e3 = (r0 + 3.f * w) * (r0 + 3.f * w);
+    return s;
+  }
+  __device__ __forceinline__ uint32_t tag(float r2) const {
+    const uint32_t k = r2 < reach2 ? 0u : 1u + (r2 >= e1) + (r2 >= e2) + (r2 >= e3);
+    return k << 29;
+  }
+};
+
 // soup/wgsl/verlet.wgsl:53-92, thread per particle, rows of cells as contiguous slot ranges.  When
 // the walk does not wrap onto itself, each (y, z) row of cells is trimmed to the x cells that can
 // reach the list sphere (with a margin) and rows wholly outside it are skipped; the accept test is
@@ -210,10 +229,11 @@ __device__ __forceinline__ float gap_to_cell(float p, int c, float cs) {
 __global__ void __launch_bounds__(128) k_build_list(
     const float4* __restrict__ pos, const uint8_t* __restrict__ sysid, const SysParams* __restrict__ sp,
     const uint32_t* __restrict__ cell_of, const uint32_t* __restrict__ start, uint32_t N, uint32_t cap,
-    uint32_t* __restrict__ nl, uint32_t* __restrict__ nl_cnt, uint32_t* __restrict__ flags) {
+    float rmax2, uint32_t* __restrict__ nl, uint32_t* __restrict__ nl_cnt, uint32_t* __restrict__ flags) {
   uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
   if (k >= N) return;
   const SysParams& P = sp[sysid[k]];
+  const Shells sh = Shells::of(rmax2, P.list_range);
   const float4 xi = pos[k];
   const float box[3] = {P.box[0], P.box[1], P.box[2]};
   const float inv[3] = {P.inv_box[0], P.inv_box[1], P.inv_box[2]};
@@ -251,7 +271,7 @@ __global__ void __launch_bounds__(128) k_build_list(
       const float r2 = dx * dx + dy * dy + dz * dz;
       if (r2 > lr2_hi) continue;
       if (r2 >= lr2_lo && !(ex_dist(xi, xj, box) < lr)) continue;
-      if (cnt < cap) row[cnt] = j;
+      if (cnt < cap) row[cnt] = j | sh.tag(r2);
       ++cnt;
     }
   };
@@ -293,7 +313,7 @@ __global__ void __launch_bounds__(128) k_build_list(
           const float r2 = dx * dx + dy * dy + dz * dz;
           if (r2 > lr2_hi) continue;
           if (r2 >= lr2_lo && !(ex_dist(xi, xj, box) < lr)) continue;
-          if (cnt < cap) row[cnt] = j;
+          if (cnt < cap) row[cnt] = j | sh.tag(r2);
           ++cnt;
         }
       }
@@ -301,6 +321,166 @@ __global__ void __launch_bounds__(128) k_build_list(
   }
   if (cnt > cap) { flags[0] = 1u; cnt = cap; }
   nl_cnt[k] = cnt;
+}
+
+// The same list build with the neighbour cells staged, for replicas whose walk does not wrap onto
+// itself (every grid side at least 2 walk + 1 cells).  A group of 8 lanes takes one cell; its lanes
+// hold up to 8 of the cell's particles at a time.  The group walks the cell's neighbour rows in
+// k_build_list's order (z, then y, then the x cells of the row as at most two wrapped segments) and
+// stages each segment 8 particles at a time in shared memory, shifted by the periodic image of the
+// segment, so that the separation is a plain difference; every lane then tests the 8 staged beads
+// against its particle.  A particle's accepted neighbours therefore come in k_build_list's order and
+// pass its test (the fast squared distance away from the range, the exact reference arithmetic on
+// the unshifted positions within 1e-5 of it), and the rows are the same lists.  Four groups in a warp
+// take four consecutive cells of one x row, whose neighbour rows coincide.
+constexpr int kGroup = 8;
+constexpr int kGBlock = 128;
+__global__ void __launch_bounds__(kGBlock) k_build_list_cells(
+    const float4* __restrict__ pos, const SysParams* __restrict__ sp, const uint8_t* __restrict__ cell_sys,
+    const uint32_t* __restrict__ start, uint32_t ncells, uint32_t cap, float rmax2, uint32_t* __restrict__ nl,
+    uint32_t* __restrict__ nl_cnt, uint32_t* __restrict__ flags) {
+  __shared__ float4 stage[kGBlock];
+  // every loop below runs the same trip count on the whole warp (the maximum over its four groups,
+  // with the shorter groups predicated off): groups that branched apart would run one after another
+  const uint32_t cg = (blockIdx.x * blockDim.x + threadIdx.x) / kGroup;
+  const bool have = cg < ncells;
+  const uint32_t c = have ? cg : 0u;
+  const uint32_t l8 = threadIdx.x & (kGroup - 1);
+  float4* st = stage + (threadIdx.x & ~(kGroup - 1));
+  const SysParams& P = sp[cell_sys[c]];
+  const float bx = P.box[0], by = P.box[1], bz = P.box[2];
+  const float lr = P.list_range;
+  const float lr2_lo = lr * lr * (1.0f - 1e-5f), lr2_hi = lr * lr * (1.0f + 1e-5f);
+  const Shells sh = Shells::of(rmax2, lr);
+  const uint32_t cl = c - P.cell_off;
+  const int dx = P.dims[0], dy = P.dims[1], dz = P.dims[2];
+  const int qx = (int)(cl % (uint32_t)dx), qy = (int)((cl / (uint32_t)dx) % (uint32_t)dy),
+            qz = (int)(cl / ((uint32_t)dx * (uint32_t)dy));
+  const int R = P.walk;
+  // the row's x cells as at most two wrapped segments, in axis_ranges' order (qx - R .. qx + R does
+  // not wrap onto itself here), and the image shift of each: cells wrapped round a face sit one box
+  // beyond it
+  const bool wrap_lo = qx - R < 0, wrap_hi = qx + R >= dx;
+  const int nseg = (wrap_lo || wrap_hi) ? 2 : 1;
+  const int s0lo = wrap_lo ? qx - R + dx : qx - R, s0hi = (wrap_lo || wrap_hi) ? dx - 1 : qx + R;
+  const int s1hi = wrap_lo ? qx + R : qx + R - dx;
+  const float xs0 = wrap_lo ? -bx : 0.f;
+  const float xs1 = wrap_hi ? bx : 0.f;
+  const uint32_t a_i = have ? start[c] : 0u, e_i = have ? start[c + 1] : 0u;
+  const uint32_t nib = __reduce_max_sync(0xffffffffu, (e_i - a_i + kGroup - 1) / kGroup);
+  for (uint32_t ib = 0; ib < nib; ++ib) {
+    const uint32_t k = a_i + ib * kGroup + l8;
+    const bool mine = k < e_i;
+    const float4 xi = mine ? pos[k] : make_float4(0.f, 0.f, 0.f, 0.f);
+    uint32_t cnt = 0;
+    uint32_t* row = nl + (size_t)(mine ? k : 0u) * cap;
+    // R is the replica's walk; a warp spans one x row of one replica, so every bound is warp-uniform
+    for (int oz = -R; oz <= R; ++oz) {
+      const int z = qz + oz;
+      const int cz = (z + dz) % dz;
+      const float sz = z < 0 ? -bz : (z >= dz ? bz : 0.f);
+      for (int oy = -R; oy <= R; ++oy) {
+        const int y = qy + oy;
+        const int cy = (y + dy) % dy;
+        const float sy = y < 0 ? -by : (y >= dy ? by : 0.f);
+        const uint32_t rowbase = P.cell_off + (uint32_t)(dx * (cy + dy * cz));
+#pragma unroll
+        for (int sgi = 0; sgi < 2; ++sgi) {
+          uint32_t a = 0, len = 0;
+          if (have && sgi < nseg) {
+            a = start[rowbase + (sgi == 0 ? s0lo : 0)];
+            len = start[rowbase + (sgi == 0 ? s0hi : s1hi) + 1] - a;
+          }
+          const float xs = sgi == 0 ? xs0 : xs1;
+          const uint32_t mlen = __reduce_max_sync(0xffffffffu, len);
+          for (uint32_t t0 = 0; t0 < mlen; t0 += kGroup) {
+            if (t0 + l8 < len) {
+              const uint32_t j = a + t0 + l8;
+              const float4 p = pos[j];
+              st[l8] = make_float4(p.x + xs, p.y + sy, p.z + sz, __uint_as_float(j));
+            }
+            __syncwarp();
+#pragma unroll
+            for (uint32_t u = 0; u < (uint32_t)kGroup; ++u) {
+              const float4 q = st[u];
+              const uint32_t jj = __float_as_uint(q.w);
+              const float ddx = xi.x - q.x, ddy = xi.y - q.y, ddz = xi.z - q.z;
+              const float r2 = ddx * ddx + ddy * ddy + ddz * ddz;
+              if (!mine || t0 + u >= len || jj == k || r2 > lr2_hi) continue;
+              if (r2 >= lr2_lo) {
+                const float4 pj = pos[jj];
+                const float ex = ex_len(ex_mi(__fsub_rn(xi.x, pj.x), bx), ex_mi(__fsub_rn(xi.y, pj.y), by),
+                                        ex_mi(__fsub_rn(xi.z, pj.z), bz));
+                if (!(ex < lr)) continue;
+              }
+              if (cnt < cap) row[cnt] = jj | sh.tag(r2);
+              ++cnt;
+            }
+            __syncwarp();
+          }
+        }
+      }
+    }
+    if (mine) {
+      if (cnt > cap) { flags[0] = 1u; cnt = cap; }
+      nl_cnt[k] = cnt;
+    }
+  }
+}
+
+// Group every row by build-distance shell (stable: a shell keeps the build's order), strip the tags,
+// and record where shells 0..3 end.  A warp per row: a row of up to 32 * kGRegs entries is read in one
+// go into registers (every load in flight at once), a longer one (dense aggregates) is staged in
+// shared memory.
+constexpr uint32_t kGRegs = 16;
+__global__ void k_group_rows(uint32_t N, uint32_t cap, uint32_t* __restrict__ nl, const uint32_t* __restrict__ nl_cnt,
+                             uint4* __restrict__ shell_end) {
+  extern __shared__ uint32_t gbuf[];
+  const uint32_t wib = threadIdx.x >> 5, lane = threadIdx.x & 31u;
+  const uint32_t k = blockIdx.x * (blockDim.x >> 5) + wib;
+  if (k >= N) return;   // whole warps
+  uint32_t* row = nl + (size_t)k * cap;
+  const uint32_t cnt = min(nl_cnt[k], cap);
+  const uint32_t lt = (1u << lane) - 1u;
+  uint32_t out = 0, e[4];
+  if (cnt <= 32u * kGRegs) {
+    uint32_t v[kGRegs];
+#pragma unroll
+    for (uint32_t c = 0; c < kGRegs; ++c) {
+      const uint32_t s = 32u * c + lane;
+      v[c] = s < cnt ? row[s] : 0xFFFFFFFFu;   // tag 7: no shell
+    }
+    __syncwarp();
+#pragma unroll
+    for (uint32_t b = 0; b < 5; ++b) {
+#pragma unroll
+      for (uint32_t c = 0; c < kGRegs; ++c) {
+        if (32u * c >= cnt) break;
+        const bool hit = (v[c] >> 29) == b;
+        const uint32_t m = __ballot_sync(0xffffffffu, hit);
+        if (hit) row[out + __popc(m & lt)] = v[c] & 0x1FFFFFFFu;
+        out += __popc(m);
+      }
+      if (b < 4) e[b] = out;
+    }
+  } else {
+    uint32_t* sb = gbuf + (size_t)wib * cap;
+    for (uint32_t s = lane; s < cnt; s += 32u) sb[s] = row[s];
+    __syncwarp();
+#pragma unroll
+    for (uint32_t b = 0; b < 5; ++b) {
+      for (uint32_t s0 = 0; s0 < cnt; s0 += 32u) {
+        const uint32_t s = s0 + lane;
+        const uint32_t v = s < cnt ? sb[s] : 0xFFFFFFFFu;
+        const bool hit = (v >> 29) == b;
+        const uint32_t m = __ballot_sync(0xffffffffu, hit);
+        if (hit) row[out + __popc(m & lt)] = v & 0x1FFFFFFFu;
+        out += __popc(m);
+      }
+      if (b < 4) e[b] = out;
+    }
+  }
+  if (lane == 0) shell_end[k] = make_uint4(e[0], e[1], e[2], e[3]);
 }
 
 // heads: bin into the coarse head grid (replica-local cells), deterministic order inside a cell
@@ -340,6 +520,18 @@ __global__ void k_head_sort_cells(const uint32_t* __restrict__ hstart, uint32_t 
   }
 }
 
+// the heads in head-cell order with their positions: the list build reads one 16-byte record per
+// candidate instead of the index, the head's slot and its position one after another
+__global__ void k_head_gather_sorted(const uint32_t* __restrict__ hsorted, uint32_t H,
+                                     const uint32_t* __restrict__ head_slot, const float4* __restrict__ pos,
+                                     float4* __restrict__ xg) {
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= H) return;
+  const uint32_t g = hsorted[t];
+  const float4 p = pos[head_slot[g]];
+  xg[t] = make_float4(p.x, p.y, p.z, __uint_as_float(g));
+}
+
 // soup/wgsl/electrostatics-long.wgsl:31-56 head list at rc_es + skin, via the head grid, a warp per
 // head: lanes test 32 candidates at a time, hits are compacted with a ballot.  Entries are the
 // neighbours' HEAD indices (head_slot maps them to slots); membership uses the exact test near the
@@ -347,7 +539,7 @@ __global__ void k_head_sort_cells(const uint32_t* __restrict__ hstart, uint32_t 
 __global__ void __launch_bounds__(256) k_build_es_list(const uint32_t* __restrict__ head_sys, uint32_t H,
                                                        const uint32_t* __restrict__ head_slot, const float4* __restrict__ pos,
                                                        const SysParams* __restrict__ sp, const uint32_t* __restrict__ hcell_of,
-                                                       const uint32_t* __restrict__ hstart, const uint32_t* __restrict__ hsorted,
+                                                       const uint32_t* __restrict__ hstart, const float4* __restrict__ hxg,
                                                        uint32_t cap, uint32_t* __restrict__ es_nl, uint32_t* __restrict__ es_cnt,
                                                        uint32_t* __restrict__ flags) {
   const uint32_t h = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -381,9 +573,9 @@ __global__ void __launch_bounds__(256) k_build_es_list(const uint32_t* __restric
       bool hit = false;
       uint32_t g = 0;
       if (t < e0) {
-        g = hsorted[t];
+        const float4 xj = hxg[t];
+        g = __float_as_uint(xj.w);
         if (g != h) {
-          const float4 xj = pos[head_slot[g]];
           const float dx = fast_mi(xi.x - xj.x, box[0], inv[0]);
           const float dy = fast_mi(xi.y - xj.y, box[1], inv[1]);
           const float dz = fast_mi(xi.z - xj.z, box[2], inv[2]);
@@ -463,8 +655,22 @@ void launch_sort_and_gather(Batch& b) {
 void launch_build_lists(Batch& b) {
   b.launches += 1;
   prof_begin(b, SOUP_K_LIST);
-  k_build_list<<<nblocks(b.N, 128), 128, 0, b.stream>>>(b.pos, b.sysid, b.sp, b.cell_of_slot, b.cell_start, b.N,
-                                                        b.list_cap, b.nl, b.nl_cnt, b.flags);
+  if (b.list_by_cell && b.list_cells)
+    k_build_list_cells<<<nblocks((uint64_t)b.ncells * kGroup, kGBlock), kGBlock, 0, b.stream>>>(
+        b.pos, b.sp, b.cell_sys, b.cell_start, b.ncells, b.list_cap, b.hs.rmax2, b.nl, b.nl_cnt, b.flags);
+  else
+    k_build_list<<<nblocks(b.N, 128), 128, 0, b.stream>>>(b.pos, b.sysid, b.sp, b.cell_of_slot, b.cell_start, b.N,
+                                                          b.list_cap, b.hs.rmax2, b.nl, b.nl_cnt, b.flags);
+  // rows grouped by shell: four warps per block while four staged rows fit the shared memory
+  const uint32_t wpb = 16u * b.list_cap <= 200u * 1024u ? 4u : 1u;
+  const size_t smem = (size_t)wpb * b.list_cap * 4u;
+  if (smem > 48u * 1024u && b.group_smem_set < smem) {
+    SOUP_CUDA_TRY(cudaFuncSetAttribute(k_group_rows, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    b.group_smem_set = smem;
+  }
+  k_group_rows<<<(unsigned)((b.N + wpb - 1) / wpb), 32u * wpb, smem, b.stream>>>(b.N, b.list_cap, b.nl, b.nl_cnt,
+                                                                                b.nl_shell);
+  b.launches += 1;
   prof_end(b);
 }
 
@@ -478,10 +684,11 @@ void launch_build_es_lists(Batch& b) {
   cudaMemsetAsync(b.hcell_cursor, 0, sizeof(uint32_t) * b.nhcells, b.stream);
   k_head_scatter<<<nblocks(b.H), kBlock, 0, b.stream>>>(b.hcell_of, b.hcell_start, b.H, b.hcell_cursor, b.hsorted);
   k_head_sort_cells<<<nblocks(b.nhcells), kBlock, 0, b.stream>>>(b.hcell_start, b.nhcells, b.hsorted);
+  k_head_gather_sorted<<<nblocks(b.H), kBlock, 0, b.stream>>>(b.hsorted, b.H, b.head_slot, b.pos, b.hsorted_xg);
   k_build_es_list<<<nblocks((uint64_t)b.H * 32, 256), 256, 0, b.stream>>>(b.head_sys, b.H, b.head_slot, b.pos, b.sp,
-                                                                         b.hcell_of, b.hcell_start, b.hsorted, b.es_cap,
-                                                                         b.es_nl, b.es_cnt, b.flags);
-  b.launches += 5 + scans;
+                                                                         b.hcell_of, b.hcell_start, b.hsorted_xg,
+                                                                         b.es_cap, b.es_nl, b.es_cnt, b.flags);
+  b.launches += 6 + scans;
   prof_end(b);
 }
 

@@ -89,6 +89,9 @@ Shared make_shared(const SoupConfig& c) {
       PairConst& p = s.pair[i * SOUP_KMAX + j];
       p.wcut = w; p.wcut2 = w * w; p.b2 = b * b;
       p.attr = (float)c.attr_scale[s.cls[i]][s.cls[j]];
+      PairW& q = s.pw[i * SOUP_KMAX + j];
+      q.b2 = p.b2; q.wcut2 = p.wcut2; q.amp = p.attr * s.attr_amp;
+      q.polar = (s.cls[i] == 1u && s.cls[j] == 1u) ? 1.f : 0.f;
       if (i < c.n_kinds && j < c.n_kinds) rmax = std::max(rmax, (float)w);
     }
   if (c.es_enabled) rmax = std::max(rmax, (float)c.es_split_radius);
@@ -178,7 +181,7 @@ namespace {
 
 // ---- batch construction ----------------------------------------------------------------------
 void alloc_grids(Batch& b) {
-  dfree(b.cell_count); dfree(b.cell_start); dfree(b.cell_cursor); dfree(b.scan_tmp);
+  dfree(b.cell_count); dfree(b.cell_start); dfree(b.cell_cursor); dfree(b.scan_tmp); dfree(b.cell_sys);
   dfree(b.hcell_count); dfree(b.hcell_start); dfree(b.hcell_cursor);
   uint64_t nc = 0, nh = 0;
   for (uint32_t r = 0; r < b.R; ++r) {
@@ -193,6 +196,17 @@ void alloc_grids(Batch& b) {
   b.cell_count = dalloc<uint32_t>(nc + 1);
   b.cell_start = dalloc<uint32_t>(nc + 1);
   b.cell_cursor = dalloc<uint32_t>(nc + 1);
+  {
+    std::vector<uint8_t> cs((size_t)nc);
+    b.list_by_cell = true;
+    for (uint32_t r = 0; r < b.R; ++r) {
+      const SysParams& p = b.hsp[r];
+      std::fill(cs.begin() + p.cell_off, cs.begin() + p.cell_off + cells_of(p.dims), (uint8_t)r);
+      for (int a = 0; a < 3; ++a) b.list_by_cell = b.list_by_cell && p.dims[a] >= 2 * p.walk + 1;
+    }
+    b.cell_sys = dalloc<uint8_t>(nc);
+    SOUP_CUDA_TRY(cudaMemcpy(b.cell_sys, cs.data(), nc, cudaMemcpyHostToDevice));
+  }
   b.hcell_count = dalloc<uint32_t>(nh + 1);
   b.hcell_start = dalloc<uint32_t>(nh + 1);
   b.hcell_cursor = dalloc<uint32_t>(nh + 1);
@@ -348,6 +362,8 @@ Batch* make_batch(const SoupConfig* cfgs, const SoupInitState* inits, uint32_t R
   if (const char* e = std::getenv("SOUP_NO_GRAPH")) b.graphs_enabled = std::atoi(e) == 0;
 
   const size_t n = b.N;
+  // a list entry carries its build-distance shell in its top three bits until the row is grouped
+  if (n >= (1ull << 29)) fail(SOUP_E_ARG, "at most 2^29 - 1 particles per batch");
   b.pos = dalloc<float4>(n); b.vel = dalloc<float4>(n); b.force = dalloc<float4>(n); b.pos_ref = dalloc<float4>(n);
   b.charge = dalloc<float>(n); b.slots = dalloc<uint32_t>(3 * n); b.center = dalloc<uint32_t>(n);
   b.held = dalloc<uint32_t>(n); b.brng = dalloc<uint32_t>(n); b.trng = dalloc<uint32_t>(n); b.frozen = dalloc<uint8_t>(n);
@@ -356,7 +372,7 @@ Batch* make_batch(const SoupConfig* cfgs, const SoupInitState* inits, uint32_t R
   b.slots2 = dalloc<uint32_t>(3 * n); b.center2 = dalloc<uint32_t>(n); b.held2 = dalloc<uint32_t>(n);
   b.brng2 = dalloc<uint32_t>(n); b.trng2 = dalloc<uint32_t>(n); b.frozen2 = dalloc<uint8_t>(n); b.id2 = dalloc<uint32_t>(n);
   b.cell_of_slot = dalloc<uint32_t>(n); b.perm = dalloc<uint32_t>(n);
-  b.nl = dalloc<uint32_t>(n * (size_t)b.list_cap); b.nl_cnt = dalloc<uint32_t>(n);
+  b.nl = dalloc<uint32_t>(n * (size_t)b.list_cap); b.nl_cnt = dalloc<uint32_t>(n); b.nl_shell = dalloc<uint4>(n);
   b.sysid = dalloc<uint8_t>(n);
   b.sp = dalloc<SysParams>(R); b.shared = dalloc<Shared>(1);
   b.flags = dalloc<uint32_t>(FLAG_WORDS + 2 * (size_t)R);
@@ -414,7 +430,7 @@ Batch* make_batch(const SoupConfig* cfgs, const SoupInitState* inits, uint32_t R
   sweep_prepare(b);
   b.es_nl = dalloc<uint32_t>((size_t)b.H * std::max<uint32_t>(b.es_cap, 1)); b.es_cnt = dalloc<uint32_t>(b.H);
   b.head_d = dalloc<long long>((size_t)b.H * std::max<uint32_t>(b.es_cap, 1));
-  b.hcell_of = dalloc<uint32_t>(b.H); b.hsorted = dalloc<uint32_t>(b.H);
+  b.hcell_of = dalloc<uint32_t>(b.H); b.hsorted = dalloc<uint32_t>(b.H); b.hsorted_xg = dalloc<float4>(b.H);
   if (b.H) {
     SOUP_CUDA_TRY(cudaMemcpy(b.heads, hall.data(), 4 * (size_t)b.H, cudaMemcpyHostToDevice));
     SOUP_CUDA_TRY(cudaMemcpy(b.head_sys, hsys.data(), 4 * (size_t)b.H, cudaMemcpyHostToDevice));
@@ -426,6 +442,8 @@ Batch* make_batch(const SoupConfig* cfgs, const SoupInitState* inits, uint32_t R
   b.tpp = 4;
   if (const char* e = std::getenv("SOUP_TPP")) b.tpp = std::atoi(e);
   if (const char* e = std::getenv("SOUP_FORCE_QUEUED")) b.queued = std::atoi(e) != 0;
+  if (const char* e = std::getenv("SOUP_LIST_BY_CELL")) b.list_cells = std::atoi(e) != 0;
+  if (const char* e = std::getenv("SOUP_FULL_ROWS")) b.prune = std::atoi(e) == 0;
   force_pass(b);   // priming pass (soup/src/sim.ts:396-408)
   SOUP_CUDA_TRY(cudaStreamSynchronize(b.stream));
   SOUP_CUDA_TRY(cudaGetLastError());
@@ -447,9 +465,9 @@ void destroy_batch(Batch* b) {
   if (b->cap_stream) cudaStreamDestroy(b->cap_stream);
   void* ptrs[] = {b->rebuild_count, b->pos, b->vel, b->force, b->pos_ref, b->charge, b->slots, b->center, b->held, b->brng, b->trng,
                   b->frozen, b->id, b->slot_of, b->pos2, b->vel2, b->force2, b->charge2, b->slots2, b->center2,
-                  b->held2, b->brng2, b->trng2, b->frozen2, b->id2, b->cell_of_slot, b->cell_count, b->cell_start,
-                  b->cell_cursor, b->perm, b->scan_tmp, b->nl, b->nl_cnt, b->heads, b->head_sys, b->es_nl,
-                  b->es_cnt, b->head_slot, b->head_e, b->head_pos, b->head_xq, b->head_d, b->head_flag, b->draw_site, b->sweep_band, b->hcell_count, b->hcell_start, b->hcell_cursor, b->hsorted, b->hcell_of, b->flags,
+                  b->held2, b->brng2, b->trng2, b->frozen2, b->id2, b->cell_of_slot, b->cell_count, b->cell_start, b->cell_sys,
+                  b->cell_cursor, b->perm, b->scan_tmp, b->nl, b->nl_cnt, b->nl_shell, b->heads, b->head_sys, b->es_nl,
+                  b->es_cnt, b->head_slot, b->head_e, b->head_pos, b->head_xq, b->head_d, b->head_flag, b->draw_site, b->sweep_band, b->hcell_count, b->hcell_start, b->hcell_cursor, b->hsorted, b->hsorted_xg, b->hcell_of, b->flags,
                   b->events, b->desorb, b->drift_bits, b->bond_items, b->bond_nitems, b->uf_parent, b->comp_min,
                   b->item_done, b->has_item, b->sweep_out, b->prot_rng_dev, b->sp, b->shared, b->sysid, b->an_buf[0],
                   b->an_buf[1]};
@@ -1421,7 +1439,7 @@ int soup_autotune(SoupHandle* h, uint32_t steps, SoupTuneResult* out) {
     double best = 1e30;
     for (int q = 0; q < 2; ++q)
       for (int t : tpps) {
-        if (q && t == 8) continue;
+        if (q && t != 1) continue;   // the compacted kernel is one lane per particle
         b.tpp = t;
         b.queued = q != 0;
         const double ms = tune_time(b, 5, [&] { launch_force_list(b); });
@@ -1430,14 +1448,21 @@ int soup_autotune(SoupHandle* h, uint32_t steps, SoupTuneResult* out) {
     b.tpp = (int)res.tpp;
     b.queued = res.queued != 0;
     drop_graphs(b);
-    // cell size: the list-walk radius (cell = list range / walk), timed on the list build
+    // cell size (the list-walk radius: cell = list range / walk) and the list build (a thread per
+    // particle, or a group of lanes per cell), timed on the list build
     best = 1e30;
-    for (int w : {2, 3}) {
-      tune_plan(b, planned, w);
-      force_pass(b);
-      const double ms = tune_time(b, 3, [&] { launch_cell_index(b); launch_build_lists(b); });
-      if (ms < best) { best = ms; res.walk = (uint32_t)w; }
-    }
+    bool cells_best = false;
+    for (int w : {2, 3})
+      for (int lc = 0; lc < 2; ++lc) {
+        tune_plan(b, planned, w);
+        if (lc && !b.list_by_cell) continue;
+        b.list_cells = lc != 0;
+        force_pass(b);
+        const double ms = tune_time(b, 3, [&] { launch_cell_index(b); launch_build_lists(b); });
+        if (ms < best) { best = ms; res.walk = (uint32_t)w; cells_best = lc != 0; }
+      }
+    b.list_cells = cells_best;
+    res.list_cells = cells_best ? 1u : 0u;
     // skin (drift-triggered rebuilds only): at most the planned one, which sized the list capacity;
     // timed on whole steps, rebuilds and sweeps included
     res.skin_scale = 1.0;
@@ -1478,6 +1503,7 @@ int soup_apply_tuning(SoupHandle* h, const SoupTuneResult* t) {
       fail(SOUP_E_ARG, "tuning: the skin can only be scaled with drift-triggered rebuilds");
     b.tpp = (int)t->tpp;
     b.queued = t->queued != 0;
+    b.list_cells = t->list_cells != 0;
     std::vector<double> sk(b.R);
     for (uint32_t r = 0; r < b.R; ++r) sk[r] = b.cfg[r].skin * t->skin_scale;
     tune_plan(b, sk, (int)t->walk);

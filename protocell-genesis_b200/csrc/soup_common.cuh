@@ -54,8 +54,16 @@ struct PairConst {
   float b2;      // b^2
   float attr;    // class-table depth
 };
+// The list force's per-kind-pair numbers, premultiplied for the pair loop.
+struct PairW {
+  float b2;      // b^2
+  float wcut2;   // (c6 * b)^2
+  float amp;     // class-table depth * eps * pi / (2 wc)
+  float polar;   // 1 when both kinds are of the polar class (the acid-soap depth applies), else 0
+};
 struct Shared {
   PairConst pair[SOUP_KMAX * SOUP_KMAX];
+  PairW pw[SOUP_KMAX * SOUP_KMAX];
   float radius[SOUP_KMAX];
   uint32_t cls[SOUP_KMAX];
   float sigma, eps, b_tt, k_fene, r_inf, k_bend, r_bend, wc, c6;
@@ -136,29 +144,55 @@ struct PairP {
   }
 };
 
-// Scalar s such that the pair force on i is s * d (d = mi(xi - xj)), for every term the
-// neighbour list carries: WCA, class attraction (+ acid-soap depth), near-half screened Coulomb.
-// WCA and the attraction are evaluated unconditionally and selected (no divergent branches); the
-// screened Coulomb term only exists between charged beads and stays a branch.
-template <class PP>
-__device__ __forceinline__ float pair_scalar(const Shared& S, const PP& P, const PairConst& pc,
-                                             float r2, int ki, int kj, float qi, float qj) {
+// The pair loop's constants of one replica, held in registers (batch-wide numbers from Shared, the
+// replica's acid-soap depth and screened-Coulomb numbers from its SysParams).
+struct PairLean {
+  float c48, c24;         // 48 eps, 24 eps
+  float k2, k2rc;         // sin argument 2 (r - rc) pi / (2 wc) = r k2 - k2rc
+  float rc2, rcw2;        // the attraction window [rc, rc + wc], squared
+  float acid_amp;         // acid-soap depth * eps * pi / (2 wc), 0 without it
+  float es_A, es_kappa, es_fc, es_lim2;   // near screened Coulomb below min(split, rc)^2 (-1: none)
+  __device__ __forceinline__ static PairLean of(const Shared& S, const SysParams& P) {
+    PairLean L;
+    L.c48 = 48.0f * S.eps;
+    L.c24 = 24.0f * S.eps;
+    L.k2 = 2.0f * S.attr_k;
+    L.k2rc = L.k2 * S.rc_attr;
+    L.rc2 = S.rc_attr * S.rc_attr;
+    const float rcw = S.rc_attr + S.wc;
+    L.rcw2 = rcw * rcw;
+    L.acid_amp = P.acid > 0.f ? P.acid * S.attr_amp : 0.f;
+    L.es_A = P.es_A; L.es_kappa = P.es_kappa; L.es_fc = P.es_fc;
+    const float lim = fminf(P.es_split, P.es_rc);
+    L.es_lim2 = P.es_A != 0.f ? lim * lim : -1.f;
+    return L;
+  }
+};
+
+// Scalar s such that the pair force on i is s * d (d = mi(xi - xj)), for every term the neighbour
+// list carries (soup/wgsl/pair.wgsl:168-204 nonbondedSoup): WCA below c6 b (forces.wgsl:19-23,
+// -wca_dv(r)/r = 24 eps (2 (b/r)^12 - (b/r)^6) / r^2), the class attraction on [rc, rc + wc] with the
+// acid-soap depth added between two polar beads of which exactly one is charged (forces.wgsl:32-37,
+// pair.wgsl:151-160, 188: -(A + acid) eps pi / (2 wc) sin(pi (r - rc) / wc) / r), and the near half of
+// the screened Coulomb force between charged beads (electrostatics.wgsl:65-83).  WCA and the
+// attraction are selected, not branched on; the windows are tested on r^2 (both forces vanish at
+// their edges).  The screened Coulomb term only exists between charged beads and stays a branch.
+// qi_nz: the owner's charge is nonzero.
+__device__ __forceinline__ float pair_lean(const PairW& pc, const PairLean& L, float r2, bool qi_nz, float qi,
+                                           float qj) {
   const float rinv = rsqrtf(r2);
   const float r = r2 * rinv;
   const float rinv2 = rinv * rinv;
-  const float s2 = pc.b2 * rinv2;                         // forces.wgsl:19-23: -wca_dv(r)/r
+  const float s2 = pc.b2 * rinv2;
   const float s6 = s2 * s2 * s2;
-  const float fw = 24.0f * S.eps * (2.0f * s6 * s6 - s6) * rinv2;
-  float s = (r2 < pc.wcut2) ? fw : 0.f;
-  float scale = pc.attr;                                  // pair.wgsl:188 class depth + acid-soap depth
-  if (P.acid > 0.f && ((qi != 0.f) != (qj != 0.f)) && S.cls[ki] == 1u && S.cls[kj] == 1u) scale += P.acid;
-  const float x = (r - S.rc_attr) * S.attr_k;            // forces.wgsl:32-37
-  const float fa = scale * S.attr_amp * __sinf(2.0f * x) * rinv;
-  s -= (r >= S.rc_attr && r <= S.rc_attr + S.wc) ? fa : 0.f;
-  const float qq = qi * qj;                               // electrostatics.wgsl:65-83, near half
-  if (qq != 0.f && r < P.es_split && r < P.es_rc && P.es_A != 0.f) {
-    const float u = P.es_A * __expf(-P.es_kappa * r) * rinv;
-    s += qq * (u * (rinv + P.es_kappa) - P.es_fc) * rinv;
+  float s = (r2 < pc.wcut2) ? (L.c48 * s6 - L.c24) * s6 * rinv2 : 0.f;
+  const float amp = pc.amp + ((pc.polar != 0.f && (qi_nz != (qj != 0.f))) ? L.acid_amp : 0.f);
+  const float sn = __sinf(fmaf(r, L.k2, -L.k2rc));
+  s -= (r2 >= L.rc2 && r2 <= L.rcw2) ? amp * sn * rinv : 0.f;
+  const float qq = qi * qj;
+  if (qq != 0.f && r2 < L.es_lim2) {
+    const float u = L.es_A * __expf(-L.es_kappa * r) * rinv;
+    s += qq * (u * (rinv + L.es_kappa) - L.es_fc) * rinv;
   }
   return s;
 }

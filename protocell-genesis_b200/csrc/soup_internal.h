@@ -11,7 +11,9 @@
 //   center u32 ORIGINAL id                held, bond_rng, thermo_rng u32;  frozen u8
 //   id     u32 slot -> original id        slot_of u32 original id -> slot
 //   pos_ref float4 positions at the last rebuild (drift reference)
-//   nl     u32 [slot][list_cap] Verlet neighbours as SLOT indices; nl_cnt u32 [slot]
+//   nl     u32 [slot][list_cap] Verlet neighbours as SLOT indices; nl_cnt u32 [slot]; each row is
+//          grouped by build distance (shell 0: inside the force's reach; shells 1-4: the skin in four
+//          equal widths), nl_shell uint4 [slot] the ends of shells 0..3
 //   heads  u32 original ids of titratable beads (ascending; static);  es_nl [head][es_cap] slots
 #pragma once
 #include <algorithm>
@@ -88,11 +90,17 @@ struct Batch {
   // grid + list
   uint32_t ncells = 0;               // total list-build cells over the batch
   uint32_t *cell_of_slot = nullptr, *cell_count = nullptr, *cell_start = nullptr, *cell_cursor = nullptr;
+  uint8_t* cell_sys = nullptr;       // replica of each list-build cell
+  bool list_by_cell = false;         // every replica's walk fits its grid: the cell-group build can run
+  bool list_cells = false;           // use it (the autotuner's choice; SOUP_LIST_BY_CELL=1)
   uint32_t* perm = nullptr;          // new slot -> old slot
   uint32_t* scan_tmp = nullptr;
   uint32_t list_cap = 0;             // row stride of nl (max over replicas, rounded to 32)
   uint32_t* nl = nullptr;
   uint32_t* nl_cnt = nullptr;
+  uint4* nl_shell = nullptr;
+  size_t group_smem_set = 0;         // dynamic shared memory k_group_rows was opened to
+  bool prune = true;                 // force passes read only the shells the drift can have brought in range         // per slot: ends of the row's build-distance shells 0..3 (shell 4 ends at nl_cnt)
 
   // heads / long-range electrostatics
   uint32_t H = 0;                    // total heads
@@ -112,6 +120,7 @@ struct Batch {
   uint32_t* es_cnt = nullptr;
   uint32_t nhcells = 0;
   uint32_t *hcell_count = nullptr, *hcell_start = nullptr, *hcell_cursor = nullptr, *hsorted = nullptr;
+  float4* hsorted_xg = nullptr;      // the heads in head-cell order: position, head index as w bits
   uint32_t* hcell_of = nullptr;
 
   // counters and flags (device): [0] list overflow, [1] es overflow, [2..3] nonfinite pos/vel,
@@ -148,7 +157,7 @@ struct Batch {
   uint64_t rebuilds = 0, sweeps = 0;
   bool force_fresh = false;          // force array matches positions+charges+lists
   int tpp = 4;                       // threads per particle in the list force
-  bool queued = false;               // list force with the in-range pairs queued per lane (k_force_q)
+  bool queued = false;               // list force with the in-range pairs compacted per warp (k_force_w)
   uint32_t wait_limit = 0;           // polls of a bounded device-side handoff before it gives up (0: default)
   DiffWindow diff;
   // captured step chunks (CUDA graphs), keyed by length and schedule phase; the drift-triggered

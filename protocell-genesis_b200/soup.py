@@ -553,6 +553,7 @@ def _apply_tuning(lib, h, tuning):
     r = _abi.SoupTuneResult()
     r.tpp, r.walk, r.skin_scale = int(tuning["tpp"]), int(tuning["walk"]), float(tuning["skin_scale"])
     r.queued = int(tuning.get("queued", 0))
+    r.list_cells = int(tuning.get("list_cells", 0))
     _check(lib, h, lib.soup_apply_tuning(h, C.byref(r)))
 
 
@@ -561,7 +562,8 @@ def _autotune(lib, h, steps):
     _check(lib, h, lib.soup_autotune(h, int(steps), C.byref(r)))
     return dict(tpp=r.tpp, walk=r.walk, tpp_before=r.tpp_before, walk_before=r.walk_before,
                 skin_scale=r.skin_scale, ms_per_step_before=r.ms_per_step_before,
-                ms_per_step_after=r.ms_per_step_after, queued=r.queued, queued_before=r.queued_before)
+                ms_per_step_after=r.ms_per_step_after, queued=r.queued, queued_before=r.queued_before,
+                list_cells=r.list_cells)
 
 
 class SoupBatch:

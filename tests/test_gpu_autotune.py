@@ -110,12 +110,16 @@ def test_apply_tuning_reproduces_the_tuned_shape():
     b.dispose()
 
 
-@pytest.mark.parametrize("tpp", [1, 2, 4])
-def test_queued_force_is_bit_identical_to_the_plain_one(tpp):
-    """The list force with the in-range pairs queued per lane (k_force_q) accumulates every lane's
-    terms in k_force's order: the forces are the same bits, for all particles and for the heads-only
-    recompute after a sweep, on compositions with charges, catalysts and a confining wall."""
+def test_compacted_force_is_bit_identical_to_the_plain_one():
+    """The list force with each warp's in-range pairs compacted and evaluated by every lane (k_force_w)
+    accumulates every particle's terms in k_force<1>'s order with k_force<1>'s arithmetic: the forces
+    are the same bits, for all particles and for the heads-only recompute after a sweep, on compositions
+    with charges, catalysts and a confining wall (whose warps take both the minimum-image path and the
+    direct one of warps inside the box).  In a batch, the warp that spans two replicas evaluates each
+    owner's pairs on the owner's lane: the batch's forces are its replicas' own."""
     from helpers import charged_opts, confined_opts
+    from protocell_genesis_b200.soup import SoupBatch
+    states = []
     for opts in (charged_opts(rebuild_on_drift=True, sweep_every=10, chunk_steps=10),
                  confined_opts(rebuild_on_drift=True, sweep_every=10, chunk_steps=10)):
         cfg = cfgm.resolve(opts, P)
@@ -124,10 +128,11 @@ def test_queued_force_is_bit_identical_to_the_plain_one(tpp):
         o.step(20)
         st = dict(positions=o.read(ob.F_POS), velocities=o.read(ob.F_VEL), bond_slots=o.read(ob.F_SLOTS),
                   center_link=o.read(ob.F_CENTER), charges=o.read(ob.F_CHARGES))
+        states.append((cfg, st))
         out = []
         for q in (0, 1):
             g = SoupSystem(cfg, st)
-            g.apply_tuning(dict(tpp=tpp, walk=2, skin_scale=1.0, queued=q))
+            g.apply_tuning(dict(tpp=1, walk=2, skin_scale=1.0, queued=q))
             f = g.forces_no_rebuild()
             g.step(30)                          # sweeps every 10 steps recompute the heads' forces only
             out.append((f, g.forces_no_rebuild(), g.charges()))
@@ -135,3 +140,62 @@ def test_queued_force_is_bit_identical_to_the_plain_one(tpp):
         assert np.array_equal(out[0][0].view(np.uint32), out[1][0].view(np.uint32))
         assert np.array_equal(out[0][2], out[1][2])
         assert np.array_equal(out[0][1].view(np.uint32), out[1][1].view(np.uint32))
+    # two replicas of the charged composition (different seeds' states are not needed: the second
+    # replica's slots start mid-warp unless its first replica's count is a multiple of 32)
+    cfg, st = states[0]
+    assert cfg.n % 32 != 0
+    b = SoupBatch([cfg, cfg], [st, st])
+    b.apply_tuning(dict(tpp=1, walk=2, skin_scale=1.0, queued=1))
+    g = SoupSystem(cfg, st)
+    g.apply_tuning(dict(tpp=1, walk=2, skin_scale=1.0, queued=1))
+    fg = g.forces_no_rebuild().view(np.uint32)
+    for r in b.replicas:
+        assert np.array_equal(r.forces_no_rebuild().view(np.uint32), fg)
+    g.dispose()
+    b.dispose()
+
+
+def test_pruned_rows_change_no_bit(monkeypatch):
+    """Force passes read a list row only up to the build-distance shells that the largest displacement
+    since the build can have brought within the force's reach; the entries skipped are beyond it, so
+    a trajectory with the pruning equals one that reads every row whole (SOUP_FULL_ROWS=1), bit for
+    bit, across drift-triggered rebuilds, charge sweeps and bond passes."""
+    from helpers import confined_opts
+    opts = confined_opts(rebuild_on_drift=True, sweep_every=10, chunk_steps=10)
+    cfg = cfgm.resolve(opts, P)
+    o = ob.OracleSystem(_abi, cfg)
+    o.relax(20, 0.1)
+    st = dict(positions=o.read(ob.F_POS), velocities=o.read(ob.F_VEL), bond_slots=o.read(ob.F_SLOTS),
+              center_link=o.read(ob.F_CENTER), charges=o.read(ob.F_CHARGES))
+    out = []
+    for full in ("0", "1"):
+        monkeypatch.setenv("SOUP_FULL_ROWS", full)
+        g = SoupSystem(cfg, st)
+        g.step(60)
+        out.append((g.particles(), g.velocities(), g.forces_no_rebuild(), g.charges(), g.info()["rebuilds"]))
+        g.dispose()
+    assert out[0][4] == out[1][4] and out[0][4] >= 3
+    for a, b in zip(out[0][:4], out[1][:4]):
+        assert np.array_equal(a.view(np.uint32), b.view(np.uint32))
+
+
+@pytest.mark.parametrize("maker", ["charged_opts", "confined_opts"])
+def test_cell_group_list_build_gives_the_oracle_sets(maker, monkeypatch):
+    """The list build with a group of lanes per cell and the neighbour rows staged in shared memory
+    (SOUP_LIST_BY_CELL=1, an autotuner choice) gives the oracle's Verlet sets, as the build with a
+    thread per particle does."""
+    import helpers
+    monkeypatch.setenv("SOUP_LIST_BY_CELL", "1")
+    cfg = cfgm.resolve(getattr(helpers, maker)(), P)
+    o = ob.OracleSystem(_abi, cfg)
+    o.relax(20, 0.1)
+    o.step(20)
+    st = dict(positions=o.read(ob.F_POS), velocities=o.read(ob.F_VEL), bond_slots=o.read(ob.F_SLOTS),
+              center_link=o.read(ob.F_CENTER), charges=o.read(ob.F_CHARGES))
+    g = SoupSystem(cfg, st)
+    o2 = ob.OracleSystem(_abi, cfg, st)
+    gc, gl = g.verlet_lists()
+    oc, ol = o2.verlet()
+    assert np.array_equal(gc, oc) and np.array_equal(gl, ol)
+    g.dispose()
+    o2.close()
