@@ -27,7 +27,7 @@ sys.path.insert(0, ROOT)
 sys.path.insert(0, os.path.join(ROOT, "tests"))
 
 METRIC = "particle-steps/s at 483k beads, plain vs batched, at <=1e-5 force err"
-SKIN = 0.8                 # the Verlet skin of the plain workload, both arms (rebuilt on half-skin drift)
+SKIN = 1.0                 # the Verlet skin of the plain workload, both arms (rebuilt on half-skin drift)
 RELAX_ITERATIONS = 50      # cold-start relax of the fresh lattice, both arms (untimed)
 E2E_MIN_STEPS = 200        # the end-to-end sample covers at least one analysis period
 UNIT = "particle-steps/s"

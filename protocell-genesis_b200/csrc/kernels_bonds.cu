@@ -281,23 +281,16 @@ __device__ __forceinline__ int item_set(const uint32_t* rec, const uint32_t* cen
   return n;
 }
 
-// Phase B, one CTA
-__global__ void __launch_bounds__(1024) k_bond_claims(
-    const Shared* __restrict__ Sg, const SysParams* __restrict__ sp, const uint8_t* __restrict__ sysid,
-    const float4* __restrict__ pos, uint32_t* __restrict__ slots, uint32_t* __restrict__ center,
-    uint32_t* __restrict__ held, const uint32_t* __restrict__ slot_of, uint32_t* __restrict__ items,
-    uint32_t* __restrict__ nitems, uint32_t item_cap, uint32_t* __restrict__ has_item, uint32_t* __restrict__ parent,
-    uint32_t* __restrict__ comp_min, uint8_t* __restrict__ done, uint32_t* __restrict__ events,
-    uint32_t* __restrict__ desorb, uint32_t* __restrict__ flags) {
-  __shared__ Shared S;
-  for (int w = threadIdx.x; w < (int)(sizeof(Shared) / 4); w += blockDim.x)
-    reinterpret_cast<uint32_t*>(&S)[w] = reinterpret_cast<const uint32_t*>(Sg)[w];
-  __syncthreads();
-  const uint32_t M0 = min(*nitems, item_cap);
-  // every particle an item may touch runs its own desorption check in its turn, so it needs an item
-  // too (proposal partners are the only ones the walk does not already cover)
+// Phase B.  Every particle an item may touch runs its own desorption check in its turn, so it needs
+// an item too (proposal partners are the only ones the walk does not already cover): added here, by
+// the whole grid, before the claims.
+// nitems[1] holds the walk's item count: only the walk's items add partners (nitems[0] grows meanwhile).
+__global__ void k_bond_partners(const uint32_t* __restrict__ center, const uint32_t* __restrict__ slot_of,
+                                uint32_t* __restrict__ items, uint32_t* __restrict__ nitems, uint32_t item_cap,
+                                uint32_t* __restrict__ has_item, uint32_t* __restrict__ flags) {
+  const uint32_t M0 = min(nitems[1], item_cap);
   uint32_t setbuf[2 * (2 + SOUP_CAND_CAP)];
-  for (uint32_t t = threadIdx.x; t < M0; t += blockDim.x) {
+  for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < M0; t += gridDim.x * blockDim.x) {
     const int n = item_set(items + (size_t)t * REC, center, slot_of, setbuf);
     for (int q = 0; q < n; ++q) {
       const uint32_t x = setbuf[q];
@@ -313,20 +306,68 @@ __global__ void __launch_bounds__(1024) k_bond_claims(
       }
     }
   }
+}
+
+// The claims of one replica per CTA (an item's set of particles never leaves its replica, so the
+// replicas' components are disjoint and resolve independently).  The CTA collects its items, joins the
+// items whose particle sets meet (union-find over the sets closed under centre links), and then in
+// rounds executes the minimum-id pending item of every component: the serial ascending order within
+// each component, which is all the serial order decides.
+constexpr uint32_t kClaimLocal = 8192;   // a replica's items held as a list in shared memory
+__global__ void __launch_bounds__(1024) k_bond_claims(
+    const Shared* __restrict__ Sg, const SysParams* __restrict__ sp, const uint8_t* __restrict__ sysid,
+    const float4* __restrict__ pos, uint32_t* __restrict__ slots, uint32_t* __restrict__ center,
+    uint32_t* __restrict__ held, const uint32_t* __restrict__ slot_of, uint32_t* __restrict__ items,
+    const uint32_t* __restrict__ nitems, uint32_t item_cap, uint32_t* __restrict__ parent,
+    uint32_t* __restrict__ comp_min, uint8_t* __restrict__ done, uint32_t* __restrict__ events,
+    uint32_t* __restrict__ desorb) {
+  __shared__ Shared S;
+  __shared__ uint32_t mine[kClaimLocal];
+  __shared__ uint32_t nmine;
+  for (int w = threadIdx.x; w < (int)(sizeof(Shared) / 4); w += blockDim.x)
+    reinterpret_cast<uint32_t*>(&S)[w] = reinterpret_cast<const uint32_t*>(Sg)[w];
+  if (threadIdx.x == 0) nmine = 0;
   __syncthreads();
+  const uint32_t r = blockIdx.x;
   const uint32_t M = min(*nitems, item_cap);
-  for (uint32_t t = threadIdx.x; t < M; t += blockDim.x) {
+  // this replica's items (any order: the rounds below depend on item ids, not positions); a batch of
+  // one replica takes them all as they are
+  const bool all = gridDim.x == 1;
+  if (!all) {
+    for (uint32_t t = threadIdx.x; t < M; t += blockDim.x)
+      if (sysid[slot_of[items[(size_t)t * REC]]] == r) {
+        const uint32_t at = atomicAdd(&nmine, 1u);
+        if (at < kClaimLocal) mine[at] = t;
+      }
+  }
+  __syncthreads();
+  const bool local = !all && nmine <= kClaimLocal;
+  const uint32_t L = local ? nmine : M;
+  // item u of this CTA, or NONE for another replica's item (when the list did not fit)
+  auto item = [&](uint32_t u) -> uint32_t {
+    if (all) return u;
+    if (local) return mine[u];
+    return sysid[slot_of[items[(size_t)u * REC]]] == r ? u : NONE;
+  };
+  uint32_t setbuf[2 * (2 + SOUP_CAND_CAP)];
+  for (uint32_t u = threadIdx.x; u < L; u += blockDim.x) {
+    const uint32_t t = item(u);
+    if (t == NONE) continue;
     const int n = item_set(items + (size_t)t * REC, center, slot_of, setbuf);
     for (int q = 0; q < n; ++q) parent[setbuf[q]] = setbuf[q];
     done[t] = 0;
   }
   __syncthreads();
-  for (uint32_t t = threadIdx.x; t < M; t += blockDim.x) {
+  for (uint32_t u = threadIdx.x; u < L; u += blockDim.x) {
+    const uint32_t t = item(u);
+    if (t == NONE) continue;
     const int n = item_set(items + (size_t)t * REC, center, slot_of, setbuf);
     for (int q = 1; q < n; ++q) uf_union(parent, setbuf[0], setbuf[q]);
   }
   __syncthreads();
-  for (uint32_t t = threadIdx.x; t < M; t += blockDim.x) {
+  for (uint32_t u = threadIdx.x; u < L; u += blockDim.x) {
+    const uint32_t t = item(u);
+    if (t == NONE) continue;
     uint32_t* rec = items + (size_t)t * REC;
     const uint32_t root = uf_find(parent, rec[0]);
     rec[9] = root;
@@ -336,19 +377,24 @@ __global__ void __launch_bounds__(1024) k_bond_claims(
   St st{S, sp, sysid, pos, slots, center, held, slot_of, events, desorb};
   for (int round = 0;; ++round) {
     int pending = 0;
-    for (uint32_t t = threadIdx.x; t < M; t += blockDim.x) {
-      if (done[t]) continue;
+    for (uint32_t u = threadIdx.x; u < L; u += blockDim.x) {
+      const uint32_t t = item(u);
+      if (t == NONE || done[t]) continue;
       pending = 1;
       atomicMin(&comp_min[items[(size_t)t * REC + 9]], items[(size_t)t * REC]);
     }
     if (!__syncthreads_or(pending)) break;
-    for (uint32_t t = threadIdx.x; t < M; t += blockDim.x) {
-      if (done[t]) continue;
+    for (uint32_t u = threadIdx.x; u < L; u += blockDim.x) {
+      const uint32_t t = item(u);
+      if (t == NONE || done[t]) continue;
       const uint32_t* rec = items + (size_t)t * REC;
       if (comp_min[rec[9]] == rec[0]) { st.run(rec); done[t] = 1; }
     }
     __syncthreads();
-    for (uint32_t t = threadIdx.x; t < M; t += blockDim.x) comp_min[items[(size_t)t * REC + 9]] = NONE;
+    for (uint32_t u = threadIdx.x; u < L; u += blockDim.x) {
+      const uint32_t t = item(u);
+      if (t != NONE) comp_min[items[(size_t)t * REC + 9]] = NONE;
+    }
     __syncthreads();
   }
 }
@@ -388,7 +434,7 @@ __global__ void k_bond_break(const Shared* __restrict__ Sg, const uint8_t* __res
 }  // namespace
 
 void launch_bonds(Batch& b) {
-  b.launches += 3;
+  b.launches += 4;
   prof_begin(b, SOUP_K_BONDS);
   cudaMemsetAsync(b.bond_nitems, 0, sizeof(uint32_t), b.stream);
   cudaMemsetAsync(b.has_item, 0, sizeof(uint32_t) * b.N, b.stream);
@@ -396,9 +442,12 @@ void launch_bonds(Batch& b) {
   k_bond_walk<<<nblocks(b.N, 128), 128, 0, b.stream>>>(b.shared, b.sp, b.sysid, b.N, b.pos, b.id, b.slots, b.center,
                                                        b.nl, b.nl_cnt, b.list_cap, b.brng, b.bond_items,
                                                        b.bond_nitems, has_item);
-  k_bond_claims<<<1, 1024, 0, b.stream>>>(b.shared, b.sp, b.sysid, b.pos, b.slots, b.center, b.held, b.slot_of,
-                                          b.bond_items, b.bond_nitems, b.N, has_item, b.uf_parent, b.comp_min,
-                                          b.item_done, b.events, b.desorb, b.flags);
+  cudaMemcpyAsync(b.bond_nitems + 1, b.bond_nitems, sizeof(uint32_t), cudaMemcpyDeviceToDevice, b.stream);
+  k_bond_partners<<<std::max(1u, std::min(nblocks(b.N, 256) / 8u, 592u)), 256, 0, b.stream>>>(
+      b.center, b.slot_of, b.bond_items, b.bond_nitems, b.N, has_item, b.flags);
+  k_bond_claims<<<b.R, 1024, 0, b.stream>>>(b.shared, b.sp, b.sysid, b.pos, b.slots, b.center, b.held, b.slot_of,
+                                            b.bond_items, b.bond_nitems, b.N, b.uf_parent, b.comp_min, b.item_done,
+                                            b.events, b.desorb);
   k_bond_break<<<nblocks(b.N), kBlock, 0, b.stream>>>(b.shared, b.sysid, b.N, b.pos, b.id, b.slot_of, b.slots,
                                                       b.brng, b.events);
   prof_end(b);

@@ -368,15 +368,7 @@ __global__ void __launch_bounds__(256) k_es_far(const SysParams* __restrict__ sp
     const float sc = qi * qj * (u * (rinv + P.es_kappa) - P.es_fc) * rinv;
     fx += sc * dx; fy += sc * dy; fz += sc * dz;
   };
-  // lane takes entries lane, lane + 32, ... in order; four of them per pass have every index and
-  // every gather in flight before the first is evaluated
-  uint32_t s = (uint32_t)lane;
-  for (; s + 96u < cnt; s += 128u) {
-    const uint32_t i0 = __ldg(row + s), i1 = __ldg(row + s + 32u), i2 = __ldg(row + s + 64u), i3 = __ldg(row + s + 96u);
-    const float4 x0 = __ldg(xq + i0), x1 = __ldg(xq + i1), x2 = __ldg(xq + i2), x3 = __ldg(xq + i3);
-    add(x0); add(x1); add(x2); add(x3);
-  }
-  for (; s < cnt; s += 32u) add(__ldg(xq + __ldg(row + s)));
+  for (uint32_t s = (uint32_t)lane; s < cnt; s += 32u) add(__ldg(xq + __ldg(row + s)));
   for (int o = 16; o > 0; o >>= 1) {
     fx += __shfl_xor_sync(0xffffffffu, fx, o);
     fy += __shfl_xor_sync(0xffffffffu, fy, o);

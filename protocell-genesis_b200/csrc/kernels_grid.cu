@@ -428,11 +428,17 @@ __global__ void __launch_bounds__(kGBlock) k_build_list_cells(
   }
 }
 
-// Group every row by build-distance shell (stable: a shell keeps the build's order), strip the tags,
-// and record where shells 0..3 end.  A warp per row: a row of up to 32 * kGRegs entries is read in one
-// go into registers (every load in flight at once), a longer one (dense aggregates) is staged in
-// shared memory.
+// Group every row by build-distance shell, strip the tags, and record where shells 0..3 end.  A warp
+// per row.  A row of up to 32 * kGRegs entries is read in one go into registers, lane l holding
+// entries l, l + 32, ..; each lane counts its entries per shell (five 12-bit fields of one 64-bit word:
+// a row holds fewer than 4096 entries), one warp scan of those words gives every lane the place of its
+// entries, and each shell receives its entries lane by lane (lane 0's first, each lane's in row order),
+// a deterministic order.  A longer row (dense aggregates) is grouped in shared memory, shell by shell
+// with ballots, keeping the build's order inside a shell.
 constexpr uint32_t kGRegs = 16;
+__device__ __forceinline__ uint32_t field12(unsigned long long w, uint32_t t) {
+  return (uint32_t)(w >> (12u * t)) & 0xFFFu;
+}
 __global__ void k_group_rows(uint32_t N, uint32_t cap, uint32_t* __restrict__ nl, const uint32_t* __restrict__ nl_cnt,
                              uint4* __restrict__ shell_end) {
   extern __shared__ uint32_t gbuf[];
@@ -441,32 +447,49 @@ __global__ void k_group_rows(uint32_t N, uint32_t cap, uint32_t* __restrict__ nl
   if (k >= N) return;   // whole warps
   uint32_t* row = nl + (size_t)k * cap;
   const uint32_t cnt = min(nl_cnt[k], cap);
-  const uint32_t lt = (1u << lane) - 1u;
-  uint32_t out = 0, e[4];
+  uint32_t e[4];
   if (cnt <= 32u * kGRegs) {
     uint32_t v[kGRegs];
+    unsigned long long mine = 0;
 #pragma unroll
     for (uint32_t c = 0; c < kGRegs; ++c) {
       const uint32_t s = 32u * c + lane;
-      v[c] = s < cnt ? row[s] : 0xFFFFFFFFu;   // tag 7: no shell
+      v[c] = s < cnt ? row[s] : 0xFFFFFFFFu;
     }
-    __syncwarp();
 #pragma unroll
-    for (uint32_t b = 0; b < 5; ++b) {
+    for (uint32_t c = 0; c < kGRegs; ++c)
+      if (v[c] != 0xFFFFFFFFu) mine += 1ull << (12u * (v[c] >> 29));
+    unsigned long long incl = mine;
 #pragma unroll
-      for (uint32_t c = 0; c < kGRegs; ++c) {
-        if (32u * c >= cnt) break;
-        const bool hit = (v[c] >> 29) == b;
-        const uint32_t m = __ballot_sync(0xffffffffu, hit);
-        if (hit) row[out + __popc(m & lt)] = v[c] & 0x1FFFFFFFu;
-        out += __popc(m);
-      }
-      if (b < 4) e[b] = out;
+    for (int o = 1; o < 32; o <<= 1) {
+      const unsigned long long y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= (uint32_t)o) incl += y;
+    }
+    const unsigned long long tot = __shfl_sync(0xffffffffu, incl, 31);
+    // the shells' first places, packed like the counts
+    unsigned long long bases = 0;
+    uint32_t run = 0;
+#pragma unroll
+    for (uint32_t t = 0; t < 5; ++t) {
+      bases |= (unsigned long long)run << (12u * t);
+      run += field12(tot, t);
+      if (t < 4) e[t] = run;
+    }
+    unsigned long long at = bases + (incl - mine);   // this lane's first place in every shell
+    __syncwarp();                                     // every lane has read its entries
+#pragma unroll
+    for (uint32_t c = 0; c < kGRegs; ++c) {
+      if (v[c] == 0xFFFFFFFFu) continue;
+      const uint32_t t = v[c] >> 29;
+      row[field12(at, t)] = v[c] & 0x1FFFFFFFu;
+      at += 1ull << (12u * t);
     }
   } else {
     uint32_t* sb = gbuf + (size_t)wib * cap;
     for (uint32_t s = lane; s < cnt; s += 32u) sb[s] = row[s];
     __syncwarp();
+    const uint32_t lt = (1u << lane) - 1u;
+    uint32_t out = 0;
 #pragma unroll
     for (uint32_t b = 0; b < 5; ++b) {
       for (uint32_t s0 = 0; s0 < cnt; s0 += 32u) {

@@ -96,6 +96,70 @@ __global__ void __launch_bounds__(kBlock) k_kick_thermo(const SysParams* __restr
   vel[k] = v;
 }
 
+// kick_thermostat_main of one step and kick_drift_wrap_main of the next in one pass, for the steps of a
+// chunk (the force they both read is the same array: nothing between them changes it).  The operations
+// are k_kick_thermo's and then k_kick_drift's, in order, so the results are the same bits.
+__global__ void __launch_bounds__(kBlock) k_thermo_drift(const SysParams* __restrict__ sp, const uint8_t* __restrict__ sysid,
+                                                         uint32_t N, float4* __restrict__ pos, float4* __restrict__ vel,
+                                                         const float4* __restrict__ force, const uint8_t* __restrict__ frozen,
+                                                         uint32_t* __restrict__ trng, const float4* __restrict__ pos_ref,
+                                                         uint32_t* __restrict__ drift_bits) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  uint32_t dbits = 0;
+  uint32_t r = 0;
+  if (k < N) {
+    r = sysid[k];
+    const SysParams& P = sp[r];
+    float4 x = pos[k];
+    if (frozen[k]) {
+      vel[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+    } else {
+      const float4 f = force[k];
+      float4 v = vel[k];
+      // step.wgsl:110-142
+      float w[3] = {__fadd_rn(v.x, __fmul_rn(P.hdt, f.x)), __fadd_rn(v.y, __fmul_rn(P.hdt, f.y)),
+                    __fadd_rn(v.z, __fmul_rn(P.hdt, f.z))};
+      uint32_t s = trng[k];
+      float noise[3];
+#pragma unroll
+      for (int a = 0; a < 3; ++a) {
+        s = pcg_hash(s);
+        const float u1 = fmaxf(u01(s), 1e-7f);
+        s = pcg_hash(s);
+        const float u2 = u01(s);
+        noise[a] = __fmul_rn(sqrtf(__fmul_rn(-2.0f, logf(u1))), cosf(__fmul_rn(6.28318531f, u2)));
+      }
+      trng[k] = s;
+      v.x = __fadd_rn(__fsub_rn(w[0], __fmul_rn(P.gdt, w[0])), __fmul_rn(P.sigma_v, noise[0]));
+      v.y = __fadd_rn(__fsub_rn(w[1], __fmul_rn(P.gdt, w[1])), __fmul_rn(P.sigma_v, noise[1]));
+      v.z = __fadd_rn(__fsub_rn(w[2], __fmul_rn(P.gdt, w[2])), __fmul_rn(P.sigma_v, noise[2]));
+      // step.wgsl:96-108 of the next step
+      v.x = __fadd_rn(v.x, __fmul_rn(P.hdt, f.x));
+      v.y = __fadd_rn(v.y, __fmul_rn(P.hdt, f.y));
+      v.z = __fadd_rn(v.z, __fmul_rn(P.hdt, f.z));
+      v.w = 0.f;
+      vel[k] = v;
+      float y;
+      y = __fadd_rn(x.x, __fmul_rn(P.dt, v.x)); x.x = __fsub_rn(y, __fmul_rn(floorf(__fdiv_rn(y, P.box[0])), P.box[0]));
+      y = __fadd_rn(x.y, __fmul_rn(P.dt, v.y)); x.y = __fsub_rn(y, __fmul_rn(floorf(__fdiv_rn(y, P.box[1])), P.box[1]));
+      y = __fadd_rn(x.z, __fmul_rn(P.dt, v.z)); x.z = __fsub_rn(y, __fmul_rn(floorf(__fdiv_rn(y, P.box[2])), P.box[2]));
+      pos[k] = x;
+    }
+    const float4 p0 = pos_ref[k];
+    const float dx = ex_mi(__fsub_rn(x.x, p0.x), P.box[0]);
+    const float dy = ex_mi(__fsub_rn(x.y, p0.y), P.box[1]);
+    const float dz = ex_mi(__fsub_rn(x.z, p0.z), P.box[2]);
+    dbits = __float_as_uint(__fadd_rn(__fadd_rn(__fmul_rn(dx, dx), __fmul_rn(dy, dy)), __fmul_rn(dz, dz)));
+  }
+  const uint32_t r0 = __shfl_sync(0xffffffffu, r, 0);
+  if (__all_sync(0xffffffffu, r == r0)) {
+    uint32_t m = warp_max(dbits);
+    if ((threadIdx.x & 31) == 0 && k < N + 31) atomicMax(&drift_bits[r0], m);
+  } else if (k < N) {
+    atomicMax(&drift_bits[r], dbits);
+  }
+}
+
 // verlet.wgsl:113-122 as a standalone pass (used by the single-phase entry point)
 __global__ void k_max_drift(const SysParams* __restrict__ sp, const uint8_t* __restrict__ sysid, uint32_t N,
                             const float4* __restrict__ pos, const float4* __restrict__ pos_ref,
@@ -175,6 +239,13 @@ void launch_kick_thermo(Batch& b) {
   b.launches += 1;
   prof_begin(b, SOUP_K_KICK_THERMO);
   k_kick_thermo<<<nblocks(b.N), kBlock, 0, b.stream>>>(b.sp, b.sysid, b.N, b.vel, b.force, b.frozen, b.trng);
+  prof_end(b);
+}
+void launch_thermo_drift(Batch& b) {
+  b.launches += 1;
+  prof_begin(b, SOUP_K_KICK_THERMO);
+  k_thermo_drift<<<nblocks(b.N), kBlock, 0, b.stream>>>(b.sp, b.sysid, b.N, b.pos, b.vel, b.force, b.frozen, b.trng,
+                                                         b.pos_ref, b.drift_bits);
   prof_end(b);
 }
 void launch_max_drift(Batch& b) {

@@ -379,7 +379,7 @@ Batch* make_batch(const SoupConfig* cfgs, const SoupInitState* inits, uint32_t R
   b.events = dalloc<uint32_t>(2 * SOUP_MAX_RULES * (size_t)R);
   b.desorb = dalloc<uint32_t>(2 * (size_t)R);
   b.drift_bits = dalloc<uint32_t>(R);
-  b.bond_items = dalloc<uint32_t>(10 * n); b.bond_nitems = dalloc<uint32_t>(1);
+  b.bond_items = dalloc<uint32_t>(10 * n); b.bond_nitems = dalloc<uint32_t>(2);   // [0] item count, [1] the walk's count
   b.uf_parent = dalloc<uint32_t>(n); b.comp_min = dalloc<uint32_t>(n); b.item_done = dalloc<uint8_t>(n);
   b.has_item = dalloc<uint32_t>(n);
   b.prot_rng_dev = dalloc<uint32_t>(R);
@@ -605,7 +605,7 @@ Batch::ChunkGraph capture_chunk(Batch& b, uint64_t chunk, uint64_t start, uint64
   try {
     for (uint64_t k = 0; k < chunk; ++k) {
       const uint64_t g = start + k;
-      launch_kick_drift(b);
+      if (k == 0) launch_kick_drift(b);   // later steps' kick and drift ride on the previous thermostat
       if (c0.rebuild_on_drift) {
         cudaStreamCaptureStatus st;
         cudaGraph_t cg = nullptr;
@@ -640,7 +640,8 @@ Batch::ChunkGraph capture_chunk(Batch& b, uint64_t chunk, uint64_t start, uint64
       }
       launch_force(b);
       if (g % c0.bond_interval == 0) launch_bonds(b);
-      launch_kick_thermo(b);
+      if (k + 1 < chunk) launch_thermo_drift(b);
+      else launch_kick_thermo(b);
     }
   } catch (...) {
     b.stream = main;
@@ -722,14 +723,15 @@ void step_batch(Batch& b, uint64_t n) {
       for (uint64_t k = 0; k < chunk; ++k) {
         const uint64_t g = b.step[0];
         const bool bonds = g % c0.bond_interval == 0;
-        launch_kick_drift(b);
+        if (k == 0) launch_kick_drift(b);
         bool reb;
         if (c0.rebuild_on_drift) reb = drift_exceeds(b);
         else reb = g % c0.rebuild_every == 0;
         if (reb) rebuild(b);
         launch_force(b);
         if (bonds) launch_bonds(b);
-        launch_kick_thermo(b);
+        if (k + 1 < chunk) launch_thermo_drift(b);
+        else launch_kick_thermo(b);
         for (uint32_t r = 0; r < b.R; ++r) b.step[r]++;
       }
     }
@@ -1458,7 +1460,13 @@ int soup_autotune(SoupHandle* h, uint32_t steps, SoupTuneResult* out) {
         if (lc && !b.list_by_cell) continue;
         b.list_cells = lc != 0;
         force_pass(b);
-        const double ms = tune_time(b, 3, [&] { launch_cell_index(b); launch_build_lists(b); });
+        // the walk sets the slot order the force gathers in: a rebuild and the ten force passes of a
+        // typical rebuild interval
+        const double ms = tune_time(b, 3, [&] {
+          launch_cell_index(b);
+          launch_build_lists(b);
+          for (int f = 0; f < 10; ++f) launch_force_list(b);
+        });
         if (ms < best) { best = ms; res.walk = (uint32_t)w; cells_best = lc != 0; }
       }
     b.list_cells = cells_best;

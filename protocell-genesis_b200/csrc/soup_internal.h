@@ -218,6 +218,7 @@ void launch_es_far(Batch& b);
 void launch_force_brute(Batch& b);
 void launch_kick_drift(Batch& b);
 void launch_kick_thermo(Batch& b);
+void launch_thermo_drift(Batch& b);   // the thermostat kick of one step + the kick and drift of the next
 void launch_rebuild_decide(Batch& b, cudaGraphConditionalHandle h);
 void launch_max_drift(Batch& b);
 void launch_nonfinite(Batch& b);
