@@ -261,13 +261,22 @@ __global__ void __launch_bounds__(128) k_build_list(
   }
   uint32_t cnt = 0;
   uint32_t* row = nl + (size_t)k * cap;
+  // a warp whose particles lie at least the list range inside every face screens with plain
+  // differences: a candidate within the range sits at its stored coordinates (fast_mi would return the
+  // same difference), and one beyond it by the plain difference is beyond it by the minimum image too
+  const float rm = lr * (1.0f + 1e-5f) + 1e-3f;
+  const bool direct = __all_sync(__activemask(), xi.x >= rm && xi.x <= box[0] - rm && xi.y >= rm &&
+                                                   xi.y <= box[1] - rm && xi.z >= rm && xi.z <= box[2] - rm);
   auto take = [&](uint32_t a, uint32_t e) {
     for (uint32_t j = a; j < e; ++j) {
       if (j == k) continue;
       const float4 xj = pos[j];
-      const float dx = fast_mi(xi.x - xj.x, box[0], inv[0]);
-      const float dy = fast_mi(xi.y - xj.y, box[1], inv[1]);
-      const float dz = fast_mi(xi.z - xj.z, box[2], inv[2]);
+      float dx = xi.x - xj.x, dy = xi.y - xj.y, dz = xi.z - xj.z;
+      if (!direct) {
+        dx = fast_mi(dx, box[0], inv[0]);
+        dy = fast_mi(dy, box[1], inv[1]);
+        dz = fast_mi(dz, box[2], inv[2]);
+      }
       const float r2 = dx * dx + dy * dy + dz * dz;
       if (r2 > lr2_hi) continue;
       if (r2 >= lr2_lo && !(ex_dist(xi, xj, box) < lr)) continue;
