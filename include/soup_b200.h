@@ -463,7 +463,9 @@ int soup_diff_forward_strided(SoupHandle* h, uint32_t steps, uint32_t checkpoint
  * (w ignored), device memory.  theta_grad receives dJ/dtheta
  * (SOUP_DIFF_NPARAM doubles, host); dx0_device / dv0_device (device, n float4, may be NULL) receive
  * dJ/dx_0 and dJ/dv_0.  The Langevin noise is fixed by the window's seeds (the adjoint does not depend
- * on it).  The system is left at the window's end state. */
+ * on it).  The system is left at the window's end state.  The sensitivity of a chaotic window grows
+ * exponentially with its length: SOUP_E_NONFINITE when a parameter gradient is no longer finite (the
+ * FP32 adjoint state overflowed; theta_grad still receives the sums). */
 int soup_diff_backward(SoupHandle* h, const float* dldx_device, double* theta_grad, float* dx0_device,
                        float* dv0_device);
 

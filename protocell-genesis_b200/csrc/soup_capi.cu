@@ -1795,6 +1795,12 @@ int soup_diff_backward(SoupHandle* h, const float* dldx_device, double* theta_gr
     b.prot_rng = w.prot_rng;
     SOUP_CUDA_TRY(cudaStreamSynchronize(b.stream));
     for (int p = 0; p < SOUP_DIFF_NPARAM; ++p) theta_grad[p] = theta[p];
+    // the sensitivity of a chaotic window grows exponentially with its length; once the FP32 adjoint
+    // state overflows, the sum is no gradient
+    for (int p = 0; p < SOUP_DIFF_NPARAM; ++p)
+      if (!std::isfinite(theta[p]))
+        fail(SOUP_E_NONFINITE, "adjoint: the parameter gradient is not finite (the window's sensitivity overflowed "
+                               "the FP32 adjoint state); differentiate a shorter window");
   });
 }
 

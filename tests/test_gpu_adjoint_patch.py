@@ -78,7 +78,10 @@ def test_displacement_gradient_over_20_steps_at_full_size(patch):
     win = tr.SoupWindow64(cfg, start, steps, device="cuda")
     loss64, grad64 = win.loss_and_grad(theta0, w)
     fd = _fd(theta0, lambda t: win.loss(t, w))
-    assert float(loss.detach()) == pytest.approx(loss64, rel=1e-4)
+    # the functional is a signed sum of 2 million terms that cancels to a small value, so the FP32
+    # window's value is held to its terms' own scale (their root sum of squares), not to the sum's
+    scale = float(torch.sqrt(((d.detach() * w.cuda()) ** 2).sum()))
+    assert abs(float(loss.detach()) - loss64) <= 1e-4 * scale, (float(loss.detach()), loss64, scale)
     _check("displacement functional, 20 steps, 32,768 beads", grad, grad64, fd)
 
 
