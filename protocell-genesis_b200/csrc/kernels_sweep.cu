@@ -137,20 +137,26 @@ __global__ void __launch_bounds__(256) k_sweep_init(const SysParams* __restrict_
   if (lane == 0) E[h] = to_fix(P.d_kT * 2.302585092994046 * (P.d_pka - P.d_ph) + (es + w));
 }
 
-// u < exp(-dG/kT) for dG > 0.  For -dG/kT > -20 an FP32 estimate decides when u is more than 1e-5
-// (relative) away from it: __expf's error there is below 2 + 1.16*20 ulp and the FP32 rounding of
-// the exponent adds 1e-6, together under 5e-6.  Below -20 only u < 1e-8 can pass.  Otherwise, and
-// near the threshold, FP64 decides.
-__device__ __forceinline__ bool metropolis(double dG, double kT, double inv_kT, double u) {
-  const double xd = -dG * inv_kT;
-  if (xd > -20.0) {
-    const double est = (double)__expf((float)xd);
-    if (u < est * (1.0 - 1e-5)) return true;
-    if (u > est * (1.0 + 1e-5)) return false;
-  } else if (u >= 1e-8) {
-    return false;                 // exp(-dG/kT) <= e^-20 (1 + 1e-15) < 2.1e-9
+// u < exp(-dG/kT) for dG > 0, with dG = g 2^-40 (g the fixed-point energy, g > 0) and u = v 2^-32 (v the
+// draw's 32 output bits).  The walk's chain takes this decision once per attempt and again whenever
+// an earlier flip of its window changes the site's energy, so the common case runs in FP32 and
+// integers: for -dG/kT > -20 an FP32 estimate decides when u is more than 2e-5 (relative) away from
+// it.  The estimate's error is below 6.8e-6: the exponent -g * (2^-40 / kT) carries three FP32
+// roundings (1.8e-7 relative, 3.6e-6 absolute at |x| < 20), __expf adds at most 2 + 1.173 |x| ulp
+// (3.0e-6), the draw's and the margin's roundings 2e-7.  Below -20 only u < 1e-8 can pass (v < 43).
+// Otherwise, and near the threshold, FP64 decides: exp(-dG / kT) with dG and u exactly as the
+// reference forms them.
+__device__ __forceinline__ bool metropolis(long long g, uint32_t v, float x_scale, double kT) {
+  const float xf = -(float)g * x_scale;
+  if (xf > -20.f) {
+    const float est = __expf(xf);
+    const float u = (float)v * 2.3283064365386963e-10f;
+    if (u < est * (1.f - 2e-5f)) return true;
+    if (u > est * (1.f + 2e-5f)) return false;
+  } else if (v >= 43u) {
+    return false;                 // u >= 1.0012e-8 > exp(-20 + 4e-6)
   }
-  return u < exp(-dG / kT);
+  return (double)v * 2.3283064365386963e-10 < exp(-((double)g * kUnfix) / kT);
 }
 
 // the pcgNext LCG (state' = a state + c mod 2^32) advanced n steps at once
@@ -164,10 +170,10 @@ __device__ __forceinline__ Lcg lcg_pow(uint32_t n) {
   }
   return acc;
 }
-__device__ __forceinline__ double pcg_out(uint32_t v) {
+// pcgNext's output bits; the draw is u = bits / 2^32
+__device__ __forceinline__ uint32_t pcg_bits(uint32_t v) {
   v = ((v >> ((v >> 28u) + 4u)) ^ v) * 277803737u;
-  v = (v >> 22u) ^ v;
-  return (double)v / 4294967296.0;
+  return (v >> 22u) ^ v;
 }
 
 constexpr int kWalkThreads = 512;
@@ -200,8 +206,10 @@ __device__ __forceinline__ size_t band_row0(const SysParams& P, uint32_t r) {
 __device__ __forceinline__ size_t draw_site0(const SysParams& P, uint32_t r) {
   return 2 * (size_t)P.head_off + 2 * (size_t)kBand * r;
 }
-__device__ __forceinline__ uint32_t site_of(double u, uint32_t H) {
-  return (uint32_t)fmin((double)(H - 1), floor(u * (double)H));
+// the reference's min(H - 1, floor(u H)) for u = bits / 2^32: u H = bits H / 2^32 is exact in FP64
+// (bits H < 2^52), so its floor is the high word of the 64-bit product, always below H
+__device__ __forceinline__ uint32_t site_of(uint32_t bits, uint32_t H) {
+  return (uint32_t)(((uint64_t)bits * H) >> 32);
 }
 
 // the site every draw of the sweep's stream selects when it is a site draw (all SMs)
@@ -214,7 +222,7 @@ __global__ void k_sweep_draws(const SysParams* __restrict__ sp, const uint32_t* 
   const uint32_t d = blockIdx.x * blockDim.x + threadIdx.x;
   if (d >= 2 * H + 2 * kBand) return;
   const Lcg j = lcg_pow(d + 1u);
-  draw_site[draw_site0(P, r) + d] = site_of(pcg_out(j.a * rng_io[r] + j.c), H);
+  draw_site[draw_site0(P, r) + d] = site_of(pcg_bits(j.a * rng_io[r] + j.c), H);
 }
 
 // band[d][k] (k = 1..63): the change of draw d+k's site energy when draw d's site deprotonates
@@ -255,25 +263,24 @@ __global__ void k_sweep_band(const SysParams* __restrict__ sp, const float4* __r
   out[lane + 32u] = m1;
 }
 
-// one draw of the stream as a lane holds it: the LCG state that produced it, the draw, the site it
-// selects when it is a site draw and that site's head-list length
+// one draw of the stream as a lane holds it: the LCG state that produced it, its output bits, the
+// site it selects when it is a site draw and that site's head-list length
 struct Draw {
-  uint32_t st, site, cnt;
-  double u;
+  uint32_t st, v, site, cnt;
 };
 __device__ __forceinline__ void draw_from(Draw& d, uint32_t st, uint32_t H, uint32_t off,
                                           const uint32_t* __restrict__ es_cnt) {
   d.st = st;
-  d.u = pcg_out(st);
-  d.site = site_of(d.u, H);
+  d.v = pcg_bits(st);
+  d.site = site_of(d.v, H);
   d.cnt = es_cnt[off + d.site];
 }
 __device__ __forceinline__ Draw shfl_draw(const Draw& d, int src) {
   Draw o;
   o.st = __shfl_sync(0xffffffffu, d.st, src);
+  o.v = __shfl_sync(0xffffffffu, d.v, src);
   o.site = __shfl_sync(0xffffffffu, d.site, src);
   o.cnt = __shfl_sync(0xffffffffu, d.cnt, src);
-  o.u = __shfl_sync(0xffffffffu, d.u, src);
   return o;
 }
 
@@ -310,12 +317,12 @@ __device__ __forceinline__ uint32_t attempt_mask(uint32_t need_m, uint32_t p) {
 
 // one attempt's decision from its site energy: bit 1 accepted, bit 2 took an acceptance draw,
 // bit 4 its acceptance draw is the next window's first (lane 31; decided there)
-__device__ __forceinline__ int decide(long long e, uint32_t f, double u_acc, double kT, double inv_kT, int lane) {
-  const double Es = (double)e * kUnfix;
-  const double dG = f != 0 ? -Es : Es;
-  if (dG <= 0.0) return 1;
+// (dG = E_s for a neutral site, -E_s for a charged one; its sign is the fixed-point value's)
+__device__ __forceinline__ int decide(long long e, uint32_t f, uint32_t v_acc, float x_scale, double kT, int lane) {
+  const long long g = f != 0 ? -e : e;
+  if (g <= 0) return 1;
   if (lane == 31) return 4;
-  return (metropolis(dG, kT, inv_kT, u_acc) ? 1 : 0) | 2;
+  return (metropolis(g, v_acc, x_scale, kT) ? 1 : 0) | 2;
 }
 
 // add the flips of G to the energies of their neighbours (global int64, reductions in L2): `t` of
@@ -440,7 +447,8 @@ __global__ void __launch_bounds__(kWalkThreads) k_sweep_walk(const SysParams* __
   const bool lead_scatters = csize == 1u;
   const uint32_t nscat = lead_scatters ? kWalkThreads - 32u : (csize - 1u) * kWalkThreads;
   const uint32_t tscat = lead ? threadIdx.x - 32u : (crank - 1u) * kWalkThreads + threadIdx.x;
-  const double kT = P.d_kT, inv_kT = 1.0 / P.d_kT;
+  const double kT = P.d_kT;
+  const float x_scale = (float)(kUnfix / P.d_kT);   // -dG/kT per fixed-point unit of dG
   const double dGintr = kT * 2.302585092994046 * (P.d_pka - P.d_ph);
   const double cut2 = P.d_rc * P.d_rc, reach = P.d_rcattr + P.d_wc, reach2 = reach * reach;
   const uint32_t s0 = rng_io[r];
@@ -482,8 +490,8 @@ __global__ void __launch_bounds__(kWalkThreads) k_sweep_walk(const SysParams* __
   };
   // R: resolve the window, record its flips, slide the draws
   auto chain_R = [&](Flips& Fc) {
-      const double u_acc = __shfl_down_sync(0xffffffffu, A.u, 1);   // lane l: draw consumed+l+1 (l < 31)
-      int res = decide(e, f, u_acc, kT, inv_kT, lane);
+      const uint32_t v_acc = __shfl_down_sync(0xffffffffu, A.v, 1);   // lane l: draw consumed+l+1 (l < 31)
+      int res = decide(e, f, v_acc, x_scale, kT, lane);
       uint32_t acc_m = __ballot_sync(0xffffffffu, res & 1), need_m = __ballot_sync(0xffffffffu, res & 2);
       uint32_t nxt_m = __ballot_sync(0xffffffffu, res & 4);
       uint32_t flipped = 0, p = 0, my_fo = 0;
@@ -531,18 +539,118 @@ __global__ void __launch_bounds__(kWalkThreads) k_sweep_walk(const SysParams* __
             if (m != 0) { e += m; ch = true; }
           }
         }
-        if (ch) res = decide(e, f, u_acc, kT, inv_kT, lane);
+        if (ch) res = decide(e, f, v_acc, x_scale, kT, lane);
         if (__ballot_sync(0xffffffffu, ch)) {
           acc_m = __ballot_sync(0xffffffffu, res & 1);
           need_m = __ballot_sync(0xffffffffu, res & 2);
           nxt_m = __ballot_sync(0xffffffffu, res & 4);
         }
       };
-      if (H - attempts > 32u) {
-        // the attempt limit cannot fall inside this window.  From lane p the attempts run up to the
-        // first one that takes an acceptance draw, skip that draw, and so on.  Every flip before the
-        // first flip that changes some later lane (inter_m) resolves at once; that flip resolves
-        // alone, and the scan starts again behind it.
+      // the changes of the flips of lanes X (ascending) on every later lane's site energy or charge
+      // state: E_, F_ as they stand before those flips (standard charges only)
+      auto apply = [&](uint32_t X, long long& E_, uint32_t& F_) {
+        for (uint32_t mm = X; mm; mm &= mm - 1u) {
+          const uint32_t q = (uint32_t)(__ffs(mm) - 1);
+          const uint32_t fq = __shfl_sync(0xffffffffu, F_, (int)q);
+          if ((uint32_t)lane > q) {
+            const long long mq = ring[(consumed + q) & (kRing - 1)][(uint32_t)lane - q];
+            if (mq == kSameSite) F_ ^= 1u;
+            else E_ += fq == 0 ? mq : -mq;
+          }
+        }
+      };
+      // the window's flips m, once e and f hold every lane's final energy and state: the charge
+      // states (a site drawn twice takes the state its last flip left), the records' values and the
+      // next window's corrections, kNcBatch flips' band entries in flight at a time
+      auto commit_final = [&](uint32_t m) {
+        const bool fl = (m >> lane) & 1u;
+        const uint32_t same = __match_any_sync(0xffffffffu, fl ? A.site : (0x80000000u | (uint32_t)lane));
+        if (fl) {
+          my_fo = f; my_e = e;
+          if ((same >> lane) == 1u) flag[A.site] = f != 0 ? 0 : 1;
+        }
+        flipped |= m;
+        constexpr int kNcBatch = 4;
+        for (uint32_t mm = m; mm;) {
+          uint32_t q[kNcBatch], fq[kNcBatch];
+          long long v1[kNcBatch], v2[kNcBatch];
+#pragma unroll
+          for (int t = 0; t < kNcBatch; ++t) {
+            q[t] = mm ? (uint32_t)(__ffs(mm) - 1) : 32u;
+            mm &= mm - 1u;
+          }
+#pragma unroll
+          for (int t = 0; t < kNcBatch; ++t) {
+            const uint32_t qq = q[t] & 31u;
+            fq[t] = __shfl_sync(0xffffffffu, f, (int)qq);
+            const long long* row = ring[(consumed + qq) & (kRing - 1)];
+            v1[t] = row[(31u + (uint32_t)lane - qq) & (kBand - 1)];
+            v2[t] = row[(63u - qq) & (kBand - 1)];
+          }
+#pragma unroll
+          for (int t = 0; t < kNcBatch; ++t) {
+            if (q[t] == 32u) continue;
+            if (31u + (uint32_t)lane != q[t] && v1[t] != kSameSite) nc += fq[t] == 0 ? v1[t] : -v1[t];
+            if (lane == 31 && v2[t] != kSameSite) nc2 += fq[t] == 0 ? v2[t] : -v2[t];
+          }
+        }
+      };
+      if (H - attempts > 32u && !__any_sync(0xffffffffu, f == 2u)) {
+        // The attempt limit cannot fall inside this window and every charge is a standard one.  From
+        // lane p the attempts run up to the first one that takes an acceptance draw, skip that draw,
+        // and so on.  The changes of every flip that changes some later lane (inter_m) are applied
+        // at once and the lanes decide again; if no lane's attempt, acceptance or deferral changed,
+        // that is the window's resolution.  Otherwise every lane up to the first one that changed
+        // has its final decision (the flips before it are the real ones), their flips' changes are
+        // kept, and the scan goes on behind it.
+        uint32_t att_fin = 0, flip_fin = 0;
+        for (;;) {
+          const uint32_t am = attempt_mask(need_m, p);
+          const uint32_t stop = am & nxt_m;                  // lane 31 decides in the next window
+          const uint32_t fm = am & acc_m & ~stop;
+          const uint32_t hits = inter_m & fm;
+          if (!hits) {
+            att_fin |= am & ~stop;
+            flip_fin |= fm;
+            p = stop ? 31u : 32u;
+            break;
+          }
+          long long es = e;
+          uint32_t fs = f;
+          apply(hits, es, fs);
+          const int rs = decide(es, fs, v_acc, x_scale, kT, lane);
+          const uint32_t acc2 = __ballot_sync(0xffffffffu, rs & 1), need2 = __ballot_sync(0xffffffffu, rs & 2);
+          const uint32_t nxt2 = __ballot_sync(0xffffffffu, rs & 4);
+          const uint32_t am2 = attempt_mask(need2, p);
+          const uint32_t stop2 = am2 & nxt2, fm2 = am2 & acc2 & ~stop2;
+          const uint32_t diff = (am ^ am2) | (fm ^ fm2) | (stop ^ stop2);
+          if (!diff) {
+            e = es;
+            f = fs;
+            att_fin |= am & ~stop;
+            flip_fin |= fm;
+            p = stop ? 31u : 32u;
+            break;
+          }
+          const uint32_t k = (uint32_t)(__ffs(diff) - 1);
+          const uint32_t upto = k == 31u ? 0xffffffffu : (2u << k) - 1u;
+          att_fin |= am2 & ~stop2 & upto;
+          flip_fin |= fm2 & upto;
+          apply(inter_m & fm2 & upto, e, f);
+          if ((stop2 >> k) & 1u) { p = 31u; break; }
+          p = k + ((((am2 & need2) >> k) & 1u) ? 2u : 1u);
+          if (p >= 32u) break;
+          res = decide(e, f, v_acc, x_scale, kT, lane);
+          acc_m = __ballot_sync(0xffffffffu, res & 1);
+          need_m = __ballot_sync(0xffffffffu, res & 2);
+          nxt_m = __ballot_sync(0xffffffffu, res & 4);
+        }
+        attempts += __popc(att_fin);
+        commit_final(flip_fin);
+      } else if (H - attempts > 32u) {
+        // a non-standard charge in the window: every flip before the first flip that changes some
+        // later lane (inter_m) resolves at once; that flip resolves alone, and the scan starts again
+        // behind it.
         while (p < 32u) {
           const uint32_t am = attempt_mask(need_m, p);
           const uint32_t stop = am & nxt_m;                  // lane 31 decides in the next window
