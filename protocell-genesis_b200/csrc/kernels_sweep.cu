@@ -187,6 +187,11 @@ __device__ __forceinline__ uint32_t ld_acquire_cluster(const uint32_t* p) {
   asm volatile("ld.acquire.cluster.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
   return v;
 }
+__device__ __forceinline__ uint32_t ld_relaxed_cluster(const uint32_t* p) {
+  uint32_t v;
+  asm volatile("ld.relaxed.cluster.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+  return v;
+}
 __device__ __forceinline__ void st_release_cluster(uint32_t* p, uint32_t v) {
   asm volatile("st.release.cluster.u32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
 }
@@ -380,6 +385,29 @@ __device__ __forceinline__ void fetch_rows(long long (*ring)[kBand], const long 
   }
 }
 
+// The D and head-list rows the flips of the draws [d0, d0 + n) would scatter, into L2 (their flips
+// are scattered a window or two later): `t` of `nt` threads.  Every prefetched address lies inside
+// its row.
+__device__ __forceinline__ void prefetch_rows(const SysParams& P, uint32_t r, uint32_t off, uint32_t cap,
+                                              const uint32_t* __restrict__ draw_site,
+                                              const uint32_t* __restrict__ es_cnt, const uint32_t* __restrict__ es_nl,
+                                              const long long* __restrict__ D, uint32_t d0, uint32_t n, uint32_t t,
+                                              uint32_t nt) {
+  const uint32_t lstep = nt / n, j = t % n, l0 = t / n;
+  if (l0 >= lstep) return;
+  const uint32_t site = draw_site[draw_site0(P, r) + d0 + j];
+  const uint32_t cnt = es_cnt[off + site];
+  if (cnt == 0) return;
+  const char* drow = reinterpret_cast<const char*>(D + (size_t)(off + site) * cap);
+  const char* nrow = reinterpret_cast<const char*>(es_nl + (size_t)(off + site) * cap);
+  const uint32_t db = cnt * 8u, nb = cnt * 4u;
+  const uint32_t ld = (db + 127u) / 128u + 1u, ln = (nb + 127u) / 128u + 1u;
+  for (uint32_t l = l0; l < ld + ln; l += lstep) {
+    const char* a = l < ld ? drow + min(l * 128u, db - 1u) : nrow + min((l - ld) * 128u, nb - 1u);
+    asm volatile("prefetch.global.L2 [%0];" ::"l"(a));
+  }
+}
+
 // One cluster per replica.  CTA 0 walks the chain (warp 0) and keeps the charge states and the ring of
 // band rows in shared memory; the site energies E live in global memory and every thread of the
 // cluster but warp 0 of CTA 0 scatters flips into them.  Per window (two cluster barriers):
@@ -398,6 +426,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_sweep_walk(const SysParams* __
                                                              const long long* __restrict__ D, uint32_t cap,
                                                              long long* __restrict__ Eg,
                                                              const long long* __restrict__ band,
+                                                             const uint32_t* __restrict__ draw_site,
                                                              uint32_t* __restrict__ rng_io, double* __restrict__ out,
                                                              uint32_t only, uint32_t spin_limit) {
   extern __shared__ __align__(16) unsigned char smem[];
@@ -442,6 +471,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_sweep_walk(const SysParams* __
   uint32_t* lead_cflag = cluster.map_shared_rank(&s_cflag, 0);
   uint32_t* lead_scat = cluster.map_shared_rank(&s_scat, 0);
   uint32_t* lead_timeout = cluster.map_shared_rank(&s_timeout, 0);
+  const uint32_t* lead_base = cluster.map_shared_rank(&s_base, 0);
   // scatter threads: every thread of the other CTAs, or CTA 0's warps 1.. when the cluster is one CTA
   // (then they also fetch the band rows, which is all they do otherwise)
   const bool lead_scatters = csize == 1u;
@@ -743,7 +773,11 @@ __global__ void __launch_bounds__(kWalkThreads) k_sweep_walk(const SysParams* __
     // CTA 0 of a cluster.  Warp 0 signals (s_cflag, a release at cluster scope) once its E reads of
     // window w are done, so the helper CTAs may add window w-1's flips to E, and before window w+1
     // reads E it waits (s_scat) until every helper has.  The other warps fetch the band rows.  No
-    // cluster barrier inside the loop.
+    // cluster barrier inside the loop.  Measured and dropped: relaying the signal through another
+    // warp (it took the release's fence, about 900 cycles, off the chain, but reached the helpers
+    // later); E in CTA 0's shared memory (the scatter became remote atomics into one SM, twice as
+    // slow as reductions spread over L2); each helper staging the rows of the draws it owns in its
+    // shared memory by asynchronous copies (the copies' issue took longer than the L2 reads saved).
     for (uint32_t wnd = 0;; ++wnd) {
       Flips& Fc = F[wnd & 1];
       const Flips& Fp = F[(wnd + 1) & 1];
@@ -791,6 +825,9 @@ __global__ void __launch_bounds__(kWalkThreads) k_sweep_walk(const SysParams* __
       scatter_flips(Fh, P, off, cap, es_nl, D, hpos, E, cut2, reach2, tscat, nscat);
       __syncthreads();
       if (threadIdx.x == 0) red_add_release_cluster(lead_scat, 1u);
+      // the rows of the window after the chain's current one (its draws start 31 or 32 later)
+      prefetch_rows(P, r, off, cap, draw_site, es_cnt, es_nl, D, ld_relaxed_cluster(lead_base) + 31u, 33u, tscat,
+                    nscat);
     }
   }
   if (!lead) {
@@ -869,7 +906,8 @@ void launch_sweep(Batch& b, uint32_t replica) {
   SOUP_CUDA_TRY(cudaLaunchKernelEx(&lc, k_sweep_walk, (const SysParams*)b.sp, (const uint32_t*)b.head_slot,
                                    (const float4*)b.head_pos, b.charge, (const uint32_t*)b.es_nl,
                                    (const uint32_t*)b.es_cnt, (const long long*)b.head_d, b.es_cap, b.head_e,
-                                   (const long long*)b.sweep_band, b.prot_rng_dev, b.sweep_out, replica,
+                                   (const long long*)b.sweep_band, (const uint32_t*)b.draw_site, b.prot_rng_dev,
+                                   b.sweep_out, replica,
                                    b.wait_limit ? b.wait_limit : kSpinLimit));
   prof_end(b);
 }
