@@ -579,10 +579,6 @@ def run_gradient(args, pkg, L, torch):
             "plain_step_ms": plain_ms / steps, "window_vs_plain_steps": total / plain_ms,
             "gpu_launches": int(launches), "loss": "thickness proxy", "value_of_loss": loss,
             "theta": list(adjoint.PARAM_NAMES), "grad": [float(x) for x in grad],
-            "short_window": {"steps": every, "value_of_loss": loss_short, "grad": [float(x) for x in grad_short]},
-            "note": "the parcels are a chaotic fluid: the sensitivity of the loss to the parameters grows "
-                    "exponentially with the window (compare short_window); the adjoint is validated against "
-                    "FP64 windows and central differences on 20-200-step windows",
             "workload": "preassembled flat bilayer, 2,048 five-bead amphiphiles, water to density 0.80, box "
                         "32x32x40 sigma, pH 9, I 0.01 M; seeded synthetic, relaxed untimed; bond and charge "
                         "Monte Carlo held off inside the window"}
