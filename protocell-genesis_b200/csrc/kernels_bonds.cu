@@ -39,25 +39,49 @@ __device__ __forceinline__ int match_rule(const Shared& S, float ti, float tj) {
 }
 
 // Phase A
+// A bead whose kind is in no rule has no candidate, draws nothing and, unless it is a catalyst or
+// tethered to one, leaves no item: its walk would change nothing (water, most of a campaign's beads).
+__device__ __forceinline__ bool bond_active(const Shared& S, float ti, uint32_t centre) {
+  bool in_rule = false;
+  for (int r = 0; r < 2; ++r) in_rule = in_rule || ti == S.kindA[r] || ti == S.kindB[r];
+  return in_rule || ti == S.cat_kind || centre != NONE;
+}
+
+// the active beads' slots, compacted (a warp's in one atomic); sel[0..*nsel) in no particular order
+__global__ void __launch_bounds__(256) k_bond_select(const Shared* __restrict__ Sg, uint32_t N,
+                                                     const float4* __restrict__ pos,
+                                                     const uint32_t* __restrict__ center, uint32_t* __restrict__ sel,
+                                                     uint32_t* __restrict__ nsel) {
+  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool act = k < N && bond_active(*Sg, pos[k].w, center[k]);
+  const uint32_t m = __ballot_sync(0xffffffffu, act);
+  if (!m) return;
+  const uint32_t lane = threadIdx.x & 31u;
+  uint32_t base = 0;
+  if (lane == (uint32_t)(__ffs(m) - 1)) base = atomicAdd(nsel, (uint32_t)__popc(m));
+  base = __shfl_sync(0xffffffffu, base, __ffs(m) - 1);
+  if (act) sel[base + __popc(m & ((1u << lane) - 1u))] = k;
+}
+
+// a thread per active bead (k_bond_select), so that the warps walk full
 __global__ void __launch_bounds__(128) k_bond_walk(
-    const Shared* __restrict__ Sg, const SysParams* __restrict__ sp, const uint8_t* __restrict__ sysid, uint32_t N,
+    const Shared* __restrict__ Sg, const SysParams* __restrict__ sp, const uint8_t* __restrict__ sysid,
+    const uint32_t* __restrict__ sel, const uint32_t* __restrict__ nsel,
     const float4* __restrict__ pos, const uint32_t* __restrict__ id, const uint32_t* __restrict__ slots,
     const uint32_t* __restrict__ center, const uint32_t* __restrict__ nl, const uint32_t* __restrict__ nl_cnt,
     uint32_t cap, uint32_t* __restrict__ brng, uint32_t* __restrict__ items, uint32_t* __restrict__ nitems,
     uint32_t* __restrict__ has_item) {
+  const uint32_t ns = *nsel;
+  if (blockIdx.x * blockDim.x >= ns) return;   // the whole block: past the active beads
   __shared__ Shared S;
   for (int w = threadIdx.x; w < (int)(sizeof(Shared) / 4); w += blockDim.x)
     reinterpret_cast<uint32_t*>(&S)[w] = reinterpret_cast<const uint32_t*>(Sg)[w];
   __syncthreads();
-  const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-  if (k >= N) return;
+  const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= ns) return;
+  const uint32_t k = sel[t];
   const float4 xi = pos[k];
   const float ti = xi.w;
-  // a bead whose kind is in no rule has no candidate, draws nothing and, unless it is a catalyst or
-  // tethered to one, leaves no item: its walk would change nothing (water, most of a campaign's beads)
-  bool in_rule = false;
-  for (int r = 0; r < 2; ++r) in_rule = in_rule || ti == S.kindA[r] || ti == S.kindB[r];
-  if (!in_rule && ti != S.cat_kind && center[k] == NONE) return;
   const SysParams& P = sp[sysid[k]];
   const float box[3] = {P.box[0], P.box[1], P.box[2]};
   const uint32_t gi = id[k];
@@ -73,10 +97,12 @@ __global__ void __launch_bounds__(128) k_bond_walk(
     const float4 xj = pos[js];
     const float tj = xj.w;
     const bool isCat = tj == S.cat_kind;
+    const int rk = match_rule(S, ti, tj);        // by the kinds alone
+    if (!isCat && rk < 0) continue;
     const uint32_t j = id[js];
     int r = -1;
     if (j > gi) {
-      r = match_rule(S, ti, tj);
+      r = rk;
       if (r >= 0 && (s0 == j || s1 == j || s2 == j)) r = -1;          // hasBondTo
       if (r >= 0 && nc == SOUP_CAND_CAP && j > cj[SOUP_CAND_CAP - 1]) r = -1;
     }
@@ -434,14 +460,16 @@ __global__ void k_bond_break(const Shared* __restrict__ Sg, const uint8_t* __res
 }  // namespace
 
 void launch_bonds(Batch& b) {
-  b.launches += 4;
+  b.launches += 5;
   prof_begin(b, SOUP_K_BONDS);
-  cudaMemsetAsync(b.bond_nitems, 0, sizeof(uint32_t), b.stream);
+  cudaMemsetAsync(b.bond_nitems, 0, 3 * sizeof(uint32_t), b.stream);
   cudaMemsetAsync(b.has_item, 0, sizeof(uint32_t) * b.N, b.stream);
   uint32_t* has_item = b.has_item;
-  k_bond_walk<<<nblocks(b.N, 128), 128, 0, b.stream>>>(b.shared, b.sp, b.sysid, b.N, b.pos, b.id, b.slots, b.center,
-                                                       b.nl, b.nl_cnt, b.list_cap, b.brng, b.bond_items,
-                                                       b.bond_nitems, has_item);
+  k_bond_select<<<nblocks(b.N, 256), 256, 0, b.stream>>>(b.shared, b.N, b.pos, b.center, b.bond_sel,
+                                                         b.bond_nitems + 2);
+  k_bond_walk<<<nblocks(b.N, 128), 128, 0, b.stream>>>(b.shared, b.sp, b.sysid, b.bond_sel, b.bond_nitems + 2, b.pos,
+                                                       b.id, b.slots, b.center, b.nl, b.nl_cnt, b.list_cap, b.brng,
+                                                       b.bond_items, b.bond_nitems, has_item);
   cudaMemcpyAsync(b.bond_nitems + 1, b.bond_nitems, sizeof(uint32_t), cudaMemcpyDeviceToDevice, b.stream);
   k_bond_partners<<<std::max(1u, std::min(nblocks(b.N, 256) / 8u, 592u)), 256, 0, b.stream>>>(
       b.center, b.slot_of, b.bond_items, b.bond_nitems, b.N, has_item, b.flags);

@@ -379,7 +379,8 @@ Batch* make_batch(const SoupConfig* cfgs, const SoupInitState* inits, uint32_t R
   b.events = dalloc<uint32_t>(2 * SOUP_MAX_RULES * (size_t)R);
   b.desorb = dalloc<uint32_t>(2 * (size_t)R);
   b.drift_bits = dalloc<uint32_t>(R);
-  b.bond_items = dalloc<uint32_t>(10 * n); b.bond_nitems = dalloc<uint32_t>(2);   // [0] item count, [1] the walk's count
+  // [0] item count, [1] the walk's count, [2] the active beads (k_bond_select)
+  b.bond_items = dalloc<uint32_t>(10 * n); b.bond_nitems = dalloc<uint32_t>(3); b.bond_sel = dalloc<uint32_t>(n);
   b.uf_parent = dalloc<uint32_t>(n); b.comp_min = dalloc<uint32_t>(n); b.item_done = dalloc<uint8_t>(n);
   b.has_item = dalloc<uint32_t>(n);
   b.prot_rng_dev = dalloc<uint32_t>(R);
@@ -468,7 +469,7 @@ void destroy_batch(Batch* b) {
                   b->held2, b->brng2, b->trng2, b->frozen2, b->id2, b->cell_of_slot, b->cell_count, b->cell_start, b->cell_sys,
                   b->cell_cursor, b->perm, b->scan_tmp, b->nl, b->nl_cnt, b->nl_shell, b->heads, b->head_sys, b->es_nl,
                   b->es_cnt, b->head_slot, b->head_e, b->head_pos, b->head_xq, b->head_d, b->head_flag, b->draw_site, b->sweep_band, b->hcell_count, b->hcell_start, b->hcell_cursor, b->hsorted, b->hsorted_xg, b->hcell_of, b->flags,
-                  b->events, b->desorb, b->drift_bits, b->bond_items, b->bond_nitems, b->uf_parent, b->comp_min,
+                  b->events, b->desorb, b->drift_bits, b->bond_items, b->bond_nitems, b->bond_sel, b->uf_parent, b->comp_min,
                   b->item_done, b->has_item, b->sweep_out, b->prot_rng_dev, b->sp, b->shared, b->sysid, b->an_buf[0],
                   b->an_buf[1]};
   for (void* p : ptrs) if (p) cudaFree(p);

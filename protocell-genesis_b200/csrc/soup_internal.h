@@ -133,6 +133,7 @@ struct Batch {
   // bond pass scratch
   uint32_t* bond_items = nullptr;    // item records
   uint32_t* bond_nitems = nullptr;
+  uint32_t* bond_sel = nullptr;      // the active beads of a bond pass, compacted
   uint32_t* uf_parent = nullptr;     // per original id
   uint32_t* comp_min = nullptr;      // per original id
   uint8_t* item_done = nullptr;
