@@ -503,8 +503,14 @@ __global__ void __launch_bounds__(kWalkThreads) k_sweep_walk(const SysParams* __
 
   // ---- the chain's two phases of a window (warp 0 of CTA 0) ----
   // C: E and the charge states of this window's sites, with the previous window's flips added
-  auto chain_C = [&](const Flips& Fp) {
+  // sig != 0: the helpers' signal for this window, released as soon as the E loads are issued (the
+  // release waits for them; the rest of C and the fence then overlap)
+  auto chain_C = [&](const Flips& Fp, uint32_t sig) {
       e = (long long)__ldcg(reinterpret_cast<const unsigned long long*>(E + A.site));
+      if (sig) {
+        __syncwarp();
+        if (lane == 0) st_release_cluster(&s_cflag, sig);
+      }
       f = flag[A.site];
       // the previous window's flips, accumulated for this window's draws while they were taken; a
       // flip from a charge other than the standard one is rare and evaluated here.  A site's own
@@ -759,7 +765,7 @@ __global__ void __launch_bounds__(kWalkThreads) k_sweep_walk(const SysParams* __
       const Flips& Fp = F[(wnd + 1) & 1];
       if (s_done) break;
       const uint32_t base = s_base;
-      if (chain) chain_C(Fp);
+      if (chain) chain_C(Fp, 0u);
       __syncthreads();
       if (chain) {
         chain_R(Fc);
@@ -787,9 +793,8 @@ __global__ void __launch_bounds__(kWalkThreads) k_sweep_walk(const SysParams* __
       }
       const uint32_t base = s_base;
       if (chain) {
-        chain_C(Fp);
+        chain_C(Fp, wnd + 1u);
         __syncwarp();
-        if (lane == 0) st_release_cluster(&s_cflag, wnd + 1u);
         chain_R(Fc);
         if (lane == 0) {
           const uint32_t want = (csize - 1u) * (wnd + 1u);
